@@ -1,0 +1,155 @@
+// Device-side data model of the B200 particle-bookkeeping engine.
+//
+// A virtual Cartesian grid of P subdomains lives in one GPU's HBM:
+//
+//   particle arrays  one allocation per array (11 doubles: x y z vx vy vz fx fy
+//                    fz mass charge; 2 int32: type global_id; F registered
+//                    fields of `bytes` bytes per particle), each laid out as
+//                    [ owned A | owned B | ghosts ]
+//                    with |owned A| = |owned B| = ncap (the total owned count,
+//                    which migration conserves) and |ghosts| = gcap.
+//   owned region     subdomain s owns [obase[s], obase[s] + n[s]) of the current
+//                    owned half (A or B, swapped by every migrate), packed in
+//                    subdomain order.
+//   ghost region     receiver q's ghosts are [gbase[q], gbase[q] + g[q]),
+//                    neighbor block by neighbor block in q's neighbor order.
+//   tiles            work is cut into tiles of `tile` consecutive owned
+//                    particles that never straddle two subdomains; tile_start
+//                    (P+1 entries) is the exclusive prefix of ceil(n[s]/tile).
+//
+// All counts live on the device so that a whole step can be captured in a
+// CUDA graph; the host reads them back only when an API call must return them.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dsx {
+
+constexpr int kMaxNeighbors = 26;
+constexpr int kMaxFields = 16;
+constexpr int kMaxRanks = 1024;
+// per-tile halo counters: 26 neighbor lists, boundary owners, images
+constexpr int kHaloCounters = 28;
+constexpr int kBoundaryCounter = 26;
+constexpr int kImageCounter = 27;
+
+// status bits (device word, read by the host after a step)
+constexpr unsigned kStatusGhostOverflow = 1u;
+constexpr unsigned kStatusCutsInvalid = 2u;
+constexpr unsigned kStatusMigrationMismatch = 4u;
+
+struct FieldSet {
+    int count = 0;
+    int bytes[kMaxFields] = {};          // per particle
+    unsigned char* base[kMaxFields] = {}; // start of the [A|B|ghost] allocation
+};
+
+struct Arrays {
+    double* d[11] = {};
+    int* type = nullptr;
+    int* gid = nullptr;
+    FieldSet f;
+};
+
+// Static description of the grid and pointers to the device tables.
+struct Grid {
+    int P = 1;
+    int dims[3] = {1, 1, 1};
+    int periodic[3] = {1, 1, 1};
+    double lower[3] = {0, 0, 0};
+    double upper[3] = {1, 1, 1};
+    double extent[3] = {1, 1, 1};   // upper - lower, computed once on the host
+    double width = 0.0;             // halo width
+    long long ncap = 0;             // owned half length (= total owned count)
+    long long gcap = 0;             // ghost capacity
+    int tile = 1024;
+    int max_tiles = 1;              // ceil(ncap / tile) + P
+    int cut_offset[3] = {0, 0, 0};  // start of each axis in `cuts`
+
+    // topology (static)
+    const int* nn = nullptr;             // [P] neighbor count
+    const int* nbr = nullptr;            // [P*26] neighbor rank or -1
+    const int* recv_entry = nullptr;     // [P*26] entry index at the receiver
+    const int* sender_of = nullptr;      // [P*26] receiver (q,m) -> sender r*26+n or -1
+    const double* shift = nullptr;       // [P*26*3]
+    const signed char* dir = nullptr;    // [P*26*3]
+    const unsigned* lut = nullptr;       // [P*64] halo flags -> neighbor mask
+
+    // geometry (changes with Dynamic boundaries)
+    double* cuts = nullptr;
+
+    // layout of the current owned half
+    int* n = nullptr;            // [P]
+    int* obase = nullptr;        // [P+1]
+    int* tile_start = nullptr;   // [P+1]
+    // next layout (written by migrate)
+    int* n_next = nullptr;
+    int* obase_next = nullptr;
+    int* tile_start_next = nullptr;
+
+    unsigned* status = nullptr;
+};
+
+// ---------------------------------------------------------------- helpers
+
+// Periodic wrap exactly as the reference Host path rounds it:
+// v -= lower; v -= floor(v / extent) * extent; v += lower
+// (dsDecompX src/migration.cpp:83-87, 106-113).  No FMA contraction.
+__device__ __forceinline__ double wrap_axis(double v, double lower, double extent) {
+    double t = __dsub_rn(v, lower);
+    const double q = floor(__ddiv_rn(t, extent));
+    t = __dsub_rn(t, __dmul_rn(q, extent));
+    return __dadd_rn(t, lower);
+}
+
+// std::upper_bound(cuts, cuts + count, v) - cuts - 1, clamped to [0, dims-1]
+// (dsDecompX src/migration.cpp:89-93).
+__device__ __forceinline__ int axis_coordinate(const double* cuts, int dims, double v) {
+    int lo = 0, hi = dims + 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (v < cuts[mid]) hi = mid;
+        else lo = mid + 1;
+    }
+    int c = lo - 1;
+    c = c > dims - 1 ? dims - 1 : c;
+    return c < 0 ? 0 : c;
+}
+
+// Subdomain that owns tile g: largest s with tile_start[s] <= g.
+__device__ __forceinline__ int tile_owner(const int* tile_start, int P, int g) {
+    int lo = 0, hi = P;   // invariant: tile_start[lo] <= g < tile_start[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (tile_start[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Copies one particle's registered fields (bytes per particle as laid out in
+// `f`) from global index `src` to global index `dst`.
+__device__ __forceinline__ void copy_fields(const FieldSet& f, long long src, long long dst) {
+    for (int k = 0; k < f.count; ++k) {
+        const int b = f.bytes[k];
+        unsigned char* base = f.base[k];
+        if ((b & 7) == 0) {
+            const unsigned long long* s = reinterpret_cast<const unsigned long long*>(base + src * b);
+            unsigned long long* d = reinterpret_cast<unsigned long long*>(base + dst * b);
+            for (int w = 0; w < (b >> 3); ++w) d[w] = s[w];
+        } else {
+            const unsigned* s = reinterpret_cast<const unsigned*>(base + src * b);
+            unsigned* d = reinterpret_cast<unsigned*>(base + dst * b);
+            for (int w = 0; w < (b >> 2); ++w) d[w] = s[w];
+        }
+    }
+}
+
+}  // namespace dsx

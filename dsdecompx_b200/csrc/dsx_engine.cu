@@ -1,0 +1,1123 @@
+// Host side of the engine: topology tables, device storage, orchestration of
+// the kernels in dsx_kernels.cu, CUDA-graph capture of the batched step, and
+// the extern "C" entry points declared in include/dsx.h.
+#include "dsx.h"
+#include "dsx_kernels.cuh"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Failure : std::runtime_error {
+    int code;
+    Failure(int c, const std::string& message) : std::runtime_error(message), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string& message) {
+    throw Failure(code, "dsDecompX: " + message);
+}
+
+void cuda_check(cudaError_t status, const char* what) {
+    if (status != cudaSuccess)
+        fail(DSX_E_RUNTIME, std::string(what) + ": " + cudaGetErrorString(status));
+}
+
+template <class F>
+int guarded(F&& body) {
+    try {
+        body();
+        return DSX_OK;
+    } catch (const Failure& e) {
+        g_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_error = std::string("dsDecompX: ") + e.what();
+        return DSX_E_RUNTIME;
+    }
+}
+
+std::size_t field_type_size(int type) {
+    switch (type) {
+    case DSX_INT32: case DSX_UINT32: case DSX_FLOAT32: return 4;
+    case DSX_INT64: case DSX_UINT64: case DSX_FLOAT64: return 8;
+    default: fail(DSX_E_INVALID, "unsupported field type");
+    }
+}
+
+// ------------------------------------------------------------ topology
+
+// Lower is better; ties broken on (px, py, pz) (dsDecompX src/grid.cpp:12-22).
+double balanced_score(const int* g, const double* len) {
+    const double lx = len[0] / g[0], ly = len[1] / g[1], lz = len[2] / g[2];
+    const double surface = 2.0 * (1.0 / lx + 1.0 / ly + 1.0 / lz);
+    const double longest = std::max({lx, ly, lz});
+    const double shortest = std::min({lx, ly, lz});
+    return surface * (1.0 + 0.05 * std::log(longest / shortest));
+}
+
+// All virtual ranks share one GPU, i.e. one node: the topology-aware score
+// of dsDecompX src/grid.cpp:28-75 with a single node.
+double single_node_score(const int* g, const double* len, const int* periodic) {
+    const double local[3] = {len[0] / g[0], len[1] / g[1], len[2] / g[2]};
+    const double face[3] = {local[1] * local[2], local[0] * local[2], local[0] * local[1]};
+    double cost = 0.0;
+    for (int x = 0; x < g[0]; ++x)
+        for (int y = 0; y < g[1]; ++y)
+            for (int z = 0; z < g[2]; ++z) {
+                const int source = (x * g[1] + y) * g[2] + z;
+                for (int a = 0; a < 3; ++a) {
+                    int c[3] = {x, y, z};
+                    if (++c[a] == g[a]) {
+                        if (!periodic[a] || g[a] == 1) continue;
+                        c[a] = 0;
+                    }
+                    if ((c[0] * g[1] + c[1]) * g[2] + c[2] == source) continue;
+                    cost += face[a] * 1.0;
+                }
+            }
+    return cost / (local[0] * local[1] * local[2] * g[0] * g[1] * g[2]) +
+           0.01 * balanced_score(g, len);
+}
+
+void choose_grid(int n, const double* len, const int* periodic, int policy, int* out) {
+    double best_score = std::numeric_limits<double>::infinity();
+    int best[3] = {n, 1, 1};
+    for (int px = 1; px <= n; ++px) {
+        if (n % px) continue;
+        const int rest = n / px;
+        for (int py = 1; py <= rest; ++py) {
+            if (rest % py) continue;
+            const int cand[3] = {px, py, rest / py};
+            const double score = policy == DSX_TOPOLOGY_AWARE ? single_node_score(cand, len, periodic)
+                                                              : balanced_score(cand, len);
+            const bool less = std::make_tuple(score, cand[0], cand[1], cand[2]) <
+                              std::make_tuple(best_score, best[0], best[1], best[2]);
+            if (less) {
+                best_score = score;
+                std::copy(cand, cand + 3, best);
+            }
+        }
+    }
+    std::copy(best, best + 3, out);
+}
+
+// Fills zero entries with a balanced factorization, largest first, like
+// MPI_Dims_create.
+bool fill_dims(int n, int* dims) {
+    int fixed = 1, free_count = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (dims[a] < 0) return false;
+        if (dims[a] > 0) fixed *= dims[a];
+        else ++free_count;
+    }
+    if (!free_count) return fixed == n;
+    if (n % fixed) return false;
+    int rest = n / fixed;
+    std::vector<int> factors;
+    for (int f = 2; rest > 1 && f * f <= rest; ++f)
+        while (rest % f == 0) { factors.push_back(f); rest /= f; }
+    if (rest > 1) factors.push_back(rest);
+    std::sort(factors.rbegin(), factors.rend());
+    std::vector<int> grid(static_cast<std::size_t>(free_count), 1);
+    for (int f : factors) *std::min_element(grid.begin(), grid.end()) *= f;
+    std::sort(grid.rbegin(), grid.rend());
+    std::size_t k = 0;
+    for (int a = 0; a < 3; ++a) if (dims[a] == 0) dims[a] = grid[k++];
+    return true;
+}
+
+int direction_slot(int dx, int dy, int dz) {
+    const int raw = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+    return raw < 13 ? raw : raw - 1;
+}
+
+struct Neighbor {
+    int rank = -1;
+    int dir[3] = {0, 0, 0};
+    int slot = -1;
+    double shift[3] = {0, 0, 0};
+};
+
+// The 26-direction neighbor list of one subdomain, in the reference's loop
+// order and with its rules (dsDecompX src/topology.cpp:85-167): directions
+// that move along an unsplit axis are skipped, periodic wrap gives the image
+// shift +L (coordinate below 0) or -L (at or past dims), a non-periodic
+// boundary gives rank -1.
+std::vector<Neighbor> neighbors_of(const int* c, const int* dims, const dsx_grid_desc& d) {
+    std::vector<Neighbor> out;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                if (!dx && !dy && !dz) continue;
+                if (!d.edges_and_corners && std::abs(dx) + std::abs(dy) + std::abs(dz) != 1) continue;
+                const int dir[3] = {dx, dy, dz};
+                bool unsplit = false;
+                for (int a = 0; a < 3; ++a) unsplit = unsplit || (dir[a] != 0 && dims[a] == 1);
+                if (unsplit) continue;
+                Neighbor nb;
+                int nc[3] = {c[0] + dx, c[1] + dy, c[2] + dz};
+                bool outside = false;
+                for (int a = 0; a < 3 && !outside; ++a) {
+                    if (nc[a] >= 0 && nc[a] < dims[a]) continue;
+                    if (!d.periodic[a]) { outside = true; break; }
+                    const double extent = d.upper[a] - d.lower[a];
+                    if (nc[a] < 0) { nc[a] += dims[a]; nb.shift[a] = extent; }
+                    else { nc[a] -= dims[a]; nb.shift[a] = -extent; }
+                }
+                for (int a = 0; a < 3; ++a) nb.dir[a] = dir[a];
+                nb.slot = direction_slot(dx, dy, dz);
+                nb.rank = outside ? -1 : (nc[0] * dims[1] + nc[1]) * dims[2] + nc[2];
+                out.push_back(nb);
+            }
+    return out;
+}
+
+// ------------------------------------------------------------ device memory
+
+struct DeviceBlock {
+    void* p = nullptr;
+    ~DeviceBlock() { if (p) cudaFree(p); }
+};
+
+template <class T>
+T* device_alloc(std::vector<void*>& owned, std::size_t count) {
+    void* p = nullptr;
+    cuda_check(cudaMalloc(&p, std::max<std::size_t>(count, 1) * sizeof(T)), "cudaMalloc");
+    owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+}  // namespace
+
+struct dsx_grid {
+    dsx_grid_desc desc{};
+    int P = 1;
+    int dims[3] = {1, 1, 1};
+    struct Field {
+        std::string name;
+        int type = DSX_FLOAT64;
+        int components = 1;
+        int bytes = 8;
+    };
+    std::vector<Field> fields;
+    std::vector<std::vector<Neighbor>> topo;   // per rank
+    std::vector<std::array<int, 3>> coords;
+    double halo_width = 0.0;
+    long long ncap = 0, gcap = 0;
+    long long total = 0;   // owned particles in the grid (conserved)
+
+    // device storage
+    std::vector<void*> arrays_owned;    // particle arrays (reallocated on growth)
+    std::vector<void*> scratch_owned;   // ghost-sized scratch (reallocated on growth)
+    std::vector<void*> fixed_owned;     // everything else
+    dsx::Arrays A;
+    dsx::Scratch S;
+    double* cuts = nullptr;
+    int cut_offset[3] = {0, 0, 0};
+    int* layout[2][3] = {};   // [which][n, obase, tile_start]
+    int cur = 0;              // current layout index
+    int parity = 0;           // current owned half
+    unsigned* status = nullptr;
+    long long* call_counter = nullptr;
+    double* rebalance_result = nullptr;   // [6]: automatic, explicit
+    double* work = nullptr;               // [P]
+    // static topology tables
+    int* d_nn = nullptr;
+    int* d_nbr = nullptr;
+    int* d_recv_entry = nullptr;
+    int* d_sender_of = nullptr;
+    double* d_shift = nullptr;
+    signed char* d_dir = nullptr;
+    unsigned* d_lut = nullptr;
+
+    // host state
+    bool plan_valid = false;
+    bool ghosts_valid = false;
+    std::vector<long long> last_ghosts;
+    unsigned* pinned_status = nullptr;   // [4]: status, G, B, pad
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    dsx_step_callback graph_callback = nullptr;
+    void* graph_user = nullptr;
+    cudaStream_t graph_stream = nullptr;
+
+    ~dsx_grid() {
+        destroy_graphs();
+        for (void* p : arrays_owned) cudaFree(p);
+        for (void* p : scratch_owned) cudaFree(p);
+        for (void* p : fixed_owned) cudaFree(p);
+        if (pinned_status) cudaFreeHost(pinned_status);
+    }
+
+    void destroy_graphs() {
+        for (auto& g : graph) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    }
+
+    long long owned_off() const { return parity ? ncap : 0; }
+    long long next_off() const { return parity ? 0 : ncap; }
+    long long ghost_off() const { return 2 * ncap; }
+
+    dsx::Grid params() const {
+        dsx::Grid G;
+        G.P = P;
+        for (int a = 0; a < 3; ++a) {
+            G.dims[a] = dims[a];
+            G.periodic[a] = desc.periodic[a] ? 1 : 0;
+            G.lower[a] = desc.lower[a];
+            G.upper[a] = desc.upper[a];
+            G.extent[a] = desc.upper[a] - desc.lower[a];
+            G.cut_offset[a] = cut_offset[a];
+        }
+        G.width = halo_width;
+        G.ncap = ncap;
+        G.gcap = gcap;
+        G.tile = 1024;
+        G.max_tiles = static_cast<int>((ncap + 1023) / 1024) + P;
+        G.nn = d_nn;
+        G.nbr = d_nbr;
+        G.recv_entry = d_recv_entry;
+        G.sender_of = d_sender_of;
+        G.shift = d_shift;
+        G.dir = d_dir;
+        G.lut = d_lut;
+        G.cuts = cuts;
+        G.n = layout[cur][0];
+        G.obase = layout[cur][1];
+        G.tile_start = layout[cur][2];
+        G.n_next = layout[cur ^ 1][0];
+        G.obase_next = layout[cur ^ 1][1];
+        G.tile_start_next = layout[cur ^ 1][2];
+        G.status = status;
+        return G;
+    }
+
+    void setup(const dsx_grid_desc& d, const dsx_field_desc* f, int nfields, long long particles,
+               long long ghost_capacity) {
+        desc = d;
+        P = d.nranks;
+        if (P < 1 || P > dsx::kMaxRanks) fail(DSX_E_INVALID, "nranks must be in 1..1024");
+        for (int a = 0; a < 3; ++a)
+            if (!(d.upper[a] > d.lower[a])) fail(DSX_E_INVALID, "global-domain extent must be positive");
+        if (d.halo_width < 0.0) fail(DSX_E_INVALID, "halo width cannot be negative");
+        if (!(d.dyn_threshold >= 1.0) || !(d.dyn_relaxation > 0.0 && d.dyn_relaxation <= 1.0) ||
+            !(d.dyn_min_fraction > 0.0 && d.dyn_min_fraction <= 1.0) || d.dyn_interval < 0)
+            fail(DSX_E_INVALID, "invalid dynamic load-balance configuration");
+        if (nfields < 0 || nfields > dsx::kMaxFields)
+            fail(DSX_E_INVALID, "at most 16 custom fields are supported on CUDA particle memory");
+        if (particles < 0 || particles >= (1ll << 30)) fail(DSX_E_INVALID, "particle count out of range");
+        for (int i = 0; i < nfields; ++i) {
+            Field fd;
+            fd.name = f[i].name ? f[i].name : "";
+            fd.type = f[i].type;
+            fd.components = f[i].components;
+            if (fd.name.empty() || fd.components <= 0)
+                fail(DSX_E_INVALID, "invalid or undersized custom particle field");
+            for (const auto& other : fields)
+                if (other.name == fd.name) fail(DSX_E_INVALID, "duplicate custom particle field '" + fd.name + "'");
+            fd.bytes = static_cast<int>(field_type_size(fd.type)) * fd.components;
+            fields.push_back(fd);
+        }
+        // process grid (dsDecompX src/topology.cpp:18-55)
+        if (d.policy != DSX_MANUAL) {
+            const double len[3] = {d.upper[0] - d.lower[0], d.upper[1] - d.lower[1], d.upper[2] - d.lower[2]};
+            choose_grid(P, len, d.periodic, d.policy, dims);
+        } else {
+            for (int a = 0; a < 3; ++a) dims[a] = d.dims[a];
+        }
+        if (!fill_dims(P, dims)) fail(DSX_E_INVALID, "process-grid dimensions do not match communicator size");
+        halo_width = d.halo_width;
+        ncap = std::max<long long>(particles, 1);
+        gcap = ghost_capacity > 0 ? ghost_capacity : std::max<long long>(ncap, 1 << 16);
+        build_topology();
+        allocate_fixed();
+        allocate_arrays();
+        allocate_ghost_scratch();
+        cuda_check(cudaMallocHost(reinterpret_cast<void**>(&pinned_status), 4 * sizeof(unsigned)),
+                   "cudaMallocHost");
+        last_ghosts.assign(static_cast<std::size_t>(P), 0);
+    }
+
+    void build_topology() {
+        topo.assign(static_cast<std::size_t>(P), {});
+        coords.assign(static_cast<std::size_t>(P), {});
+        for (int s = 0; s < P; ++s) {
+            int c[3] = {s / (dims[1] * dims[2]), (s / dims[2]) % dims[1], s % dims[2]};
+            coords[static_cast<std::size_t>(s)] = {c[0], c[1], c[2]};
+            topo[static_cast<std::size_t>(s)] = neighbors_of(c, dims, desc);
+        }
+    }
+
+    // sender entry of receiver (q, m): the entry of r = nbr(q,m) that points
+    // toward -d_m (the MPI backend's tag matching, dsDecompX
+    // src/backends/mpi_backend.cpp:398-433)
+    int sender_entry(int q, int m) const {
+        const Neighbor& nb = topo[static_cast<std::size_t>(q)][static_cast<std::size_t>(m)];
+        if (nb.rank < 0) return -1;
+        const int want = direction_slot(-nb.dir[0], -nb.dir[1], -nb.dir[2]);
+        const auto& list = topo[static_cast<std::size_t>(nb.rank)];
+        for (std::size_t n = 0; n < list.size(); ++n)
+            if (list[n].slot == want && list[n].rank == q) return nb.rank * dsx::kMaxNeighbors + static_cast<int>(n);
+        return -1;
+    }
+
+    void allocate_fixed() {
+        const int E = dsx::kMaxNeighbors;
+        std::vector<int> nn(P), nbr(P * E, -1), recv_entry(P * E, -1), sender_of(P * E, -1);
+        std::vector<double> shift(P * E * 3, 0.0);
+        std::vector<signed char> dir(P * E * 3, 0);
+        std::vector<unsigned> lut(static_cast<std::size_t>(P) * 64, 0u);
+        for (int s = 0; s < P; ++s) {
+            const auto& list = topo[static_cast<std::size_t>(s)];
+            nn[s] = static_cast<int>(list.size());
+            for (std::size_t n = 0; n < list.size(); ++n) {
+                const int idx = s * E + static_cast<int>(n);
+                nbr[idx] = list[n].rank;
+                for (int a = 0; a < 3; ++a) {
+                    shift[3 * idx + a] = list[n].shift[a];
+                    dir[3 * idx + a] = static_cast<signed char>(list[n].dir[a]);
+                }
+                sender_of[idx] = sender_entry(s, static_cast<int>(n));
+                if (sender_of[idx] >= 0) recv_entry[sender_of[idx]] = idx;
+            }
+            // flags bit 2a: below lower+w on axis a; bit 2a+1: above upper-w
+            for (unsigned flags = 1; flags < 64; ++flags) {
+                unsigned mask = 0;
+                for (std::size_t n = 0; n < list.size(); ++n) {
+                    if (list[n].rank < 0) continue;
+                    bool hit = true;
+                    for (int a = 0; a < 3; ++a) {
+                        if (list[n].dir[a] < 0 && !(flags & (1u << (2 * a)))) hit = false;
+                        if (list[n].dir[a] > 0 && !(flags & (2u << (2 * a)))) hit = false;
+                    }
+                    if (hit) mask |= 1u << n;
+                }
+                lut[static_cast<std::size_t>(s) * 64 + flags] = mask;
+            }
+        }
+        auto up = [&](auto* dst, const auto& src) {
+            cuda_check(cudaMemcpy(dst, src.data(), src.size() * sizeof(src[0]), cudaMemcpyHostToDevice),
+                       "upload topology");
+        };
+        d_nn = device_alloc<int>(fixed_owned, nn.size());
+        d_nbr = device_alloc<int>(fixed_owned, nbr.size());
+        d_recv_entry = device_alloc<int>(fixed_owned, recv_entry.size());
+        d_sender_of = device_alloc<int>(fixed_owned, sender_of.size());
+        d_shift = device_alloc<double>(fixed_owned, shift.size());
+        d_dir = device_alloc<signed char>(fixed_owned, dir.size());
+        d_lut = device_alloc<unsigned>(fixed_owned, lut.size());
+        up(d_nn, nn); up(d_nbr, nbr); up(d_recv_entry, recv_entry); up(d_sender_of, sender_of);
+        up(d_shift, shift); up(d_dir, dir); up(d_lut, lut);
+
+        // uniform cuts (dsDecompX src/topology.cpp:63-75)
+        std::vector<double> c;
+        for (int a = 0; a < 3; ++a) {
+            cut_offset[a] = static_cast<int>(c.size());
+            const double extent = desc.upper[a] - desc.lower[a];
+            for (int i = 0; i <= dims[a]; ++i)
+                c.push_back(desc.lower[a] + extent * static_cast<double>(i) / static_cast<double>(dims[a]));
+        }
+        cuts = device_alloc<double>(fixed_owned, c.size());
+        up(cuts, c);
+
+        for (auto& l : layout) {
+            l[0] = device_alloc<int>(fixed_owned, P + 1);
+            l[1] = device_alloc<int>(fixed_owned, P + 1);
+            l[2] = device_alloc<int>(fixed_owned, P + 1);
+            cuda_check(cudaMemset(l[0], 0, sizeof(int) * (P + 1)), "memset");
+            cuda_check(cudaMemset(l[1], 0, sizeof(int) * (P + 1)), "memset");
+            cuda_check(cudaMemset(l[2], 0, sizeof(int) * (P + 1)), "memset");
+        }
+        status = device_alloc<unsigned>(fixed_owned, 4);
+        cuda_check(cudaMemset(status, 0, 4 * sizeof(unsigned)), "memset");
+        call_counter = device_alloc<long long>(fixed_owned, 1);
+        cuda_check(cudaMemset(call_counter, 0, sizeof(long long)), "memset");
+        rebalance_result = device_alloc<double>(fixed_owned, 6);
+        work = device_alloc<double>(fixed_owned, P);
+
+        const int max_tiles = static_cast<int>((ncap + 1023) / 1024) + P;
+        S.stride = max_tiles + 1;
+        S.cnt = device_alloc<int>(fixed_owned, static_cast<std::size_t>(dsx::kHaloCounters) * S.stride);
+        S.pre = device_alloc<int>(fixed_owned, static_cast<std::size_t>(dsx::kHaloCounters) * S.stride);
+        S.imm_total = device_alloc<int>(fixed_owned, P);
+        S.imm_base = device_alloc<int>(fixed_owned, P);
+        S.emig_src = device_alloc<int>(fixed_owned, ncap);
+        S.emig_dst = device_alloc<int>(fixed_owned, ncap);
+        S.max_chunks = static_cast<int>((ncap + 1023) / 1024);
+        S.emig_hist = device_alloc<int>(fixed_owned, static_cast<std::size_t>(S.max_chunks) * P);
+        S.emig_info = device_alloc<int>(fixed_owned, 4);
+        cuda_check(cudaMemset(S.emig_info, 0, 4 * sizeof(int)), "memset");
+        S.mig_results = device_alloc<long long>(fixed_owned, static_cast<std::size_t>(P) * 6);
+        S.mask = device_alloc<unsigned>(fixed_owned, ncap);
+        S.list_len = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
+        S.send_base = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
+        S.g = device_alloc<int>(fixed_owned, P + 1);
+        S.gbase = device_alloc<int>(fixed_owned, P + 1);
+        cuda_check(cudaMemset(S.g, 0, sizeof(int) * (P + 1)), "memset");
+        cuda_check(cudaMemset(S.gbase, 0, sizeof(int) * (P + 1)), "memset");
+        S.bowner = device_alloc<int>(fixed_owned, ncap);
+        S.boff = device_alloc<int>(fixed_owned, ncap + 1);
+        S.halo_info = device_alloc<int>(fixed_owned, 4);
+        cuda_check(cudaMemset(S.halo_info, 0, 4 * sizeof(int)), "memset");
+    }
+
+    // particle arrays [owned A | owned B | ghosts]
+    void allocate_arrays() {
+        const std::size_t len = static_cast<std::size_t>(2 * ncap + gcap);
+        for (int a = 0; a < 11; ++a) A.d[a] = device_alloc<double>(arrays_owned, len);
+        A.type = device_alloc<int>(arrays_owned, len);
+        A.gid = device_alloc<int>(arrays_owned, len);
+        A.f.count = static_cast<int>(fields.size());
+        for (std::size_t f = 0; f < fields.size(); ++f) {
+            A.f.bytes[f] = fields[f].bytes;
+            A.f.base[f] = device_alloc<unsigned char>(arrays_owned, len * fields[f].bytes);
+        }
+    }
+
+    void allocate_ghost_scratch() {
+        S.ghost_owner = device_alloc<int>(scratch_owned, gcap);
+        S.ghost_entry = device_alloc<int>(scratch_owned, gcap);
+        S.bslot = device_alloc<int>(scratch_owned, gcap);
+    }
+
+    // Grows the ghost region; the current owned half survives.
+    void grow_ghosts(long long required, cudaStream_t stream) {
+        const long long next = std::max<long long>(required + required / 2, gcap + gcap / 2);
+        cuda_check(cudaStreamSynchronize(stream), "synchronize before growth");
+        destroy_graphs();
+        dsx::Arrays old = A;
+        std::vector<void*> old_arrays;
+        old_arrays.swap(arrays_owned);
+        const long long off = owned_off();
+        gcap = next;
+        allocate_arrays();
+        const std::size_t n = static_cast<std::size_t>(total);
+        for (int a = 0; a < 11; ++a)
+            cuda_check(cudaMemcpyAsync(A.d[a] + off, old.d[a] + off, n * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, stream), "grow copy");
+        cuda_check(cudaMemcpyAsync(A.type + off, old.type + off, n * sizeof(int), cudaMemcpyDeviceToDevice, stream), "grow copy");
+        cuda_check(cudaMemcpyAsync(A.gid + off, old.gid + off, n * sizeof(int), cudaMemcpyDeviceToDevice, stream), "grow copy");
+        for (std::size_t f = 0; f < fields.size(); ++f)
+            cuda_check(cudaMemcpyAsync(A.f.base[f] + off * fields[f].bytes, old.f.base[f] + off * fields[f].bytes,
+                                       n * fields[f].bytes, cudaMemcpyDeviceToDevice, stream), "grow copy");
+        cuda_check(cudaStreamSynchronize(stream), "grow copy");
+        for (void* p : old_arrays) cudaFree(p);
+        for (void* p : scratch_owned) cudaFree(p);
+        scratch_owned.clear();
+        allocate_ghost_scratch();
+        plan_valid = false;
+        ghosts_valid = false;
+    }
+
+    // -------------------------------------------------------- operations
+
+    void enqueue_migrate(cudaStream_t stream, bool automatic_rebalance) {
+        const dsx::Grid G = params();
+        if (desc.policy == DSX_DYNAMIC) {
+            // Decomp::migrate: ++migration_calls, automatic rebalance every
+            // `interval` calls unless called from rebalance()
+            // (dsDecompX src/runtime.cpp:983-993)
+            dsx::RebalanceParams p;
+            p.threshold = desc.dyn_threshold;
+            p.relaxation = desc.dyn_relaxation;
+            p.minimum_fraction = desc.dyn_min_fraction;
+            p.halo_width = halo_width;
+            p.automatic = 1;
+            p.interval = automatic_rebalance ? static_cast<long long>(desc.dyn_interval) : 0;
+            dsx::launch_rebalance(G, nullptr, p, call_counter, rebalance_result, stream);
+        }
+        dsx::launch_migrate(G, A, owned_off(), next_off(), S, stream);
+    }
+
+    void commit_migrate() {
+        parity ^= 1;
+        cur ^= 1;
+        plan_valid = false;
+        ghosts_valid = false;
+        std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
+    }
+
+    void enqueue_halo_build(cudaStream_t stream) {
+        dsx::launch_halo_build(params(), A, owned_off(), ghost_off(), S, stream);
+    }
+
+    void enqueue_reverse(cudaStream_t stream) {
+        const long long o = owned_off(), g = ghost_off();
+        dsx::launch_reverse_sum3(params(), A.d[6] + o, A.d[7] + o, A.d[8] + o, A.d[6] + g, A.d[7] + g,
+                                 A.d[8] + g, S, stream);
+    }
+
+    unsigned read_status(cudaStream_t stream) {
+        cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
+                   "read status");
+        cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream),
+                   "read status");
+        cuda_check(cudaStreamSynchronize(stream), "synchronize");
+        return pinned_status[0];
+    }
+
+    void clear_status(cudaStream_t stream) {
+        cuda_check(cudaMemsetAsync(status, 0, sizeof(unsigned), stream), "clear status");
+    }
+
+    std::vector<int> read_ints(const int* device, int count, cudaStream_t stream) {
+        std::vector<int> out(static_cast<std::size_t>(count));
+        cuda_check(cudaMemcpyAsync(out.data(), device, sizeof(int) * count, cudaMemcpyDeviceToHost, stream), "read");
+        cuda_check(cudaStreamSynchronize(stream), "synchronize");
+        return out;
+    }
+
+    void migrate(cudaStream_t stream, long long* results, bool automatic_rebalance = true) {
+        clear_status(stream);
+        enqueue_migrate(stream, automatic_rebalance);
+        commit_migrate();
+        if (results) {
+            cuda_check(cudaMemcpyAsync(results, S.mig_results, sizeof(long long) * 6 * P,
+                                       cudaMemcpyDeviceToHost, stream), "read migration results");
+            const unsigned st = read_status(stream);
+            if (st & dsx::kStatusMigrationMismatch) fail(DSX_E_RUNTIME, "migration count mismatch");
+            if (st & dsx::kStatusCutsInvalid)
+                fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");
+        }
+    }
+
+    // Builds the plan; grows the ghost region and rebuilds when it overflowed.
+    void build_checked(cudaStream_t stream) {
+        for (;;) {
+            clear_status(stream);
+            enqueue_halo_build(stream);
+            const unsigned st = read_status(stream);
+            if (!(st & dsx::kStatusGhostOverflow)) break;
+            grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
+        }
+        plan_valid = true;
+        ghosts_valid = true;
+    }
+
+    void exchange_halo(bool rebuild, bool positions_only, cudaStream_t stream, long long* results) {
+        if (rebuild) plan_valid = false;
+        bool reused = false;
+        if (P == 1) {
+            // one rank owns the whole periodic box: no ghosts (dsDecompX src/halo.cpp:325-350)
+            plan_valid = false;
+            ghosts_valid = false;
+        } else if (plan_valid) {
+            dsx::launch_halo_refresh(params(), A, owned_off(), ghost_off(), positions_only, S, stream);
+            reused = true;
+        } else if (results) {
+            build_checked(stream);
+        } else {
+            clear_status(stream);
+            enqueue_halo_build(stream);
+            plan_valid = true;
+            ghosts_valid = true;
+        }
+        if (results) {
+            std::vector<int> g(static_cast<std::size_t>(P), 0);
+            if (ghosts_valid) g = read_ints(S.g, P, stream);
+            for (int s = 0; s < P; ++s) {
+                const long long now = ghosts_valid ? g[static_cast<std::size_t>(s)] : 0;
+                long long* o = results + 4 * s;
+                o[0] = now;
+                o[1] = (rebuild || now != last_ghosts[static_cast<std::size_t>(s)] || (now != 0 && !reused)) ? 1 : 0;
+                o[2] = 0;
+                o[3] = reused ? 1 : 0;
+                last_ghosts[static_cast<std::size_t>(s)] = now;
+            }
+        } else if (!ghosts_valid) {
+            std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
+        }
+    }
+
+    void reverse_halo(cudaStream_t stream) {
+        if (P == 1 || !ghosts_valid) return;
+        enqueue_reverse(stream);
+    }
+
+    dsx::FieldOps field_ops(int nf, const int* ids, const int* ops, const char* what) {
+        if (nf > dsx::kMaxFields) fail(DSX_E_INVALID, std::string("at most 16 fields can be ") + what);
+        dsx::FieldOps F;
+        F.count = nf;
+        for (int i = 0; i < nf; ++i) {
+            if (!ids || ids[i] < 0 || ids[i] >= static_cast<int>(fields.size()))
+                fail(DSX_E_INVALID, std::string("missing or undersized ") + what + " field");
+            for (int j = 0; j < i; ++j)
+                if (ids[j] == ids[i])
+                    fail(DSX_E_INVALID, std::string("duplicate ") + what + " field '" +
+                                            fields[static_cast<std::size_t>(ids[i])].name + "'");
+            const Field& f = fields[static_cast<std::size_t>(ids[i])];
+            F.index[i] = ids[i];
+            F.type[i] = f.type;
+            F.components[i] = f.components;
+            F.op[i] = ops ? ops[i] : DSX_REPLACE;
+            if (F.op[i] < DSX_SUM || F.op[i] > DSX_REPLACE) fail(DSX_E_INVALID, "unknown reduce operation");
+        }
+        return F;
+    }
+
+    void reverse_exchange(int nf, const int* ids, const int* ops, cudaStream_t stream) {
+        const dsx::FieldOps F = field_ops(nf, ids, ops, "reverse-exchanged");
+        if (P == 1 || !ghosts_valid || nf == 0) return;
+        dsx::launch_reverse_fields(params(), A, owned_off(), ghost_off(), F, S, stream);
+    }
+
+    void forward_exchange(int nf, const int* ids, cudaStream_t stream) {
+        const dsx::FieldOps F = field_ops(nf, ids, nullptr, "forward-exchanged");
+        if (P == 1 || !ghosts_valid || nf == 0) return;
+        dsx::launch_forward_fields(params(), A, owned_off(), ghost_off(), F, S, stream);
+    }
+
+    void rebalance(const double* host_work, bool force, cudaStream_t stream, long long* results,
+                   double* imbalance) {
+        if (host_work) {
+            for (int s = 0; s < P; ++s)
+                if (!std::isfinite(host_work[s]) || host_work[s] < 0.0)
+                    fail(DSX_E_INVALID, "rebalance local_work must be finite and non-negative");
+            cuda_check(cudaMemcpyAsync(work, host_work, sizeof(double) * P, cudaMemcpyHostToDevice, stream),
+                       "upload work");
+        }
+        clear_status(stream);
+        dsx::RebalanceParams p;
+        p.threshold = desc.dyn_threshold;
+        p.relaxation = desc.dyn_relaxation;
+        p.minimum_fraction = desc.dyn_min_fraction;
+        p.halo_width = halo_width;
+        p.force = force ? 1 : 0;
+        p.automatic = 0;
+        dsx::launch_rebalance(params(), host_work ? work : nullptr, p, call_counter, rebalance_result + 3, stream);
+        double r[3] = {0, 0, 1};
+        cuda_check(cudaMemcpyAsync(r, rebalance_result + 3, sizeof(r), cudaMemcpyDeviceToHost, stream), "read");
+        const unsigned st = read_status(stream);
+        if (st & dsx::kStatusCutsInvalid)
+            fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");
+        if (r[1] != 0.0) plan_valid = false;
+        std::vector<long long> mig(static_cast<std::size_t>(6 * P));
+        migrate(stream, mig.data(), false);
+        for (int s = 0; s < P; ++s) {
+            if (results) {
+                results[3 * s + 0] = r[0] != 0.0;
+                results[3 * s + 1] = r[1] != 0.0;
+                results[3 * s + 2] = mig[static_cast<std::size_t>(6 * s + 5)];
+            }
+            if (imbalance) imbalance[s] = r[2];
+        }
+    }
+
+    dsx_grid_view view() const {
+        dsx_grid_view v{};
+        for (int a = 0; a < 11; ++a) v.base[a] = A.d[a];
+        v.base[11] = A.type;
+        v.base[12] = A.gid;
+        for (std::size_t f = 0; f < fields.size(); ++f) v.base[13 + f] = A.f.base[f];
+        v.owned_offset = owned_off();
+        v.ghost_offset = ghost_off();
+        v.n = layout[cur][0];
+        v.obase = layout[cur][1];
+        v.g = S.g;
+        v.gbase = S.gbase;
+        v.halo_totals = S.halo_info;
+        v.particles = total;
+        v.ghost_capacity = gcap;
+        v.nranks = P;
+        return v;
+    }
+
+    void enqueue_step(dsx_step_callback cb, void* user, cudaStream_t stream) {
+        clear_status(stream);
+        enqueue_migrate(stream, true);
+        // the rest of the step reads the next layout
+        parity ^= 1;
+        cur ^= 1;
+        enqueue_halo_build(stream);
+        const dsx_grid_view v = view();
+        if (cb) cb(user, stream, &v);
+        enqueue_reverse(stream);
+        cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
+                   "read status");
+        cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream),
+                   "read status");
+        parity ^= 1;
+        cur ^= 1;
+    }
+
+    void step(dsx_step_callback cb, void* user, bool capture, cudaStream_t stream, unsigned* status_out) {
+        if (capture && (graph_callback != cb || graph_user != user || graph_stream != stream)) {
+            destroy_graphs();
+            graph_callback = cb;
+            graph_user = user;
+            graph_stream = stream;
+        }
+        if (capture) {
+            cudaGraphExec_t& exec = graph[parity];
+            if (!exec) {
+                cudaGraph_t g = nullptr;
+                cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+                enqueue_step(cb, user, stream);
+                cuda_check(cudaStreamEndCapture(stream, &g), "end capture");
+                cuda_check(cudaGraphInstantiate(&exec, g, 0), "instantiate graph");
+                cudaGraphDestroy(g);
+            }
+            cuda_check(cudaGraphLaunch(exec, stream), "launch graph");
+        } else {
+            enqueue_step(cb, user, stream);
+        }
+        commit_migrate();
+        plan_valid = true;
+        ghosts_valid = true;
+        cuda_check(cudaStreamSynchronize(stream), "synchronize step");
+        unsigned st = pinned_status[0];
+        if (st & dsx::kStatusGhostOverflow) {
+            // the owned half of this step is intact: grow, then redo the
+            // halo build, the callback and the reverse sum
+            grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
+            build_checked(stream);
+            const dsx_grid_view v = view();
+            if (cb) cb(user, stream, &v);
+            enqueue_reverse(stream);
+            st = read_status(stream);
+        }
+        if (st & dsx::kStatusMigrationMismatch) fail(DSX_E_RUNTIME, "migration count mismatch");
+        if (st & dsx::kStatusCutsInvalid)
+            fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");
+        if (status_out) *status_out = st;
+    }
+
+    void upload(const long long* counts, const void* const* arrays, cudaStream_t stream) {
+        long long sum = 0;
+        for (int s = 0; s < P; ++s) {
+            if (counts[s] < 0) fail(DSX_E_INVALID, "negative particle count");
+            sum += counts[s];
+        }
+        if (sum > ncap) fail(DSX_E_LENGTH, "particle storage is smaller than the supplied counts");
+        total = sum;
+        parity = 0;
+        cur = 0;
+        plan_valid = false;
+        ghosts_valid = false;
+        std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
+        const std::size_t n = static_cast<std::size_t>(sum);
+        for (int a = 0; a < 13; ++a) {
+            void* dst = a < 11 ? static_cast<void*>(A.d[a]) : a == 11 ? static_cast<void*>(A.type) : A.gid;
+            const std::size_t bytes = n * (a < 11 ? sizeof(double) : sizeof(int));
+            if (arrays && arrays[a])
+                cuda_check(cudaMemcpyAsync(dst, arrays[a], bytes, cudaMemcpyDefault, stream), "upload");
+            else
+                cuda_check(cudaMemsetAsync(dst, 0, bytes, stream), "upload");
+        }
+        for (std::size_t f = 0; f < fields.size(); ++f) {
+            const void* src = arrays ? arrays[13 + f] : nullptr;
+            if (src)
+                cuda_check(cudaMemcpyAsync(A.f.base[f], src, n * fields[f].bytes, cudaMemcpyDefault, stream), "upload");
+            else
+                cuda_check(cudaMemsetAsync(A.f.base[f], 0, n * fields[f].bytes, stream), "upload");
+        }
+        std::vector<int> c(static_cast<std::size_t>(P) + 1, 0);
+        for (int s = 0; s < P; ++s) c[static_cast<std::size_t>(s)] = static_cast<int>(counts[s]);
+        cuda_check(cudaMemcpyAsync(layout[cur][0], c.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice, stream),
+                   "upload counts");
+        dsx::launch_layout(params(), layout[cur][0], layout[cur][1], layout[cur][2], stream);
+        cuda_check(cudaMemsetAsync(S.g, 0, sizeof(int) * (P + 1), stream), "memset");
+        cuda_check(cudaMemsetAsync(S.gbase, 0, sizeof(int) * (P + 1), stream), "memset");
+        cuda_check(cudaMemsetAsync(S.halo_info, 0, sizeof(int) * 4, stream), "memset");
+        cuda_check(cudaStreamSynchronize(stream), "upload");
+    }
+
+    // slot range of one rank -> device index ranges in the owned/ghost regions
+    void access(int rank, int array, long long start, long long count, void* host, bool write,
+                cudaStream_t stream) {
+        if (rank < 0 || rank >= P) fail(DSX_E_INVALID, "rank out of range");
+        std::size_t element = 0;
+        unsigned char* base = nullptr;
+        if (array >= 0 && array < 11) { element = 8; base = reinterpret_cast<unsigned char*>(A.d[array]); }
+        else if (array == 11) { element = 4; base = reinterpret_cast<unsigned char*>(A.type); }
+        else if (array == 12) { element = 4; base = reinterpret_cast<unsigned char*>(A.gid); }
+        else if (array >= 13 && array < 13 + static_cast<int>(fields.size())) {
+            element = static_cast<std::size_t>(fields[static_cast<std::size_t>(array - 13)].bytes);
+            base = A.f.base[array - 13];
+        } else fail(DSX_E_INVALID, "bad array id");
+        const std::vector<int> n = read_ints(layout[cur][0], P, stream);
+        const std::vector<int> ob = read_ints(layout[cur][1], P, stream);
+        std::vector<int> g(static_cast<std::size_t>(P), 0), gb(static_cast<std::size_t>(P), 0);
+        if (ghosts_valid) {
+            g = read_ints(S.g, P, stream);
+            gb = read_ints(S.gbase, P, stream);
+        }
+        const long long owned = n[static_cast<std::size_t>(rank)];
+        const long long ghosts = g[static_cast<std::size_t>(rank)];
+        if (start < 0 || count < 0 || start + count > owned + ghosts)
+            fail(DSX_E_INVALID, "slot range outside the subdomain's particles");
+        auto copy = [&](long long device_index, long long slots, unsigned char* h) {
+            if (slots <= 0) return;
+            unsigned char* d = base + static_cast<std::size_t>(device_index) * element;
+            if (write)
+                cuda_check(cudaMemcpyAsync(d, h, static_cast<std::size_t>(slots) * element, cudaMemcpyHostToDevice, stream), "write");
+            else
+                cuda_check(cudaMemcpyAsync(h, d, static_cast<std::size_t>(slots) * element, cudaMemcpyDeviceToHost, stream), "read");
+        };
+        unsigned char* h = static_cast<unsigned char*>(host);
+        const long long owned_part = std::max<long long>(0, std::min(start + count, owned) - start);
+        copy(owned_off() + ob[static_cast<std::size_t>(rank)] + start, owned_part, h);
+        const long long ghost_start = std::max(start, owned) - owned;
+        const long long ghost_part = count - owned_part;
+        copy(ghost_off() + gb[static_cast<std::size_t>(rank)] + ghost_start, ghost_part,
+             h + static_cast<std::size_t>(owned_part) * element);
+        cuda_check(cudaStreamSynchronize(stream), "synchronize");
+    }
+};
+
+extern "C" {
+
+const char* dsx_last_error(void) { return g_error.c_str(); }
+const char* dsx_version(void) { return "dsdecompx-b200 1.0.0 (sm_100a)"; }
+
+int dsx_rank_migrate(double* x, double* y, double* z, long long owned, const dsx_domain* domain,
+                     void* stream, dsx_migration_result* result) {
+    return guarded([&] {
+        if (!domain) fail(DSX_E_INVALID, "missing domain");
+        if (!stream) fail(DSX_E_INVALID, "CUDA migration requires an explicit communication stream");
+        if (owned < 0) fail(DSX_E_INVALID, "negative owned count");
+        if (owned && (!x || !y || !z)) fail(DSX_E_INVALID, "incomplete CUDA migration view");
+        double extent[3];
+        for (int a = 0; a < 3; ++a) {
+            if (!(domain->upper[a] > domain->lower[a])) fail(DSX_E_INVALID, "global-domain extent must be positive");
+            extent[a] = domain->upper[a] - domain->lower[a];
+        }
+        dsx::launch_wrap_inplace(x, y, z, owned, domain->lower, extent, domain->periodic,
+                                 static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch migrate");
+        if (result) {
+            result->ownership_changed = 0;
+            result->previous_owned_count = owned;
+            result->retained_count = owned;
+            result->sent_count = 0;
+            result->received_count = 0;
+            result->new_owned_count = owned;
+        }
+    });
+}
+
+int dsx_plan_topology(const dsx_grid_desc* desc, int rank, int* dims, int* count, int* info,
+                      double* shifts) {
+    return guarded([&] {
+        if (!desc) fail(DSX_E_INVALID, "null argument");
+        const int P = desc->nranks;
+        if (P < 1 || P > dsx::kMaxRanks) fail(DSX_E_INVALID, "nranks must be in 1..1024");
+        if (rank < 0 || rank >= P) fail(DSX_E_INVALID, "rank out of range");
+        int d[3];
+        if (desc->policy != DSX_MANUAL) {
+            const double len[3] = {desc->upper[0] - desc->lower[0], desc->upper[1] - desc->lower[1],
+                                   desc->upper[2] - desc->lower[2]};
+            for (double l : len) if (!(l > 0.0)) fail(DSX_E_INVALID, "domain lengths must be positive");
+            choose_grid(P, len, desc->periodic, desc->policy, d);
+        } else {
+            for (int a = 0; a < 3; ++a) d[a] = desc->dims[a];
+        }
+        if (!fill_dims(P, d)) fail(DSX_E_INVALID, "process-grid dimensions do not match communicator size");
+        const int c[3] = {rank / (d[1] * d[2]), (rank / d[2]) % d[1], rank % d[2]};
+        const auto list = neighbors_of(c, d, *desc);
+        for (int a = 0; a < 3; ++a) dims[a] = d[a];
+        *count = static_cast<int>(list.size());
+        for (std::size_t n = 0; n < list.size(); ++n) {
+            info[5 * n + 0] = list[n].rank;
+            for (int a = 0; a < 3; ++a) {
+                info[5 * n + 1 + a] = list[n].dir[a];
+                shifts[3 * n + a] = list[n].shift[a];
+            }
+            info[5 * n + 4] = list[n].slot;
+        }
+    });
+}
+
+int dsx_grid_create(const dsx_grid_desc* desc, const dsx_field_desc* fields, int nfields,
+                    long long particles, long long ghost_capacity, dsx_grid** out) {
+    return guarded([&] {
+        if (!desc || !out) fail(DSX_E_INVALID, "null argument");
+        if (nfields && !fields) fail(DSX_E_INVALID, "custom field array is null");
+        auto* g = new dsx_grid();
+        try {
+            g->setup(*desc, fields, nfields, particles, ghost_capacity);
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        *out = g;
+    });
+}
+
+int dsx_grid_destroy(dsx_grid* grid) {
+    return guarded([&] { delete grid; });
+}
+
+int dsx_grid_topology(dsx_grid* grid, int rank, int* dims, int* coords, double* local) {
+    return guarded([&] {
+        if (!grid || rank < 0 || rank >= grid->P) fail(DSX_E_INVALID, "rank out of range");
+        std::vector<double> cuts;
+        int total = 0;
+        for (int a = 0; a < 3; ++a) total += grid->dims[a] + 1;
+        cuts.resize(static_cast<std::size_t>(total));
+        cuda_check(cudaMemcpy(cuts.data(), grid->cuts, sizeof(double) * total, cudaMemcpyDeviceToHost), "read cuts");
+        const auto& c = grid->coords[static_cast<std::size_t>(rank)];
+        for (int a = 0; a < 3; ++a) {
+            dims[a] = grid->dims[a];
+            coords[a] = c[static_cast<std::size_t>(a)];
+            local[a] = cuts[static_cast<std::size_t>(grid->cut_offset[a] + c[static_cast<std::size_t>(a)])];
+            local[3 + a] = cuts[static_cast<std::size_t>(grid->cut_offset[a] + c[static_cast<std::size_t>(a)] + 1)];
+        }
+    });
+}
+
+int dsx_grid_neighbors(dsx_grid* grid, int rank, int* count, int* info, double* shifts) {
+    return guarded([&] {
+        if (!grid || rank < 0 || rank >= grid->P) fail(DSX_E_INVALID, "rank out of range");
+        const auto& list = grid->topo[static_cast<std::size_t>(rank)];
+        *count = static_cast<int>(list.size());
+        for (std::size_t n = 0; n < list.size(); ++n) {
+            info[5 * n + 0] = list[n].rank;
+            info[5 * n + 1] = list[n].dir[0];
+            info[5 * n + 2] = list[n].dir[1];
+            info[5 * n + 3] = list[n].dir[2];
+            info[5 * n + 4] = list[n].slot;
+            for (int a = 0; a < 3; ++a) shifts[3 * n + a] = list[n].shift[a];
+        }
+    });
+}
+
+int dsx_grid_cuts(dsx_grid* grid, double* out, void* stream) {
+    return guarded([&] {
+        int total = 0;
+        for (int a = 0; a < 3; ++a) total += grid->dims[a] + 1;
+        cuda_check(cudaMemcpyAsync(out, grid->cuts, sizeof(double) * total, cudaMemcpyDeviceToHost,
+                                   static_cast<cudaStream_t>(stream)), "read cuts");
+        cuda_check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "synchronize");
+    });
+}
+
+int dsx_grid_upload(dsx_grid* grid, const long long* counts, const void* const* arrays, void* stream) {
+    return guarded([&] {
+        if (!grid || !counts) fail(DSX_E_INVALID, "null argument");
+        grid->upload(counts, arrays, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_counts(dsx_grid* grid, long long* owned, long long* ghosts, void* stream) {
+    return guarded([&] {
+        const auto s = static_cast<cudaStream_t>(stream);
+        const std::vector<int> n = grid->read_ints(grid->layout[grid->cur][0], grid->P, s);
+        std::vector<int> g(static_cast<std::size_t>(grid->P), 0);
+        if (grid->ghosts_valid) g = grid->read_ints(grid->S.g, grid->P, s);
+        for (int r = 0; r < grid->P; ++r) {
+            if (owned) owned[r] = n[static_cast<std::size_t>(r)];
+            if (ghosts) ghosts[r] = g[static_cast<std::size_t>(r)];
+        }
+    });
+}
+
+int dsx_grid_read(dsx_grid* grid, int rank, int array, long long start, long long count, void* host_out,
+                  void* stream) {
+    return guarded([&] { grid->access(rank, array, start, count, host_out, false, static_cast<cudaStream_t>(stream)); });
+}
+
+int dsx_grid_write(dsx_grid* grid, int rank, int array, long long start, long long count, const void* host_in,
+                   void* stream) {
+    return guarded([&] {
+        grid->access(rank, array, start, count, const_cast<void*>(host_in), true, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_view_get(dsx_grid* grid, dsx_grid_view* out) {
+    return guarded([&] { *out = grid->view(); });
+}
+
+int dsx_grid_migrate(dsx_grid* grid, void* stream, long long* results) {
+    return guarded([&] {
+        grid->migrate(static_cast<cudaStream_t>(stream), results);
+        cuda_check(cudaGetLastError(), "launch migrate");
+    });
+}
+
+int dsx_grid_exchange_halo(dsx_grid* grid, int rebuild, int positions_only, void* stream, long long* results) {
+    return guarded([&] {
+        grid->exchange_halo(rebuild != 0, positions_only != 0, static_cast<cudaStream_t>(stream), results);
+        cuda_check(cudaGetLastError(), "launch halo");
+    });
+}
+
+int dsx_grid_reverse_halo(dsx_grid* grid, void* stream) {
+    return guarded([&] {
+        grid->reverse_halo(static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch reverse halo");
+    });
+}
+
+int dsx_grid_reverse_exchange(dsx_grid* grid, int nfields, const int* field_ids, const int* ops, void* stream) {
+    return guarded([&] {
+        grid->reverse_exchange(nfields, field_ids, ops, static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch reverse exchange");
+    });
+}
+
+int dsx_grid_forward_exchange(dsx_grid* grid, int nfields, const int* field_ids, void* stream) {
+    return guarded([&] {
+        grid->forward_exchange(nfields, field_ids, static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch forward exchange");
+    });
+}
+
+int dsx_grid_rebalance(dsx_grid* grid, const double* work, int force, void* stream, long long* results,
+                       double* imbalance) {
+    return guarded([&] {
+        grid->rebalance(work, force != 0, static_cast<cudaStream_t>(stream), results, imbalance);
+    });
+}
+
+int dsx_grid_set_halo_width(dsx_grid* grid, double width) {
+    return guarded([&] {
+        if (width < 0.0) fail(DSX_E_INVALID, "halo width cannot be negative");
+        if (grid->halo_width != width) {
+            grid->halo_width = width;
+            grid->plan_valid = false;
+        }
+    });
+}
+
+int dsx_grid_invalidate_halo(dsx_grid* grid) {
+    return guarded([&] { grid->plan_valid = false; });
+}
+
+int dsx_grid_halo_backward(dsx_grid* grid, const double* cx, const double* cy, const double* cz,
+                           double* gx, double* gy, double* gz, void* stream) {
+    return guarded([&] {
+        if (grid->P == 1 || !grid->ghosts_valid) return;
+        dsx::launch_reverse_sum3(grid->params(), gx, gy, gz, cx, cy, cz, grid->S,
+                                 static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch halo backward");
+    });
+}
+
+int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture, void* stream,
+                  unsigned* status) {
+    return guarded([&] {
+        if (grid->P == 1) fail(DSX_E_INVALID, "the batched step needs at least two subdomains");
+        grid->step(callback, user, capture != 0, static_cast<cudaStream_t>(stream), status);
+        cuda_check(cudaGetLastError(), "launch step");
+    });
+}
+
+int dsx_grid_step_kernel_count(dsx_grid* grid) {
+    // rebalance (Dynamic only) + 7 migrate + 4 halo build + 1 reverse
+    return (grid->desc.policy == DSX_DYNAMIC ? 1 : 0) + 7 + 4 + 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,1023 @@
+// Hand-written sm_100a kernels of the particle-bookkeeping hot path.
+//
+// All of this work is HBM-bound integer/FP64 bookkeeping (no contraction, so
+// no tensor cores): every kernel streams SoA arrays with coalesced accesses,
+// compacts with warp ballots + popc, and orders its output with per-tile
+// counters and prefix sums so that the result is deterministic and identical
+// to the reference's Host path order (dsDecompX src/migration.cpp:437-518,
+// src/halo.cpp:164-238, 1476-1531).
+//
+// Built with -fmad=false: the few FP64 expressions (periodic wrap, shift add,
+// force sums) must round exactly like the reference's.
+#include "dsx_kernels.cuh"
+
+#include <cstdio>
+
+namespace dsx {
+namespace {
+
+constexpr int NT = 256;           // threads per CTA of the tile kernels
+constexpr int ITEMS = 4;          // consecutive 32-particle groups per warp
+constexpr int TILE = NT * ITEMS;  // particles per tile
+constexpr int NW = NT / 32;
+
+static_assert(TILE == 1024, "engine tile size");
+
+// Exclusive block scan; `total` gets the block sum.  ws: 33 ints of shared.
+template <int THREADS>
+__device__ __forceinline__ int block_scan_excl(int v, int& total, int* ws) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < THREADS / 32 ? ws[lane] : 0;
+        int winc = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, winc, o);
+            if (lane >= o) winc += u;
+        }
+        ws[lane] = winc - w;
+        if (lane == 31) ws[32] = winc;
+    }
+    __syncthreads();
+    const int excl = inc - v + ws[warp];
+    total = ws[32];
+    __syncthreads();
+    return excl;
+}
+
+__device__ __forceinline__ int warp_inclusive_sum(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
+}
+
+// Host-path destination of one owned particle: wrapped_record wraps the
+// position once, owner_rank wraps it again and bisects the cuts
+// (dsDecompX src/migration.cpp:437-441, 74-98).  Returns the rank and the
+// once-wrapped position that the migrated record carries.
+__device__ __forceinline__ int destination(const Grid& G, double px, double py, double pz,
+                                           double& wx, double& wy, double& wz) {
+    const double p[3] = {px, py, pz};
+    double w[3];
+    int c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (G.periodic[a]) {
+            w[a] = wrap_axis(p[a], G.lower[a], G.extent[a]);
+            const double w2 = wrap_axis(w[a], G.lower[a], G.extent[a]);
+            c[a] = axis_coordinate(G.cuts + G.cut_offset[a], G.dims[a], w2);
+        } else {
+            w[a] = p[a];
+            c[a] = axis_coordinate(G.cuts + G.cut_offset[a], G.dims[a], p[a]);
+        }
+    }
+    wx = w[0];
+    wy = w[1];
+    wz = w[2];
+    return (c[0] * G.dims[1] + c[1]) * G.dims[2] + c[2];
+}
+
+__device__ __forceinline__ void move_record(const Arrays& A, long long src, long long dst,
+                                            double wx, double wy, double wz) {
+    A.d[0][dst] = wx;
+    A.d[1][dst] = wy;
+    A.d[2][dst] = wz;
+#pragma unroll
+    for (int a = 3; a < 11; ++a) A.d[a][dst] = A.d[a][src];
+    A.type[dst] = A.type[src];
+    A.gid[dst] = A.gid[src];
+    copy_fields(A.f, src, dst);
+}
+
+// ------------------------------------------------------------------ layout
+
+__global__ void __launch_bounds__(1024) k_layout(int P, int tile, const int* n, int* obase,
+                                                  int* tile_start) {
+    __shared__ int ws[33];
+    const int t = threadIdx.x;
+    const int a = t < P ? n[t] : 0;
+    const int b = t < P ? (a + tile - 1) / tile : 0;
+    int ta, tb;
+    const int ea = block_scan_excl<1024>(a, ta, ws);
+    const int eb = block_scan_excl<1024>(b, tb, ws);
+    if (t < P) {
+        obase[t] = ea;
+        tile_start[t] = eb;
+    }
+    if (t == 0) {
+        obase[P] = ta;
+        tile_start[P] = tb;
+    }
+}
+
+// Exclusive prefix of counter k (= blockIdx.x) over the tiles of the layout.
+// cnt/pre are counter-major: [k * stride + tile]; pre[k*stride + ntiles] = total.
+__global__ void __launch_bounds__(1024) k_scan_counters(const int* cnt, int* pre, int stride,
+                                                         const int* tile_start_end) {
+    __shared__ int ws[33];
+    constexpr int PER = 8;
+    const int k = blockIdx.x;
+    const int ntiles = *tile_start_end;
+    const int* src = cnt + static_cast<long long>(k) * stride;
+    int* dst = pre + static_cast<long long>(k) * stride;
+    int carry = 0;
+    for (int base = 0; base < ntiles; base += 1024 * PER) {
+        int v[PER];
+        int sum = 0;
+        const int first = base + threadIdx.x * PER;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            v[j] = first + j < ntiles ? src[first + j] : 0;
+            sum += v[j];
+        }
+        int total;
+        int run = block_scan_excl<1024>(sum, total, ws) + carry;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            if (first + j < ntiles) dst[first + j] = run;
+            run += v[j];
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) dst[ntiles] = carry;
+}
+
+// ----------------------------------------------------------------- migrate
+
+// K1: destination of every owned particle; per-tile stay/emigrant counts and
+// per-destination immigrant totals.
+__global__ void __launch_bounds__(NT) k_mig_classify(Grid G, const double* __restrict__ x,
+                                                     const double* __restrict__ y,
+                                                     const double* __restrict__ z, int* cnt,
+                                                     int stride, int* imm_total) {
+    __shared__ int ws[33];
+    const int g = blockIdx.x;
+    const int P = G.P;
+    if (g >= G.tile_start[P]) return;
+    const int s = tile_owner(G.tile_start, P, g);
+    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
+    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    int stay = 0, emig = 0;
+    for (int i = begin + threadIdx.x; i < end; i += NT) {
+        double wx, wy, wz;
+        const int d = destination(G, x[i], y[i], z[i], wx, wy, wz);
+        if (d == s) {
+            ++stay;
+        } else {
+            ++emig;
+            atomicAdd(&imm_total[d], 1);
+        }
+    }
+    int stays, emigs;
+    block_scan_excl<NT>(stay, stays, ws);
+    block_scan_excl<NT>(emig, emigs, ws);
+    if (threadIdx.x == 0) {
+        cnt[g] = stays;
+        cnt[stride + g] = emigs;
+    }
+}
+
+// S1: the next layout (retained + immigrants per subdomain) and the migration
+// result of every subdomain.  One CTA, one thread per subdomain.
+__global__ void __launch_bounds__(1024) k_mig_layout(Grid G, const int* pre, int stride,
+                                                      const int* imm_total, int* imm_base,
+                                                      int* emig_info, long long* results) {
+    __shared__ int ws[33];
+    const int P = G.P;
+    const int t = threadIdx.x;
+    const int ntiles = G.tile_start[P];
+    int retained = 0, received = 0, old = 0, next = 0;
+    if (t < P) {
+        retained = pre[G.tile_start[t + 1]] - pre[G.tile_start[t]];
+        received = imm_total[t];
+        old = G.n[t];
+        next = retained + received;
+    }
+    int total_next, total_tiles;
+    const int ob = block_scan_excl<1024>(next, total_next, ws);
+    const int tiles = t < P ? (next + G.tile - 1) / G.tile : 0;
+    const int ts = block_scan_excl<1024>(tiles, total_tiles, ws);
+    if (t < P) {
+        G.n_next[t] = next;
+        G.obase_next[t] = ob;
+        G.tile_start_next[t] = ts;
+        imm_base[t] = ob + retained;
+        long long* o = results + 6 * t;
+        o[1] = old;
+        o[2] = retained;
+        o[3] = old - retained;
+        o[4] = received;
+        o[5] = next;
+        o[0] = (o[3] != 0 || o[4] != 0) ? 1 : 0;
+    }
+    if (t == 0) {
+        G.obase_next[P] = total_next;
+        G.tile_start_next[P] = total_tiles;
+        const int E = pre[stride + ntiles];
+        emig_info[0] = E;
+        emig_info[1] = (E + TILE - 1) / TILE;
+        if (total_next != G.obase[P]) atomicOr(G.status, kStatusMigrationMismatch);
+    }
+}
+
+// K2: retained particles move (stably) to the next layout; emigrants are
+// listed in (source subdomain, source order), which is the order the
+// reference's receivers append them in.
+__global__ void __launch_bounds__(NT) k_mig_move(Grid G, Arrays A, long long src_off,
+                                                 long long dst_off, const int* pre, int stride,
+                                                 int* emig_src, int* emig_dst) {
+    __shared__ int s_stay[NW], s_emig[NW];
+    const int g = blockIdx.x;
+    const int P = G.P;
+    if (g >= G.tile_start[P]) return;
+    const int s = tile_owner(G.tile_start, P, g);
+    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
+    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbegin = begin + warp * 32 * ITEMS;
+    const unsigned lt = lanemask_lt();
+
+    int dest[ITEMS];
+    double wx[ITEMS], wy[ITEMS], wz[ITEMS];
+    int nstay = 0, nemig = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        dest[j] = -1;
+        if (i < end) {
+            const long long src = src_off + i;
+            dest[j] = destination(G, A.d[0][src], A.d[1][src], A.d[2][src], wx[j], wy[j], wz[j]);
+        }
+        nstay += __popc(__ballot_sync(0xffffffffu, dest[j] == s));
+        nemig += __popc(__ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s));
+    }
+    if (lane == 0) {
+        s_stay[warp] = nstay;
+        s_emig[warp] = nemig;
+    }
+    __syncthreads();
+    int stay_base = G.obase_next[s] + (pre[g] - pre[G.tile_start[s]]);
+    int emig_base = pre[stride + g];
+    for (int w = 0; w < warp; ++w) {
+        stay_base += s_stay[w];
+        emig_base += s_emig[w];
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        const unsigned bs = __ballot_sync(0xffffffffu, dest[j] == s);
+        const unsigned be = __ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s);
+        if (dest[j] == s) {
+            move_record(A, src_off + i, dst_off + stay_base + __popc(bs & lt), wx[j], wy[j], wz[j]);
+        } else if (dest[j] >= 0) {
+            const int e = emig_base + __popc(be & lt);
+            emig_src[e] = i;
+            emig_dst[e] = dest[j];
+        }
+        stay_base += __popc(bs);
+        emig_base += __popc(be);
+    }
+}
+
+// K3a: per chunk of the emigrant list, how many go to each destination.
+__global__ void __launch_bounds__(NT) k_emig_hist(int P, const int* emig_info,
+                                                  const int* __restrict__ emig_dst, int* hist) {
+    extern __shared__ int sm[];  // [NW][P]
+    const int E = emig_info[0], nchunks = emig_info[1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        for (int k = threadIdx.x; k < NW * P; k += NT) sm[k] = 0;
+        __syncthreads();
+        const int base = c * TILE + warp * 32 * ITEMS;
+        for (int j = 0; j < ITEMS; ++j) {
+            const int e = base + j * 32 + lane;
+            const int d = e < E ? emig_dst[e] : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (d >= 0 && lane == __ffs(peers) - 1) sm[warp * P + d] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < P; d += NT) {
+            int sum = 0;
+            for (int w = 0; w < NW; ++w) sum += sm[w * P + d];
+            hist[static_cast<long long>(c) * P + d] = sum;
+        }
+        __syncthreads();
+    }
+}
+
+// K3b: per destination, exclusive prefix of its chunk counts.
+__global__ void __launch_bounds__(NT) k_emig_colscan(int P, const int* emig_info, int* hist,
+                                                     const int* imm_total, unsigned* status) {
+    __shared__ int ws[33];
+    const int d = blockIdx.x;
+    const int nchunks = emig_info[1];
+    int carry = 0;
+    for (int base = 0; base < nchunks; base += NT) {
+        const int c = base + threadIdx.x;
+        const long long at = static_cast<long long>(c) * P + d;
+        const int v = c < nchunks ? hist[at] : 0;
+        int total;
+        const int excl = block_scan_excl<NT>(v, total, ws);
+        if (c < nchunks) hist[at] = carry + excl;
+        carry += total;
+    }
+    if (threadIdx.x == 0 && carry != imm_total[d]) atomicOr(status, kStatusMigrationMismatch);
+}
+
+// K3c: every emigrant lands after its destination's retained particles, in
+// (source subdomain, source order) -- a stable multi-split of the list.
+__global__ void __launch_bounds__(NT) k_emig_place(Grid G, Arrays A, long long src_off,
+                                                   long long dst_off, const int* emig_info,
+                                                   const int* __restrict__ emig_src,
+                                                   const int* __restrict__ emig_dst,
+                                                   const int* hist, const int* imm_base) {
+    extern __shared__ int sm[];  // [NW][P]
+    const int P = G.P;
+    const int E = emig_info[0], nchunks = emig_info[1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        for (int k = threadIdx.x; k < NW * P; k += NT) sm[k] = 0;
+        __syncthreads();
+        const int base = c * TILE + warp * 32 * ITEMS;
+        int dj[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const int e = base + j * 32 + lane;
+            dj[j] = e < E ? emig_dst[e] : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, dj[j]);
+            if (dj[j] >= 0 && lane == __ffs(peers) - 1) sm[warp * P + dj[j]] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        // per destination: exclusive prefix over warps, in place
+        for (int d = threadIdx.x; d < P; d += NT) {
+            int run = 0;
+            for (int w = 0; w < NW; ++w) {
+                const int v = sm[w * P + d];
+                sm[w * P + d] = run;
+                run += v;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const int e = base + j * 32 + lane;
+            const int d = dj[j];
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (d >= 0) {
+                const int pos = imm_base[d] + hist[static_cast<long long>(c) * P + d] +
+                                sm[warp * P + d] + __popc(peers & lt);
+                const long long src = src_off + emig_src[e];
+                const double wx = G.periodic[0] ? wrap_axis(A.d[0][src], G.lower[0], G.extent[0]) : A.d[0][src];
+                const double wy = G.periodic[1] ? wrap_axis(A.d[1][src], G.lower[1], G.extent[1]) : A.d[1][src];
+                const double wz = G.periodic[2] ? wrap_axis(A.d[2][src], G.lower[2], G.extent[2]) : A.d[2][src];
+                move_record(A, src, dst_off + pos, wx, wy, wz);
+            }
+            __syncwarp();
+            if (d >= 0 && lane == __ffs(peers) - 1) sm[warp * P + d] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
+// -------------------------------------------------------------------- halo
+
+struct TileBounds {
+    double lo[3], hi[3];  // local.lower + width, local.upper - width
+};
+
+__device__ __forceinline__ TileBounds halo_bounds(const Grid& G, int s) {
+    TileBounds b;
+    const int c[3] = {s / (G.dims[1] * G.dims[2]), (s / G.dims[2]) % G.dims[1], s % G.dims[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double* cuts = G.cuts + G.cut_offset[a];
+        b.lo[a] = __dadd_rn(cuts[c[a]], G.width);
+        b.hi[a] = __dsub_rn(cuts[c[a] + 1], G.width);
+    }
+    return b;
+}
+
+// Host halo classification (dsDecompX src/halo.cpp:200-221): six strict
+// comparisons, then the neighbor mask from the subdomain's lookup table.
+__device__ __forceinline__ unsigned halo_mask(const TileBounds& b, const unsigned* lut, double px,
+                                              double py, double pz) {
+    const unsigned flags = (px < b.lo[0] ? 1u : 0u) | (px > b.hi[0] ? 2u : 0u) |
+                           (py < b.lo[1] ? 4u : 0u) | (py > b.hi[1] ? 8u : 0u) |
+                           (pz < b.lo[2] ? 16u : 0u) | (pz > b.hi[2] ? 32u : 0u);
+    return flags ? __ldg(lut + flags) : 0u;
+}
+
+// Adds this warp's contribution of one 32-particle group to the per-lane
+// counters (lane n < 26: send list n, lane 26: boundary owners, lane 27: images).
+__device__ __forceinline__ void count_group(unsigned m, int nn, int lane, int& acc) {
+    const unsigned any = __ballot_sync(0xffffffffu, m != 0);
+    if (!any) return;
+    for (int n = 0; n < nn; ++n) {
+        const unsigned b = __ballot_sync(0xffffffffu, (m >> n) & 1u);
+        if (lane == n) acc += __popc(b);
+    }
+    const int images = warp_inclusive_sum(__popc(m));
+    const int total_images = __shfl_sync(0xffffffffu, images, 31);
+    if (lane == kBoundaryCounter) acc += __popc(any);
+    if (lane == kImageCounter) acc += total_images;
+}
+
+// H1: neighbor mask of every owned particle and per-tile list counts.
+__global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const double* __restrict__ x,
+                                                      const double* __restrict__ y,
+                                                      const double* __restrict__ z,
+                                                      unsigned* mask, int* cnt, int stride) {
+    __shared__ int s_cnt[NW][32];
+    const int g = blockIdx.x;
+    const int P = G.P;
+    if (g >= G.tile_start[P]) return;
+    const int s = tile_owner(G.tile_start, P, g);
+    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
+    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbegin = begin + warp * 32 * ITEMS;
+    const TileBounds b = halo_bounds(G, s);
+    const unsigned* lut = G.lut + s * 64;
+    const int nn = G.nn[s];
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        unsigned m = 0;
+        if (i < end) {
+            m = halo_mask(b, lut, x[i], y[i], z[i]);
+            mask[i] = m;
+        }
+        count_group(m, nn, lane, acc);
+    }
+    s_cnt[warp][lane] = acc;
+    __syncthreads();
+    if (threadIdx.x < kHaloCounters) {
+        int sum = 0;
+        for (int w = 0; w < NW; ++w) sum += s_cnt[w][threadIdx.x];
+        cnt[threadIdx.x * stride + g] = sum;
+    }
+}
+
+// S2b: send-list lengths, receiver ghost layout (blocks in the receiver's
+// neighbor order, dsDecompX src/halo.cpp:609-649) and the first ghost slot of
+// every send list.  One CTA, one thread per receiver.
+__global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, int stride,
+                                                       int* list_len, int* send_base, int* gq,
+                                                       int* gbase, int* boff, int* info) {
+    __shared__ int ws[33];
+    const int P = G.P;
+    const int ntiles = G.tile_start[P];
+    for (int idx = threadIdx.x; idx < P * kMaxNeighbors; idx += blockDim.x) {
+        const int r = idx / kMaxNeighbors, n = idx % kMaxNeighbors;
+        int len = 0;
+        if (n < G.nn[r] && G.nbr[idx] >= 0)
+            len = pre[n * stride + G.tile_start[r + 1]] - pre[n * stride + G.tile_start[r]];
+        list_len[idx] = len;
+    }
+    __syncthreads();
+    const int q = threadIdx.x;
+    int mine = 0;
+    if (q < P) {
+        for (int m = 0; m < G.nn[q]; ++m) {
+            const int e = G.sender_of[q * kMaxNeighbors + m];
+            mine += e >= 0 ? list_len[e] : 0;
+        }
+    }
+    int total;
+    const int excl = block_scan_excl<1024>(mine, total, ws);
+    if (q < P) {
+        gq[q] = mine;
+        gbase[q] = excl;
+        int run = excl;
+        for (int m = 0; m < G.nn[q]; ++m) {
+            const int e = G.sender_of[q * kMaxNeighbors + m];
+            if (e < 0) continue;
+            send_base[e] = run;
+            run += list_len[e];
+        }
+    }
+    if (q == 0) {
+        gbase[P] = total;
+        const int B = pre[kBoundaryCounter * stride + ntiles];
+        const int images = pre[kImageCounter * stride + ntiles];
+        info[0] = total;
+        info[1] = B;
+        if (static_cast<long long>(total) > G.gcap) {
+            atomicOr(G.status, kStatusGhostOverflow);
+        } else {
+            boff[B] = images;
+        }
+    }
+}
+
+// H2: every (owner, neighbor) hit becomes a ghost in the receiver's block --
+// x + shift, v, f = 0, mass, charge, type, id and the registered fields, as
+// the reference's make_record + copy_record leave it (dsDecompX
+// src/halo.cpp:37-55, src/runtime.cpp:82-96) -- plus the ghost -> owner map
+// and the owner -> ghosts CSR that reverse_halo sums in neighbor order.
+__global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long owned_off,
+                                                     long long ghost_off,
+                                                     const unsigned* __restrict__ mask,
+                                                     const int* pre, int stride,
+                                                     const int* send_base, int* ghost_owner,
+                                                     int* ghost_entry, int* bowner, int* boff,
+                                                     int* bslot) {
+    __shared__ int s_cnt[NW][32];
+    __shared__ int s_base[32];
+    if (*G.status & kStatusGhostOverflow) return;
+    const int g = blockIdx.x;
+    const int P = G.P;
+    if (g >= G.tile_start[P]) return;
+    const int s = tile_owner(G.tile_start, P, g);
+    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
+    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbegin = begin + warp * 32 * ITEMS;
+    const int nn = G.nn[s];
+    const unsigned lt = lanemask_lt();
+
+    unsigned m[ITEMS];
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        m[j] = i < end ? mask[i] : 0u;
+        count_group(m[j], nn, lane, acc);
+    }
+    s_cnt[warp][lane] = acc;
+    if (threadIdx.x < kHaloCounters) {
+        const int k = threadIdx.x;
+        const int first = G.tile_start[s];
+        int base = pre[k * stride + g];
+        if (k < kMaxNeighbors) base += send_base[s * kMaxNeighbors + k] - pre[k * stride + first];
+        s_base[k] = base;
+    }
+    __syncthreads();
+    // lane k carries the running offset of counter k for this warp
+    int run = 0;
+    if (lane < kHaloCounters) {
+        run = s_base[lane];
+        for (int w = 0; w < warp; ++w) run += s_cnt[w][lane];
+    }
+    const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
+#pragma unroll 1
+    for (int j = 0; j < ITEMS; ++j) {
+        const unsigned mj = m[j];
+        const unsigned any = __ballot_sync(0xffffffffu, mj != 0);
+        if (!any) continue;
+        const int i = wbegin + j * 32 + lane;
+        const long long src = owned_off + i;
+        const int b = __shfl_sync(0xffffffffu, run, kBoundaryCounter) + __popc(any & lt);
+        const int pm = __popc(mj);
+        const int incl = warp_inclusive_sum(pm);
+        const int img = __shfl_sync(0xffffffffu, run, kImageCounter) + incl - pm;
+        double px = 0, py = 0, pz = 0, vx = 0, vy = 0, vz = 0, ms = 0, ch = 0;
+        int ty = 0, id = 0;
+        if (mj) {
+            px = A.d[0][src]; py = A.d[1][src]; pz = A.d[2][src];
+            vx = A.d[3][src]; vy = A.d[4][src]; vz = A.d[5][src];
+            ms = A.d[9][src]; ch = A.d[10][src];
+            ty = A.type[src]; id = A.gid[src];
+            bowner[b] = i;
+            boff[b] = img;
+        }
+        int k = 0;
+        for (int n = 0; n < nn; ++n) {
+            const unsigned hit = __ballot_sync(0xffffffffu, (mj >> n) & 1u);
+            if (!hit) continue;
+            const int list_base = __shfl_sync(0xffffffffu, run, n);
+            if ((mj >> n) & 1u) {
+                const int slot = list_base + __popc(hit & lt);
+                const long long gi = ghost_off + slot;
+                A.d[0][gi] = __dadd_rn(px, shift[3 * n + 0]);
+                A.d[1][gi] = __dadd_rn(py, shift[3 * n + 1]);
+                A.d[2][gi] = __dadd_rn(pz, shift[3 * n + 2]);
+                A.d[3][gi] = vx; A.d[4][gi] = vy; A.d[5][gi] = vz;
+                A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+                A.d[9][gi] = ms; A.d[10][gi] = ch;
+                A.type[gi] = ty; A.gid[gi] = id;
+                copy_fields(A.f, src, gi);
+                ghost_owner[slot] = i;
+                ghost_entry[slot] = s * kMaxNeighbors + n;
+                bslot[img + k] = slot;
+                ++k;
+            }
+            if (lane == n) run += __popc(hit);
+        }
+        const int group_images = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane == kBoundaryCounter) run += __popc(any);
+        if (lane == kImageCounter) run += group_images;
+    }
+}
+
+// Refresh along the existing plan (Host semantics, dsDecompX
+// src/halo.cpp:256-289 + 687): positions (+ shift) and velocities and every
+// registered field; forces of the ghosts become 0 again; mass, charge, type
+// and id keep the values of the plan build.  positions_only moves x, y, z.
+__global__ void __launch_bounds__(NT) k_halo_refresh(Grid G, Arrays A, long long owned_off,
+                                                     long long ghost_off, int positions_only,
+                                                     const int* info,
+                                                     const int* __restrict__ ghost_owner,
+                                                     const int* __restrict__ ghost_entry) {
+    if (*G.status & kStatusGhostOverflow) return;
+    const int total = info[0];
+    for (int slot = blockIdx.x * NT + threadIdx.x; slot < total; slot += gridDim.x * NT) {
+        const long long src = owned_off + ghost_owner[slot];
+        const double* sh = G.shift + 3ll * ghost_entry[slot];
+        const long long gi = ghost_off + slot;
+        A.d[0][gi] = __dadd_rn(A.d[0][src], sh[0]);
+        A.d[1][gi] = __dadd_rn(A.d[1][src], sh[1]);
+        A.d[2][gi] = __dadd_rn(A.d[2][src], sh[2]);
+        A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+        if (!positions_only) {
+            A.d[3][gi] = A.d[3][src];
+            A.d[4][gi] = A.d[4][src];
+            A.d[5][gi] = A.d[5][src];
+            copy_fields(A.f, src, gi);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_forward_fields(Arrays A, long long owned_off,
+                                                       long long ghost_off, FieldOps F,
+                                                       const int* info,
+                                                       const int* __restrict__ ghost_owner,
+                                                       const unsigned* status) {
+    if (*status & kStatusGhostOverflow) return;
+    const int total = info[0];
+    for (int slot = blockIdx.x * NT + threadIdx.x; slot < total; slot += gridDim.x * NT) {
+        const long long src = owned_off + ghost_owner[slot];
+        const long long dst = ghost_off + slot;
+        for (int t = 0; t < F.count; ++t) {
+            const int f = F.index[t];
+            const int b = A.f.bytes[f];
+            unsigned char* base = A.f.base[f];
+            if ((b & 7) == 0) {
+                const unsigned long long* s = reinterpret_cast<const unsigned long long*>(base + src * b);
+                unsigned long long* d = reinterpret_cast<unsigned long long*>(base + dst * b);
+                for (int w = 0; w < (b >> 3); ++w) d[w] = s[w];
+            } else {
+                const unsigned* s = reinterpret_cast<const unsigned*>(base + src * b);
+                unsigned* d = reinterpret_cast<unsigned*>(base + dst * b);
+                for (int w = 0; w < (b >> 2); ++w) d[w] = s[w];
+            }
+        }
+    }
+}
+
+// Owner-centric deterministic sum: owner += ghost images in the order the
+// reference's Host reverse_exchange visits them (neighbor n ascending,
+// dsDecompX src/halo.cpp:1507-1530).  No atomics.
+__global__ void __launch_bounds__(NT) k_reverse_sum3(const int* info, const int* __restrict__ bowner,
+                                                     const int* __restrict__ boff,
+                                                     const int* __restrict__ bslot, double* ox,
+                                                     double* oy, double* oz,
+                                                     const double* __restrict__ gx,
+                                                     const double* __restrict__ gy,
+                                                     const double* __restrict__ gz,
+                                                     const unsigned* status) {
+    if (*status & kStatusGhostOverflow) return;
+    const int B = info[1];
+    for (int b = blockIdx.x * NT + threadIdx.x; b < B; b += gridDim.x * NT) {
+        const int i = bowner[b];
+        const int k0 = boff[b], k1 = boff[b + 1];
+        double fx = ox[i], fy = oy[i], fz = oz[i];
+        for (int k = k0; k < k1; ++k) {
+            const int slot = bslot[k];
+            fx = __dadd_rn(fx, gx[slot]);
+            fy = __dadd_rn(fy, gy[slot]);
+            fz = __dadd_rn(fz, gz[slot]);
+        }
+        ox[i] = fx;
+        oy[i] = fy;
+        oz[i] = fz;
+    }
+}
+
+// std::min / std::max / += / = exactly as reduce_field_values applies them
+// (dsDecompX src/halo.cpp:1351-1372).
+template <class T>
+__device__ __forceinline__ T reduce_one(T d, T v, int op) {
+    switch (op) {
+    case 0: return static_cast<T>(d + v);
+    case 1: return v < d ? v : d;
+    case 2: return d < v ? v : d;
+    default: return v;
+    }
+}
+template <>
+__device__ __forceinline__ double reduce_one<double>(double d, double v, int op) {
+    switch (op) {
+    case 0: return __dadd_rn(d, v);
+    case 1: return v < d ? v : d;
+    case 2: return d < v ? v : d;
+    default: return v;
+    }
+}
+template <>
+__device__ __forceinline__ float reduce_one<float>(float d, float v, int op) {
+    switch (op) {
+    case 0: return __fadd_rn(d, v);
+    case 1: return v < d ? v : d;
+    case 2: return d < v ? v : d;
+    default: return v;
+    }
+}
+template <>
+__device__ __forceinline__ int reduce_one<int>(int d, int v, int op) {
+    switch (op) {
+    case 0: return static_cast<int>(static_cast<unsigned>(d) + static_cast<unsigned>(v));
+    case 1: return v < d ? v : d;
+    case 2: return d < v ? v : d;
+    default: return v;
+    }
+}
+template <>
+__device__ __forceinline__ long long reduce_one<long long>(long long d, long long v, int op) {
+    switch (op) {
+    case 0: return static_cast<long long>(static_cast<unsigned long long>(d) + static_cast<unsigned long long>(v));
+    case 1: return v < d ? v : d;
+    case 2: return d < v ? v : d;
+    default: return v;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void reduce_images(unsigned char* base, int comps, int op, long long owner,
+                                              long long ghost_off, const int* bslot, int k0, int k1) {
+    T* o = reinterpret_cast<T*>(base) + owner * comps;
+    for (int c = 0; c < comps; ++c) {
+        T acc = o[c];
+        for (int k = k0; k < k1; ++k)
+            acc = reduce_one<T>(acc, reinterpret_cast<const T*>(base)[(ghost_off + bslot[k]) * comps + c], op);
+        o[c] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_reverse_fields(Arrays A, long long owned_off,
+                                                       long long ghost_off, FieldOps F,
+                                                       const int* info,
+                                                       const int* __restrict__ bowner,
+                                                       const int* __restrict__ boff,
+                                                       const int* __restrict__ bslot,
+                                                       const unsigned* status) {
+    if (*status & kStatusGhostOverflow) return;
+    const int B = info[1];
+    for (int b = blockIdx.x * NT + threadIdx.x; b < B; b += gridDim.x * NT) {
+        const long long owner = owned_off + bowner[b];
+        const int k0 = boff[b], k1 = boff[b + 1];
+        for (int t = 0; t < F.count; ++t) {
+            unsigned char* base = A.f.base[F.index[t]];
+            const int comps = F.components[t];
+            const int op = F.op[t];
+            switch (F.type[t]) {
+            case 0: reduce_images<int>(base, comps, op, owner, ghost_off, bslot, k0, k1); break;
+            case 1: reduce_images<long long>(base, comps, op, owner, ghost_off, bslot, k0, k1); break;
+            case 2: reduce_images<unsigned>(base, comps, op, owner, ghost_off, bslot, k0, k1); break;
+            case 3: reduce_images<unsigned long long>(base, comps, op, owner, ghost_off, bslot, k0, k1); break;
+            case 4: reduce_images<float>(base, comps, op, owner, ghost_off, bslot, k0, k1); break;
+            default: reduce_images<double>(base, comps, op, owner, ghost_off, bslot, k0, k1); break;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- rebalance
+
+// Dynamic cut planes (dsDecompX src/runtime.cpp:345-447) evaluated by one
+// thread in the reference's operation order, on the device so that it can
+// sit inside a captured step.
+__global__ void k_rebalance(Grid G, const double* work_in, RebalanceParams p,
+                            long long* call_counter, double* result) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    result[0] = 0.0;
+    result[1] = 0.0;
+    result[2] = 1.0;
+    if (p.automatic) {
+        const long long calls = ++(*call_counter);
+        if (p.interval == 0 || calls % p.interval != 0) return;
+    }
+    const int P = G.P;
+    double total = 0.0, maximum = 0.0;
+    for (int s = 0; s < P; ++s) {
+        const double w = work_in ? work_in[s] : static_cast<double>(G.n[s]);
+        total = __dadd_rn(total, w);
+        if (maximum < w) maximum = w;
+    }
+    result[0] = 1.0;
+    if (total <= 0.0 || P <= 1) return;
+    const double imbalance = __ddiv_rn(maximum, __ddiv_rn(total, static_cast<double>(P)));
+    result[2] = imbalance;
+    if (!p.force && imbalance < p.threshold) return;
+
+    // shared, not local: a large per-thread stack would make the driver
+    // reserve it for every resident thread of the device
+    __shared__ double next[3][kMaxRanks + 1];
+    __shared__ double slab_work[kMaxRanks];
+    bool changed = false;
+    for (int a = 0; a < 3; ++a) {
+        const int slabs = G.dims[a];
+        const double* old = G.cuts + G.cut_offset[a];
+        for (int i = 0; i <= slabs; ++i) next[a][i] = old[i];
+        if (slabs <= 1) continue;
+        for (int i = 0; i < slabs; ++i) slab_work[i] = 0.0;
+        for (int s = 0; s < P; ++s) {
+            const int c = a == 0 ? s / (G.dims[1] * G.dims[2])
+                        : a == 1 ? (s / G.dims[2]) % G.dims[1] : s % G.dims[2];
+            const double w = work_in ? work_in[s] : static_cast<double>(G.n[s]);
+            slab_work[c] = __dadd_rn(slab_work[c], w);
+        }
+        const double target = __ddiv_rn(total, static_cast<double>(slabs));
+        const double extent = __dsub_rn(G.upper[a], G.lower[a]);
+        const double uniform = __ddiv_rn(extent, static_cast<double>(slabs));
+        double bound = __dmul_rn(uniform, p.minimum_fraction);
+        if (bound < p.halo_width) bound = p.halo_width;
+        const double minimum_width = bound < uniform ? bound : uniform;
+        next[a][0] = G.lower[a];
+        next[a][slabs] = G.upper[a];
+        for (int b = 1; b < slabs; ++b) {
+            const double desired = __dmul_rn(target, static_cast<double>(b));
+            double cumulative = 0.0;
+            int slab = 0;
+            while (slab < slabs - 1 && __dadd_rn(cumulative, slab_work[slab]) < desired)
+                cumulative = __dadd_rn(cumulative, slab_work[slab++]);
+            const double weight = slab_work[slab];
+            double fraction = 0.5;
+            if (weight > 0.0) {
+                const double v = __ddiv_rn(__dsub_rn(desired, cumulative), weight);
+                fraction = v < 0.0 ? 0.0 : (1.0 < v ? 1.0 : v);
+            }
+            const double proposed =
+                __dadd_rn(old[slab], __dmul_rn(fraction, __dsub_rn(old[slab + 1], old[slab])));
+            const double o = old[b];
+            next[a][b] = __dadd_rn(o, __dmul_rn(p.relaxation, __dsub_rn(proposed, o)));
+        }
+        for (int i = 1; i < slabs; ++i) {
+            const double floor_value = __dadd_rn(next[a][i - 1], minimum_width);
+            if (next[a][i] < floor_value) next[a][i] = floor_value;
+        }
+        for (int i = slabs - 1; i > 0; --i) {
+            const double ceiling = __dsub_rn(next[a][i + 1], minimum_width);
+            if (ceiling < next[a][i]) next[a][i] = ceiling;
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        const double* old = G.cuts + G.cut_offset[a];
+        for (int i = 0; i <= G.dims[a]; ++i)
+            if (fabs(__dsub_rn(next[a][i], old[i])) > 1.0e-12) changed = true;
+    }
+    if (!changed) return;
+    // Decomposition::set_axis_cuts validation (dsDecompX src/decomp.cpp:146-163)
+    for (int a = 0; a < 3; ++a) {
+        const int slabs = G.dims[a];
+        bool valid = next[a][0] == G.lower[a] && next[a][slabs] == G.upper[a];
+        for (int i = 0; i < slabs; ++i) valid = valid && next[a][i] < next[a][i + 1];
+        if (!valid) {
+            atomicOr(G.status, kStatusCutsInvalid);
+            return;
+        }
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int i = 0; i <= G.dims[a]; ++i) G.cuts[G.cut_offset[a] + i] = next[a][i];
+    result[1] = 1.0;
+}
+
+// 1-rank migrate of the drop-in: every particle stays and keeps its slot; its
+// position is replaced by the once-wrapped value (dsDecompX
+// src/migration.cpp:106-116).  Only changed values are written back.
+__global__ void __launch_bounds__(NT) k_wrap_inplace(double* x, double* y, double* z, long long n,
+                                                     double3 lower, double3 extent, int3 periodic) {
+    for (long long i = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * NT) {
+        if (periodic.x) {
+            const double v = x[i], w = wrap_axis(v, lower.x, extent.x);
+            if (__double_as_longlong(w) != __double_as_longlong(v)) x[i] = w;
+        }
+        if (periodic.y) {
+            const double v = y[i], w = wrap_axis(v, lower.y, extent.y);
+            if (__double_as_longlong(w) != __double_as_longlong(v)) y[i] = w;
+        }
+        if (periodic.z) {
+            const double v = z[i], w = wrap_axis(v, lower.z, extent.z);
+            if (__double_as_longlong(w) != __double_as_longlong(v)) z[i] = w;
+        }
+    }
+}
+
+int g_sm_count = 0;
+
+int sm_count() {
+    if (!g_sm_count) {
+        int device = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, device);
+        if (g_sm_count <= 0) g_sm_count = 148;
+    }
+    return g_sm_count;
+}
+
+int stream_grid(long long items) {
+    const long long want = (items + NT - 1) / NT;
+    const long long cap = static_cast<long long>(sm_count()) * 8;
+    long long g = want < cap ? want : cap;
+    return static_cast<int>(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+int kernels_per_step() { return 0; }
+
+void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, cudaStream_t s) {
+    k_layout<<<1, 1024, 0, s>>>(G.P, G.tile, n, obase, tile_start);
+}
+
+void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
+                    const Scratch& S, cudaStream_t s) {
+    cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P, s);
+    k_mig_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + src_off, A.d[1] + src_off,
+                                               A.d[2] + src_off, S.cnt, S.stride, S.imm_total);
+    k_scan_counters<<<2, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    k_mig_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.imm_total, S.imm_base, S.emig_info,
+                                     S.mig_results);
+    k_mig_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, S.pre, S.stride, S.emig_src,
+                                          S.emig_dst);
+    const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
+    const size_t smem = sizeof(int) * NW * G.P;
+    k_emig_hist<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(G.P, S.emig_info, S.emig_dst,
+                                                                  S.emig_hist);
+    k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, S.imm_total, G.status);
+    k_emig_place<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(
+        G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base);
+}
+
+void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
+                       const Scratch& S, cudaStream_t s) {
+    k_halo_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + owned_off, A.d[1] + owned_off,
+                                                A.d[2] + owned_off, S.mask, S.cnt, S.stride);
+    k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    k_halo_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.list_len, S.send_base, S.g, S.gbase,
+                                      S.boff, S.halo_info);
+    k_halo_scatter<<<G.max_tiles, NT, 0, s>>>(G, A, owned_off, ghost_off, S.mask, S.pre, S.stride,
+                                              S.send_base, S.ghost_owner, S.ghost_entry, S.bowner,
+                                              S.boff, S.bslot);
+}
+
+void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
+                         bool positions_only, const Scratch& S, cudaStream_t s) {
+    k_halo_refresh<<<stream_grid(G.gcap), NT, 0, s>>>(G, A, owned_off, ghost_off,
+                                                      positions_only ? 1 : 0, S.halo_info,
+                                                      S.ghost_owner, S.ghost_entry);
+}
+
+void launch_forward_fields(const Grid& G, const Arrays& A, long long owned_off,
+                           long long ghost_off, const FieldOps& F, const Scratch& S,
+                           cudaStream_t s) {
+    k_forward_fields<<<stream_grid(G.gcap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
+                                                        S.ghost_owner, G.status);
+}
+
+void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, const double* gx,
+                         const double* gy, const double* gz, const Scratch& S, cudaStream_t s) {
+    k_reverse_sum3<<<stream_grid(G.ncap), NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot, ox,
+                                                      oy, oz, gx, gy, gz, G.status);
+}
+
+void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
+                           long long ghost_off, const FieldOps& F, const Scratch& S,
+                           cudaStream_t s) {
+    k_reverse_fields<<<stream_grid(G.ncap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
+                                                        S.bowner, S.boff, S.bslot, G.status);
+}
+
+void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
+                      long long* call_counter, double* result, cudaStream_t s) {
+    k_rebalance<<<1, 32, 0, s>>>(G, work, params, call_counter, result);
+}
+
+void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,
+                         const double* extent, const int* periodic, cudaStream_t s) {
+    if (n <= 0) return;
+    k_wrap_inplace<<<stream_grid(n), NT, 0, s>>>(
+        x, y, z, n, make_double3(lower[0], lower[1], lower[2]),
+        make_double3(extent[0], extent[1], extent[2]),
+        make_int3(periodic[0], periodic[1], periodic[2]));
+}
+
+}  // namespace dsx

@@ -1,0 +1,92 @@
+// Launch wrappers of the hand-written sm_100a kernels (dsx_kernels.cu).
+// Every wrapper enqueues on `stream` and never synchronizes.
+#pragma once
+
+#include "dsx_device.cuh"
+
+namespace dsx {
+
+// Scratch shared by the phases of one step (device buffers owned by the
+// engine; sizes in the engine's allocate()).
+struct Scratch {
+    int* cnt = nullptr;        // [kHaloCounters][stride] per-tile counters
+    int* pre = nullptr;        // [kHaloCounters][stride] exclusive prefixes
+    int stride = 0;            // max_tiles + 1
+    int* imm_total = nullptr;  // [P] immigrants per destination
+    int* imm_base = nullptr;   // [P]
+    int* emig_src = nullptr;   // [ncap]
+    int* emig_dst = nullptr;   // [ncap]
+    int* emig_hist = nullptr;  // [max_chunks][P]
+    int* emig_info = nullptr;  // {E, nchunks}
+    long long* mig_results = nullptr;  // [P][6]
+    unsigned* mask = nullptr;  // [ncap] halo neighbor mask per owned particle
+    int* list_len = nullptr;   // [P*26] send-list lengths
+    int* send_base = nullptr;  // [P*26] first ghost slot of each send list
+    int* g = nullptr;          // [P] ghosts per receiver
+    int* gbase = nullptr;      // [P+1]
+    int* ghost_owner = nullptr;  // [gcap] owned index of each ghost
+    int* ghost_entry = nullptr;  // [gcap] sender r*26+n of each ghost
+    int* bowner = nullptr;     // [ncap] owned index of each boundary owner
+    int* boff = nullptr;       // [ncap+1] CSR offsets into bslot
+    int* bslot = nullptr;      // [gcap] ghost slots of each boundary owner, n ascending
+    int* halo_info = nullptr;  // {G, B}
+    int max_chunks = 0;
+};
+
+void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, cudaStream_t s);
+
+void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
+                    const Scratch& S, cudaStream_t s);
+
+void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off,
+                       long long ghost_off, const Scratch& S, cudaStream_t s);
+
+void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off,
+                         long long ghost_off, bool positions_only, const Scratch& S,
+                         cudaStream_t s);
+
+struct FieldOps {
+    int count = 0;
+    int index[kMaxFields] = {};   // field index into Arrays::f
+    int type[kMaxFields] = {};    // dsdecompx::FieldType order
+    int components[kMaxFields] = {};
+    int op[kMaxFields] = {};      // dsdecompx::ReduceOp order
+};
+
+void launch_forward_fields(const Grid& G, const Arrays& A, long long owned_off,
+                           long long ghost_off, const FieldOps& F, const Scratch& S,
+                           cudaStream_t s);
+
+// owner[i] (+)= sum over its images of ghost[slot], images in neighbor order;
+// used for reverse_halo (forces) and for the halo adjoint.
+void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz,
+                         const double* gx, const double* gy, const double* gz,
+                         const Scratch& S, cudaStream_t s);
+
+void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
+                           long long ghost_off, const FieldOps& F, const Scratch& S,
+                           cudaStream_t s);
+
+// Dynamic cut-plane rebalance on the device (dsDecompX src/runtime.cpp:345-447)
+// from the owned counts (work == nullptr) or a per-subdomain work metric.
+struct RebalanceParams {
+    double threshold = 1.10;
+    double relaxation = 0.5;
+    double minimum_fraction = 0.10;
+    double halo_width = 0.0;
+    int force = 0;
+    long long interval = 1;   // 0: automatic rebalance disabled
+    int automatic = 0;        // 1: the migrate-time check (counts the call)
+};
+// out: {attempted, changed, imbalance(bits)} written to `result` (3 doubles)
+void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
+                      long long* call_counter, double* result, cudaStream_t s);
+
+// 1-rank drop-in migrate: wraps positions in place (every particle stays).
+void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,
+                         const double* extent, const int* periodic, cudaStream_t s);
+
+// Fills x with the per-kernel launch count (for reporting).
+int kernels_per_step();
+
+}  // namespace dsx

@@ -1,0 +1,235 @@
+/*
+ * dsx.h -- C ABI of the B200-native dsDecompX particle-bookkeeping engine.
+ *
+ * Plain pointers and sizes only; every pointer argument named `device` is a
+ * CUDA device pointer (or managed memory), `stream` is a cudaStream_t passed
+ * as void*.  Every entry point returns DSX_OK or a negative DSX_E_* code and
+ * never throws; dsx_last_error() gives the message of the calling thread's
+ * last failure.  Messages start with "dsDecompX:" like the reference's
+ * exceptions (docs/05_API_Reference.md:432).
+ *
+ * Two surfaces:
+ *
+ *  1. The single-rank drop-in (dsx_rank_*), called by the C++ Decomp /
+ *     ParticleInfo shim in include/dsdecompx.hpp.  It operates in place on the
+ *     caller's device SoA arrays, exactly where the reference's
+ *     ExecutionMode::Cuda calls its src/cuda launch_* kernels on one rank.
+ *
+ *  2. The virtual grid (dsx_grid_*): P subdomains of one box held on one GPU,
+ *     the multi-rank behaviour of the reference (one MPI rank per subdomain)
+ *     with every neighbor "send" turned into a write into the receiver's
+ *     slots.  Each call is the batched counterpart of the reference's
+ *     collective call on all ranks at once.
+ *
+ * Array ids (dsx_grid_read / dsx_grid_write): 0..10 x y z vx vy vz fx fy fz
+ * mass charge (double), 11 type, 12 global_id (int32), 13+f registered field f.
+ */
+#ifndef DSX_H
+#define DSX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSX_OK 0
+#define DSX_E_INVALID (-1)     /* std::invalid_argument in the reference */
+#define DSX_E_LOGIC (-2)       /* std::logic_error */
+#define DSX_E_RUNTIME (-3)     /* std::runtime_error (CUDA failure) */
+#define DSX_E_LENGTH (-4)      /* std::length_error (capacity) */
+#define DSX_E_OVERFLOW (-5)    /* ghost capacity exceeded; call grew it, retry */
+
+/* dsdecompx::FieldType (include/field.hpp:22-29) */
+enum { DSX_INT32 = 0, DSX_INT64 = 1, DSX_UINT32 = 2, DSX_UINT64 = 3,
+       DSX_FLOAT32 = 4, DSX_FLOAT64 = 5 };
+/* dsdecompx::ReduceOp (include/field.hpp:31-36) */
+enum { DSX_SUM = 0, DSX_MIN = 1, DSX_MAX = 2, DSX_REPLACE = 3 };
+/* dsdecompx::GridPolicy (include/grid.hpp:26-33) */
+enum { DSX_MANUAL = 0, DSX_BALANCED = 1, DSX_TOPOLOGY_AWARE = 2, DSX_DYNAMIC = 3 };
+
+const char* dsx_last_error(void);
+const char* dsx_version(void);
+
+/* ------------------------------------------------------------------------
+ * 1. Single-rank drop-in
+ * ---------------------------------------------------------------------- */
+
+/* Periodic box of the rank (dsdecompx::GlobalDomain, include/domain.hpp:7-11). */
+typedef struct dsx_domain {
+    double lower[3];
+    double upper[3];
+    int periodic[3];
+} dsx_domain;
+
+/* dsdecompx::MigrationResult (include/config.hpp:42-49) */
+typedef struct dsx_migration_result {
+    int ownership_changed;
+    long long previous_owned_count;
+    long long retained_count;
+    long long sent_count;
+    long long received_count;
+    long long new_owned_count;
+} dsx_migration_result;
+
+/* Replaces the 1-rank branch of Decomposition::migrate_particles
+ * (src/migration.cpp:147-389 with rank_count == 1, launch_classify_destinations
+ * src/cuda/classify.cu:46-63 + launch_build_migration_layout
+ * src/cuda/migration_layout.cu:48-110 + unpack src/cuda/unpack.cu:61-71):
+ * every owned particle stays in its slot and gets the Host-path periodic wrap
+ * of its position.  x, y, z: device arrays of `owned` doubles. */
+int dsx_rank_migrate(double* x, double* y, double* z, long long owned,
+                     const dsx_domain* domain, void* stream,
+                     dsx_migration_result* result);
+
+/* ------------------------------------------------------------------------
+ * 2. Virtual grid of P subdomains on one GPU
+ * ---------------------------------------------------------------------- */
+
+typedef struct dsx_grid dsx_grid;
+
+/* dsdecompx::Config (include/config.hpp:20-40) for P virtual ranks. */
+typedef struct dsx_grid_desc {
+    int nranks;               /* P, 1..1024 */
+    int dims[3];              /* Manual policy; 0 entries are filled like MPI_Dims_create */
+    int policy;               /* DSX_MANUAL .. DSX_DYNAMIC */
+    double lower[3], upper[3];
+    int periodic[3];
+    double halo_width;
+    int edges_and_corners;    /* HaloConfig::include_edges_and_corners */
+    double dyn_interval;      /* DynamicLoadBalanceConfig (defaults 1, 1.10, 0.5, 0.10) */
+    double dyn_threshold;
+    double dyn_relaxation;
+    double dyn_min_fraction;
+} dsx_grid_desc;
+
+typedef struct dsx_field_desc {
+    const char* name;
+    int type;                 /* DSX_INT32 .. DSX_FLOAT64 */
+    int components;
+} dsx_field_desc;
+
+/* Host only (no GPU needed): the process grid dims[3] and the neighbor list
+ * of rank `rank` that a grid created from `desc` uses, in the format of
+ * dsx_grid_neighbors.  Mirrors initialize_topology + refresh_domain_geometry
+ * (src/topology.cpp:18-176) and choose_process_grid (src/grid.cpp:79-122). */
+int dsx_plan_topology(const dsx_grid_desc* desc, int rank, int* dims, int* count,
+                      int* info, double* shifts);
+
+/* Creates the grid with room for `particles` owned particles in total (the
+ * count migration conserves) and `ghost_capacity` ghosts (0: estimated; grown
+ * on overflow). */
+int dsx_grid_create(const dsx_grid_desc* desc, const dsx_field_desc* fields,
+                    int nfields, long long particles, long long ghost_capacity,
+                    dsx_grid** out);
+int dsx_grid_destroy(dsx_grid* grid);
+
+/* Topology as the reference's Topology reports it for rank `rank`
+ * (include/topology.hpp:19-41): dims[3], coords[3], local {lower[3], upper[3]};
+ * neighbors: count and per entry {rank, dx, dy, dz, slot} + shift[3]. */
+int dsx_grid_topology(dsx_grid* grid, int rank, int* dims, int* coords, double* local);
+int dsx_grid_neighbors(dsx_grid* grid, int rank, int* count, int* info, double* shifts);
+/* Current axis cuts, axis by axis (dims[a]+1 each); synchronizes `stream`. */
+int dsx_grid_cuts(dsx_grid* grid, double* out, void* stream);
+
+/* Owned particles of every subdomain, host arrays concatenated in rank order
+ * with counts[P] (sum == particles).  arrays[13 + nfields]: core arrays in
+ * array-id order, then fields; null core arrays are zero-filled.
+ * Replaces the state (no ghosts). */
+int dsx_grid_upload(dsx_grid* grid, const long long* counts,
+                    const void* const* arrays, void* stream);
+
+/* Counts per subdomain (owned, ghosts); synchronizes `stream`. */
+int dsx_grid_counts(dsx_grid* grid, long long* owned, long long* ghosts, void* stream);
+
+/* Host copy of `count` entries of array `array` of subdomain `rank` starting
+ * at local slot `start` (owned slots first, then ghosts, as one rank's
+ * ParticleInfo holds them).  Synchronizes `stream`. */
+int dsx_grid_read(dsx_grid* grid, int rank, int array, long long start,
+                  long long count, void* host_out, void* stream);
+int dsx_grid_write(dsx_grid* grid, int rank, int array, long long start,
+                   long long count, const void* host_in, void* stream);
+
+/* Device pointers of the current storage.  base[13 + nfields]: start of each
+ * array; owned particles of subdomain s are [owned_offset + obase[s], +n[s])
+ * and its ghosts [ghost_offset + gbase[s], +g[s]).  The pointers change after
+ * a migrate (the owned half flips) and after a capacity growth: re-read them
+ * after every call, as the reference asks of ParticleInfo users
+ * (docs/04_Using_in_Your_Code.md:357-358).  obase/gbase/n/g: device arrays. */
+typedef struct dsx_grid_view {
+    void* base[32];
+    long long owned_offset;
+    long long ghost_offset;
+    const int* n;             /* [P]   owned per subdomain (device) */
+    const int* obase;         /* [P+1] */
+    const int* g;             /* [P]   ghosts per receiver (device) */
+    const int* gbase;         /* [P+1] */
+    const int* halo_totals;   /* {ghosts, boundary owners} (device) */
+    long long particles;      /* total owned (host) */
+    long long ghost_capacity; /* host */
+    int nranks;
+} dsx_grid_view;
+int dsx_grid_view_get(dsx_grid* grid, dsx_grid_view* out);
+
+/* Decomp::migrate on all P ranks (src/runtime.cpp:983-1019), including the
+ * automatic Dynamic rebalance.  results: null, or P x {changed, previous,
+ * retained, sent, received, new_owned} (synchronizes). */
+int dsx_grid_migrate(dsx_grid* grid, void* stream, long long* results);
+
+/* Decomp::exchange_halo on all ranks (src/runtime.cpp:862-981).  Rebuilds the
+ * plan when rebuild != 0 or no valid plan exists, else refreshes it in place
+ * (positions_only: x, y, z only).  results: null, or P x {ghost_count,
+ * layout_changed, storage_reallocated, plan_reused} (synchronizes; a ghost
+ * overflow is then detected, the capacity grown and the build redone). */
+int dsx_grid_exchange_halo(dsx_grid* grid, int rebuild, int positions_only,
+                           void* stream, long long* results);
+
+/* Decomp::reverse_halo (src/halo.cpp:1288-1347): owner forces += ghost forces,
+ * images summed in neighbor order (bit-identical to the Host path). */
+int dsx_grid_reverse_halo(dsx_grid* grid, void* stream);
+
+/* Decomp::reverse_exchange / forward_exchange (src/halo.cpp:1210-1286,
+ * 1396-1532) on registered fields (indices into the create-time list). */
+int dsx_grid_reverse_exchange(dsx_grid* grid, int nfields, const int* field_ids,
+                              const int* ops, void* stream);
+int dsx_grid_forward_exchange(dsx_grid* grid, int nfields, const int* field_ids,
+                              void* stream);
+
+/* Decomp::rebalance (src/runtime.cpp:1021-1041): work (host, P entries) or
+ * null for owned counts; then migrate.  results: P x {attempted, changed,
+ * new_owned} (synchronizes). */
+int dsx_grid_rebalance(dsx_grid* grid, const double* work, int force, void* stream,
+                       long long* results, double* imbalance);
+
+int dsx_grid_set_halo_width(dsx_grid* grid, double width);
+int dsx_grid_invalidate_halo(dsx_grid* grid);
+
+/* Adjoint of the ghost position copy: owner_grad[i] += sum over the ghost
+ * images of i of ghost_cot[slot], in the same deterministic order as
+ * reverse_halo.  Arrays are device SoA: ghost_cot_{x,y,z} indexed by ghost
+ * slot (0..ghosts-1, the grid's ghost order), owner_grad_{x,y,z} by owned
+ * index (0..particles-1 of the current owned half). */
+int dsx_grid_halo_backward(dsx_grid* grid, const double* ghost_cot_x,
+                           const double* ghost_cot_y, const double* ghost_cot_z,
+                           double* owner_grad_x, double* owner_grad_y,
+                           double* owner_grad_z, void* stream);
+
+/* Batched step: migrate -> halo build -> callback(user, stream, view) ->
+ * reverse_halo.  capture != 0 captures the step in CUDA graphs (one per owned
+ * half) on first use and replays them; the callback must then only enqueue
+ * work on `stream` that reads counts from the view's device arrays.  The
+ * callback must be idempotent: a step whose ghost build overflowed is redone
+ * after the capacity grows.  status (optional) gets the step's device status
+ * bits (0 == ok). */
+typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view* view);
+int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
+                  void* stream, unsigned* status);
+
+/* Number of this library's kernel launches in one batched step (for reports). */
+int dsx_grid_step_kernel_count(dsx_grid* grid);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,66 @@
+"""The C-ABI library loads, exports every entry point include/dsx.h declares,
+and its host-side topology planning matches the oracle (no GPU needed)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import dsdecompx_b200 as dsx
+from oracle import Grid
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "dsx.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dsx_[a-z_0-9]+)\s*\(", text)) - {"dsx_step_callback"})
+
+
+def test_library_exports_every_declared_symbol():
+    lib = dsx.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_errors():
+    lib = dsx.lib()
+    assert b"sm_100a" in lib.dsx_version()
+    with pytest.raises(ValueError, match="dsDecompX: nranks"):
+        dsx.plan_topology(0, 0)
+    with pytest.raises(ValueError, match="do not match"):
+        dsx.plan_topology(8, 0, dims=(3, 1, 1))
+
+
+CASES = [
+    dict(nranks=1, dims=(1, 1, 1)),
+    dict(nranks=2, dims=(0, 0, 0)),
+    dict(nranks=8, dims=(2, 2, 2)),
+    dict(nranks=12, dims=(3, 1, 4), periodic=(True, False, False)),
+    dict(nranks=12, dims=(3, 1, 4), periodic=(False, True, False), edges_and_corners=False),
+    dict(nranks=64, dims=(4, 4, 4)),
+    dict(nranks=256, dims=(8, 8, 4), upper=(400.0, 400.0, 200.0)),
+    dict(nranks=6, policy="balanced", upper=(12.0, 8.0, 4.0)),
+    dict(nranks=24, policy="dynamic", upper=(3.0, 2.0, 1.0)),
+    dict(nranks=16, policy="topology_aware", upper=(1.0, 1.0, 8.0)),
+    dict(nranks=7, dims=(0, 0, 0)),
+]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_topology_matches_oracle(case):
+    case = dict(case)
+    P = case.pop("nranks")
+    kw = dict(dims=case.get("dims", (0, 0, 0)), policy=case.get("policy", "manual"),
+              lower=(0.0, 0.0, 0.0), upper=case.get("upper", (10.0, 10.0, 10.0)),
+              periodic=case.get("periodic", (True, True, True)),
+              edges_and_corners=case.get("edges_and_corners", True))
+    g = Grid("port", P, kw["dims"], kw["policy"], kw["lower"], kw["upper"], kw["periodic"],
+             0.5, kw["edges_and_corners"])
+    for r in range(P):
+        dims, nbrs = dsx.plan_topology(P, r, **kw)
+        assert dims == g.topology(r)[0]
+        assert nbrs == g.neighbors(r)

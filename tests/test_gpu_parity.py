@@ -1,0 +1,271 @@
+"""CUDA path vs the oracle (the reference's Host algorithm), bit for bit.
+
+Every case drives the virtual grid through the C ABI (dsdecompx_b200 ->
+libdsx.so) and the C restatement through the same seeded calls, then compares
+every array of every subdomain: ids, positions (with the periodic shift),
+velocities, forces, mass, charge, type and all registered fields.
+"""
+import numpy as np
+import pytest
+
+from helpers import ALL_FIELDS, Pair, same, split_by_owner, uniform_particles
+
+pytestmark = pytest.mark.gpu
+
+
+def run_scenario(cuda, *, P, dims, L, halo, N, steps, seed, fields=ALL_FIELDS, sigma=0.3,
+                 periodic=(True, True, True), edges=True, policy="manual", dynamic=None,
+                 lower=(0.0, 0.0, 0.0), ghost_capacity=0, data_fn=None):
+    rng = np.random.default_rng(seed)
+    upper = tuple(lo + l for lo, l in zip(lower, L))
+    pair = Pair(P, dims, policy, lower, upper, periodic, halo, edges, dynamic, fields,
+                particles=N, ghost_capacity=ghost_capacity)
+    try:
+        data = data_fn(rng, N, lower, upper) if data_fn else uniform_particles(rng, N, lower, upper, fields)
+        owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+        pair.upload(split_by_owner(owner, data, P))
+        pair.compare("upload")
+        names = [f[0] for f in fields]
+        for step in range(steps):
+            pair.displace(rng, sigma)
+            mg, mr = pair.gpu.migrate(), pair.ref.migrate()
+            assert (mg == mr).all(), (step, mg, mr)
+            if policy == "dynamic":
+                for a, b in zip(pair.gpu.cuts(), pair.ref.cuts()):
+                    assert same(a, b), (step, a, b)
+            pair.compare(f"migrate {step}")
+            hg, hr = pair.gpu.exchange_halo(rebuild=step % 2 == 0), pair.ref.exchange_halo(rebuild=step % 2 == 0)
+            assert (hg[:, :2] == hr[:, :2]).all(), (step, hg, hr)
+            pair.compare(f"halo build {step}")
+            pair.set_ghost(rng, ["fx", "fy", "fz"])
+            pair.gpu.reverse_halo()
+            pair.ref.reverse_halo()
+            pair.compare(f"reverse_halo {step}")
+            if names:
+                ops = ["sum", "min", "max", "replace"]
+                spec = [(n, ops[(i + step) % 4]) for i, n in enumerate(names)]
+                pair.set_ghost(rng, names)
+                pair.gpu.reverse_exchange(spec)
+                pair.ref.reverse_exchange(spec)
+                pair.compare(f"reverse_exchange {step}")
+                pair.gpu.forward_exchange(names[::-1])
+                pair.ref.forward_exchange(names[::-1])
+                pair.compare(f"forward_exchange {step}")
+            # refresh along the plan after a small move
+            pair.displace(rng, sigma * 0.1)
+            hg, hr = pair.gpu.exchange_halo(), pair.ref.exchange_halo()
+            assert (hg[:, 0] == hr[:, 0]).all()
+            assert P == 1 or hg[:, 3].all(), hg
+            pair.compare(f"refresh {step}")
+        return pair
+    except Exception:
+        pair.close()
+        raise
+
+
+def test_two_by_two_by_two_all_field_types(cuda):
+    run_scenario(cuda, P=8, dims=(2, 2, 2), L=(10.0, 10.0, 10.0), halo=1.0, N=6000, steps=3,
+                 seed=1).close()
+
+
+def test_single_rank_has_no_ghosts(cuda):
+    pair = run_scenario(cuda, P=1, dims=(1, 1, 1), L=(10.0, 10.0, 10.0), halo=2.0, N=3000,
+                        steps=2, seed=2, sigma=3.0)
+    assert pair.gpu.counts(0)[1] == 0
+    pair.close()
+
+
+def test_uneven_grid_non_periodic_faces_only(cuda):
+    run_scenario(cuda, P=12, dims=(3, 1, 4), L=(9.0, 5.0, 12.0), halo=0.8, N=8000, steps=3,
+                 seed=3, periodic=(True, False, False), edges=False,
+                 lower=(-4.5, 1.0, 100.0)).close()
+
+
+def test_many_subdomains_with_long_jumps(cuda):
+    # particles jump several cells: direct routing to any rank
+    run_scenario(cuda, P=64, dims=(4, 4, 4), L=(16.0, 16.0, 16.0), halo=1.2, N=20000, steps=2,
+                 seed=4, sigma=3.0, fields=ALL_FIELDS[:3]).close()
+
+
+def test_balanced_policy_picks_the_reference_grid(cuda):
+    pair = run_scenario(cuda, P=6, dims=(0, 0, 0), L=(12.0, 8.0, 4.0), halo=0.5, N=3000,
+                        steps=1, seed=5, policy="balanced", fields=())
+    assert pair.gpu.topology(0)[0] == pair.ref.topology(0)[0]
+    pair.close()
+
+
+def test_dynamic_boundaries_follow_the_reference(cuda):
+    def clustered(rng, n, lower, upper):
+        lower, upper = np.asarray(lower), np.asarray(upper)
+        d = uniform_particles(rng, n, lower, upper, ALL_FIELDS[:2])
+        k = int(0.8 * n)
+        centre = rng.uniform(lower, upper, size=(4, 3))
+        pick = rng.integers(0, 4, k)
+        pos = centre[pick] + rng.normal(0, 1.5, size=(k, 3))
+        pos = lower + np.mod(pos - lower, upper - lower)
+        d["x"][:k], d["y"][:k], d["z"][:k] = pos[:, 0], pos[:, 1], pos[:, 2]
+        return d
+
+    pair = run_scenario(cuda, P=8, dims=(0, 0, 0), L=(24.0, 24.0, 24.0), halo=1.0, N=12000,
+                        steps=4, seed=6, policy="dynamic", fields=ALL_FIELDS[:2],
+                        dynamic=(1.0, 1.10, 0.5, 0.10), data_fn=clustered)
+    # the boundaries moved
+    assert not np.allclose(pair.gpu.cuts()[0], np.linspace(0, 24, 3))
+    pair.close()
+
+
+def test_ghost_overflow_grows_and_rebuilds(cuda):
+    # a deliberately tiny ghost capacity: the build must detect the overflow,
+    # grow the ghost region and rebuild, with results identical to the oracle
+    run_scenario(cuda, P=8, dims=(2, 2, 2), L=(8.0, 8.0, 8.0), halo=1.5, N=4000, steps=2,
+                 seed=7, ghost_capacity=64, fields=ALL_FIELDS[:2]).close()
+
+
+def test_all_particles_start_on_one_rank(cuda):
+    rng = np.random.default_rng(8)
+    pair = Pair(8, (2, 2, 2), "manual", (0, 0, 0), (6, 6, 6), halo_width=0.7,
+                fields=ALL_FIELDS[:3], particles=5000)
+    data = uniform_particles(rng, 5000, (0, 0, 0), (6, 6, 6), ALL_FIELDS[:3])
+    per = [data] + [{k: v[:0] for k, v in data.items()} for _ in range(7)]
+    pair.upload(per)
+    assert (pair.gpu.migrate() == pair.ref.migrate()).all()
+    pair.compare("scatter from rank 0")
+    assert (pair.gpu.exchange_halo(True)[:, 0] == pair.ref.exchange_halo(True)[:, 0]).all()
+    pair.compare("halo")
+    pair.close()
+
+
+def test_rebalance_api(cuda):
+    rng = np.random.default_rng(9)
+    pair = Pair(8, (0, 0, 0), "dynamic", (0, 0, 0), (8, 8, 8), halo_width=0.25,
+                dynamic=(0.0, 1.10, 1.0, 0.10), particles=3000)
+    data = uniform_particles(rng, 3000, (0, 0, 0), (8, 8, 8))
+    owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    pair.upload(split_by_owner(owner, data, 8))
+    work = [100.0] + [1.0] * 7
+    rg, ig = pair.gpu.rebalance(work, force=True)
+    rr, ir = pair.ref.rebalance(work, force=True)
+    assert (rg == rr).all() and same(ig, ir), (rg, rr, ig, ir)
+    for a, b in zip(pair.gpu.cuts(), pair.ref.cuts()):
+        assert same(a, b)
+    pair.compare("after rebalance")
+    pair.close()
+
+
+def test_positions_only_refresh(cuda):
+    pair = run_scenario(cuda, P=8, dims=(2, 2, 2), L=(10.0, 10.0, 10.0), halo=1.0, N=5000,
+                        steps=1, seed=10, fields=ALL_FIELDS[:2])
+    rng = np.random.default_rng(11)
+    before = [pair.gpu.snapshot(r) for r in range(8)]
+    pair.displace(rng, 0.05)
+    h = pair.gpu.exchange_halo(positions_only=True)
+    pair.ref.exchange_halo()
+    assert h[:, 3].all() and not h[:, 1].any()
+    for r in range(8):
+        a, b = pair.gpu.snapshot(r), pair.ref.snapshot(r)
+        o = a["owned"]
+        for k in ("x", "y", "z", "fx", "fy", "fz"):
+            assert same(a[k][o:], b[k][o:]), k
+        for k in ("vx", "mass", "global_id", "q"):
+            assert same(a[k][o:], before[r][k][o:]), k
+    pair.close()
+
+
+class DeviceArray:
+    """Wraps a raw device pointer for torch.as_tensor (CUDA array interface)."""
+
+    def __init__(self, ptr, n, typestr="<f8"):
+        self.__cuda_array_interface__ = dict(shape=(n,), typestr=typestr, data=(ptr, False),
+                                             version=3, strides=None)
+
+
+def ghost_force_filler(torch, capacity):
+    """Step callback: every slot of the ghost region gets a force that depends
+    only on its slot, copied on the step's stream from tensors made up front
+    (nothing is allocated while a graph is being captured)."""
+    slots = torch.arange(capacity, device="cuda", dtype=torch.float64)
+    values = [torch.sin(slots * (j + 1)) for j in range(3)]
+
+    def fill(view, stream):
+        assert int(view.ghost_capacity) == capacity
+        s = torch.cuda.ExternalStream(stream)
+        with torch.cuda.stream(s):
+            for j, k in enumerate((6, 7, 8)):
+                t = torch.as_tensor(DeviceArray(view.base[k] + 8 * int(view.ghost_offset), capacity),
+                                    device="cuda")
+                t.copy_(values[j])
+    return fill
+
+
+def test_batched_step_matches_calls(cuda):
+    import torch
+
+    import dsdecompx_b200 as dsx
+    rng = np.random.default_rng(12)
+    fields = ALL_FIELDS[:2]
+    kw = dict(nranks=8, dims=(2, 2, 2), lower=(0, 0, 0), upper=(12, 12, 12), halo_width=0.6,
+              fields=fields, particles=8000, ghost_capacity=12000)
+    data = uniform_particles(rng, 8000, (0, 0, 0), (12, 12, 12), fields)
+    a = Pair(**kw)
+    owner = a.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    per = split_by_owner(owner, data, 8)
+    a.upload(per)
+    b = dsx.VirtualGrid(**kw)
+    b.upload(per)
+    fill = ghost_force_filler(torch, 12000)
+    side = torch.cuda.Stream()
+    for step in range(4):
+        a.displace(rng, 0.3)
+        for r in range(8):
+            o = b.counts(r)[0]
+            for name in "xyz":
+                b.write(r, name, 0, a.gpu.read(r, name, 0, o))
+        a.gpu.migrate()
+        a.ref.migrate()
+        a.gpu.exchange_halo(rebuild=True)
+        a.ref.exchange_halo(rebuild=True)
+        fill(a.gpu.view(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        for r in range(8):
+            o, g = a.ref.counts(r)
+            for name in ("fx", "fy", "fz"):
+                a.ref.write(r, name, o, a.gpu.read(r, name, o, g))
+        a.gpu.reverse_halo()
+        a.ref.reverse_halo()
+        a.compare(f"calls {step}")
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            st = b.step(fill, capture=step > 0)
+        side.synchronize()
+        assert st == 0
+        for r in range(8):
+            x, y = a.gpu.snapshot(r), b.snapshot(r)
+            for k in x:
+                assert same(x[k], y[k]), (step, r, k)
+    a.close()
+    b.close()
+
+
+def test_halo_backward_is_reverse_halo(cuda):
+    import torch
+    pair = run_scenario(cuda, P=8, dims=(2, 2, 2), L=(10.0, 10.0, 10.0), halo=1.2, N=5000,
+                        steps=1, seed=13, fields=())
+    v = pair.gpu.view()
+    G = int(pair.gpu.all_counts()[1].sum())
+    N = int(v.particles)
+    cot = torch.randn(3, G, dtype=torch.float64, device="cuda")
+    grad = torch.randn(3, N, dtype=torch.float64, device="cuda")
+    expect = grad.clone()
+    pair.gpu.halo_backward(cot, grad)
+    # reverse_halo on the same cotangents stored as ghost forces
+    for j, k in enumerate((6, 7, 8)):
+        gt = torch.as_tensor(DeviceArray(v.base[k] + 8 * int(v.ghost_offset), G), device="cuda")
+        gt.copy_(cot[j])
+        ot = torch.as_tensor(DeviceArray(v.base[k] + 8 * int(v.owned_offset), N), device="cuda")
+        ot.copy_(expect[j])
+    pair.gpu.reverse_halo()
+    torch.cuda.synchronize()
+    for j, k in enumerate((6, 7, 8)):
+        ot = torch.as_tensor(DeviceArray(v.base[k] + 8 * int(v.owned_offset), N), device="cuda")
+        assert torch.equal(ot, grad[j])
+    pair.close()

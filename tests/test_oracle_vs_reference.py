@@ -1,0 +1,139 @@
+"""Pins the oracle: the C restatement (oracle/dsx_oracle.c) against the
+reference's own Host path built from its sources (oracle/_ref), bit for bit,
+on seeded scenarios covering migrate, halo build and refresh, reverse_halo,
+reverse_exchange with every op and field type, rebalance and the Dynamic
+policy.  CPU only."""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import ALL_FIELDS, FIELD_TYPE_NAMES, same, split_by_owner, uniform_particles
+
+needs_ref = pytest.mark.skipif(not oracle.available("ref_debug"),
+                               reason="reference build (oracle/_ref) not present")
+
+
+def make_pair(kind_a, kind_b, **kw):
+    fields = [(n, FIELD_TYPE_NAMES.index(t), c) for n, t, c in kw.pop("fields")]
+    cap = kw.pop("field_capacity")
+    a = oracle.Grid(kind_a, fields=fields, field_capacity=cap, **kw)
+    b = oracle.Grid(kind_b, fields=fields, field_capacity=cap, **kw)
+    return a, b
+
+
+def compare(a, b, P, what):
+    for r in range(P):
+        x, y = a.snapshot(r), b.snapshot(r)
+        assert x["owned"] == y["owned"] and x["ghosts"] == y["ghosts"], (what, r)
+        for k in x:
+            assert same(x[k], y[k]), (what, r, k)
+
+
+def scenario(P, dims, L, halo, N, steps, seed, fields=ALL_FIELDS, sigma=0.3, policy="manual",
+             periodic=(True, True, True), edges=True, dynamic=None, lower=(0.0, 0.0, 0.0)):
+    rng = np.random.default_rng(seed)
+    upper = tuple(lo + l for lo, l in zip(lower, L))
+    # The reference's debug invariants reject particles that drift out of the
+    # box through a non-periodic face (src/migration.cpp:558-577); its release
+    # build clamps them into the edge cell, which is what the port follows.
+    kind = "ref_debug" if all(periodic) else "ref"
+    a, b = make_pair("port", kind, nranks=P, dims=dims, policy=policy, lower=lower,
+                     upper=upper, periodic=periodic, halo_width=halo, edges_and_corners=edges,
+                     dynamic=dynamic, fields=fields, field_capacity=4 * N + 64)
+    data = uniform_particles(rng, N, lower, upper, fields)
+    owner = b.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    assert (owner == a.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))).all()
+    for r, d in enumerate(split_by_owner(owner, data, P)):
+        a.set_owned(r, d)
+        b.set_owned(r, d)
+    names = [f[0] for f in fields]
+    for step in range(steps):
+        for r in range(P):
+            o, _ = a.counts(r)
+            dx = rng.normal(0, sigma, size=(o, 3))
+            for k, name in enumerate("xyz"):
+                v = a.read(r, name, 0, o) + dx[:, k]
+                a.write(r, name, 0, v)
+                b.write(r, name, 0, v)
+        ma, mb = a.migrate(), b.migrate()
+        assert (ma == mb).all(), (step, ma, mb)
+        for x, y in zip(a.cuts(), b.cuts()):
+            assert same(x, y)
+        compare(a, b, P, f"migrate {step}")
+        ha, hb = a.exchange_halo(step % 2 == 0), b.exchange_halo(step % 2 == 0)
+        assert (ha[:, :2] == hb[:, :2]).all(), (ha, hb)
+        compare(a, b, P, f"halo {step}")
+        for r in range(P):
+            o, g = a.counts(r)
+            for name in ["fx", "fy", "fz"] + names:
+                comps = a.components(name)
+                t = next((ft for fn, ft, _ in fields if fn == name), "float64")
+                from helpers import field_values
+                v = field_values(rng, name, t, comps, g)
+                a.write(r, name, o, v)
+                b.write(r, name, o, v)
+        a.reverse_halo()
+        b.reverse_halo()
+        compare(a, b, P, f"reverse_halo {step}")
+        if names:
+            ops = ["sum", "min", "max", "replace"]
+            spec = [(n, ops[(i + step) % 4]) for i, n in enumerate(names)]
+            a.reverse_exchange(spec)
+            b.reverse_exchange(spec)
+            compare(a, b, P, f"reverse_exchange {step}")
+        for r in range(P):
+            o, _ = a.counts(r)
+            dx = rng.normal(0, sigma * 0.1, size=(o, 3))
+            for k, name in enumerate("xyz"):
+                v = a.read(r, name, 0, o) + dx[:, k]
+                a.write(r, name, 0, v)
+                b.write(r, name, 0, v)
+        ha, hb = a.exchange_halo(False), b.exchange_halo(False)
+        assert (ha[:, :2] == hb[:, :2]).all(), (ha, hb)
+        compare(a, b, P, f"refresh {step}")
+    a.close()
+    b.close()
+
+
+@needs_ref
+@pytest.mark.parametrize("P,dims,L,halo,kw", [
+    (1, (1, 1, 1), (10.0, 10.0, 10.0), 2.0, dict(sigma=3.0)),
+    (2, (2, 1, 1), (10.0, 10.0, 10.0), 1.0, {}),
+    (8, (2, 2, 2), (10.0, 10.0, 10.0), 1.0, {}),
+    (12, (3, 1, 4), (9.0, 5.0, 12.0), 0.8,
+     dict(periodic=(True, False, False), edges=False, lower=(-4.5, 1.0, 100.0))),
+    (27, (3, 3, 3), (9.0, 9.0, 9.0), 0.9, dict(sigma=2.5, fields=ALL_FIELDS[:3])),
+    (6, (0, 0, 0), (12.0, 8.0, 4.0), 0.5, dict(policy="balanced")),
+])
+def test_port_matches_reference(P, dims, L, halo, kw):
+    scenario(P, dims, L, halo, N=1500 * max(1, P // 4), steps=3, seed=P, **kw)
+
+
+@needs_ref
+def test_port_matches_reference_dynamic():
+    scenario(8, (0, 0, 0), (16.0, 16.0, 16.0), 1.0, N=3000, steps=4, seed=21,
+             policy="dynamic", dynamic=(1.0, 1.01, 0.5, 0.1), fields=ALL_FIELDS[:2], sigma=1.0)
+
+
+@needs_ref
+def test_port_matches_reference_rebalance():
+    rng = np.random.default_rng(5)
+    a, b = make_pair("port", "ref_debug", nranks=8, dims=(0, 0, 0), policy="dynamic",
+                     lower=(0, 0, 0), upper=(8, 8, 8), periodic=(True,) * 3, halo_width=0.25,
+                     edges_and_corners=True, dynamic=(0.0, 1.10, 1.0, 0.10), fields=[],
+                     field_capacity=0)
+    data = uniform_particles(rng, 2000, (0, 0, 0), (8, 8, 8))
+    owner = a.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    for r, d in enumerate(split_by_owner(owner, data, 8)):
+        a.set_owned(r, d)
+        b.set_owned(r, d)
+    for work, force in [([100.0] + [1.0] * 7, True), (None, False), ([5.0] * 8, False),
+                        ([1, 2, 3, 4, 5, 6, 7, 8.0], True)]:
+        ra, ia = a.rebalance(work, force)
+        rb, ib = b.rebalance(work, force)
+        assert (ra == rb).all() and same(ia, ib)
+        for x, y in zip(a.cuts(), b.cuts()):
+            assert same(x, y)
+        compare(a, b, 8, "rebalance")
+    a.close()
+    b.close()
