@@ -1,0 +1,483 @@
+#!/usr/bin/env python
+"""Throughput of the particle-bookkeeping step on B200.
+
+One step = migrate (with the Dynamic rebalance when the workload has it) ->
+exchange_halo (plan build) -> the synthetic "user" work (ghost forces N(0,1),
+field exchanges when the workload names them, the next N(0,sigma) drift) ->
+reverse_halo, run as the batched, CUDA-graph-captured step of the virtual grid
+(dsx_grid_step).  Prints one JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+                  [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank runs its own replica of the workload; there
+is no data-path collective (the path does not shard across GPUs in this
+build), only a barrier and the max-over-ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "M particles/s per migrate+halo+reverse step"
+DEFAULT_WORKLOAD = "clustered_64"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--particles", type=int, default=0,
+                    help="override the workload's particle count (small profiling cases)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while running."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={CLOCK_QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "20"], stdout=self.file,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.file:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def algorithmic_bytes(S, N, E, G, B):
+    """Bytes each kernel must move at minimum (reads + writes) for one step
+    of N owned particles (E emigrants), G ghosts and B boundary owners, with
+    S bytes per particle record (96 core + registered fields)."""
+    R = N - E
+    return {
+        "mig_classify": 24 * N,                               # positions
+        "mig_move": 24 * N + (S - 24) * R + S * R + 8 * E,    # read all, write retained, list emigrants
+        "emig_place": E * (8 + 2 * S),
+        "halo_classify": 24 * N + 4 * N,                      # positions in, mask out
+        "halo_scatter": 4 * N + S * B + (S + 12) * G + 8 * B,  # masks, owners, ghosts + maps
+        "reverse_sum": 8 * B + 4 * G + 24 * G + 48 * B,       # CSR, ghost forces, owner RMW
+    }
+
+
+# ------------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, device):
+    import numpy as np
+    import torch
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import workloads as W
+
+    w = W.WORKLOADS[args.workload]
+    if args.particles:
+        import dataclasses
+        w = dataclasses.replace(w, particles=args.particles)
+    wl = W.harness()
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream(device)
+    if w.nranks == 1:
+        return run_drop_in(args, w, wl, stream, rank, world)
+
+    dims, _ = dsx.plan_topology(w.nranks, 0, w.dims, w.policy, w.lower, w.upper)
+    data = W.generate(w, seed=args.seed)
+    owner = W.initial_owner(w, dims, data["x"], data["y"], data["z"])
+    counts, grouped = W.group_by_owner(data, owner, w.nranks)
+    del data, owner
+    N = int(counts.sum())
+    S = w.record_bytes()
+    names = dsx.ARRAYS + [f[0] for f in w.fields]
+    # pinned host copies of the state (the e2e leg copies them every step)
+    pinned = []
+    for name in names:
+        if name in grouped:
+            t = torch.from_numpy(np.ascontiguousarray(grouped[name])).pin_memory()
+        else:
+            t = torch.zeros(N, dtype=torch.float64).pin_memory()
+        pinned.append(t)
+    del grouped
+    grid = dsx.VirtualGrid(w.nranks, w.dims, w.policy, w.lower, w.upper, halo_width=w.halo,
+                           fields=w.fields, particles=N, ghost_capacity=int(0.9 * N))
+    ptrs = [t.data_ptr() for t in pinned]
+    with torch.cuda.stream(stream):
+        grid.upload_flat(counts, ptrs)
+    field_ids = list(range(len(w.fields))) if w.field_exchange else []
+    seed = args.seed + 1000 * rank
+
+    def user_work(view, s):
+        vp = C.byref(view)
+        wl.dsxw_ghost_forces(vp, seed, 0, s)
+        if field_ids:
+            grid.forward_exchange([w.fields[i][0] for i in field_ids], stream=s)
+            grid.reverse_exchange([(w.fields[i][0], "sum") for i in field_ids], stream=s)
+        wl.dsxw_drift(vp, seed, 0, w.drift, s)
+        wl.dsxw_advance(s)
+
+    harness_kernels = 3 + (0 if not field_ids else 2)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            status = grid.step(user_work, capture=True)
+            assert status == 0, status
+        grid.profile(True)
+        grid.step(user_work, capture=True)   # re-capture both halves with the timing marks
+        grid.step(user_work, capture=True)
+    stream.synchronize()
+
+    per_kernel = {}
+    totals_acc = {"particles": 0, "emigrants": 0, "ghosts": 0, "boundary": 0}
+    launches = 0
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clocks:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for _ in range(args.steps):
+                status = grid.step(user_work, capture=True)
+                assert status == 0, status
+                for name, ms in grid.kernel_times():
+                    per_kernel.setdefault(name, []).append(ms)
+                for k, v in grid.totals(stream=stream).items():
+                    totals_acc[k] += v
+            end.record(stream)
+        torch.cuda.synchronize(device)
+    elapsed_ms = start.elapsed_time(end)
+    barrier()
+    clock = clocks.summary()
+    kernels_per_step = grid.step_kernel_count()
+    launches = args.steps * (kernels_per_step + harness_kernels)
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = world * N / (ms_per_step / 1e3) / 1e6
+
+    avg = {k: sum(v) / len(v) for k, v in per_kernel.items()}
+    mean_tot = {k: v / args.steps for k, v in totals_acc.items()}
+    alg = algorithmic_bytes(S, N, mean_tot["emigrants"], mean_tot["ghosts"], mean_tot["boundary"])
+    ours = {k: v for k, v in avg.items() if k not in ("callback",)}
+    dominant = max(ours, key=ours.get)
+    peak, peak_kind = peaks()
+    step_bytes = sum(alg.values())
+    ours_ms = sum(ours.values())
+    roof = None
+    if dominant in alg:
+        achieved = alg[dominant] / (avg[dominant] / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": int(alg[dominant]),
+                "avg_launch_ms": round(avg[dominant], 4),
+                "traffic": traffic_from_profiles(dominant, N, mean_tot)}
+
+    # e2e: the same step through the C ABI with the state in pinned host memory
+    e2e = None
+    if args.e2e_steps > 0:
+        h2d = N * S + 8 * w.nranks
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cnt = counts.copy()
+        with torch.cuda.stream(stream):
+            cnt = grid.download_flat(ptrs)
+            barrier()
+            e0.record(stream)
+            for _ in range(args.e2e_steps):
+                grid.upload_flat(cnt, ptrs)
+                status = grid.step(user_work, capture=True)
+                assert status == 0, status
+                cnt = grid.download_flat(ptrs)
+            e1.record(stream)
+        torch.cuda.synchronize(device)
+        e_ms = e0.elapsed_time(e1) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([e_ms], device=f"cuda:{device}")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": round(world * N / (e_ms / 1e3) / 1e6, 3), "unit": "M particles/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(N * S + 8 * w.nranks),
+               "ms_per_step": round(e_ms, 3),
+               "path": "dsx_grid_upload (pinned host) -> dsx_grid_step -> dsx_grid_download"}
+
+    # per-call path (every call returns its counts synchronously, no graph)
+    plain = None
+    if args.plain_steps > 0:
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        grid.profile(False)
+        with torch.cuda.stream(stream):
+            p0.record(stream)
+            for _ in range(args.plain_steps):
+                grid.migrate(stream=stream)
+                grid.exchange_halo(rebuild=True, stream=stream)
+                user_work(grid.view(), stream.cuda_stream)
+                grid.reverse_halo(stream=stream)
+                grid.all_counts(stream=stream)
+            p1.record(stream)
+        torch.cuda.synchronize(device)
+        plain = round(p0.elapsed_time(p1) / args.plain_steps, 3)
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "M particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded numpy PCG64 + counter-based device deviates)",
+        "config": {"workload": w.name, "description": w.description, "subdomains": w.nranks,
+                   "grid": list(dims), "particles": N, "record_bytes": S,
+                   "step": "graph-captured batched step (dsx_grid_step)",
+                   "l2": "inputs larger than L2 (%.2f GB of owned records)" % (N * S / 1e9),
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "roofline": roof,
+        "step_roofline": {"algorithmic_bytes": int(step_bytes),
+                          "kernels_ms": round(ours_ms, 4),
+                          "achieved_gbs": round(step_bytes / (ours_ms / 1e3) / 1e9, 1),
+                          "frac_of_peak": round(step_bytes / (ours_ms / 1e3) / 1e9 / peak, 4),
+                          "achieved_gbs_wall": round(step_bytes / (ms_per_step / 1e3) / 1e9, 1)},
+        "kernel_ms": {k: round(v, 4) for k, v in avg.items()},
+        "totals_per_step": {k: int(v) for k, v in mean_tot.items()},
+        "per_call_ms_per_step": plain,
+        "clocks": clock,
+        "e2e": e2e,
+        "gpu_launches": launches,
+    }
+    return line
+
+
+def traffic_from_profiles(kernel, N, totals):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/traffic.json), scaled to this launch's particle count."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        entry = data[kernel]
+        return int(entry["dram_bytes_per_particle"] * N)
+    except Exception:
+        return None
+
+
+def run_drop_in(args, w, wl, stream, rank, world):
+    """Single-rank drop-in: drift + dsx_rank_migrate in place (no ghosts at
+    one rank, so exchange_halo and reverse_halo do no work)."""
+    import numpy as np
+    import torch
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import workloads as W
+
+    data = W.generate(w, seed=args.seed)
+    N = w.particles
+    dev = torch.device("cuda", torch.cuda.current_device())
+    x, y, z = (torch.from_numpy(data[k]).to(dev) for k in "xyz")
+    gid = torch.from_numpy(data["global_id"]).to(dev)
+    seed = args.seed + 1000 * rank
+
+    def step():
+        wl.dsxw_drift_arrays(x.data_ptr(), y.data_ptr(), z.data_ptr(), gid.data_ptr(), N, seed, 0,
+                             w.drift, stream.cuda_stream)
+        wl.dsxw_advance(stream.cuda_stream)
+        dsx.rank_migrate(x, y, z, N, w.lower, w.upper, stream=stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            for _ in range(args.steps):
+                step()
+            b.record(stream)
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    return {"metric": METRIC, "value": round(world * N / (ms / 1e3) / 1e6, 3),
+            "unit": "M particles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "description": w.description},
+            "clocks": clocks.summary(), "gpu_launches": 3 * args.steps, "roofline": None,
+            "e2e": None}
+
+
+# --------------------------------------------------------- reference (CPU)
+
+def reference_rate(w, seed, steps, warmup, budget_s=120.0):
+    """The reference's own Host path (oracle/_ref, built from its sources)
+    with one thread per subdomain: M particles/s of migrate + exchange_halo
+    (rebuild) + reverse_halo, timed like its communication_test (slowest rank
+    per call), on a sample of the workload sized to fit `budget_s`."""
+    import numpy as np
+
+    import oracle
+    from dsdecompx_b200 import workloads as W
+
+    if not oracle.available("ref"):
+        return None, "reference build oracle/_ref/libdsx_ref.so is missing"
+    import dsdecompx_b200 as dsx
+    dims, _ = dsx.plan_topology(w.nranks, 0, w.dims, w.policy, w.lower, w.upper)
+    fields = [(n, ["int32", "int64", "uint32", "uint64", "float32", "float64"].index(t), c)
+              for n, t, c in w.fields]
+
+    def run(n_sample, nsteps, nwarm):
+        data = W.generate(w, seed=seed, particles=n_sample)
+        owner = W.initial_owner(w, dims, data["x"], data["y"], data["z"])
+        counts = np.bincount(owner, minlength=w.nranks)
+        cap = int(max(4 * counts.max(), 3 * n_sample // w.nranks) + 4096)
+        g = oracle.Grid("ref", w.nranks, w.dims, w.policy, w.lower, w.upper, (True,) * 3, w.halo,
+                        fields=fields, field_capacity=cap)
+        for r in range(w.nranks):
+            m = owner == r
+            g.set_owned(r, {k: v[m] for k, v in data.items()})
+        rng = np.random.default_rng(seed + 1)
+        times = []
+        for step in range(nwarm + nsteps):
+            for r in range(w.nranks):       # drift (harness, not timed)
+                o, _ = g.counts(r)
+                if o:
+                    for name in "xyz":
+                        g.write(r, name, 0, g.read(r, name, 0, o) + rng.normal(0, w.drift, o))
+            t = g.timed("migrate") + g.timed("halo_rebuild")
+            for r in range(w.nranks):       # ghost forces (harness, not timed)
+                o, gh = g.counts(r)
+                for name in ("fx", "fy", "fz"):
+                    g.write(r, name, o, rng.normal(size=gh))
+            t += g.timed("reverse_halo")
+            if step >= nwarm:
+                times.append(t)
+        g.close()
+        return n_sample / statistics.mean(times) / 1e6, statistics.mean(times)
+
+    probe_n = min(w.particles, 1_000_000)
+    rate, _ = run(probe_n, 1, 1)
+    # size the sample so that (steps + warmup) steps fit the budget
+    per_particle = 1.0 / (rate * 1e6)
+    n_sample = int(min(w.particles, max(probe_n, budget_s / (steps + warmup) / per_particle)))
+    rate, step_s = run(n_sample, steps, warmup)
+    sample = (f"{n_sample} of the {w.particles}-particle {w.name} workload (same box, grid, halo "
+              f"and distributions), {steps} timed steps after {warmup} warm-up; "
+              f"{w.nranks} thread-ranks on {os.cpu_count()} host CPUs; "
+              f"{step_s:.3f} s per step")
+    return {"value": round(rate, 4), "unit": "M particles/s", "cores": w.nranks,
+            "kind": "reference", "sample": sample}, None
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from dsdecompx_b200 import workloads as W
+        w = W.WORKLOADS[args.workload]
+        base, why = reference_rate(w, args.seed, max(1, min(args.steps, 5)), 1)
+        if base is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        line = {"metric": METRIC, "value": base["value"], "unit": base["unit"],
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": w.name, "description": w.description},
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": base["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line = run_ours(args, rank, world, local)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            from dsdecompx_b200 import workloads as W
+            base, why = reference_rate(W.WORKLOADS[args.workload], args.seed, 2, 1, budget_s=25.0)
+            line["cpu_baseline"] = base if base else {"unavailable": why}
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

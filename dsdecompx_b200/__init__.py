@@ -100,6 +100,8 @@ def lib() -> C.CDLL:
             "dsx_grid_cuts": [vp, dp, vp],
             "dsx_grid_upload": [vp, llp, C.POINTER(vp), vp],
             "dsx_grid_counts": [vp, llp, llp, vp],
+            "dsx_grid_download": [vp, llp, C.POINTER(vp), vp],
+            "dsx_grid_totals": [vp, llp, vp],
             "dsx_grid_read": [vp, C.c_int, C.c_int, C.c_longlong, C.c_longlong, vp, vp],
             "dsx_grid_write": [vp, C.c_int, C.c_int, C.c_longlong, C.c_longlong, vp, vp],
             "dsx_grid_view_get": [vp, C.POINTER(GridView)],
@@ -114,6 +116,8 @@ def lib() -> C.CDLL:
             "dsx_grid_halo_backward": [vp, vp, vp, vp, vp, vp, vp, vp],
             "dsx_grid_step": [vp, STEP_CALLBACK, vp, C.c_int, vp, C.POINTER(C.c_uint)],
             "dsx_grid_step_kernel_count": [vp],
+            "dsx_grid_profile": [vp, C.c_int],
+            "dsx_grid_kernel_times": [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -277,6 +281,29 @@ class VirtualGrid:
         _check(self.L.dsx_grid_upload(self.h, counts.ctypes.data_as(C.POINTER(C.c_longlong)), ptrs,
                                       _stream(stream)))
 
+    def upload_flat(self, counts, arrays: List[Optional[int]], stream=None):
+        """Upload from raw host/device pointers (arrays[13 + nfields], None
+        entries zero-filled), owned particles concatenated in rank order."""
+        c = np.ascontiguousarray(counts, dtype=np.int64)
+        ptrs = (C.c_void_p * (13 + len(self.fields)))(*[a or None for a in arrays])
+        _check(self.L.dsx_grid_upload(self.h, c.ctypes.data_as(C.POINTER(C.c_longlong)), ptrs,
+                                      _stream(stream)))
+
+    def download_flat(self, arrays: List[Optional[int]], stream=None) -> np.ndarray:
+        """Inverse of upload_flat; returns the per-rank owned counts."""
+        c = np.zeros(self.nranks, dtype=np.int64)
+        ptrs = (C.c_void_p * (13 + len(self.fields)))(*[a or None for a in arrays])
+        _check(self.L.dsx_grid_download(self.h, c.ctypes.data_as(C.POINTER(C.c_longlong)), ptrs,
+                                        _stream(stream)))
+        return c
+
+    def totals(self, stream=None) -> Dict[str, int]:
+        out = np.zeros(4, dtype=np.int64)
+        _check(self.L.dsx_grid_totals(self.h, out.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                      _stream(stream)))
+        return dict(particles=int(out[0]), emigrants=int(out[1]), ghosts=int(out[2]),
+                    boundary=int(out[3]))
+
     def all_counts(self, stream=None):
         o = np.zeros(self.nranks, dtype=np.int64)
         g = np.zeros(self.nranks, dtype=np.int64)
@@ -389,6 +416,18 @@ class VirtualGrid:
         _check(self.L.dsx_grid_step(self.h, cb, None, 1 if capture else 0, _stream(stream),
                                     C.byref(st)))
         return st.value
+
+    def profile(self, enable: bool = True):
+        _check(self.L.dsx_grid_profile(self.h, 1 if enable else 0))
+
+    def kernel_times(self) -> List[Tuple[str, float]]:
+        """(name, ms) of every kernel interval of the last profiled step."""
+        names = (C.c_char_p * 64)()
+        ms = (C.c_float * 64)()
+        n = self.L.dsx_grid_kernel_times(self.h, 64, names, ms)
+        if n < 0:
+            _check(n)
+        return [(names[i].decode(), float(ms[i])) for i in range(n)]
 
     def step_kernel_count(self) -> int:
         return self.L.dsx_grid_step_kernel_count(self.h)

@@ -58,6 +58,22 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+WORKLOAD_LIB = os.path.join(LIBDIR, "libdsx_workload.so")
+WORKLOAD_SRC = os.path.join(PKG, "workload", "workload.cu")
+
+
+def build_workload(force: bool = False, verbose: bool = False) -> str:
+    """Benchmark-harness kernels (synthetic drift and ghost forces)."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    if force or _stale(WORKLOAD_LIB, [WORKLOAD_SRC, os.path.join(INCLUDE, "dsx.h")]):
+        cmd = [nvcc()] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                                 "-I" + INCLUDE, "-o", WORKLOAD_LIB, WORKLOAD_SRC]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return WORKLOAD_LIB
+
+
 def build_cpp_tests(force: bool = False, verbose: bool = False) -> List[str]:
     """C++ programs under tests/cpp that exercise the drop-in API like the
     reference's own sanity checks."""
@@ -76,4 +92,5 @@ def build_cpp_tests(force: bool = False, verbose: bool = False) -> List[str]:
 
 def build(force: bool = False, verbose: bool = False) -> None:
     build_library(force=force, verbose=verbose)
+    build_workload(force=force, verbose=verbose)
     build_cpp_tests(force=force, verbose=verbose)

@@ -247,12 +247,14 @@ struct dsx_grid {
     std::vector<long long> last_ghosts;
     unsigned* pinned_status = nullptr;   // [4]: status, G, B, pad
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    dsx::Marks marks;
     dsx_step_callback graph_callback = nullptr;
     void* graph_user = nullptr;
     cudaStream_t graph_stream = nullptr;
 
     ~dsx_grid() {
         destroy_graphs();
+        for (auto& e : marks.ev) if (e) cudaEventDestroy(e);
         for (void* p : arrays_owned) cudaFree(p);
         for (void* p : scratch_owned) cudaFree(p);
         for (void* p : fixed_owned) cudaFree(p);
@@ -347,6 +349,7 @@ struct dsx_grid {
         allocate_ghost_scratch();
         cuda_check(cudaMallocHost(reinterpret_cast<void**>(&pinned_status), 4 * sizeof(unsigned)),
                    "cudaMallocHost");
+        S.marks = &marks;
         last_ghosts.assign(static_cast<std::size_t>(P), 0);
     }
 
@@ -537,6 +540,7 @@ struct dsx_grid {
             p.automatic = 1;
             p.interval = automatic_rebalance ? static_cast<long long>(desc.dyn_interval) : 0;
             dsx::launch_rebalance(G, nullptr, p, call_counter, rebalance_result, stream);
+            dsx::mark(S, stream, "rebalance");
         }
         dsx::launch_migrate(G, A, owned_off(), next_off(), S, stream);
     }
@@ -735,14 +739,23 @@ struct dsx_grid {
     }
 
     void enqueue_step(dsx_step_callback cb, void* user, cudaStream_t stream) {
+        marks.count = 0;
         clear_status(stream);
+        marks.mark(stream, "start");
         enqueue_migrate(stream, true);
         // the rest of the step reads the next layout
         parity ^= 1;
         cur ^= 1;
         enqueue_halo_build(stream);
         const dsx_grid_view v = view();
+        // inside the callback the new plan is the current one (field
+        // exchanges called from it act on these ghosts)
+        const bool saved_plan = plan_valid, saved_ghosts = ghosts_valid;
+        plan_valid = ghosts_valid = true;
         if (cb) cb(user, stream, &v);
+        plan_valid = saved_plan;
+        ghosts_valid = saved_ghosts;
+        marks.mark(stream, "callback");
         enqueue_reverse(stream);
         cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
                    "read status");
@@ -1011,6 +1024,42 @@ int dsx_grid_upload(dsx_grid* grid, const long long* counts, const void* const* 
     });
 }
 
+int dsx_grid_download(dsx_grid* grid, long long* counts, void* const* arrays, void* stream) {
+    return guarded([&] {
+        const auto s = static_cast<cudaStream_t>(stream);
+        const std::vector<int> n = grid->read_ints(grid->layout[grid->cur][0], grid->P, s);
+        for (int r = 0; r < grid->P; ++r) if (counts) counts[r] = n[static_cast<std::size_t>(r)];
+        const std::size_t total = static_cast<std::size_t>(grid->total);
+        const long long off = grid->owned_off();
+        for (int a = 0; a < 13 + static_cast<int>(grid->fields.size()); ++a) {
+            if (!arrays || !arrays[a]) continue;
+            const void* src;
+            std::size_t element;
+            if (a < 11) { src = grid->A.d[a] + off; element = 8; }
+            else if (a == 11) { src = grid->A.type + off; element = 4; }
+            else if (a == 12) { src = grid->A.gid + off; element = 4; }
+            else {
+                element = static_cast<std::size_t>(grid->fields[static_cast<std::size_t>(a - 13)].bytes);
+                src = grid->A.f.base[a - 13] + off * static_cast<long long>(element);
+            }
+            cuda_check(cudaMemcpyAsync(arrays[a], src, total * element, cudaMemcpyDefault, s), "download");
+        }
+        cuda_check(cudaStreamSynchronize(s), "download");
+    });
+}
+
+int dsx_grid_totals(dsx_grid* grid, long long* out4, void* stream) {
+    return guarded([&] {
+        const auto s = static_cast<cudaStream_t>(stream);
+        const std::vector<int> e = grid->read_ints(grid->S.emig_info, 1, s);
+        const std::vector<int> h = grid->read_ints(grid->S.halo_info, 2, s);
+        out4[0] = grid->total;
+        out4[1] = e[0];
+        out4[2] = h[0];
+        out4[3] = h[1];
+    });
+}
+
 int dsx_grid_counts(dsx_grid* grid, long long* owned, long long* ghosts, void* stream) {
     return guarded([&] {
         const auto s = static_cast<cudaStream_t>(stream);
@@ -1113,6 +1162,32 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
         grid->step(callback, user, capture != 0, static_cast<cudaStream_t>(stream), status);
         cuda_check(cudaGetLastError(), "launch step");
     });
+}
+
+int dsx_grid_profile(dsx_grid* grid, int enable) {
+    return guarded([&] {
+        if (enable && !grid->marks.ev[0])
+            for (auto& e : grid->marks.ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        if ((enable != 0) != grid->marks.on) grid->destroy_graphs();
+        grid->marks.on = enable != 0;
+        grid->marks.count = 0;
+    });
+}
+
+int dsx_grid_kernel_times(dsx_grid* grid, int max, const char** names, float* ms) {
+    int n = 0;
+    const int status = guarded([&] {
+        const dsx::Marks& m = grid->marks;
+        if (!m.on || m.count < 2) return;
+        cuda_check(cudaEventSynchronize(m.ev[m.count - 1]), "event synchronize");
+        for (int k = 1; k < m.count && n < max; ++k, ++n) {
+            float t = 0.0f;
+            cuda_check(cudaEventElapsedTime(&t, m.ev[k - 1], m.ev[k]), "event elapsed");
+            if (names) names[n] = m.name[k];
+            if (ms) ms[n] = t;
+        }
+    });
+    return status == DSX_OK ? n : status;
 }
 
 int dsx_grid_step_kernel_count(dsx_grid* grid) {

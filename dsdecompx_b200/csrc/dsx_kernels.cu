@@ -953,30 +953,41 @@ void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long
     cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P, s);
     k_mig_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + src_off, A.d[1] + src_off,
                                                A.d[2] + src_off, S.cnt, S.stride, S.imm_total);
+    if (S.marks) S.marks->mark(s, "mig_classify");
     k_scan_counters<<<2, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    if (S.marks) S.marks->mark(s, "mig_scan");
     k_mig_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.imm_total, S.imm_base, S.emig_info,
                                      S.mig_results);
+    if (S.marks) S.marks->mark(s, "mig_layout");
     k_mig_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, S.pre, S.stride, S.emig_src,
                                           S.emig_dst);
+    if (S.marks) S.marks->mark(s, "mig_move");
     const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
     const size_t smem = sizeof(int) * NW * G.P;
     k_emig_hist<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(G.P, S.emig_info, S.emig_dst,
                                                                   S.emig_hist);
+    if (S.marks) S.marks->mark(s, "emig_hist");
     k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, S.imm_total, G.status);
+    if (S.marks) S.marks->mark(s, "emig_colscan");
     k_emig_place<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(
         G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base);
+    if (S.marks) S.marks->mark(s, "emig_place");
 }
 
 void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                        const Scratch& S, cudaStream_t s) {
     k_halo_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + owned_off, A.d[1] + owned_off,
                                                 A.d[2] + owned_off, S.mask, S.cnt, S.stride);
+    if (S.marks) S.marks->mark(s, "halo_classify");
     k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    if (S.marks) S.marks->mark(s, "halo_scan");
     k_halo_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.list_len, S.send_base, S.g, S.gbase,
                                       S.boff, S.halo_info);
+    if (S.marks) S.marks->mark(s, "halo_layout");
     k_halo_scatter<<<G.max_tiles, NT, 0, s>>>(G, A, owned_off, ghost_off, S.mask, S.pre, S.stride,
                                               S.send_base, S.ghost_owner, S.ghost_entry, S.bowner,
                                               S.boff, S.bslot);
+    if (S.marks) S.marks->mark(s, "halo_scatter");
 }
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
@@ -997,6 +1008,7 @@ void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, cons
                          const double* gy, const double* gz, const Scratch& S, cudaStream_t s) {
     k_reverse_sum3<<<stream_grid(G.ncap), NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot, ox,
                                                       oy, oz, gx, gy, gz, G.status);
+    if (S.marks) S.marks->mark(s, "reverse_sum");
 }
 
 void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
@@ -1009,6 +1021,10 @@ void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
 void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
                       long long* call_counter, double* result, cudaStream_t s) {
     k_rebalance<<<1, 32, 0, s>>>(G, work, params, call_counter, result);
+}
+
+void mark(const Scratch& S, cudaStream_t s, const char* what) {
+    if (S.marks) S.marks->mark(s, what);
 }
 
 void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,

@@ -6,6 +6,24 @@
 
 namespace dsx {
 
+// Optional per-kernel timing: when `on`, every launch wrapper records an
+// event after its kernel (inside a captured graph these become event-record
+// nodes), so that the host can read each kernel's duration of the last step.
+struct Marks {
+    static constexpr int kMax = 48;
+    cudaEvent_t ev[kMax] = {};
+    const char* name[kMax] = {};
+    int count = 0;
+    bool on = false;
+    void mark(cudaStream_t s, const char* what) {
+        if (!on || count >= kMax || !ev[count]) return;
+        name[count] = what;
+        // external: inside stream capture this becomes a real event-record
+        // node that every replay of the graph executes
+        cudaEventRecordWithFlags(ev[count++], s, cudaEventRecordExternal);
+    }
+};
+
 // Scratch shared by the phases of one step (device buffers owned by the
 // engine; sizes in the engine's allocate()).
 struct Scratch {
@@ -31,6 +49,7 @@ struct Scratch {
     int* bslot = nullptr;      // [gcap] ghost slots of each boundary owner, n ascending
     int* halo_info = nullptr;  // {G, B}
     int max_chunks = 0;
+    Marks* marks = nullptr;
 };
 
 void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, cudaStream_t s);
@@ -86,7 +105,9 @@ void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
 void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,
                          const double* extent, const int* periodic, cudaStream_t s);
 
-// Fills x with the per-kernel launch count (for reporting).
+// Records a named timing mark on `s` (no-op unless S.marks->on).
+void mark(const Scratch& S, cudaStream_t s, const char* what);
+
 int kernels_per_step();
 
 }  // namespace dsx

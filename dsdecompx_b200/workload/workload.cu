@@ -1,0 +1,106 @@
+// Synthetic-workload kernels for the benchmark harness (not part of the
+// bookkeeping path): the per-step drift of the owned particles and the ghost
+// forces that stand in for a user's force computation.  Both draw N(0,1)
+// deviates from a counter-based generator (splitmix64 of seed, step, particle
+// id and axis, then Box-Muller), so a step's inputs do not depend on the order
+// the particles sit in and the kernels can be captured in a CUDA graph.
+#include "dsx.h"
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace {
+
+// step number of the synthetic inputs; advanced on the device so that a
+// captured step draws fresh deviates at every replay
+__device__ unsigned long long g_step = 0;
+
+__device__ __forceinline__ std::uint64_t splitmix64(std::uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Standard normal deviate number `axis` (0..2) of counter `id` at `step`.
+__device__ __forceinline__ double normal(std::uint64_t seed, std::uint64_t step, std::uint64_t id,
+                                         int axis) {
+    const std::uint64_t key = splitmix64(seed ^ splitmix64(step * 0x100000001B3ull + id * 4 + axis));
+    const double u1 = (static_cast<double>(key >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+    const double u2 = static_cast<double>(splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
+__global__ void k_drift(double* x, double* y, double* z, const int* gid, long long n,
+                        std::uint64_t seed, std::uint64_t step, double sigma) {
+    step += g_step;
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += gridDim.x * 256ll) {
+        const std::uint64_t id = static_cast<std::uint32_t>(gid[i]);
+        x[i] += sigma * normal(seed, step, id, 0);
+        y[i] += sigma * normal(seed, step, id, 1);
+        z[i] += sigma * normal(seed, step, id, 2);
+    }
+}
+
+__global__ void k_ghost_forces(double* fx, double* fy, double* fz, const int* totals,
+                               std::uint64_t seed, std::uint64_t step) {
+    step += g_step;
+    const long long n = totals[0];
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += gridDim.x * 256ll) {
+        fx[i] = normal(seed, step, static_cast<std::uint64_t>(i), 0);
+        fy[i] = normal(seed, step, static_cast<std::uint64_t>(i), 1);
+        fz[i] = normal(seed, step, static_cast<std::uint64_t>(i), 2);
+    }
+}
+
+__global__ void k_advance() { ++g_step; }
+
+int grid_for(long long n) {
+    int sms = 148, device = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const long long want = (n + 255) / 256;
+    const long long cap = static_cast<long long>(sms) * 8;
+    return static_cast<int>(want < 1 ? 1 : (want < cap ? want : cap));
+}
+
+}  // namespace
+
+extern "C" {
+
+// owned x, y, z += sigma * N(0,1), keyed by global_id
+int dsxw_drift(const dsx_grid_view* v, unsigned long long seed, long long step, double sigma,
+               void* stream) {
+    const long long o = v->owned_offset;
+    k_drift<<<grid_for(v->particles), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<double*>(v->base[0]) + o, static_cast<double*>(v->base[1]) + o,
+        static_cast<double*>(v->base[2]) + o, static_cast<const int*>(v->base[12]) + o,
+        v->particles, seed, static_cast<std::uint64_t>(step), sigma);
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+// drift of plain device arrays (the single-rank drop-in workload)
+int dsxw_drift_arrays(double* x, double* y, double* z, const int* gid, long long n,
+                      unsigned long long seed, long long step, double sigma, void* stream) {
+    k_drift<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        x, y, z, gid, n, seed, static_cast<std::uint64_t>(step), sigma);
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+// ghost forces of the current halo = N(0,1), keyed by ghost slot
+int dsxw_ghost_forces(const dsx_grid_view* v, unsigned long long seed, long long step,
+                      void* stream) {
+    const long long g = v->ghost_offset;
+    k_ghost_forces<<<grid_for(v->ghost_capacity), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<double*>(v->base[6]) + g, static_cast<double*>(v->base[7]) + g,
+        static_cast<double*>(v->base[8]) + g, v->halo_totals, seed, static_cast<std::uint64_t>(step));
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+// moves the device step counter on (call once per step, after the draws)
+int dsxw_advance(void* stream) {
+    k_advance<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>();
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+}  // extern "C"

@@ -139,6 +139,15 @@ int dsx_grid_cuts(dsx_grid* grid, double* out, void* stream);
 int dsx_grid_upload(dsx_grid* grid, const long long* counts,
                     const void* const* arrays, void* stream);
 
+/* Inverse of dsx_grid_upload: counts[P] and the owned particles of every
+ * subdomain, concatenated in rank order, into host (or device) arrays of at
+ * least `particles` entries; null entries are skipped.  Synchronizes. */
+int dsx_grid_download(dsx_grid* grid, long long* counts, void* const* arrays, void* stream);
+
+/* Totals of the last migrate / halo build: {owned particles, emigrants,
+ * ghosts, boundary owners}; synchronizes `stream`. */
+int dsx_grid_totals(dsx_grid* grid, long long* out4, void* stream);
+
 /* Counts per subdomain (owned, ghosts); synchronizes `stream`. */
 int dsx_grid_counts(dsx_grid* grid, long long* owned, long long* ghosts, void* stream);
 
@@ -224,6 +233,14 @@ int dsx_grid_halo_backward(dsx_grid* grid, const double* ghost_cot_x,
 typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view* view);
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
                   void* stream, unsigned* status);
+
+/* Per-kernel timing of the batched step, for benchmarks: enable != 0 makes
+ * the next steps record a CUDA event after every kernel (inside a captured
+ * graph they are event-record nodes; captured graphs are rebuilt when the
+ * setting changes).  dsx_grid_kernel_times fills names/ms (milliseconds) for
+ * the intervals of the last step, in launch order, and returns how many. */
+int dsx_grid_profile(dsx_grid* grid, int enable);
+int dsx_grid_kernel_times(dsx_grid* grid, int max, const char** names, float* ms);
 
 /* Number of this library's kernel launches in one batched step (for reports). */
 int dsx_grid_step_kernel_count(dsx_grid* grid);
