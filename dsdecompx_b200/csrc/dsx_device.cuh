@@ -96,9 +96,14 @@ struct Grid {
 // Periodic wrap exactly as the reference Host path rounds it:
 // v -= lower; v -= floor(v / extent) * extent; v += lower
 // (dsDecompX src/migration.cpp:83-87, 106-113).  No FMA contraction.
+//
+// Fast path: for 0 <= t < extent the correctly rounded quotient t / extent is
+// at most 1 - 2^-53, so floor() of it is a zero carrying t's sign; the FP64
+// division (a long instruction sequence) is skipped without changing a bit of
+// the result.  Every other input (outside the box, NaN, inf) divides.
 __device__ __forceinline__ double wrap_axis(double v, double lower, double extent) {
     double t = __dsub_rn(v, lower);
-    const double q = floor(__ddiv_rn(t, extent));
+    const double q = (t >= 0.0 && t < extent) ? copysign(0.0, t) : floor(__ddiv_rn(t, extent));
     t = __dsub_rn(t, __dmul_rn(q, extent));
     return __dadd_rn(t, lower);
 }
@@ -134,6 +139,11 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
+// Read-only (non-coherent) load: the copy kernels read one region and write
+// another, so source loads may be reordered past the stores.
+template <class T>
+__device__ __forceinline__ T ro(const T* p) { return __ldg(p); }
+
 // Copies one particle's registered fields (bytes per particle as laid out in
 // `f`) from global index `src` to global index `dst`.
 __device__ __forceinline__ void copy_fields(const FieldSet& f, long long src, long long dst) {
@@ -143,11 +153,11 @@ __device__ __forceinline__ void copy_fields(const FieldSet& f, long long src, lo
         if ((b & 7) == 0) {
             const unsigned long long* s = reinterpret_cast<const unsigned long long*>(base + src * b);
             unsigned long long* d = reinterpret_cast<unsigned long long*>(base + dst * b);
-            for (int w = 0; w < (b >> 3); ++w) d[w] = s[w];
+            for (int w = 0; w < (b >> 3); ++w) d[w] = ro(s + w);
         } else {
             const unsigned* s = reinterpret_cast<const unsigned*>(base + src * b);
             unsigned* d = reinterpret_cast<unsigned*>(base + dst * b);
-            for (int w = 0; w < (b >> 2); ++w) d[w] = s[w];
+            for (int w = 0; w < (b >> 2); ++w) d[w] = ro(s + w);
         }
     }
 }

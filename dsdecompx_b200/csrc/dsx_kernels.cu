@@ -91,13 +91,17 @@ __device__ __forceinline__ int destination(const Grid& G, double px, double py, 
 
 __device__ __forceinline__ void move_record(const Arrays& A, long long src, long long dst,
                                             double wx, double wy, double wz) {
+    double v[8];
+#pragma unroll
+    for (int a = 3; a < 11; ++a) v[a - 3] = ro(A.d[a] + src);
+    const int ty = ro(A.type + src), id = ro(A.gid + src);
     A.d[0][dst] = wx;
     A.d[1][dst] = wy;
     A.d[2][dst] = wz;
 #pragma unroll
-    for (int a = 3; a < 11; ++a) A.d[a][dst] = A.d[a][src];
-    A.type[dst] = A.type[src];
-    A.gid[dst] = A.gid[src];
+    for (int a = 3; a < 11; ++a) A.d[a][dst] = v[a - 3];
+    A.type[dst] = ty;
+    A.gid[dst] = id;
     copy_fields(A.f, src, dst);
 }
 
@@ -170,9 +174,22 @@ __global__ void __launch_bounds__(NT) k_mig_classify(Grid G, const double* __res
     const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
     const int end = min(begin + TILE, G.obase[s] + G.n[s]);
     int stay = 0, emig = 0;
-    for (int i = begin + threadIdx.x; i < end; i += NT) {
+    double px[ITEMS], py[ITEMS], pz[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = begin + threadIdx.x + j * NT;
+        if (i < end) {
+            px[j] = ro(x + i);
+            py[j] = ro(y + i);
+            pz[j] = ro(z + i);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = begin + threadIdx.x + j * NT;
+        if (i >= end) continue;
         double wx, wy, wz;
-        const int d = destination(G, x[i], y[i], z[i], wx, wy, wz);
+        const int d = destination(G, px[j], py[j], pz[j], wx, wy, wz);
         if (d == s) {
             ++stay;
         } else {
@@ -258,7 +275,8 @@ __global__ void __launch_bounds__(NT) k_mig_move(Grid G, Arrays A, long long src
         dest[j] = -1;
         if (i < end) {
             const long long src = src_off + i;
-            dest[j] = destination(G, A.d[0][src], A.d[1][src], A.d[2][src], wx[j], wy[j], wz[j]);
+            dest[j] = destination(G, ro(A.d[0] + src), ro(A.d[1] + src), ro(A.d[2] + src), wx[j],
+                                  wy[j], wz[j]);
         }
         nstay += __popc(__ballot_sync(0xffffffffu, dest[j] == s));
         nemig += __popc(__ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s));
@@ -382,9 +400,10 @@ __global__ void __launch_bounds__(NT) k_emig_place(Grid G, Arrays A, long long s
                 const int pos = imm_base[d] + hist[static_cast<long long>(c) * P + d] +
                                 sm[warp * P + d] + __popc(peers & lt);
                 const long long src = src_off + emig_src[e];
-                const double wx = G.periodic[0] ? wrap_axis(A.d[0][src], G.lower[0], G.extent[0]) : A.d[0][src];
-                const double wy = G.periodic[1] ? wrap_axis(A.d[1][src], G.lower[1], G.extent[1]) : A.d[1][src];
-                const double wz = G.periodic[2] ? wrap_axis(A.d[2][src], G.lower[2], G.extent[2]) : A.d[2][src];
+                const double ox = ro(A.d[0] + src), oy = ro(A.d[1] + src), oz = ro(A.d[2] + src);
+                const double wx = G.periodic[0] ? wrap_axis(ox, G.lower[0], G.extent[0]) : ox;
+                const double wy = G.periodic[1] ? wrap_axis(oy, G.lower[1], G.extent[1]) : oy;
+                const double wz = G.periodic[2] ? wrap_axis(oz, G.lower[2], G.extent[2]) : oz;
                 move_record(A, src, dst_off + pos, wx, wy, wz);
             }
             __syncwarp();
@@ -456,12 +475,22 @@ __global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const double* __re
     const unsigned* lut = G.lut + s * 64;
     const int nn = G.nn[s];
     int acc = 0;
+    double px[ITEMS], py[ITEMS], pz[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        if (i < end) {
+            px[j] = ro(x + i);
+            py[j] = ro(y + i);
+            pz[j] = ro(z + i);
+        }
+    }
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = wbegin + j * 32 + lane;
         unsigned m = 0;
         if (i < end) {
-            m = halo_mask(b, lut, x[i], y[i], z[i]);
+            m = halo_mask(b, lut, px[j], py[j], pz[j]);
             mask[i] = m;
         }
         count_group(m, nn, lane, acc);
@@ -527,11 +556,37 @@ __global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, in
     }
 }
 
+// Ghost images a tile stages in shared memory before writing them out; a tile
+// with more images (only possible with a halo wider than half a cell) writes
+// them directly instead.
+constexpr int kStageCap = 6144;
+
+__device__ __forceinline__ void write_ghost(const Arrays& A, long long src, long long gi,
+                                            const double* sh) {
+    const double px = ro(A.d[0] + src), py = ro(A.d[1] + src), pz = ro(A.d[2] + src);
+    const double vx = ro(A.d[3] + src), vy = ro(A.d[4] + src), vz = ro(A.d[5] + src);
+    const double ms = ro(A.d[9] + src), ch = ro(A.d[10] + src);
+    const int ty = ro(A.type + src), id = ro(A.gid + src);
+    A.d[0][gi] = __dadd_rn(px, sh[0]);
+    A.d[1][gi] = __dadd_rn(py, sh[1]);
+    A.d[2][gi] = __dadd_rn(pz, sh[2]);
+    A.d[3][gi] = vx; A.d[4][gi] = vy; A.d[5][gi] = vz;
+    A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+    A.d[9][gi] = ms; A.d[10][gi] = ch;
+    A.type[gi] = ty; A.gid[gi] = id;
+    copy_fields(A.f, src, gi);
+}
+
 // H2: every (owner, neighbor) hit becomes a ghost in the receiver's block --
 // x + shift, v, f = 0, mass, charge, type, id and the registered fields, as
 // the reference's make_record + copy_record leave it (dsDecompX
 // src/halo.cpp:37-55, src/runtime.cpp:82-96) -- plus the ghost -> owner map
 // and the owner -> ghosts CSR that reverse_halo sums in neighbor order.
+//
+// The warps first rank every hit (ballot + popc) and stage the tile's images
+// in shared memory list by list; the whole CTA then writes each list's slice
+// of the ghost region with consecutive threads on consecutive slots, so every
+// array is written with full, coalesced runs.
 __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long owned_off,
                                                      long long ghost_off,
                                                      const unsigned* __restrict__ mask,
@@ -541,6 +596,8 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
                                                      int* bslot) {
     __shared__ int s_cnt[NW][32];
     __shared__ int s_base[32];
+    __shared__ int s_off[kMaxNeighbors + 1];
+    __shared__ unsigned short s_own[kStageCap];
     if (*G.status & kStatusGhostOverflow) return;
     const int g = blockIdx.x;
     const int P = G.P;
@@ -554,13 +611,14 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
     const unsigned lt = lanemask_lt();
 
     unsigned m[ITEMS];
-    int acc = 0;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = wbegin + j * 32 + lane;
         m[j] = i < end ? mask[i] : 0u;
-        count_group(m[j], nn, lane, acc);
     }
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) count_group(m[j], nn, lane, acc);
     s_cnt[warp][lane] = acc;
     if (threadIdx.x < kHaloCounters) {
         const int k = threadIdx.x;
@@ -570,11 +628,27 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
         s_base[k] = base;
     }
     __syncthreads();
-    // lane k carries the running offset of counter k for this warp
-    int run = 0;
+    if (threadIdx.x == 0) {
+        int q = 0;
+        for (int n = 0; n < nn; ++n) {
+            s_off[n] = q;
+            for (int w = 0; w < NW; ++w) q += s_cnt[w][n];
+        }
+        s_off[nn] = q;
+    }
+    __syncthreads();
+    const int Q = s_off[nn];
+    const bool staged = Q <= kStageCap;
+    // lane k carries counter k's running offset for this warp: the global
+    // slot (run) and, for lists, the position in the staged array (lrun)
+    int run = 0, lrun = 0;
     if (lane < kHaloCounters) {
         run = s_base[lane];
-        for (int w = 0; w < warp; ++w) run += s_cnt[w][lane];
+        if (lane < nn) lrun = s_off[lane];
+        for (int w = 0; w < warp; ++w) {
+            run += s_cnt[w][lane];
+            lrun += s_cnt[w][lane];
+        }
     }
     const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
 #pragma unroll 1
@@ -583,18 +657,11 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
         const unsigned any = __ballot_sync(0xffffffffu, mj != 0);
         if (!any) continue;
         const int i = wbegin + j * 32 + lane;
-        const long long src = owned_off + i;
         const int b = __shfl_sync(0xffffffffu, run, kBoundaryCounter) + __popc(any & lt);
         const int pm = __popc(mj);
         const int incl = warp_inclusive_sum(pm);
         const int img = __shfl_sync(0xffffffffu, run, kImageCounter) + incl - pm;
-        double px = 0, py = 0, pz = 0, vx = 0, vy = 0, vz = 0, ms = 0, ch = 0;
-        int ty = 0, id = 0;
         if (mj) {
-            px = A.d[0][src]; py = A.d[1][src]; pz = A.d[2][src];
-            vx = A.d[3][src]; vy = A.d[4][src]; vz = A.d[5][src];
-            ms = A.d[9][src]; ch = A.d[10][src];
-            ty = A.type[src]; id = A.gid[src];
             bowner[b] = i;
             boff[b] = img;
         }
@@ -603,27 +670,44 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
             const unsigned hit = __ballot_sync(0xffffffffu, (mj >> n) & 1u);
             if (!hit) continue;
             const int list_base = __shfl_sync(0xffffffffu, run, n);
+            const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
             if ((mj >> n) & 1u) {
-                const int slot = list_base + __popc(hit & lt);
-                const long long gi = ghost_off + slot;
-                A.d[0][gi] = __dadd_rn(px, shift[3 * n + 0]);
-                A.d[1][gi] = __dadd_rn(py, shift[3 * n + 1]);
-                A.d[2][gi] = __dadd_rn(pz, shift[3 * n + 2]);
-                A.d[3][gi] = vx; A.d[4][gi] = vy; A.d[5][gi] = vz;
-                A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
-                A.d[9][gi] = ms; A.d[10][gi] = ch;
-                A.type[gi] = ty; A.gid[gi] = id;
-                copy_fields(A.f, src, gi);
-                ghost_owner[slot] = i;
-                ghost_entry[slot] = s * kMaxNeighbors + n;
+                const int rank = __popc(hit & lt);
+                const int slot = list_base + rank;
                 bslot[img + k] = slot;
                 ++k;
+                if (staged) {
+                    s_own[stage_base + rank] = static_cast<unsigned short>(i - begin);
+                } else {
+                    write_ghost(A, owned_off + i, ghost_off + slot, shift + 3 * n);
+                    ghost_owner[slot] = i;
+                    ghost_entry[slot] = s * kMaxNeighbors + n;
+                }
             }
-            if (lane == n) run += __popc(hit);
+            if (lane == n) {
+                run += __popc(hit);
+                lrun += __popc(hit);
+            }
         }
         const int group_images = __shfl_sync(0xffffffffu, incl, 31);
         if (lane == kBoundaryCounter) run += __popc(any);
         if (lane == kImageCounter) run += group_images;
+    }
+    if (!staged) return;
+    __syncthreads();
+    for (int q = threadIdx.x; q < Q; q += NT) {
+        int lo = 0, hi = nn;   // largest n with s_off[n] <= q
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_off[mid] <= q) lo = mid;
+            else hi = mid;
+        }
+        const int n = lo;
+        const int slot = s_base[n] + (q - s_off[n]);
+        const int i = begin + s_own[q];
+        write_ghost(A, owned_off + i, ghost_off + slot, shift + 3 * n);
+        ghost_owner[slot] = i;
+        ghost_entry[slot] = s * kMaxNeighbors + n;
     }
 }
 

@@ -22,23 +22,35 @@ __device__ __forceinline__ std::uint64_t splitmix64(std::uint64_t z) {
     return z ^ (z >> 31);
 }
 
-// Standard normal deviate number `axis` (0..2) of counter `id` at `step`.
-__device__ __forceinline__ double normal(std::uint64_t seed, std::uint64_t step, std::uint64_t id,
-                                         int axis) {
-    const std::uint64_t key = splitmix64(seed ^ splitmix64(step * 0x100000001B3ull + id * 4 + axis));
-    const double u1 = (static_cast<double>(key >> 11) + 1.0) * (1.0 / 9007199254740992.0);
-    const double u2 = static_cast<double>(splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
-    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+// Three standard normal deviates for counter `id` at `step`: two Box-Muller
+// pairs in FP32 arithmetic (synthetic inputs only; the values are then used as
+// FP64 displacements and forces).
+__device__ __forceinline__ void normals3(std::uint64_t seed, std::uint64_t step, std::uint64_t id,
+                                         double& a, double& b, double& c) {
+    const std::uint64_t k1 = splitmix64(seed ^ splitmix64(step * 0x100000001B3ull + id));
+    const std::uint64_t k2 = splitmix64(k1);
+    const float u1 = (static_cast<float>(k1 >> 40) + 1.0f) * (1.0f / 16777216.0f);
+    const float u2 = static_cast<float>((k1 >> 16) & 0xFFFFFFull) * (1.0f / 16777216.0f);
+    const float u3 = (static_cast<float>(k2 >> 40) + 1.0f) * (1.0f / 16777216.0f);
+    const float u4 = static_cast<float>((k2 >> 16) & 0xFFFFFFull) * (1.0f / 16777216.0f);
+    const float r1 = sqrtf(-2.0f * __logf(u1)), r2 = sqrtf(-2.0f * __logf(u3));
+    float s1, c1, s2, c2;
+    __sincosf(6.2831853f * u2, &s1, &c1);
+    __sincosf(6.2831853f * u4, &s2, &c2);
+    a = r1 * c1;
+    b = r1 * s1;
+    c = r2 * c2;
 }
 
 __global__ void k_drift(double* x, double* y, double* z, const int* gid, long long n,
                         std::uint64_t seed, std::uint64_t step, double sigma) {
     step += g_step;
     for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += gridDim.x * 256ll) {
-        const std::uint64_t id = static_cast<std::uint32_t>(gid[i]);
-        x[i] += sigma * normal(seed, step, id, 0);
-        y[i] += sigma * normal(seed, step, id, 1);
-        z[i] += sigma * normal(seed, step, id, 2);
+        double a, b, c;
+        normals3(seed, step, static_cast<std::uint32_t>(gid[i]), a, b, c);
+        x[i] += sigma * a;
+        y[i] += sigma * b;
+        z[i] += sigma * c;
     }
 }
 
@@ -47,9 +59,11 @@ __global__ void k_ghost_forces(double* fx, double* fy, double* fz, const int* to
     step += g_step;
     const long long n = totals[0];
     for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += gridDim.x * 256ll) {
-        fx[i] = normal(seed, step, static_cast<std::uint64_t>(i), 0);
-        fy[i] = normal(seed, step, static_cast<std::uint64_t>(i), 1);
-        fz[i] = normal(seed, step, static_cast<std::uint64_t>(i), 2);
+        double a, b, c;
+        normals3(seed, step, static_cast<std::uint64_t>(i), a, b, c);
+        fx[i] = a;
+        fy[i] = b;
+        fz[i] = c;
     }
 }
 
