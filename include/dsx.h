@@ -245,6 +245,40 @@ int dsx_grid_kernel_times(dsx_grid* grid, int max, const char** names, float* ms
 /* Number of this library's kernel launches in one batched step (for reports). */
 int dsx_grid_step_kernel_count(dsx_grid* grid);
 
+/* ------------------------------------------------------------------------
+ * Allocation-free migrate.  No counterpart in the reference (its migrate grows
+ * device buffers with cudaMalloc as needed).
+ *
+ * For callers that cannot allocate device memory: a solver whose framework
+ * owns all GPU memory through its own pool, a latency-critical loop where an
+ * allocation's implicit device synchronization is not acceptable, or a plugin
+ * that must not change the process's memory footprint.  Such a caller cannot
+ * create a dsx_grid (which allocates its storage); this call migrates the
+ * caller's own arrays instead: the owned particles of `desc->nranks`
+ * subdomains, concatenated in rank order (counts_in[P] on the host; arrays_in
+ * and arrays_out: the 13 core device arrays in array-id order, no registered
+ * fields), into arrays_out in the migrated order -- the same result as
+ * dsx_grid_migrate on the same grid, cuts and particles.  cuts: host array of
+ * the axis cuts (dims[a]+1 per axis) or null for uniform cuts; desc->dims must
+ * be explicit; there is no automatic Dynamic rebalance.  counts_out[P] and
+ * results (null or P x 6, as dsx_grid_migrate) are host arrays; the call
+ * synchronizes `stream`.
+ *
+ * Limits: at most 64 subdomains and 262144 particles (DSX_E_LENGTH beyond).
+ * Scratch: one fixed 2.2 MB device array inside the library, reserved on every
+ * GPU that loads it until the process exits; nothing else is allocated.  The
+ * first call on a device looks up that array's device address (and may make
+ * the driver load the library's device code): make the first call before any
+ * CUDA-graph capture.  All calls share the array and it keeps the previous
+ * call's contents, so calls that overlap on the GPU (other streams or host
+ * threads) race: serialize them.  Errors: a DSX_E_* code and, if `error` is
+ * not null, a message in the caller's buffer of `error_capacity` bytes. */
+int dsx_migrate_noalloc(const dsx_grid_desc* desc, const double* cuts,
+                        const long long* counts_in, const void* const* arrays_in,
+                        long long* counts_out, void* const* arrays_out,
+                        long long* results, void* stream, char* error,
+                        int error_capacity);
+
 #ifdef __cplusplus
 }
 #endif
