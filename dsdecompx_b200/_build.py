@@ -19,6 +19,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libdsx.so")
 INCLUDE = os.path.join(ROOT, "include")
+# header-only single-process <mpi.h> for the C++ drop-in where no MPI exists
+MPI_STUB = os.path.join(INCLUDE, "dsx_mpi_stub")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # -fmad=false: the FP64 wrap / shift / sum expressions must round like the
@@ -50,8 +52,8 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) \
         + glob.glob(os.path.join(INCLUDE, "*.h")) + glob.glob(os.path.join(INCLUDE, "*.hpp"))
     if force or _stale(LIB, deps):
-        cmd = [nvcc()] + NVCC_FLAGS + ["-shared", "-I" + INCLUDE, "-I" + CSRC, "-o", LIB] \
-            + sources() + ["-lcuda"]
+        cmd = [nvcc()] + NVCC_FLAGS + ["-shared", "-I" + INCLUDE, "-I" + MPI_STUB, "-I" + CSRC,
+                                       "-o", LIB] + sources() + ["-lcuda"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
@@ -81,7 +83,7 @@ def build_cpp_tests(force: bool = False, verbose: bool = False) -> List[str]:
     for src in sorted(glob.glob(os.path.join(ROOT, "tests", "cpp", "*.cpp"))):
         exe = os.path.join(LIBDIR, os.path.splitext(os.path.basename(src))[0])
         if force or _stale(exe, [src, LIB]):
-            cmd = [nvcc()] + ARCH + ["-O2", "-std=c++17", "-I" + INCLUDE, "-o", exe, src,
+            cmd = [nvcc()] + ARCH + ["-O2", "-std=c++17", "-I" + INCLUDE, "-I" + MPI_STUB, "-o", exe, src,
                                      "-L" + LIBDIR, "-ldsx", "-Xlinker", "-rpath=" + LIBDIR]
             if verbose:
                 print(" ".join(cmd))
