@@ -128,6 +128,10 @@ def algorithmic_bytes(S, N, E, G, B):
         "halo_classify": 24 * N + 4 * N,                      # positions in, mask out
         "halo_scatter": 4 * N + S * B + (S + 12) * G + 8 * B,  # masks, owners, ghosts + maps
         "reverse_sum": 8 * B + 4 * G + 24 * G + 48 * B,       # CSR, ghost forces, owner RMW
+        # fused step (migrate + plan build in one pipeline)
+        "step_classify": 24 * N + 6 * N,                      # positions in; destination + mask out
+        "step_move": 6 * N + S * R + S * R + 8 * E + (S + 12) * G + 8 * B,
+        "immigrant_halo": E * (24 + 4),
     }
 
 
@@ -235,7 +239,7 @@ def run_ours(args, rank, world, device):
     ours = {k: v for k, v in avg.items() if k not in ("callback",)}
     dominant = max(ours, key=ours.get)
     peak, peak_kind = peaks()
-    step_bytes = sum(alg.values())
+    step_bytes = sum(v for k, v in alg.items() if k in ours)
     ours_ms = sum(ours.values())
     roof = None
     if dominant in alg:

@@ -83,10 +83,14 @@ struct Grid {
     int* n = nullptr;            // [P]
     int* obase = nullptr;        // [P+1]
     int* tile_start = nullptr;   // [P+1]
+    // per tile of the current layout: {subdomain, first particle, end, first
+    // tile of that subdomain}, so a CTA finds its work with one 16-byte load
+    const int4* tiles = nullptr;
     // next layout (written by migrate)
     int* n_next = nullptr;
     int* obase_next = nullptr;
     int* tile_start_next = nullptr;
+    int4* tiles_next = nullptr;
 
     unsigned* status = nullptr;
 };

@@ -226,6 +226,7 @@ struct dsx_grid {
     double* cuts = nullptr;
     int cut_offset[3] = {0, 0, 0};
     int* layout[2][3] = {};   // [which][n, obase, tile_start]
+    int4* layout_tiles[2] = {};   // per-tile descriptors of each layout
     int cur = 0;              // current layout index
     int parity = 0;           // current owned half
     unsigned* status = nullptr;
@@ -299,9 +300,11 @@ struct dsx_grid {
         G.n = layout[cur][0];
         G.obase = layout[cur][1];
         G.tile_start = layout[cur][2];
+        G.tiles = layout_tiles[cur];
         G.n_next = layout[cur ^ 1][0];
         G.obase_next = layout[cur ^ 1][1];
         G.tile_start_next = layout[cur ^ 1][2];
+        G.tiles_next = layout_tiles[cur ^ 1];
         G.status = status;
         return G;
     }
@@ -443,6 +446,8 @@ struct dsx_grid {
             cuda_check(cudaMemset(l[1], 0, sizeof(int) * (P + 1)), "memset");
             cuda_check(cudaMemset(l[2], 0, sizeof(int) * (P + 1)), "memset");
         }
+        const int tiles_cap = static_cast<int>((ncap + 1023) / 1024) + P;
+        for (auto& t : layout_tiles) t = device_alloc<int4>(fixed_owned, tiles_cap);
         status = device_alloc<unsigned>(fixed_owned, 4);
         cuda_check(cudaMemset(status, 0, 4 * sizeof(unsigned)), "memset");
         call_counter = device_alloc<long long>(fixed_owned, 1);
@@ -452,9 +457,20 @@ struct dsx_grid {
 
         const int max_tiles = static_cast<int>((ncap + 1023) / 1024) + P;
         S.stride = max_tiles + 1;
-        S.cnt = device_alloc<int>(fixed_owned, static_cast<std::size_t>(dsx::kHaloCounters) * S.stride);
-        S.pre = device_alloc<int>(fixed_owned, static_cast<std::size_t>(dsx::kHaloCounters) * S.stride);
-        S.imm_total = device_alloc<int>(fixed_owned, P);
+        // 30 counters per tile: the fused step's (28 halo + stays + emigrants)
+        S.cnt = device_alloc<int>(fixed_owned, static_cast<std::size_t>(30) * S.stride);
+        S.pre = device_alloc<int>(fixed_owned, static_cast<std::size_t>(30) * S.stride);
+        S.cnt2 = device_alloc<int>(fixed_owned, static_cast<std::size_t>(dsx::kHaloCounters) * S.stride);
+        S.pre2 = device_alloc<int>(fixed_owned, static_cast<std::size_t>(dsx::kHaloCounters) * S.stride);
+        // immigrant totals, per-list, boundary and image counts in one block
+        S.imm_total = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * (3 + dsx::kMaxNeighbors));
+        S.imm_list = S.imm_total + P;
+        S.imm_bnd = S.imm_list + static_cast<std::size_t>(P) * dsx::kMaxNeighbors;
+        S.imm_img = S.imm_bnd + P;
+        S.list_ret = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
+        S.cbase_imm = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * dsx::kHaloCounters);
+        S.imm_tile_start = device_alloc<int>(fixed_owned, P + 1);
+        S.imm_tiles = device_alloc<int4>(fixed_owned, static_cast<std::size_t>(max_tiles));
         S.imm_base = device_alloc<int>(fixed_owned, P);
         S.emig_src = device_alloc<int>(fixed_owned, ncap);
         S.emig_dst = device_alloc<int>(fixed_owned, ncap);
@@ -464,6 +480,7 @@ struct dsx_grid {
         cuda_check(cudaMemset(S.emig_info, 0, 4 * sizeof(int)), "memset");
         S.mig_results = device_alloc<long long>(fixed_owned, static_cast<std::size_t>(P) * 6);
         S.mask = device_alloc<unsigned>(fixed_owned, ncap);
+        S.dest16 = device_alloc<unsigned short>(fixed_owned, ncap);
         S.list_len = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
         S.send_base = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
         S.g = device_alloc<int>(fixed_owned, P + 1);
@@ -472,6 +489,7 @@ struct dsx_grid {
         cuda_check(cudaMemset(S.gbase, 0, sizeof(int) * (P + 1)), "memset");
         S.bowner = device_alloc<int>(fixed_owned, ncap);
         S.boff = device_alloc<int>(fixed_owned, ncap + 1);
+        S.cbase = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * dsx::kHaloCounters);
         S.halo_info = device_alloc<int>(fixed_owned, 4);
         cuda_check(cudaMemset(S.halo_info, 0, 4 * sizeof(int)), "memset");
     }
@@ -527,6 +545,11 @@ struct dsx_grid {
     // -------------------------------------------------------- operations
 
     void enqueue_migrate(cudaStream_t stream, bool automatic_rebalance) {
+        enqueue_rebalance(stream, automatic_rebalance);
+        dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream);
+    }
+
+    void enqueue_rebalance(cudaStream_t stream, bool automatic_rebalance) {
         const dsx::Grid G = params();
         if (desc.policy == DSX_DYNAMIC) {
             // Decomp::migrate: ++migration_calls, automatic rebalance every
@@ -542,7 +565,6 @@ struct dsx_grid {
             dsx::launch_rebalance(G, nullptr, p, call_counter, rebalance_result, stream);
             dsx::mark(S, stream, "rebalance");
         }
-        dsx::launch_migrate(G, A, owned_off(), next_off(), S, stream);
     }
 
     void commit_migrate() {
@@ -742,11 +764,17 @@ struct dsx_grid {
         marks.count = 0;
         clear_status(stream);
         marks.mark(stream, "start");
-        enqueue_migrate(stream, true);
+        enqueue_rebalance(stream, true);
+        {
+            const dsx::Grid G = params();
+            cur ^= 1;
+            const dsx::Grid Gn = params();
+            cur ^= 1;
+            dsx::launch_fused_step(G, Gn, A, owned_off(), next_off(), ghost_off(), S, stream);
+        }
         // the rest of the step reads the next layout
         parity ^= 1;
         cur ^= 1;
-        enqueue_halo_build(stream);
         const dsx_grid_view v = view();
         // inside the callback the new plan is the current one (field
         // exchanges called from it act on these ghosts)
@@ -840,7 +868,8 @@ struct dsx_grid {
         for (int s = 0; s < P; ++s) c[static_cast<std::size_t>(s)] = static_cast<int>(counts[s]);
         cuda_check(cudaMemcpyAsync(layout[cur][0], c.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice, stream),
                    "upload counts");
-        dsx::launch_layout(params(), layout[cur][0], layout[cur][1], layout[cur][2], stream);
+        dsx::launch_layout(params(), layout[cur][0], layout[cur][1], layout[cur][2], layout_tiles[cur],
+                           stream);
         cuda_check(cudaMemsetAsync(S.g, 0, sizeof(int) * (P + 1), stream), "memset");
         cuda_check(cudaMemsetAsync(S.gbase, 0, sizeof(int) * (P + 1), stream), "memset");
         cuda_check(cudaMemsetAsync(S.halo_info, 0, sizeof(int) * 4, stream), "memset");

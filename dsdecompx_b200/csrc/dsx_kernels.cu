@@ -63,25 +63,51 @@ __device__ __forceinline__ int warp_inclusive_sum(int v) {
     return v;
 }
 
+// One subdomain's cell: its grid coordinates and cut planes.
+struct Cell {
+    int c[3];
+    double lo[3], hi[3];
+};
+
+__device__ __forceinline__ Cell cell_of(const Grid& G, int s) {
+    Cell cell;
+    cell.c[0] = s / (G.dims[1] * G.dims[2]);
+    cell.c[1] = (s / G.dims[2]) % G.dims[1];
+    cell.c[2] = s % G.dims[2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double* cuts = G.cuts + G.cut_offset[a];
+        cell.lo[a] = cuts[cell.c[a]];
+        cell.hi[a] = cuts[cell.c[a] + 1];
+    }
+    return cell;
+}
+
 // Host-path destination of one owned particle: wrapped_record wraps the
 // position once, owner_rank wraps it again and bisects the cuts
 // (dsDecompX src/migration.cpp:437-441, 74-98).  Returns the rank and the
-// once-wrapped position that the migrated record carries.
-__device__ __forceinline__ int destination(const Grid& G, double px, double py, double pz,
-                                           double& wx, double& wy, double& wz) {
+// once-wrapped position that the migrated record carries.  `cell` is where
+// the particle most likely still is: inside its cut planes upper_bound's
+// answer is the cell's own coordinate (the cuts are strictly increasing), so
+// the bisection runs only for particles that left it.
+__device__ __forceinline__ int destination_near(const Grid& G, const Cell& cell, double px,
+                                                double py, double pz, double& wx, double& wy,
+                                                double& wz) {
     const double p[3] = {px, py, pz};
     double w[3];
     int c[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+        double v = p[a];
         if (G.periodic[a]) {
             w[a] = wrap_axis(p[a], G.lower[a], G.extent[a]);
-            const double w2 = wrap_axis(w[a], G.lower[a], G.extent[a]);
-            c[a] = axis_coordinate(G.cuts + G.cut_offset[a], G.dims[a], w2);
+            v = wrap_axis(w[a], G.lower[a], G.extent[a]);
         } else {
             w[a] = p[a];
-            c[a] = axis_coordinate(G.cuts + G.cut_offset[a], G.dims[a], p[a]);
         }
+        c[a] = (cell.lo[a] <= v && v < cell.hi[a])
+                   ? cell.c[a]
+                   : axis_coordinate(G.cuts + G.cut_offset[a], G.dims[a], v);
     }
     wx = w[0];
     wy = w[1];
@@ -107,9 +133,28 @@ __device__ __forceinline__ void move_record(const Arrays& A, long long src, long
 
 // ------------------------------------------------------------------ layout
 
+// Writes the per-tile descriptors {s, begin, end, first tile of s} of a
+// layout whose counts, bases and tile starts sit in shared memory.
+__device__ __forceinline__ void fill_tiles(int P, int tile, const int* s_n, const int* s_ob,
+                                           const int* s_ts, int4* tiles) {
+    const int total = s_ts[P];
+    for (int g = threadIdx.x; g < total; g += blockDim.x) {
+        int lo = 0, hi = P;   // largest s with s_ts[s] <= g
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_ts[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        const int begin = s_ob[lo] + (g - s_ts[lo]) * tile;
+        const int end = min(begin + tile, s_ob[lo] + s_n[lo]);
+        tiles[g] = make_int4(lo, begin, end, s_ts[lo]);
+    }
+}
+
 __global__ void __launch_bounds__(1024) k_layout(int P, int tile, const int* n, int* obase,
-                                                  int* tile_start) {
+                                                  int* tile_start, int4* tiles) {
     __shared__ int ws[33];
+    __shared__ int s_n[kMaxRanks + 1], s_ob[kMaxRanks + 1], s_ts[kMaxRanks + 1];
     const int t = threadIdx.x;
     const int a = t < P ? n[t] : 0;
     const int b = t < P ? (a + tile - 1) / tile : 0;
@@ -119,11 +164,18 @@ __global__ void __launch_bounds__(1024) k_layout(int P, int tile, const int* n, 
     if (t < P) {
         obase[t] = ea;
         tile_start[t] = eb;
+        s_n[t] = a;
+        s_ob[t] = ea;
+        s_ts[t] = eb;
     }
     if (t == 0) {
         obase[P] = ta;
         tile_start[P] = tb;
+        s_ob[P] = ta;
+        s_ts[P] = tb;
     }
+    __syncthreads();
+    fill_tiles(P, tile, s_n, s_ob, s_ts, tiles);
 }
 
 // Exclusive prefix of counter k (= blockIdx.x) over the tiles of the layout.
@@ -162,7 +214,7 @@ __global__ void __launch_bounds__(1024) k_scan_counters(const int* cnt, int* pre
 
 // K1: destination of every owned particle; per-tile stay/emigrant counts and
 // per-destination immigrant totals.
-__global__ void __launch_bounds__(NT) k_mig_classify(Grid G, const double* __restrict__ x,
+__global__ void __launch_bounds__(NT, 4) k_mig_classify(Grid G, const double* __restrict__ x,
                                                      const double* __restrict__ y,
                                                      const double* __restrict__ z, int* cnt,
                                                      int stride, int* imm_total) {
@@ -170,10 +222,10 @@ __global__ void __launch_bounds__(NT) k_mig_classify(Grid G, const double* __res
     const int g = blockIdx.x;
     const int P = G.P;
     if (g >= G.tile_start[P]) return;
-    const int s = tile_owner(G.tile_start, P, g);
-    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
-    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    const int4 td = G.tiles[g];
+    const int s = td.x, begin = td.y, end = td.z;
     int stay = 0, emig = 0;
+    const Cell cell = cell_of(G, s);
     double px[ITEMS], py[ITEMS], pz[ITEMS];
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
@@ -189,7 +241,7 @@ __global__ void __launch_bounds__(NT) k_mig_classify(Grid G, const double* __res
         const int i = begin + threadIdx.x + j * NT;
         if (i >= end) continue;
         double wx, wy, wz;
-        const int d = destination(G, px[j], py[j], pz[j], wx, wy, wz);
+        const int d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
         if (d == s) {
             ++stay;
         } else {
@@ -222,11 +274,15 @@ __global__ void __launch_bounds__(1024) k_mig_layout(Grid G, const int* pre, int
         old = G.n[t];
         next = retained + received;
     }
+    __shared__ int s_n[kMaxRanks + 1], s_ob[kMaxRanks + 1], s_ts[kMaxRanks + 1];
     int total_next, total_tiles;
     const int ob = block_scan_excl<1024>(next, total_next, ws);
     const int tiles = t < P ? (next + G.tile - 1) / G.tile : 0;
     const int ts = block_scan_excl<1024>(tiles, total_tiles, ws);
     if (t < P) {
+        s_n[t] = next;
+        s_ob[t] = ob;
+        s_ts[t] = ts;
         G.n_next[t] = next;
         G.obase_next[t] = ob;
         G.tile_start_next[t] = ts;
@@ -240,6 +296,8 @@ __global__ void __launch_bounds__(1024) k_mig_layout(Grid G, const int* pre, int
         o[0] = (o[3] != 0 || o[4] != 0) ? 1 : 0;
     }
     if (t == 0) {
+        s_ob[P] = total_next;
+        s_ts[P] = total_tiles;
         G.obase_next[P] = total_next;
         G.tile_start_next[P] = total_tiles;
         const int E = pre[stride + ntiles];
@@ -247,21 +305,22 @@ __global__ void __launch_bounds__(1024) k_mig_layout(Grid G, const int* pre, int
         emig_info[1] = (E + TILE - 1) / TILE;
         if (total_next != G.obase[P]) atomicOr(G.status, kStatusMigrationMismatch);
     }
+    __syncthreads();
+    fill_tiles(P, G.tile, s_n, s_ob, s_ts, G.tiles_next);
 }
 
 // K2: retained particles move (stably) to the next layout; emigrants are
 // listed in (source subdomain, source order), which is the order the
 // reference's receivers append them in.
-__global__ void __launch_bounds__(NT) k_mig_move(Grid G, Arrays A, long long src_off,
+__global__ void __launch_bounds__(NT, 4) k_mig_move(Grid G, Arrays A, long long src_off,
                                                  long long dst_off, const int* pre, int stride,
                                                  int* emig_src, int* emig_dst) {
     __shared__ int s_stay[NW], s_emig[NW];
     const int g = blockIdx.x;
     const int P = G.P;
     if (g >= G.tile_start[P]) return;
-    const int s = tile_owner(G.tile_start, P, g);
-    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
-    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    const int4 td = G.tiles[g];
+    const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wbegin = begin + warp * 32 * ITEMS;
     const unsigned lt = lanemask_lt();
@@ -269,14 +328,15 @@ __global__ void __launch_bounds__(NT) k_mig_move(Grid G, Arrays A, long long src
     int dest[ITEMS];
     double wx[ITEMS], wy[ITEMS], wz[ITEMS];
     int nstay = 0, nemig = 0;
+    const Cell cell = cell_of(G, s);
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = wbegin + j * 32 + lane;
         dest[j] = -1;
         if (i < end) {
             const long long src = src_off + i;
-            dest[j] = destination(G, ro(A.d[0] + src), ro(A.d[1] + src), ro(A.d[2] + src), wx[j],
-                                  wy[j], wz[j]);
+            dest[j] = destination_near(G, cell, ro(A.d[0] + src), ro(A.d[1] + src), ro(A.d[2] + src),
+                                       wx[j], wy[j], wz[j]);
         }
         nstay += __popc(__ballot_sync(0xffffffffu, dest[j] == s));
         nemig += __popc(__ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s));
@@ -286,7 +346,7 @@ __global__ void __launch_bounds__(NT) k_mig_move(Grid G, Arrays A, long long src
         s_emig[warp] = nemig;
     }
     __syncthreads();
-    int stay_base = G.obase_next[s] + (pre[g] - pre[G.tile_start[s]]);
+    int stay_base = G.obase_next[s] + (pre[g] - pre[td.w]);
     int emig_base = pre[stride + g];
     for (int w = 0; w < warp; ++w) {
         stay_base += s_stay[w];
@@ -445,9 +505,14 @@ __device__ __forceinline__ unsigned halo_mask(const TileBounds& b, const unsigne
 // Adds this warp's contribution of one 32-particle group to the per-lane
 // counters (lane n < 26: send list n, lane 26: boundary owners, lane 27: images).
 __device__ __forceinline__ void count_group(unsigned m, int nn, int lane, int& acc) {
+    (void)nn;
     const unsigned any = __ballot_sync(0xffffffffu, m != 0);
     if (!any) return;
-    for (int n = 0; n < nn; ++n) {
+    // only the neighbors some lane of the warp sends to (a face particle of a
+    // warp rarely touches more than a few of the 26)
+    const unsigned used = __reduce_or_sync(0xffffffffu, m);
+    for (unsigned rest = used; rest; rest &= rest - 1) {
+        const int n = __ffs(rest) - 1;
         const unsigned b = __ballot_sync(0xffffffffu, (m >> n) & 1u);
         if (lane == n) acc += __popc(b);
     }
@@ -458,17 +523,19 @@ __device__ __forceinline__ void count_group(unsigned m, int nn, int lane, int& a
 }
 
 // H1: neighbor mask of every owned particle and per-tile list counts.
-__global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const double* __restrict__ x,
+// `tiles`/`ntiles`: the tiles to classify (all owned particles of a layout,
+// or the immigrant segments of a fused step).
+__global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const int4* __restrict__ tiles,
+                                                      const int* ntiles,
+                                                      const double* __restrict__ x,
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z,
                                                       unsigned* mask, int* cnt, int stride) {
     __shared__ int s_cnt[NW][32];
     const int g = blockIdx.x;
-    const int P = G.P;
-    if (g >= G.tile_start[P]) return;
-    const int s = tile_owner(G.tile_start, P, g);
-    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
-    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    if (g >= *ntiles) return;
+    const int4 td = tiles[g];
+    const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wbegin = begin + warp * 32 * ITEMS;
     const TileBounds b = halo_bounds(G, s);
@@ -509,7 +576,8 @@ __global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const double* __re
 // every send list.  One CTA, one thread per receiver.
 __global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, int stride,
                                                        int* list_len, int* send_base, int* gq,
-                                                       int* gbase, int* boff, int* info) {
+                                                       int* gbase, int* boff, int* info,
+                                                       int* cbase) {
     __shared__ int ws[33];
     const int P = G.P;
     const int ntiles = G.tile_start[P];
@@ -554,6 +622,16 @@ __global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, in
             boff[B] = images;
         }
     }
+    __syncthreads();
+    // per subdomain and counter, the value that turns a tile prefix into the
+    // global index: first slot of each send list, boundary/image prefixes
+    for (int idx = threadIdx.x; idx < P * kHaloCounters; idx += blockDim.x) {
+        const int r = idx / kHaloCounters, k = idx % kHaloCounters;
+        int v;
+        if (k < kMaxNeighbors) v = (k < G.nn[r] && G.nbr[r * kMaxNeighbors + k] >= 0) ? send_base[r * kMaxNeighbors + k] : 0;
+        else v = pre[k * stride + G.tile_start[r]];
+        cbase[idx] = v;
+    }
 }
 
 // Ghost images a tile stages in shared memory before writing them out; a tile
@@ -589,9 +667,11 @@ __device__ __forceinline__ void write_ghost(const Arrays& A, long long src, long
 // array is written with full, coalesced runs.
 __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long owned_off,
                                                      long long ghost_off,
+                                                     const int4* __restrict__ tiles,
+                                                     const int* ntiles,
                                                      const unsigned* __restrict__ mask,
                                                      const int* pre, int stride,
-                                                     const int* send_base, int* ghost_owner,
+                                                     const int* cbase, int* ghost_owner,
                                                      int* ghost_entry, int* bowner, int* boff,
                                                      int* bslot) {
     __shared__ int s_cnt[NW][32];
@@ -600,11 +680,9 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
     __shared__ unsigned short s_own[kStageCap];
     if (*G.status & kStatusGhostOverflow) return;
     const int g = blockIdx.x;
-    const int P = G.P;
-    if (g >= G.tile_start[P]) return;
-    const int s = tile_owner(G.tile_start, P, g);
-    const int begin = G.obase[s] + (g - G.tile_start[s]) * TILE;
-    const int end = min(begin + TILE, G.obase[s] + G.n[s]);
+    if (g >= *ntiles) return;
+    const int4 td = tiles[g];
+    const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wbegin = begin + warp * 32 * ITEMS;
     const int nn = G.nn[s];
@@ -622,19 +700,18 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
     s_cnt[warp][lane] = acc;
     if (threadIdx.x < kHaloCounters) {
         const int k = threadIdx.x;
-        const int first = G.tile_start[s];
-        int base = pre[k * stride + g];
-        if (k < kMaxNeighbors) base += send_base[s * kMaxNeighbors + k] - pre[k * stride + first];
-        s_base[k] = base;
+        s_base[k] = cbase[s * kHaloCounters + k] + pre[k * stride + g] - pre[k * stride + td.w];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int q = 0;
-        for (int n = 0; n < nn; ++n) {
-            s_off[n] = q;
-            for (int w = 0; w < NW; ++w) q += s_cnt[w][n];
-        }
-        s_off[nn] = q;
+    if (warp == 0) {
+        // staging offsets of the lists: lane n sums its list over the warps,
+        // then an exclusive scan over the lanes
+        int tot = 0;
+        if (lane < nn)
+            for (int w = 0; w < NW; ++w) tot += s_cnt[w][lane];
+        const int incl = warp_inclusive_sum(tot);
+        if (lane < nn) s_off[lane] = incl - tot;
+        if (lane == 31) s_off[nn] = incl;
     }
     __syncthreads();
     const int Q = s_off[nn];
@@ -666,9 +743,10 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
             boff[b] = img;
         }
         int k = 0;
-        for (int n = 0; n < nn; ++n) {
+        const unsigned used = __reduce_or_sync(0xffffffffu, mj);
+        for (unsigned rest = used; rest; rest &= rest - 1) {
+            const int n = __ffs(rest) - 1;
             const unsigned hit = __ballot_sync(0xffffffffu, (mj >> n) & 1u);
-            if (!hit) continue;
             const int list_base = __shfl_sync(0xffffffffu, run, n);
             const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
             if ((mj >> n) & 1u) {
@@ -707,6 +785,421 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
         const int i = begin + s_own[q];
         write_ghost(A, owned_off + i, ghost_off + slot, shift + 3 * n);
         ghost_owner[slot] = i;
+        ghost_entry[slot] = s * kMaxNeighbors + n;
+    }
+}
+
+// ------------------------------------------------------------- fused step
+//
+// A batched step runs migrate and the plan build as one pipeline, so each
+// owned record is read once: the classify pass already knows every
+// particle's destination and its halo mask there (the mask of the particle's
+// NEW owner, computed from its wrapped position), the move pass writes a
+// retained particle to its new slot and, from the same registers, its ghost
+// images; the few immigrants get theirs in a small pass over their segments.
+// The result is the same as migrate followed by a rebuild: a send list
+// L(r, n) is r's retained particles with bit n (old order, which is their new
+// order) followed by r's immigrants with bit n (immigrant order).
+
+// counters per tile of the old layout: 0..25 retained send lists, 26 retained
+// boundary owners, 27 retained images, 28 stays, 29 emigrants
+constexpr int kStepCounters = 30;
+constexpr int kStepStay = 28;
+constexpr int kStepEmig = 29;
+
+__device__ __forceinline__ double wrap_if(const Grid& G, int a, double v) {
+    return G.periodic[a] ? wrap_axis(v, G.lower[a], G.extent[a]) : v;
+}
+
+// F1: destination and new-owner halo mask of every owned particle; per-tile
+// counters; per-destination totals of the emigrants (atomics: only sums).
+__global__ void __launch_bounds__(NT, 4) k_step_classify(Grid G, const double* __restrict__ x,
+                                                      const double* __restrict__ y,
+                                                      const double* __restrict__ z, int* cnt,
+                                                      int stride, int* imm_total, int* imm_list,
+                                                      int* imm_bnd, int* imm_img,
+                                                      unsigned short* __restrict__ dest_out,
+                                                      unsigned* __restrict__ mask_out) {
+    __shared__ int s_cnt[NW][32];
+    const int g = blockIdx.x;
+    if (g >= G.tile_start[G.P]) return;
+    const int4 td = G.tiles[g];
+    const int s = td.x, begin = td.y, end = td.z;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbegin = begin + warp * 32 * ITEMS;
+    const TileBounds bs = halo_bounds(G, s);
+    const Cell cell = cell_of(G, s);
+    const unsigned* lut = G.lut + s * 64;
+    const int nn = G.nn[s];
+    double px[ITEMS], py[ITEMS], pz[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        if (i < end) {
+            px[j] = ro(x + i);
+            py[j] = ro(y + i);
+            pz[j] = ro(z + i);
+        }
+    }
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        int d = -1;
+        unsigned m = 0;
+        if (i < end) {
+            double wx, wy, wz;
+            d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
+            dest_out[i] = static_cast<unsigned short>(d);
+            if (d == s) {
+                m = halo_mask(bs, lut, wx, wy, wz);
+                mask_out[i] = m;
+            } else {
+                const unsigned me = halo_mask(halo_bounds(G, d), G.lut + d * 64, wx, wy, wz);
+                atomicAdd(&imm_total[d], 1);
+                if (me) {
+                    atomicAdd(&imm_bnd[d], 1);
+                    atomicAdd(&imm_img[d], __popc(me));
+                    for (unsigned r = me; r; r &= r - 1)
+                        atomicAdd(&imm_list[d * kMaxNeighbors + __ffs(r) - 1], 1);
+                }
+            }
+        }
+        count_group(m, nn, lane, acc);
+        const int stays = __popc(__ballot_sync(0xffffffffu, d == s));
+        const int emigs = __popc(__ballot_sync(0xffffffffu, d >= 0 && d != s));
+        if (lane == kStepStay) acc += stays;
+        if (lane == kStepEmig) acc += emigs;
+    }
+    s_cnt[warp][lane] = acc;
+    __syncthreads();
+    if (threadIdx.x < kStepCounters) {
+        int sum = 0;
+        for (int w = 0; w < NW; ++w) sum += s_cnt[w][threadIdx.x];
+        cnt[threadIdx.x * stride + g] = sum;
+    }
+}
+
+// F3: the new owned layout, the ghost layout of the whole plan (retained +
+// immigrant parts of every send list), the CSR bases and the immigrant
+// segments.  One CTA, one thread per subdomain.
+struct StepTables {
+    int* imm_total;
+    int* imm_list;
+    int* imm_bnd;
+    int* imm_img;
+    int* imm_base;
+    int* emig_info;
+    long long* results;
+    int* list_ret;
+    int* list_len;
+    int* send_base;
+    int* gq;
+    int* gbase;
+    int* boff;
+    int* info;
+    int* cbase_ret;
+    int* cbase_imm;
+    int* imm_tile_start;
+    int4* imm_tiles;
+};
+
+__global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, int stride,
+                                                       StepTables T) {
+    __shared__ int ws[33];
+    __shared__ int s_n[kMaxRanks + 1], s_ob[kMaxRanks + 1], s_ts[kMaxRanks + 1];
+    __shared__ int s_in[kMaxRanks + 1], s_ib[kMaxRanks + 1], s_its[kMaxRanks + 1];
+    const int P = G.P;
+    const int t = threadIdx.x;
+    const int ntiles = G.tile_start[P];
+    const int* ts_old = G.tile_start;
+    auto tile_sum = [&](int k, int r) {
+        return pre[k * stride + ts_old[r + 1]] - pre[k * stride + ts_old[r]];
+    };
+    // new owned layout and migration results
+    int retained = 0, received = 0, old = 0, next = 0;
+    if (t < P) {
+        retained = tile_sum(kStepStay, t);
+        received = T.imm_total[t];
+        old = G.n[t];
+        next = retained + received;
+    }
+    int total_next, total_tiles, total_imm_tiles;
+    const int ob = block_scan_excl<1024>(next, total_next, ws);
+    const int ntl = t < P ? (next + G.tile - 1) / G.tile : 0;
+    const int ts = block_scan_excl<1024>(ntl, total_tiles, ws);
+    const int itl = t < P ? (received + G.tile - 1) / G.tile : 0;
+    const int its = block_scan_excl<1024>(itl, total_imm_tiles, ws);
+    if (t < P) {
+        s_n[t] = next;
+        s_ob[t] = ob;
+        s_ts[t] = ts;
+        s_in[t] = received;
+        s_ib[t] = ob + retained;
+        s_its[t] = its;
+        G.n_next[t] = next;
+        G.obase_next[t] = ob;
+        G.tile_start_next[t] = ts;
+        T.imm_base[t] = ob + retained;
+        T.imm_tile_start[t] = its;
+        long long* o = T.results + 6 * t;
+        o[1] = old;
+        o[2] = retained;
+        o[3] = old - retained;
+        o[4] = received;
+        o[5] = next;
+        o[0] = (o[3] != 0 || o[4] != 0) ? 1 : 0;
+    }
+    if (t == 0) {
+        s_ob[P] = total_next;
+        s_ts[P] = total_tiles;
+        s_its[P] = total_imm_tiles;
+        G.obase_next[P] = total_next;
+        G.tile_start_next[P] = total_tiles;
+        T.imm_tile_start[P] = total_imm_tiles;
+        const int E = pre[kStepEmig * stride + ntiles];
+        T.emig_info[0] = E;
+        T.emig_info[1] = (E + TILE - 1) / TILE;
+        if (total_next != G.obase[P]) atomicOr(G.status, kStatusMigrationMismatch);
+    }
+    // send-list lengths: retained part from the tile prefixes, immigrant part
+    // from the atomics of F1
+    for (int idx = t; idx < P * kMaxNeighbors; idx += blockDim.x) {
+        const int r = idx / kMaxNeighbors, n = idx % kMaxNeighbors;
+        const bool active = n < G.nn[r] && G.nbr[idx] >= 0;
+        const int ret = active ? tile_sum(n, r) : 0;
+        T.list_ret[idx] = ret;
+        T.list_len[idx] = active ? ret + T.imm_list[idx] : 0;
+    }
+    __syncthreads();
+    fill_tiles(P, G.tile, s_n, s_ob, s_ts, G.tiles_next);
+    fill_tiles(P, G.tile, s_in, s_ib, s_its, T.imm_tiles);
+    // receivers: blocks in the receiver's neighbor order
+    int mine = 0;
+    if (t < P) {
+        for (int m = 0; m < G.nn[t]; ++m) {
+            const int e = G.sender_of[t * kMaxNeighbors + m];
+            mine += e >= 0 ? T.list_len[e] : 0;
+        }
+    }
+    int total_ghosts;
+    const int gb = block_scan_excl<1024>(mine, total_ghosts, ws);
+    if (t < P) {
+        T.gq[t] = mine;
+        T.gbase[t] = gb;
+        int run = gb;
+        for (int m = 0; m < G.nn[t]; ++m) {
+            const int e = G.sender_of[t * kMaxNeighbors + m];
+            if (e < 0) continue;
+            T.send_base[e] = run;
+            run += T.list_len[e];
+        }
+    }
+    // boundary owners and images: retained part first, then the immigrants
+    int bret = 0, bimm = 0, iret = 0, iimm = 0;
+    if (t < P) {
+        bret = tile_sum(kBoundaryCounter, t);
+        bimm = T.imm_bnd[t];
+        iret = tile_sum(kImageCounter, t);
+        iimm = T.imm_img[t];
+    }
+    int total_b, total_i;
+    const int bb = block_scan_excl<1024>(bret + bimm, total_b, ws);
+    const int ib = block_scan_excl<1024>(iret + iimm, total_i, ws);   // syncs: send_base complete
+    if (t < P) {
+        int* cr = T.cbase_ret + t * kHaloCounters;
+        int* ci = T.cbase_imm + t * kHaloCounters;
+        for (int n = 0; n < kMaxNeighbors; ++n) {
+            const int e = t * kMaxNeighbors + n;
+            const bool active = n < G.nn[t] && G.nbr[e] >= 0;
+            cr[n] = active ? T.send_base[e] : 0;
+            ci[n] = active ? T.send_base[e] + T.list_ret[e] : 0;
+        }
+        cr[kBoundaryCounter] = bb;
+        ci[kBoundaryCounter] = bb + bret;
+        cr[kImageCounter] = ib;
+        ci[kImageCounter] = ib + iret;
+    }
+    if (t == 0) {
+        T.gbase[P] = total_ghosts;
+        T.info[0] = total_ghosts;
+        T.info[1] = total_b;
+        if (static_cast<long long>(total_ghosts) > G.gcap) atomicOr(G.status, kStatusGhostOverflow);
+        else T.boff[total_b] = total_i;
+    }
+}
+
+__device__ __forceinline__ void write_ghost_wrapped(const Grid& G, const Arrays& A, long long src,
+                                                    long long gi, const double* sh) {
+    const double px = wrap_if(G, 0, ro(A.d[0] + src));
+    const double py = wrap_if(G, 1, ro(A.d[1] + src));
+    const double pz = wrap_if(G, 2, ro(A.d[2] + src));
+    const double vx = ro(A.d[3] + src), vy = ro(A.d[4] + src), vz = ro(A.d[5] + src);
+    const double ms = ro(A.d[9] + src), ch = ro(A.d[10] + src);
+    const int ty = ro(A.type + src), id = ro(A.gid + src);
+    A.d[0][gi] = __dadd_rn(px, sh[0]);
+    A.d[1][gi] = __dadd_rn(py, sh[1]);
+    A.d[2][gi] = __dadd_rn(pz, sh[2]);
+    A.d[3][gi] = vx; A.d[4][gi] = vy; A.d[5][gi] = vz;
+    A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+    A.d[9][gi] = ms; A.d[10][gi] = ch;
+    A.type[gi] = ty; A.gid[gi] = id;
+    copy_fields(A.f, src, gi);
+}
+
+// F4: retained particles move to their new slots (stable) and write their
+// ghost images (staged per tile, then written list by list with coalesced
+// stores); emigrants are listed for the multi-split.  On a ghost overflow the
+// move still completes (the engine grows the ghost region and rebuilds).
+__global__ void __launch_bounds__(NT, 4) k_step_move(Grid G, Arrays A, long long src_off,
+                                                  long long dst_off, long long ghost_off,
+                                                  const int* pre, int stride, const int* cbase_ret,
+                                                  const unsigned short* __restrict__ dest_in,
+                                                  const unsigned* __restrict__ mask_in,
+                                                  int* emig_src, int* emig_dst, int* ghost_owner,
+                                                  int* ghost_entry, int* bowner, int* boff,
+                                                  int* bslot) {
+    __shared__ int s_cnt[NW][32];
+    __shared__ int s_base[32];
+    __shared__ int s_off[kMaxNeighbors + 1];
+    __shared__ unsigned short s_own[kStageCap];
+    __shared__ int s_ni[TILE];
+    const int g = blockIdx.x;
+    if (g >= G.tile_start[G.P]) return;
+    const bool ghosts = !(*G.status & kStatusGhostOverflow);
+    const int4 td = G.tiles[g];
+    const int s = td.x, begin = td.y, end = td.z, first = td.w;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbegin = begin + warp * 32 * ITEMS;
+    const int nn = G.nn[s];
+    const unsigned lt = lanemask_lt();
+
+    int dest[ITEMS];
+    unsigned msk[ITEMS];
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        dest[j] = -1;
+        msk[j] = 0;
+        if (i < end) {
+            dest[j] = dest_in[i];
+            if (dest[j] == s) msk[j] = mask_in[i];
+        }
+        count_group(msk[j], nn, lane, acc);
+        const int stays = __popc(__ballot_sync(0xffffffffu, dest[j] == s));
+        const int emigs = __popc(__ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s));
+        if (lane == kStepStay) acc += stays;
+        if (lane == kStepEmig) acc += emigs;
+    }
+    s_cnt[warp][lane] = acc;
+    if (threadIdx.x < kStepCounters) {
+        const int k = threadIdx.x;
+        int base;
+        if (k < kHaloCounters) base = cbase_ret[s * kHaloCounters + k] + pre[k * stride + g] - pre[k * stride + first];
+        else if (k == kStepStay) base = G.obase_next[s] + pre[k * stride + g] - pre[k * stride + first];
+        else base = pre[k * stride + g];
+        s_base[k] = base;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // staging offsets of the lists: lane n sums its list over the warps,
+        // then an exclusive scan over the lanes
+        int tot = 0;
+        if (lane < nn)
+            for (int w = 0; w < NW; ++w) tot += s_cnt[w][lane];
+        const int incl = warp_inclusive_sum(tot);
+        if (lane < nn) s_off[lane] = incl - tot;
+        if (lane == 31) s_off[nn] = incl;
+    }
+    __syncthreads();
+    const int Q = s_off[nn];
+    const bool staged = Q <= kStageCap;
+    int run = 0, lrun = 0;
+    if (lane < kStepCounters) {
+        run = s_base[lane];
+        if (lane < nn) lrun = s_off[lane];
+        for (int w = 0; w < warp; ++w) {
+            run += s_cnt[w][lane];
+            lrun += s_cnt[w][lane];
+        }
+    }
+    const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        const bool stay = dest[j] == s;
+        const bool emig = dest[j] >= 0 && !stay;
+        const unsigned bs_ = __ballot_sync(0xffffffffu, stay);
+        const unsigned be = __ballot_sync(0xffffffffu, emig);
+        const int ni = __shfl_sync(0xffffffffu, run, kStepStay) + __popc(bs_ & lt);
+        const int eb = __shfl_sync(0xffffffffu, run, kStepEmig) + __popc(be & lt);
+        if (stay) {
+            const long long src = src_off + i;
+            move_record(A, src, dst_off + ni, wrap_if(G, 0, ro(A.d[0] + src)),
+                        wrap_if(G, 1, ro(A.d[1] + src)), wrap_if(G, 2, ro(A.d[2] + src)));
+            s_ni[i - begin] = ni;
+        } else if (emig) {
+            emig_src[eb] = i;
+            emig_dst[eb] = dest[j];
+        }
+        const unsigned mj = ghosts ? msk[j] : 0u;
+        const unsigned any = __ballot_sync(0xffffffffu, mj != 0);
+        if (any) {
+            const int b = __shfl_sync(0xffffffffu, run, kBoundaryCounter) + __popc(any & lt);
+            const int pm = __popc(mj);
+            const int incl = warp_inclusive_sum(pm);
+            const int img = __shfl_sync(0xffffffffu, run, kImageCounter) + incl - pm;
+            if (mj) {
+                bowner[b] = ni;
+                boff[b] = img;
+            }
+            int k = 0;
+            const unsigned used = __reduce_or_sync(0xffffffffu, mj);
+            for (unsigned rest = used; rest; rest &= rest - 1) {
+                const int n = __ffs(rest) - 1;
+                const unsigned hit = __ballot_sync(0xffffffffu, (mj >> n) & 1u);
+                const int list_base = __shfl_sync(0xffffffffu, run, n);
+                const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
+                if ((mj >> n) & 1u) {
+                    const int rank = __popc(hit & lt);
+                    const int slot = list_base + rank;
+                    bslot[img + k] = slot;
+                    ++k;
+                    if (staged) {
+                        s_own[stage_base + rank] = static_cast<unsigned short>(i - begin);
+                    } else {
+                        write_ghost_wrapped(G, A, src_off + i, ghost_off + slot, shift + 3 * n);
+                        ghost_owner[slot] = ni;
+                        ghost_entry[slot] = s * kMaxNeighbors + n;
+                    }
+                }
+                if (lane == n) {
+                    run += __popc(hit);
+                    lrun += __popc(hit);
+                }
+            }
+            const int group_images = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == kBoundaryCounter) run += __popc(any);
+            if (lane == kImageCounter) run += group_images;
+        }
+        if (lane == kStepStay) run += __popc(bs_);
+        if (lane == kStepEmig) run += __popc(be);
+    }
+    if (!ghosts || !staged) return;
+    __syncthreads();
+    for (int q = threadIdx.x; q < Q; q += NT) {
+        int lo = 0, hi = nn;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_off[mid] <= q) lo = mid;
+            else hi = mid;
+        }
+        const int n = lo;
+        const int slot = s_base[n] + (q - s_off[n]);
+        const int l = s_own[q];
+        write_ghost_wrapped(G, A, src_off + begin + l, ghost_off + slot, shift + 3 * n);
+        ghost_owner[slot] = s_ni[l];
         ghost_entry[slot] = s * kMaxNeighbors + n;
     }
 }
@@ -1028,8 +1521,9 @@ int stream_grid(long long items) {
 
 int kernels_per_step() { return 0; }
 
-void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, cudaStream_t s) {
-    k_layout<<<1, 1024, 0, s>>>(G.P, G.tile, n, obase, tile_start);
+void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, int4* tiles,
+                   cudaStream_t s) {
+    k_layout<<<1, 1024, 0, s>>>(G.P, G.tile, n, obase, tile_start, tiles);
 }
 
 void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
@@ -1060,18 +1554,60 @@ void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long
 
 void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                        const Scratch& S, cudaStream_t s) {
-    k_halo_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + owned_off, A.d[1] + owned_off,
-                                                A.d[2] + owned_off, S.mask, S.cnt, S.stride);
+    k_halo_classify<<<G.max_tiles, NT, 0, s>>>(G, G.tiles, G.tile_start + G.P, A.d[0] + owned_off,
+                                                A.d[1] + owned_off, A.d[2] + owned_off, S.mask,
+                                                S.cnt, S.stride);
     if (S.marks) S.marks->mark(s, "halo_classify");
     k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
     if (S.marks) S.marks->mark(s, "halo_scan");
     k_halo_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.list_len, S.send_base, S.g, S.gbase,
-                                      S.boff, S.halo_info);
+                                      S.boff, S.halo_info, S.cbase);
     if (S.marks) S.marks->mark(s, "halo_layout");
-    k_halo_scatter<<<G.max_tiles, NT, 0, s>>>(G, A, owned_off, ghost_off, S.mask, S.pre, S.stride,
-                                              S.send_base, S.ghost_owner, S.ghost_entry, S.bowner,
+    k_halo_scatter<<<G.max_tiles, NT, 0, s>>>(G, A, owned_off, ghost_off, G.tiles,
+                                              G.tile_start + G.P, S.mask, S.pre, S.stride,
+                                              S.cbase, S.ghost_owner, S.ghost_entry, S.bowner,
                                               S.boff, S.bslot);
     if (S.marks) S.marks->mark(s, "halo_scatter");
+}
+
+void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
+                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
+    cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P * (3 + kMaxNeighbors), s);
+    k_step_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + src_off, A.d[1] + src_off,
+                                                A.d[2] + src_off, S.cnt, S.stride, S.imm_total,
+                                                S.imm_list, S.imm_bnd, S.imm_img, S.dest16, S.mask);
+    if (S.marks) S.marks->mark(s, "step_classify");
+    k_scan_counters<<<kStepCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    if (S.marks) S.marks->mark(s, "step_scan");
+    StepTables T{S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.imm_base, S.emig_info,
+                 S.mig_results, S.list_ret, S.list_len, S.send_base, S.g, S.gbase, S.boff,
+                 S.halo_info, S.cbase, S.cbase_imm, S.imm_tile_start, S.imm_tiles};
+    k_step_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, T);
+    if (S.marks) S.marks->mark(s, "step_layout");
+    k_step_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
+                                           S.cbase, S.dest16, S.mask, S.emig_src, S.emig_dst,
+                                           S.ghost_owner,
+                                           S.ghost_entry, S.bowner, S.boff, S.bslot);
+    if (S.marks) S.marks->mark(s, "step_move");
+    const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
+    const size_t smem = sizeof(int) * NW * G.P;
+    k_emig_hist<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(G.P, S.emig_info, S.emig_dst,
+                                                                  S.emig_hist);
+    k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, S.imm_total, G.status);
+    k_emig_place<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(
+        G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base);
+    if (S.marks) S.marks->mark(s, "emig_place");
+    // immigrants: masks, list ranks and ghost images over their segments
+    k_halo_classify<<<G.max_tiles, NT, 0, s>>>(Gn, S.imm_tiles, S.imm_tile_start + G.P,
+                                                A.d[0] + dst_off, A.d[1] + dst_off,
+                                                A.d[2] + dst_off, S.mask, S.cnt2, S.stride);
+    k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt2, S.pre2, S.stride,
+                                                   S.imm_tile_start + G.P);
+    k_halo_scatter<<<G.max_tiles, NT, 0, s>>>(Gn, A, dst_off, ghost_off, S.imm_tiles,
+                                              S.imm_tile_start + G.P, S.mask, S.pre2, S.stride,
+                                              S.cbase_imm, S.ghost_owner, S.ghost_entry,
+                                              S.bowner, S.boff, S.bslot);
+    if (S.marks) S.marks->mark(s, "immigrant_halo");
 }
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,

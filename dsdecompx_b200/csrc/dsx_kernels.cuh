@@ -38,6 +38,7 @@ struct Scratch {
     int* emig_info = nullptr;  // {E, nchunks}
     long long* mig_results = nullptr;  // [P][6]
     unsigned* mask = nullptr;  // [ncap] halo neighbor mask per owned particle
+    unsigned short* dest16 = nullptr;  // [ncap] destination of each owned particle (fused step)
     int* list_len = nullptr;   // [P*26] send-list lengths
     int* send_base = nullptr;  // [P*26] first ghost slot of each send list
     int* g = nullptr;          // [P] ghosts per receiver
@@ -48,17 +49,34 @@ struct Scratch {
     int* boff = nullptr;       // [ncap+1] CSR offsets into bslot
     int* bslot = nullptr;      // [gcap] ghost slots of each boundary owner, n ascending
     int* halo_info = nullptr;  // {G, B}
+    int* cbase = nullptr;      // [P*28] per subdomain: tile prefix -> global index
+    // fused step
+    int* imm_list = nullptr;   // [P*26] immigrants per (destination, send list)
+    int* imm_bnd = nullptr;    // [P] immigrant boundary owners per destination
+    int* imm_img = nullptr;    // [P] immigrant images per destination
+    int* list_ret = nullptr;   // [P*26] retained part of each send list
+    int* cbase_imm = nullptr;  // [P*28] bases of the immigrant parts
+    int* imm_tile_start = nullptr;  // [P+1] tiles over the immigrant segments
+    int4* imm_tiles = nullptr;      // their descriptors
+    int* cnt2 = nullptr;       // [28][stride] immigrant-tile counters
+    int* pre2 = nullptr;
     int max_chunks = 0;
     Marks* marks = nullptr;
 };
 
-void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, cudaStream_t s);
+void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, int4* tiles,
+                   cudaStream_t s);
 
 void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
                     const Scratch& S, cudaStream_t s);
 
 void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off,
                        long long ghost_off, const Scratch& S, cudaStream_t s);
+
+// migrate + plan build as one pipeline (the batched step); G: current layout,
+// Gn: the same grid with the next layout current.
+void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
+                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s);
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off,
                          long long ghost_off, bool positions_only, const Scratch& S,
