@@ -26,6 +26,8 @@
 
 namespace dsx {
 
+// particles per tile of the tile kernels (256 threads x 2 groups of 32)
+constexpr int kTile = 512;
 constexpr int kMaxNeighbors = 26;
 constexpr int kMaxFields = 16;
 constexpr int kMaxRanks = 1024;
@@ -38,6 +40,7 @@ constexpr int kImageCounter = 27;
 constexpr unsigned kStatusGhostOverflow = 1u;
 constexpr unsigned kStatusCutsInvalid = 2u;
 constexpr unsigned kStatusMigrationMismatch = 4u;
+constexpr unsigned kStatusCopyTimeout = 8u;   // a bulk copy did not complete
 
 struct FieldSet {
     int count = 0;
@@ -75,6 +78,7 @@ struct Grid {
     const double* shift = nullptr;       // [P*26*3]
     const signed char* dir = nullptr;    // [P*26*3]
     const unsigned* lut = nullptr;       // [P*64] halo flags -> neighbor mask
+    const int* coord = nullptr;          // [P] grid coordinates, 10 bits each (x<<20|y<<10|z)
 
     // geometry (changes with Dynamic boundaries)
     double* cuts = nullptr;

@@ -241,6 +241,7 @@ struct dsx_grid {
     double* d_shift = nullptr;
     signed char* d_dir = nullptr;
     unsigned* d_lut = nullptr;
+    int* d_coord = nullptr;
 
     // host state
     bool plan_valid = false;
@@ -287,8 +288,8 @@ struct dsx_grid {
         G.width = halo_width;
         G.ncap = ncap;
         G.gcap = gcap;
-        G.tile = 1024;
-        G.max_tiles = static_cast<int>((ncap + 1023) / 1024) + P;
+        G.tile = dsx::kTile;
+        G.max_tiles = static_cast<int>((ncap + dsx::kTile - 1) / dsx::kTile) + P;
         G.nn = d_nn;
         G.nbr = d_nbr;
         G.recv_entry = d_recv_entry;
@@ -296,6 +297,7 @@ struct dsx_grid {
         G.shift = d_shift;
         G.dir = d_dir;
         G.lut = d_lut;
+        G.coord = d_coord;
         G.cuts = cuts;
         G.n = layout[cur][0];
         G.obase = layout[cur][1];
@@ -424,8 +426,14 @@ struct dsx_grid {
         d_shift = device_alloc<double>(fixed_owned, shift.size());
         d_dir = device_alloc<signed char>(fixed_owned, dir.size());
         d_lut = device_alloc<unsigned>(fixed_owned, lut.size());
+        std::vector<int> coord(static_cast<std::size_t>(P));
+        for (int s = 0; s < P; ++s) {
+            const auto& c = coords[static_cast<std::size_t>(s)];
+            coord[static_cast<std::size_t>(s)] = (c[0] << 20) | (c[1] << 10) | c[2];
+        }
+        d_coord = device_alloc<int>(fixed_owned, coord.size());
         up(d_nn, nn); up(d_nbr, nbr); up(d_recv_entry, recv_entry); up(d_sender_of, sender_of);
-        up(d_shift, shift); up(d_dir, dir); up(d_lut, lut);
+        up(d_shift, shift); up(d_dir, dir); up(d_lut, lut); up(d_coord, coord);
 
         // uniform cuts (dsDecompX src/topology.cpp:63-75)
         std::vector<double> c;
@@ -446,7 +454,7 @@ struct dsx_grid {
             cuda_check(cudaMemset(l[1], 0, sizeof(int) * (P + 1)), "memset");
             cuda_check(cudaMemset(l[2], 0, sizeof(int) * (P + 1)), "memset");
         }
-        const int tiles_cap = static_cast<int>((ncap + 1023) / 1024) + P;
+        const int tiles_cap = static_cast<int>((ncap + dsx::kTile - 1) / dsx::kTile) + P;
         for (auto& t : layout_tiles) t = device_alloc<int4>(fixed_owned, tiles_cap);
         status = device_alloc<unsigned>(fixed_owned, 4);
         cuda_check(cudaMemset(status, 0, 4 * sizeof(unsigned)), "memset");
@@ -455,7 +463,7 @@ struct dsx_grid {
         rebalance_result = device_alloc<double>(fixed_owned, 6);
         work = device_alloc<double>(fixed_owned, P);
 
-        const int max_tiles = static_cast<int>((ncap + 1023) / 1024) + P;
+        const int max_tiles = static_cast<int>((ncap + dsx::kTile - 1) / dsx::kTile) + P;
         S.stride = max_tiles + 1;
         // 30 counters per tile: the fused step's (28 halo + stays + emigrants)
         S.cnt = device_alloc<int>(fixed_owned, static_cast<std::size_t>(30) * S.stride);
@@ -474,7 +482,7 @@ struct dsx_grid {
         S.imm_base = device_alloc<int>(fixed_owned, P);
         S.emig_src = device_alloc<int>(fixed_owned, ncap);
         S.emig_dst = device_alloc<int>(fixed_owned, ncap);
-        S.max_chunks = static_cast<int>((ncap + 1023) / 1024);
+        S.max_chunks = static_cast<int>((ncap + dsx::kTile - 1) / dsx::kTile);
         S.emig_hist = device_alloc<int>(fixed_owned, static_cast<std::size_t>(S.max_chunks) * P);
         S.emig_info = device_alloc<int>(fixed_owned, 4);
         cuda_check(cudaMemset(S.emig_info, 0, 4 * sizeof(int)), "memset");
@@ -495,8 +503,10 @@ struct dsx_grid {
     }
 
     // particle arrays [owned A | owned B | ghosts]
+    // Every array holds [owned A | owned B | ghosts] plus 4 elements of
+    // padding, so a tile read widened to 16-byte boundaries stays inside it.
     void allocate_arrays() {
-        const std::size_t len = static_cast<std::size_t>(2 * ncap + gcap);
+        const std::size_t len = static_cast<std::size_t>(2 * ncap + gcap) + 4;
         for (int a = 0; a < 11; ++a) A.d[a] = device_alloc<double>(arrays_owned, len);
         A.type = device_alloc<int>(arrays_owned, len);
         A.gid = device_alloc<int>(arrays_owned, len);
@@ -829,6 +839,8 @@ struct dsx_grid {
             enqueue_reverse(stream);
             st = read_status(stream);
         }
+        if (st & dsx::kStatusCopyTimeout)
+            fail(DSX_E_RUNTIME, "a bulk copy of particle records did not complete within 1 s");
         if (st & dsx::kStatusMigrationMismatch) fail(DSX_E_RUNTIME, "migration count mismatch");
         if (st & dsx::kStatusCutsInvalid)
             fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");

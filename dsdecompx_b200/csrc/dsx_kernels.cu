@@ -17,11 +17,11 @@ namespace dsx {
 namespace {
 
 constexpr int NT = 256;           // threads per CTA of the tile kernels
-constexpr int ITEMS = 4;          // consecutive 32-particle groups per warp
+constexpr int ITEMS = 2;          // consecutive 32-particle groups per warp
 constexpr int TILE = NT * ITEMS;  // particles per tile
 constexpr int NW = NT / 32;
 
-static_assert(TILE == 1024, "engine tile size");
+static_assert(TILE == kTile, "engine tile size");
 
 // Exclusive block scan; `total` gets the block sum.  ws: 33 ints of shared.
 template <int THREADS>
@@ -71,9 +71,10 @@ struct Cell {
 
 __device__ __forceinline__ Cell cell_of(const Grid& G, int s) {
     Cell cell;
-    cell.c[0] = s / (G.dims[1] * G.dims[2]);
-    cell.c[1] = (s / G.dims[2]) % G.dims[1];
-    cell.c[2] = s % G.dims[2];
+    const int packed = G.coord[s];
+    cell.c[0] = packed >> 20;
+    cell.c[1] = (packed >> 10) & 1023;
+    cell.c[2] = packed & 1023;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const double* cuts = G.cuts + G.cut_offset[a];
@@ -482,7 +483,8 @@ struct TileBounds {
 
 __device__ __forceinline__ TileBounds halo_bounds(const Grid& G, int s) {
     TileBounds b;
-    const int c[3] = {s / (G.dims[1] * G.dims[2]), (s / G.dims[2]) % G.dims[1], s % G.dims[2]};
+    const int packed = G.coord[s];
+    const int c[3] = {packed >> 20, (packed >> 10) & 1023, packed & 1023};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const double* cuts = G.cuts + G.cut_offset[a];
@@ -516,8 +518,7 @@ __device__ __forceinline__ void count_group(unsigned m, int nn, int lane, int& a
         const unsigned b = __ballot_sync(0xffffffffu, (m >> n) & 1u);
         if (lane == n) acc += __popc(b);
     }
-    const int images = warp_inclusive_sum(__popc(m));
-    const int total_images = __shfl_sync(0xffffffffu, images, 31);
+    const int total_images = __reduce_add_sync(0xffffffffu, __popc(m));
     if (lane == kBoundaryCounter) acc += __popc(any);
     if (lane == kImageCounter) acc += total_images;
 }
@@ -525,15 +526,13 @@ __device__ __forceinline__ void count_group(unsigned m, int nn, int lane, int& a
 // H1: neighbor mask of every owned particle and per-tile list counts.
 // `tiles`/`ntiles`: the tiles to classify (all owned particles of a layout,
 // or the immigrant segments of a fused step).
-__global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const int4* __restrict__ tiles,
-                                                      const int* ntiles,
-                                                      const double* __restrict__ x,
-                                                      const double* __restrict__ y,
-                                                      const double* __restrict__ z,
-                                                      unsigned* mask, int* cnt, int stride) {
+__device__ __forceinline__ void halo_classify_tile(int g, const Grid& G,
+                                                   const int4* __restrict__ tiles,
+                                                   const double* __restrict__ x,
+                                                   const double* __restrict__ y,
+                                                   const double* __restrict__ z, unsigned* mask,
+                                                   int* cnt, int stride) {
     __shared__ int s_cnt[NW][32];
-    const int g = blockIdx.x;
-    if (g >= *ntiles) return;
     const int4 td = tiles[g];
     const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -568,6 +567,21 @@ __global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const int4* __rest
         int sum = 0;
         for (int w = 0; w < NW; ++w) sum += s_cnt[w][threadIdx.x];
         cnt[threadIdx.x * stride + g] = sum;
+    }
+}
+
+// The blocks stride over the tiles, so a launch may be smaller than the tile
+// count (the immigrant segments of a step are few and counted on the device).
+__global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const int4* __restrict__ tiles,
+                                                      const int* ntiles,
+                                                      const double* __restrict__ x,
+                                                      const double* __restrict__ y,
+                                                      const double* __restrict__ z,
+                                                      unsigned* mask, int* cnt, int stride) {
+    const int nt = *ntiles;
+    for (int g = blockIdx.x; g < nt; g += gridDim.x) {
+        halo_classify_tile(g, G, tiles, x, y, z, mask, cnt, stride);
+        __syncthreads();
     }
 }
 
@@ -637,7 +651,7 @@ __global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, in
 // Ghost images a tile stages in shared memory before writing them out; a tile
 // with more images (only possible with a halo wider than half a cell) writes
 // them directly instead.
-constexpr int kStageCap = 6144;
+constexpr int kStageCap = 3072;
 
 __device__ __forceinline__ void write_ghost(const Arrays& A, long long src, long long gi,
                                             const double* sh) {
@@ -665,22 +679,17 @@ __device__ __forceinline__ void write_ghost(const Arrays& A, long long src, long
 // in shared memory list by list; the whole CTA then writes each list's slice
 // of the ghost region with consecutive threads on consecutive slots, so every
 // array is written with full, coalesced runs.
-__global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long owned_off,
-                                                     long long ghost_off,
-                                                     const int4* __restrict__ tiles,
-                                                     const int* ntiles,
-                                                     const unsigned* __restrict__ mask,
-                                                     const int* pre, int stride,
-                                                     const int* cbase, int* ghost_owner,
-                                                     int* ghost_entry, int* bowner, int* boff,
-                                                     int* bslot) {
+__device__ __forceinline__ void halo_scatter_tile(int g, const Grid& G, const Arrays& A,
+                                                  long long owned_off, long long ghost_off,
+                                                  const int4* __restrict__ tiles,
+                                                  const unsigned* __restrict__ mask,
+                                                  const int* pre, int stride, const int* cbase,
+                                                  int* ghost_owner, int* ghost_entry,
+                                                  int* bowner, int* boff, int* bslot) {
     __shared__ int s_cnt[NW][32];
     __shared__ int s_base[32];
     __shared__ int s_off[kMaxNeighbors + 1];
     __shared__ unsigned short s_own[kStageCap];
-    if (*G.status & kStatusGhostOverflow) return;
-    const int g = blockIdx.x;
-    if (g >= *ntiles) return;
     const int4 td = tiles[g];
     const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -789,6 +798,24 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
     }
 }
 
+__global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long owned_off,
+                                                     long long ghost_off,
+                                                     const int4* __restrict__ tiles,
+                                                     const int* ntiles,
+                                                     const unsigned* __restrict__ mask,
+                                                     const int* pre, int stride,
+                                                     const int* cbase, int* ghost_owner,
+                                                     int* ghost_entry, int* bowner, int* boff,
+                                                     int* bslot) {
+    if (*G.status & kStatusGhostOverflow) return;
+    const int nt = *ntiles;
+    for (int g = blockIdx.x; g < nt; g += gridDim.x) {
+        halo_scatter_tile(g, G, A, owned_off, ghost_off, tiles, mask, pre, stride, cbase,
+                          ghost_owner, ghost_entry, bowner, boff, bslot);
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------- fused step
 //
 // A batched step runs migrate and the plan build as one pipeline, so each
@@ -822,15 +849,13 @@ __global__ void __launch_bounds__(NT, 4) k_step_classify(Grid G, const double* _
                                                       unsigned* __restrict__ mask_out) {
     __shared__ int s_cnt[NW][32];
     const int g = blockIdx.x;
-    if (g >= G.tile_start[G.P]) return;
+    // the descriptor is read together with the tile count (the table has a
+    // row for every block of the launch)
     const int4 td = G.tiles[g];
+    if (g >= G.tile_start[G.P]) return;
     const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wbegin = begin + warp * 32 * ITEMS;
-    const TileBounds bs = halo_bounds(G, s);
-    const Cell cell = cell_of(G, s);
-    const unsigned* lut = G.lut + s * 64;
-    const int nn = G.nn[s];
     double px[ITEMS], py[ITEMS], pz[ITEMS];
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
@@ -841,6 +866,10 @@ __global__ void __launch_bounds__(NT, 4) k_step_classify(Grid G, const double* _
             pz[j] = ro(z + i);
         }
     }
+    const TileBounds bs = halo_bounds(G, s);
+    const Cell cell = cell_of(G, s);
+    const unsigned* lut = G.lut + s * 64;
+    const int nn = G.nn[s];
     int acc = 0;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
@@ -1199,6 +1228,300 @@ __global__ void __launch_bounds__(NT, 4) k_step_move(Grid G, Arrays A, long long
         const int slot = s_base[n] + (q - s_off[n]);
         const int l = s_own[q];
         write_ghost_wrapped(G, A, src_off + begin + l, ghost_off + slot, shift + 3 * n);
+        ghost_owner[slot] = s_ni[l];
+        ghost_entry[slot] = s * kMaxNeighbors + n;
+    }
+}
+
+// ------------------------------------------------------------ bulk staging
+// The staged move brings a tile's records into shared memory with the TMA
+// unit (cp.async.bulk, completion counted in bytes on an mbarrier) while the
+// block reads the destinations and combines its counts; the move and the ghost
+// images then read shared memory, so each record crosses HBM once and the
+// copies are in flight from the block's first instruction.
+
+constexpr int kStagedArrays = 13 + kMaxFields;
+constexpr int kStagedMaxBytes = 100 * 1024;         // dynamic shared memory cap
+constexpr unsigned long long kBulkWaitNs = 1000000000ull;   // 1 s: a copy counts as lost
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigned bytes,
+                                          unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+
+// Polls phase 0 of the mbarrier for at most kBulkWaitNs; false if it never
+// completed.
+__device__ __forceinline__ bool bulk_wait(unsigned bar) {
+    const unsigned long long start = global_ns();
+    for (;;) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+            " selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok) : "r"(bar) : "memory");
+        if (ok) return true;
+        if (global_ns() - start > kBulkWaitNs) return false;
+    }
+}
+
+// Array k of the record (0..10 doubles, 11 type, 12 id, 13.. fields).
+__device__ __forceinline__ int array_bytes(const Arrays& A, int k) {
+    return k < 11 ? 8 : k < 13 ? 4 : A.f.bytes[k - 13];
+}
+__device__ __forceinline__ const unsigned char* array_base(const Arrays& A, int k) {
+    if (k < 11) return reinterpret_cast<const unsigned char*>(A.d[k]);
+    if (k == 11) return reinterpret_cast<const unsigned char*>(A.type);
+    if (k == 12) return reinterpret_cast<const unsigned char*>(A.gid);
+    return A.f.base[k - 13];
+}
+
+__device__ __forceinline__ double srd(const unsigned char* rec, int seg, int l) {
+    return *reinterpret_cast<const double*>(rec + seg + l * 8);
+}
+__device__ __forceinline__ int sri(const unsigned char* rec, int seg, int l) {
+    return *reinterpret_cast<const int*>(rec + seg + l * 4);
+}
+
+__device__ __forceinline__ void fields_from_stage(const FieldSet& f, const unsigned char* rec,
+                                                  const int* seg, int l, long long dst) {
+    for (int k = 0; k < f.count; ++k) {
+        const int b = f.bytes[k];
+        const unsigned char* src = rec + seg[k] + l * b;
+        unsigned char* out = f.base[k] + dst * b;
+        if ((b & 7) == 0) {
+            for (int w = 0; w < (b >> 3); ++w)
+                reinterpret_cast<unsigned long long*>(out)[w] =
+                    reinterpret_cast<const unsigned long long*>(src)[w];
+        } else {
+            for (int w = 0; w < (b >> 2); ++w)
+                reinterpret_cast<unsigned*>(out)[w] = reinterpret_cast<const unsigned*>(src)[w];
+        }
+    }
+}
+
+// Owned record l of the staged tile to slot dst, positions wrapped.
+__device__ __forceinline__ void move_from_stage(const Grid& G, const Arrays& A,
+                                                const unsigned char* rec, const int* seg, int l,
+                                                long long dst) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) A.d[a][dst] = wrap_if(G, a, srd(rec, seg[a], l));
+#pragma unroll
+    for (int a = 3; a < 11; ++a) A.d[a][dst] = srd(rec, seg[a], l);
+    A.type[dst] = sri(rec, seg[11], l);
+    A.gid[dst] = sri(rec, seg[12], l);
+    fields_from_stage(A.f, rec, seg + 13, l, dst);
+}
+
+// Ghost image of record l of the staged tile (plan-build semantics: wrapped
+// position + shift, velocities, zero force, mass, charge, type, id, fields).
+__device__ __forceinline__ void ghost_from_stage(const Grid& G, const Arrays& A,
+                                                 const unsigned char* rec, const int* seg, int l,
+                                                 long long gi, const double* sh) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) A.d[a][gi] = __dadd_rn(wrap_if(G, a, srd(rec, seg[a], l)), sh[a]);
+#pragma unroll
+    for (int a = 3; a < 6; ++a) A.d[a][gi] = srd(rec, seg[a], l);
+    A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+    A.d[9][gi] = srd(rec, seg[9], l);
+    A.d[10][gi] = srd(rec, seg[10], l);
+    A.type[gi] = sri(rec, seg[11], l);
+    A.gid[gi] = sri(rec, seg[12], l);
+    fields_from_stage(A.f, rec, seg + 13, l, gi);
+}
+
+// F4 with the tile's records staged in shared memory (same output as
+// k_step_move).  Dynamic shared memory: sum over the arrays of TILE x element
+// bytes + 32.
+__global__ void __launch_bounds__(NT, 3) k_step_move_staged(
+    Grid G, Arrays A, long long src_off, long long dst_off, long long ghost_off, const int* pre,
+    int stride, const int* cbase_ret, const unsigned short* __restrict__ dest_in,
+    const unsigned* __restrict__ mask_in, int* emig_src, int* emig_dst, int* ghost_owner,
+    int* ghost_entry, int* bowner, int* boff, int* bslot) {
+    extern __shared__ __align__(16) unsigned char s_rec[];
+    __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ int s_seg[kStagedArrays];
+    __shared__ int s_cnt[NW][32];
+    __shared__ int s_base[32];
+    __shared__ int s_off[kMaxNeighbors + 1];
+    __shared__ unsigned short s_own[kStageCap];
+    __shared__ int s_ni[TILE];
+    const int g = blockIdx.x;
+    const int4 td = G.tiles[g];
+    if (g >= G.tile_start[G.P]) return;
+    const int s = td.x, begin = td.y, end = td.z, first = td.w;
+    const unsigned bar = smem_u32(&s_bar);
+    if (threadIdx.x == 0) {
+        const int narrays = 13 + A.f.count;
+        unsigned total = 0;
+        for (int k = 0; k < narrays; ++k) {
+            const int b = array_bytes(A, k);
+            const long long lo = ((src_off + begin) * b) & ~15LL;
+            const long long hi = ((src_off + end) * b + 15) & ~15LL;
+            total += static_cast<unsigned>(hi - lo);
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total)
+                     : "memory");
+        int off = 0;
+        for (int k = 0; k < narrays; ++k) {
+            const int b = array_bytes(A, k);
+            const long long gl = (src_off + begin) * b;
+            const long long lo = gl & ~15LL;
+            const long long hi = ((src_off + end) * b + 15) & ~15LL;
+            bulk_load(smem_u32(s_rec + off), array_base(A, k) + lo, static_cast<unsigned>(hi - lo),
+                      bar);
+            s_seg[k] = off + static_cast<int>(gl - lo);
+            off += TILE * b + 32;
+        }
+    }
+    const bool ghosts = !(*G.status & kStatusGhostOverflow);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbegin = begin + warp * 32 * ITEMS;
+    const int nn = G.nn[s];
+    const unsigned lt = lanemask_lt();
+
+    int dest[ITEMS];
+    unsigned msk[ITEMS];
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        dest[j] = -1;
+        msk[j] = 0;
+        if (i < end) {
+            dest[j] = dest_in[i];
+            if (dest[j] == s) msk[j] = mask_in[i];
+        }
+        count_group(msk[j], nn, lane, acc);
+        const int stays = __popc(__ballot_sync(0xffffffffu, dest[j] == s));
+        const int emigs = __popc(__ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s));
+        if (lane == kStepStay) acc += stays;
+        if (lane == kStepEmig) acc += emigs;
+    }
+    s_cnt[warp][lane] = acc;
+    if (threadIdx.x < kStepCounters) {
+        const int k = threadIdx.x;
+        int base;
+        if (k < kHaloCounters) base = cbase_ret[s * kHaloCounters + k] + pre[k * stride + g] - pre[k * stride + first];
+        else if (k == kStepStay) base = G.obase_next[s] + pre[k * stride + g] - pre[k * stride + first];
+        else base = pre[k * stride + g];
+        s_base[k] = base;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int tot = 0;
+        if (lane < nn)
+            for (int w = 0; w < NW; ++w) tot += s_cnt[w][lane];
+        const int incl = warp_inclusive_sum(tot);
+        if (lane < nn) s_off[lane] = incl - tot;
+        if (lane == 31) s_off[nn] = incl;
+    }
+    // the records must have landed before anything reads them
+    const bool lost = !bulk_wait(bar);
+    if (__syncthreads_or(lost)) {
+        if (lost) bulk_wait(bar);   // copies still in flight get one more bounded wait
+        if (threadIdx.x == 0) atomicOr(G.status, kStatusCopyTimeout);
+        return;
+    }
+    const int Q = s_off[nn];
+    const bool staged = Q <= kStageCap;
+    int run = 0, lrun = 0;
+    if (lane < kStepCounters) {
+        run = s_base[lane];
+        if (lane < nn) lrun = s_off[lane];
+        for (int w = 0; w < warp; ++w) {
+            run += s_cnt[w][lane];
+            lrun += s_cnt[w][lane];
+        }
+    }
+    const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        const int l = i - begin;
+        const bool stay = dest[j] == s;
+        const bool emig = dest[j] >= 0 && !stay;
+        const unsigned bs_ = __ballot_sync(0xffffffffu, stay);
+        const unsigned be = __ballot_sync(0xffffffffu, emig);
+        const int ni = __shfl_sync(0xffffffffu, run, kStepStay) + __popc(bs_ & lt);
+        const int eb = __shfl_sync(0xffffffffu, run, kStepEmig) + __popc(be & lt);
+        if (stay) {
+            move_from_stage(G, A, s_rec, s_seg, l, dst_off + ni);
+            s_ni[l] = ni;
+        } else if (emig) {
+            emig_src[eb] = i;
+            emig_dst[eb] = dest[j];
+        }
+        const unsigned mj = ghosts ? msk[j] : 0u;
+        const unsigned any = __ballot_sync(0xffffffffu, mj != 0);
+        if (any) {
+            const int b = __shfl_sync(0xffffffffu, run, kBoundaryCounter) + __popc(any & lt);
+            const int pm = __popc(mj);
+            const int incl = warp_inclusive_sum(pm);
+            const int img = __shfl_sync(0xffffffffu, run, kImageCounter) + incl - pm;
+            if (mj) {
+                bowner[b] = ni;
+                boff[b] = img;
+            }
+            int k = 0;
+            const unsigned used = __reduce_or_sync(0xffffffffu, mj);
+            for (unsigned rest = used; rest; rest &= rest - 1) {
+                const int n = __ffs(rest) - 1;
+                const unsigned hit = __ballot_sync(0xffffffffu, (mj >> n) & 1u);
+                const int list_base = __shfl_sync(0xffffffffu, run, n);
+                const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
+                if ((mj >> n) & 1u) {
+                    const int rank = __popc(hit & lt);
+                    const int slot = list_base + rank;
+                    bslot[img + k] = slot;
+                    ++k;
+                    if (staged) {
+                        s_own[stage_base + rank] = static_cast<unsigned short>(l);
+                    } else {
+                        ghost_from_stage(G, A, s_rec, s_seg, l, ghost_off + slot, shift + 3 * n);
+                        ghost_owner[slot] = ni;
+                        ghost_entry[slot] = s * kMaxNeighbors + n;
+                    }
+                }
+                if (lane == n) {
+                    run += __popc(hit);
+                    lrun += __popc(hit);
+                }
+            }
+            const int group_images = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == kBoundaryCounter) run += __popc(any);
+            if (lane == kImageCounter) run += group_images;
+        }
+        if (lane == kStepStay) run += __popc(bs_);
+        if (lane == kStepEmig) run += __popc(be);
+    }
+    if (!ghosts || !staged) return;
+    __syncthreads();
+    for (int q = threadIdx.x; q < Q; q += NT) {
+        int lo = 0, hi = nn;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_off[mid] <= q) lo = mid;
+            else hi = mid;
+        }
+        const int n = lo;
+        const int slot = s_base[n] + (q - s_off[n]);
+        const int l = s_own[q];
+        ghost_from_stage(G, A, s_rec, s_seg, l, ghost_off + slot, shift + 3 * n);
         ghost_owner[slot] = s_ni[l];
         ghost_entry[slot] = s * kMaxNeighbors + n;
     }
@@ -1570,6 +1893,13 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long
     if (S.marks) S.marks->mark(s, "halo_scatter");
 }
 
+// Shared memory the staged move needs for one tile of every array.
+int staged_bytes(const Arrays& A) {
+    int bytes = 11 * (TILE * 8 + 32) + 2 * (TILE * 4 + 32);
+    for (int k = 0; k < A.f.count; ++k) bytes += TILE * A.f.bytes[k] + 32;
+    return bytes;
+}
+
 void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
                        long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
     cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P * (3 + kMaxNeighbors), s);
@@ -1584,10 +1914,23 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
                  S.halo_info, S.cbase, S.cbase_imm, S.imm_tile_start, S.imm_tiles};
     k_step_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, T);
     if (S.marks) S.marks->mark(s, "step_layout");
-    k_step_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
-                                           S.cbase, S.dest16, S.mask, S.emig_src, S.emig_dst,
-                                           S.ghost_owner,
-                                           S.ghost_entry, S.bowner, S.boff, S.bslot);
+    const int staged = staged_bytes(A);
+    if (staged <= kStagedMaxBytes) {
+        static bool attribute_set = false;   // once per process (one device per process)
+        if (!attribute_set) {
+            cudaFuncSetAttribute(k_step_move_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kStagedMaxBytes);
+            attribute_set = true;
+        }
+        k_step_move_staged<<<G.max_tiles, NT, staged, s>>>(
+            G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
+            S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner, S.boff, S.bslot);
+    } else {
+        k_step_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
+                                               S.cbase, S.dest16, S.mask, S.emig_src, S.emig_dst,
+                                               S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
+                                               S.bslot);
+    }
     if (S.marks) S.marks->mark(s, "step_move");
     const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
     const size_t smem = sizeof(int) * NW * G.P;
@@ -1598,12 +1941,13 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
         G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base);
     if (S.marks) S.marks->mark(s, "emig_place");
     // immigrants: masks, list ranks and ghost images over their segments
-    k_halo_classify<<<G.max_tiles, NT, 0, s>>>(Gn, S.imm_tiles, S.imm_tile_start + G.P,
+    const int imm_grid = G.max_tiles < sm_count() * 4 ? G.max_tiles : sm_count() * 4;
+    k_halo_classify<<<imm_grid, NT, 0, s>>>(Gn, S.imm_tiles, S.imm_tile_start + G.P,
                                                 A.d[0] + dst_off, A.d[1] + dst_off,
                                                 A.d[2] + dst_off, S.mask, S.cnt2, S.stride);
     k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt2, S.pre2, S.stride,
                                                    S.imm_tile_start + G.P);
-    k_halo_scatter<<<G.max_tiles, NT, 0, s>>>(Gn, A, dst_off, ghost_off, S.imm_tiles,
+    k_halo_scatter<<<imm_grid, NT, 0, s>>>(Gn, A, dst_off, ghost_off, S.imm_tiles,
                                               S.imm_tile_start + G.P, S.mask, S.pre2, S.stride,
                                               S.cbase_imm, S.ghost_owner, S.ghost_entry,
                                               S.bowner, S.boff, S.bslot);
