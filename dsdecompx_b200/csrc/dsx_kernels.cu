@@ -1311,34 +1311,93 @@ __device__ __forceinline__ void fields_from_stage(const FieldSet& f, const unsig
     }
 }
 
-// Owned record l of the staged tile to slot dst, positions wrapped.
+// Owned record l of the staged tile to slot dst, positions wrapped.  `sg`:
+// where element 0 of each core array sits in `rec`, `fseg` the same for the
+// fields (every value is read before the first store, so the reads overlap).
 __device__ __forceinline__ void move_from_stage(const Grid& G, const Arrays& A,
-                                                const unsigned char* rec, const int* seg, int l,
-                                                long long dst) {
+                                                const unsigned char* rec, const int* sg,
+                                                const int* fseg, int l, long long dst) {
+    double v[11];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) A.d[a][dst] = wrap_if(G, a, srd(rec, seg[a], l));
+    for (int a = 0; a < 11; ++a) v[a] = srd(rec, sg[a], l);
+    const int ty = sri(rec, sg[11], l), id = sri(rec, sg[12], l);
 #pragma unroll
-    for (int a = 3; a < 11; ++a) A.d[a][dst] = srd(rec, seg[a], l);
-    A.type[dst] = sri(rec, seg[11], l);
-    A.gid[dst] = sri(rec, seg[12], l);
-    fields_from_stage(A.f, rec, seg + 13, l, dst);
+    for (int a = 0; a < 3; ++a) A.d[a][dst] = wrap_if(G, a, v[a]);
+#pragma unroll
+    for (int a = 3; a < 11; ++a) A.d[a][dst] = v[a];
+    A.type[dst] = ty;
+    A.gid[dst] = id;
+    fields_from_stage(A.f, rec, fseg, l, dst);
 }
 
 // Ghost image of record l of the staged tile (plan-build semantics: wrapped
 // position + shift, velocities, zero force, mass, charge, type, id, fields).
 __device__ __forceinline__ void ghost_from_stage(const Grid& G, const Arrays& A,
-                                                 const unsigned char* rec, const int* seg, int l,
-                                                 long long gi, const double* sh) {
+                                                 const unsigned char* rec, const int* sg,
+                                                 const int* fseg, int l, long long gi,
+                                                 const double* sh) {
+    double v[11];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) A.d[a][gi] = __dadd_rn(wrap_if(G, a, srd(rec, seg[a], l)), sh[a]);
+    for (int a = 0; a < 11; ++a)
+        if (a < 6 || a > 8) v[a] = srd(rec, sg[a], l);
+    const int ty = sri(rec, sg[11], l), id = sri(rec, sg[12], l);
+    const double s0 = sh[0], s1 = sh[1], s2 = sh[2];
+    A.d[0][gi] = __dadd_rn(wrap_if(G, 0, v[0]), s0);
+    A.d[1][gi] = __dadd_rn(wrap_if(G, 1, v[1]), s1);
+    A.d[2][gi] = __dadd_rn(wrap_if(G, 2, v[2]), s2);
 #pragma unroll
-    for (int a = 3; a < 6; ++a) A.d[a][gi] = srd(rec, seg[a], l);
+    for (int a = 3; a < 6; ++a) A.d[a][gi] = v[a];
     A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
-    A.d[9][gi] = srd(rec, seg[9], l);
-    A.d[10][gi] = srd(rec, seg[10], l);
-    A.type[gi] = sri(rec, seg[11], l);
-    A.gid[gi] = sri(rec, seg[12], l);
-    fields_from_stage(A.f, rec, seg + 13, l, gi);
+    A.d[9][gi] = v[9];
+    A.d[10][gi] = v[10];
+    A.type[gi] = ty;
+    A.gid[gi] = id;
+    fields_from_stage(A.f, rec, fseg, l, gi);
+}
+
+// Warp 0 issues the bulk copies of elements [first, last) of a tile into a
+// shared-memory buffer: lane k copies array k of the record and stores in
+// seg[k] where element 0 landed.  Lane 0 announces the byte total on the
+// mbarrier before any copy starts.
+__device__ __forceinline__ void stage_issue(const Arrays& A, long long src_off, int first,
+                                            int last, unsigned char* stage, unsigned bar,
+                                            int* seg, int lane) {
+    int b = 0;
+    const unsigned char* base = nullptr;
+    if (lane < 13 + A.f.count) {
+        b = array_bytes(A, lane);
+        base = array_base(A, lane);
+    }
+    const int size = b ? TILE * b + 32 : 0;
+    const int soff = warp_inclusive_sum(size) - size;
+    long long gl = 0, lo = 0, hi = 0;
+    if (b) {
+        gl = (src_off + first) * b;
+        lo = gl & ~15LL;
+        hi = ((src_off + last) * b + 15) & ~15LL;
+    }
+    const unsigned bytes = static_cast<unsigned>(hi - lo);
+    const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
+    if (lane == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total)
+                     : "memory");
+    __syncwarp();
+    if (b) {
+        bulk_load(smem_u32(stage + soff), base + lo, bytes, bar);
+        seg[lane] = soff + static_cast<int>(gl - lo);
+    }
+}
+
+// Value of step counter k at tile g (the global running index of the tile's
+// first entry): send-list slots, boundary/image offsets, new owned slots,
+// emigrant slots.
+__device__ __forceinline__ int tile_base(const Grid& G, const int* pre, int stride,
+                                         const int* cbase_ret, int g, int4 td, int k) {
+    const int s = td.x, first = td.w;
+    if (k < kHaloCounters)
+        return cbase_ret[s * kHaloCounters + k] + pre[k * stride + g] - pre[k * stride + first];
+    if (k == kStepStay) return G.obase_next[s] + pre[k * stride + g] - pre[k * stride + first];
+    return pre[k * stride + g];
 }
 
 // F4 with the tile's records staged in shared memory (same output as
@@ -1360,43 +1419,14 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     const int g = blockIdx.x;
     const int4 td = G.tiles[g];
     if (g >= G.tile_start[G.P]) return;
-    const int s = td.x, begin = td.y, end = td.z, first = td.w;
+    const int s = td.x, begin = td.y, end = td.z;
     const unsigned bar = smem_u32(&s_bar);
-    if (threadIdx.x == 0) {
-        const int narrays = 13 + A.f.count;
-        unsigned total = 0;
-        for (int k = 0; k < narrays; ++k) {
-            const int b = array_bytes(A, k);
-            const long long lo = ((src_off + begin) * b) & ~15LL;
-            const long long hi = ((src_off + end) * b + 15) & ~15LL;
-            total += static_cast<unsigned>(hi - lo);
-        }
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total)
-                     : "memory");
-        int off = 0;
-        for (int k = 0; k < narrays; ++k) {
-            const int b = array_bytes(A, k);
-            const long long gl = (src_off + begin) * b;
-            const long long lo = gl & ~15LL;
-            const long long hi = ((src_off + end) * b + 15) & ~15LL;
-            bulk_load(smem_u32(s_rec + off), array_base(A, k) + lo, static_cast<unsigned>(hi - lo),
-                      bar);
-            s_seg[k] = off + static_cast<int>(gl - lo);
-            off += TILE * b + 32;
-        }
-    }
-    const bool ghosts = !(*G.status & kStatusGhostOverflow);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wbegin = begin + warp * 32 * ITEMS;
-    const int nn = G.nn[s];
-    const unsigned lt = lanemask_lt();
-
+    // what the tile needs first goes out first: destinations, masks (only
+    // meaningful for a stay) and the counter bases
     int dest[ITEMS];
     unsigned msk[ITEMS];
-    int acc = 0;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = wbegin + j * 32 + lane;
@@ -1404,8 +1434,26 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         msk[j] = 0;
         if (i < end) {
             dest[j] = dest_in[i];
-            if (dest[j] == s) msk[j] = mask_in[i];
+            msk[j] = mask_in[i];
         }
+    }
+    int base = 0;
+    if (threadIdx.x < kStepCounters) base = tile_base(G, pre, stride, cbase_ret, g, td, threadIdx.x);
+    if (warp == 0) {
+        if (lane == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+        stage_issue(A, src_off, begin, end, s_rec, bar, s_seg, lane);
+    }
+    const bool ghosts = !(*G.status & kStatusGhostOverflow);
+    const int nn = G.nn[s];
+    const unsigned lt = lanemask_lt();
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        if (dest[j] != s) msk[j] = 0;
         count_group(msk[j], nn, lane, acc);
         const int stays = __popc(__ballot_sync(0xffffffffu, dest[j] == s));
         const int emigs = __popc(__ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s));
@@ -1413,14 +1461,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         if (lane == kStepEmig) acc += emigs;
     }
     s_cnt[warp][lane] = acc;
-    if (threadIdx.x < kStepCounters) {
-        const int k = threadIdx.x;
-        int base;
-        if (k < kHaloCounters) base = cbase_ret[s * kHaloCounters + k] + pre[k * stride + g] - pre[k * stride + first];
-        else if (k == kStepStay) base = G.obase_next[s] + pre[k * stride + g] - pre[k * stride + first];
-        else base = pre[k * stride + g];
-        s_base[k] = base;
-    }
+    if (threadIdx.x < kStepCounters) s_base[threadIdx.x] = base;
     __syncthreads();
     if (warp == 0) {
         int tot = 0;
@@ -1439,6 +1480,10 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     }
     const int Q = s_off[nn];
     const bool staged = Q <= kStageCap;
+    int sg[13];
+#pragma unroll
+    for (int a = 0; a < 13; ++a) sg[a] = s_seg[a];
+    const int* fseg = s_seg + 13;
     int run = 0, lrun = 0;
     if (lane < kStepCounters) {
         run = s_base[lane];
@@ -1460,7 +1505,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         const int ni = __shfl_sync(0xffffffffu, run, kStepStay) + __popc(bs_ & lt);
         const int eb = __shfl_sync(0xffffffffu, run, kStepEmig) + __popc(be & lt);
         if (stay) {
-            move_from_stage(G, A, s_rec, s_seg, l, dst_off + ni);
+            move_from_stage(G, A, s_rec, sg, fseg, l, dst_off + ni);
             s_ni[l] = ni;
         } else if (emig) {
             emig_src[eb] = i;
@@ -1492,7 +1537,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
                     if (staged) {
                         s_own[stage_base + rank] = static_cast<unsigned short>(l);
                     } else {
-                        ghost_from_stage(G, A, s_rec, s_seg, l, ghost_off + slot, shift + 3 * n);
+                        ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
                         ghost_owner[slot] = ni;
                         ghost_entry[slot] = s * kMaxNeighbors + n;
                     }
@@ -1521,7 +1566,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         const int n = lo;
         const int slot = s_base[n] + (q - s_off[n]);
         const int l = s_own[q];
-        ghost_from_stage(G, A, s_rec, s_seg, l, ghost_off + slot, shift + 3 * n);
+        ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
         ghost_owner[slot] = s_ni[l];
         ghost_entry[slot] = s * kMaxNeighbors + n;
     }

@@ -269,3 +269,60 @@ def test_halo_backward_is_reverse_halo(cuda):
         ot = torch.as_tensor(DeviceArray(v.base[k] + 8 * int(v.owned_offset), N), device="cuda")
         assert torch.equal(ot, grad[j])
     pair.close()
+
+
+@pytest.mark.parametrize("fields,particles", [(ALL_FIELDS[:2], 300_000), (ALL_FIELDS, 40_000)],
+                         ids=["staged-record", "wide-record"])
+def test_batched_step_many_tiles(cuda, fields, particles):
+    """The batched step against the per-call path and the oracle with far
+    more 512-particle tiles than SMs, once with a record that the move stages
+    in shared memory and once with a record too wide to stage (the move then
+    reads HBM directly)."""
+    import torch
+
+    import dsdecompx_b200 as dsx
+    rng = np.random.default_rng(29)
+    capacity = 2 * particles
+    kw = dict(nranks=27, dims=(3, 3, 3), lower=(0, 0, 0), upper=(12, 12, 12), halo_width=0.6,
+              fields=fields, particles=particles, ghost_capacity=capacity)
+    data = uniform_particles(rng, particles, (0, 0, 0), (12, 12, 12), fields)
+    a = Pair(**kw)
+    owner = a.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    per = split_by_owner(owner, data, 27)
+    a.upload(per)
+    b = dsx.VirtualGrid(**kw)
+    b.upload(per)
+    fill = ghost_force_filler(torch, capacity)
+    side = torch.cuda.Stream()
+    try:
+        for step in range(3):
+            a.displace(rng, 0.4)
+            for r in range(27):
+                o = b.counts(r)[0]
+                for name in "xyz":
+                    b.write(r, name, 0, a.gpu.read(r, name, 0, o))
+            a.gpu.migrate()
+            a.ref.migrate()
+            a.gpu.exchange_halo(rebuild=True)
+            a.ref.exchange_halo(rebuild=True)
+            fill(a.gpu.view(), torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            for r in range(27):
+                o, g = a.ref.counts(r)
+                for name in ("fx", "fy", "fz"):
+                    a.ref.write(r, name, o, a.gpu.read(r, name, o, g))
+            a.gpu.reverse_halo()
+            a.ref.reverse_halo()
+            a.compare(f"calls {step}")
+            torch.cuda.synchronize()
+            with torch.cuda.stream(side):
+                st = b.step(fill, capture=step > 0)
+            side.synchronize()
+            assert st == 0
+            for r in range(27):
+                x, y = a.gpu.snapshot(r), b.snapshot(r)
+                for k in x:
+                    assert same(x[k], y[k]), (step, r, k)
+    finally:
+        a.close()
+        b.close()
