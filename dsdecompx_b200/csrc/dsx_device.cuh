@@ -106,14 +106,16 @@ struct Grid {
 // (dsDecompX src/migration.cpp:83-87, 106-113).  No FMA contraction.
 //
 // Fast path: for 0 <= t < extent the correctly rounded quotient t / extent is
-// at most 1 - 2^-53, so floor() of it is a zero carrying t's sign; the FP64
-// division (a long instruction sequence) is skipped without changing a bit of
-// the result.  Every other input (outside the box, NaN, inf) divides.
+// at most 1 - 2^-53, so floor() of it is a zero q carrying t's sign; then
+// q * extent is that zero and t - q * extent is t itself, except that a zero t
+// (of either sign) gives +0.  So the fast path is (t == 0 ? +0 : t) + lower:
+// the FP64 division, multiply and subtract are skipped without changing a bit
+// of the result.  Every other input (outside the box, NaN, inf) divides.
 __device__ __forceinline__ double wrap_axis(double v, double lower, double extent) {
-    double t = __dsub_rn(v, lower);
-    const double q = (t >= 0.0 && t < extent) ? copysign(0.0, t) : floor(__ddiv_rn(t, extent));
-    t = __dsub_rn(t, __dmul_rn(q, extent));
-    return __dadd_rn(t, lower);
+    const double t = __dsub_rn(v, lower);
+    if (t >= 0.0 && t < extent) return __dadd_rn(t == 0.0 ? 0.0 : t, lower);
+    const double q = floor(__ddiv_rn(t, extent));
+    return __dadd_rn(__dsub_rn(t, __dmul_rn(q, extent)), lower);
 }
 
 // std::upper_bound(cuts, cuts + count, v) - cuts - 1, clamped to [0, dims-1]

@@ -1747,63 +1747,94 @@ __global__ void __launch_bounds__(NT) k_reverse_fields(Arrays A, long long owned
 // ---------------------------------------------------------------- rebalance
 
 // Dynamic cut planes (dsDecompX src/runtime.cpp:345-447) evaluated by one
-// thread in the reference's operation order, on the device so that it can
-// sit inside a captured step.
-__global__ void k_rebalance(Grid G, const double* work_in, RebalanceParams p,
-                            long long* call_counter, double* result) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    result[0] = 0.0;
-    result[1] = 0.0;
-    result[2] = 1.0;
-    if (p.automatic) {
-        const long long calls = ++(*call_counter);
-        if (p.interval == 0 || calls % p.interval != 0) return;
+// warp, every value with the reference's operations in the reference's
+// order, on the device so that it can sit inside a captured step.
+__global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
+                                                  RebalanceParams p, long long* call_counter,
+                                                  double* result) {
+    // one warp: the serial parts (the totals, each axis's slab sums and
+    // clamps) run in the reference's order on one lane each; the cut
+    // searches, independent per boundary, run one per lane
+    __shared__ double s_work[kMaxRanks];
+    __shared__ double s_next[kMaxRanks + 4];   // next cuts, axis a at G.cut_offset[a]
+    __shared__ double s_slab[kMaxRanks + 3];   // slab work, axis a at slab_off[a]
+    __shared__ double s_total;
+    __shared__ int s_go, s_bad;
+    const int lane = threadIdx.x;
+    if (blockIdx.x != 0) return;
+    if (lane == 0) {
+        result[0] = 0.0;
+        result[1] = 0.0;
+        result[2] = 1.0;
+        int go = 1;
+        if (p.automatic) {
+            const long long calls = ++(*call_counter);
+            if (p.interval == 0 || calls % p.interval != 0) go = 0;
+        }
+        s_go = go;
+        s_bad = 0;
     }
+    __syncwarp();
+    if (!s_go) return;
     const int P = G.P;
-    double total = 0.0, maximum = 0.0;
-    for (int s = 0; s < P; ++s) {
-        const double w = work_in ? work_in[s] : static_cast<double>(G.n[s]);
-        total = __dadd_rn(total, w);
-        if (maximum < w) maximum = w;
+    for (int s = lane; s < P; s += 32) s_work[s] = work_in ? work_in[s] : static_cast<double>(G.n[s]);
+    __syncwarp();
+    if (lane == 0) {
+        double total = 0.0, maximum = 0.0;
+        for (int s = 0; s < P; ++s) {
+            const double w = s_work[s];
+            total = __dadd_rn(total, w);
+            if (maximum < w) maximum = w;
+        }
+        result[0] = 1.0;
+        int go = 1;
+        if (total <= 0.0 || P <= 1) {
+            go = 0;
+        } else {
+            const double imbalance = __ddiv_rn(maximum, __ddiv_rn(total, static_cast<double>(P)));
+            result[2] = imbalance;
+            if (!p.force && imbalance < p.threshold) go = 0;
+        }
+        s_go = go;
+        s_total = total;
     }
-    result[0] = 1.0;
-    if (total <= 0.0 || P <= 1) return;
-    const double imbalance = __ddiv_rn(maximum, __ddiv_rn(total, static_cast<double>(P)));
-    result[2] = imbalance;
-    if (!p.force && imbalance < p.threshold) return;
-
-    // shared, not local: a large per-thread stack would make the driver
-    // reserve it for every resident thread of the device
-    __shared__ double next[3][kMaxRanks + 1];
-    __shared__ double slab_work[kMaxRanks];
-    bool changed = false;
+    __syncwarp();
+    if (!s_go) return;
+    const double total = s_total;
+    const int slab_off[3] = {0, G.dims[0], G.dims[0] + G.dims[1]};
+    const int ncuts = G.cut_offset[2] + G.dims[2] + 1;
+    for (int k = lane; k < ncuts; k += 32) s_next[k] = G.cuts[k];
+    if (lane < 3) {
+        const int a = lane, slabs = G.dims[a];
+        double* sw = s_slab + slab_off[a];
+        if (slabs > 1) {
+            for (int i = 0; i < slabs; ++i) sw[i] = 0.0;
+            const int shift = a == 0 ? 20 : a == 1 ? 10 : 0;
+            for (int s = 0; s < P; ++s) {
+                const int c = (G.coord[s] >> shift) & 1023;
+                sw[c] = __dadd_rn(sw[c], s_work[s]);
+            }
+        }
+    }
+    __syncwarp();
     for (int a = 0; a < 3; ++a) {
         const int slabs = G.dims[a];
-        const double* old = G.cuts + G.cut_offset[a];
-        for (int i = 0; i <= slabs; ++i) next[a][i] = old[i];
         if (slabs <= 1) continue;
-        for (int i = 0; i < slabs; ++i) slab_work[i] = 0.0;
-        for (int s = 0; s < P; ++s) {
-            const int c = a == 0 ? s / (G.dims[1] * G.dims[2])
-                        : a == 1 ? (s / G.dims[2]) % G.dims[1] : s % G.dims[2];
-            const double w = work_in ? work_in[s] : static_cast<double>(G.n[s]);
-            slab_work[c] = __dadd_rn(slab_work[c], w);
-        }
+        const double* old = G.cuts + G.cut_offset[a];
+        const double* sw = s_slab + slab_off[a];
+        double* next = s_next + G.cut_offset[a];
         const double target = __ddiv_rn(total, static_cast<double>(slabs));
-        const double extent = __dsub_rn(G.upper[a], G.lower[a]);
-        const double uniform = __ddiv_rn(extent, static_cast<double>(slabs));
-        double bound = __dmul_rn(uniform, p.minimum_fraction);
-        if (bound < p.halo_width) bound = p.halo_width;
-        const double minimum_width = bound < uniform ? bound : uniform;
-        next[a][0] = G.lower[a];
-        next[a][slabs] = G.upper[a];
-        for (int b = 1; b < slabs; ++b) {
+        if (lane == 0) {
+            next[0] = G.lower[a];
+            next[slabs] = G.upper[a];
+        }
+        for (int b = 1 + lane; b < slabs; b += 32) {
             const double desired = __dmul_rn(target, static_cast<double>(b));
             double cumulative = 0.0;
             int slab = 0;
-            while (slab < slabs - 1 && __dadd_rn(cumulative, slab_work[slab]) < desired)
-                cumulative = __dadd_rn(cumulative, slab_work[slab++]);
-            const double weight = slab_work[slab];
+            while (slab < slabs - 1 && __dadd_rn(cumulative, sw[slab]) < desired)
+                cumulative = __dadd_rn(cumulative, sw[slab++]);
+            const double weight = sw[slab];
             double fraction = 0.5;
             if (weight > 0.0) {
                 const double v = __ddiv_rn(__dsub_rn(desired, cumulative), weight);
@@ -1812,36 +1843,47 @@ __global__ void k_rebalance(Grid G, const double* work_in, RebalanceParams p,
             const double proposed =
                 __dadd_rn(old[slab], __dmul_rn(fraction, __dsub_rn(old[slab + 1], old[slab])));
             const double o = old[b];
-            next[a][b] = __dadd_rn(o, __dmul_rn(p.relaxation, __dsub_rn(proposed, o)));
+            next[b] = __dadd_rn(o, __dmul_rn(p.relaxation, __dsub_rn(proposed, o)));
         }
+    }
+    __syncwarp();
+    if (lane < 3 && G.dims[lane] > 1) {
+        const int a = lane, slabs = G.dims[a];
+        double* next = s_next + G.cut_offset[a];
+        const double extent = __dsub_rn(G.upper[a], G.lower[a]);
+        const double uniform = __ddiv_rn(extent, static_cast<double>(slabs));
+        double bound = __dmul_rn(uniform, p.minimum_fraction);
+        if (bound < p.halo_width) bound = p.halo_width;
+        const double minimum_width = bound < uniform ? bound : uniform;
         for (int i = 1; i < slabs; ++i) {
-            const double floor_value = __dadd_rn(next[a][i - 1], minimum_width);
-            if (next[a][i] < floor_value) next[a][i] = floor_value;
+            const double floor_value = __dadd_rn(next[i - 1], minimum_width);
+            if (next[i] < floor_value) next[i] = floor_value;
         }
         for (int i = slabs - 1; i > 0; --i) {
-            const double ceiling = __dsub_rn(next[a][i + 1], minimum_width);
-            if (ceiling < next[a][i]) next[a][i] = ceiling;
+            const double ceiling = __dsub_rn(next[i + 1], minimum_width);
+            if (ceiling < next[i]) next[i] = ceiling;
         }
     }
-    for (int a = 0; a < 3; ++a) {
-        const double* old = G.cuts + G.cut_offset[a];
-        for (int i = 0; i <= G.dims[a]; ++i)
-            if (fabs(__dsub_rn(next[a][i], old[i])) > 1.0e-12) changed = true;
-    }
-    if (!changed) return;
+    __syncwarp();
+    bool moved = false;
+    for (int k = lane; k < ncuts; k += 32)
+        if (fabs(__dsub_rn(s_next[k], G.cuts[k])) > 1.0e-12) moved = true;
+    if (!__any_sync(0xffffffffu, moved)) return;
     // Decomposition::set_axis_cuts validation (dsDecompX src/decomp.cpp:146-163)
-    for (int a = 0; a < 3; ++a) {
-        const int slabs = G.dims[a];
-        bool valid = next[a][0] == G.lower[a] && next[a][slabs] == G.upper[a];
-        for (int i = 0; i < slabs; ++i) valid = valid && next[a][i] < next[a][i + 1];
-        if (!valid) {
-            atomicOr(G.status, kStatusCutsInvalid);
-            return;
-        }
+    if (lane < 3) {
+        const int a = lane, slabs = G.dims[a];
+        const double* next = s_next + G.cut_offset[a];
+        bool valid = next[0] == G.lower[a] && next[slabs] == G.upper[a];
+        for (int i = 0; i < slabs; ++i) valid = valid && next[i] < next[i + 1];
+        if (!valid) atomicOr(&s_bad, 1);
     }
-    for (int a = 0; a < 3; ++a)
-        for (int i = 0; i <= G.dims[a]; ++i) G.cuts[G.cut_offset[a] + i] = next[a][i];
-    result[1] = 1.0;
+    __syncwarp();
+    if (s_bad) {
+        if (lane == 0) atomicOr(G.status, kStatusCutsInvalid);
+        return;
+    }
+    for (int k = lane; k < ncuts; k += 32) G.cuts[k] = s_next[k];
+    if (lane == 0) result[1] = 1.0;
 }
 
 // 1-rank migrate of the drop-in: every particle stays and keeps its slot; its
