@@ -263,7 +263,7 @@ def run_ours(args, rank, world, device):
                 else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": int(alg[dominant]),
                 "avg_launch_ms": round(avg[dominant], 4),
-                "traffic": traffic_from_profiles(dominant, N, mean_tot)}
+                "traffic": traffic_from_profiles(w.name, dominant, N)}
 
     # e2e: the same step through the C ABI with the state in pinned host memory
     e2e = None
@@ -309,6 +309,25 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize(device)
         plain = round(p0.elapsed_time(p1) / args.plain_steps, 3)
 
+    # plain launches: the same per-call operations, every tile kernel launched
+    # once per subdomain (the launch pattern of one process per subdomain)
+    per_subdomain = None
+    if args.plain_steps > 0:
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        grid.set_plain(True)
+        with torch.cuda.stream(stream):
+            q0.record(stream)
+            for _ in range(args.plain_steps):
+                grid.migrate(stream=stream)
+                grid.exchange_halo(rebuild=True, stream=stream)
+                user_work(grid.view(), stream.cuda_stream)
+                grid.reverse_halo(stream=stream)
+                grid.all_counts(stream=stream)
+            q1.record(stream)
+        torch.cuda.synchronize(device)
+        grid.set_plain(False)
+        per_subdomain = round(q0.elapsed_time(q1) / args.plain_steps, 3)
+
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "M particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -328,6 +347,8 @@ def run_ours(args, rank, world, device):
         "kernel_ms": {k: round(v, 4) for k, v in avg.items()},
         "totals_per_step": {k: int(v) for k, v in mean_tot.items()},
         "per_call_ms_per_step": plain,
+        "plain_ms_per_step": per_subdomain,
+        "batched_vs_plain": round(per_subdomain / ms_per_step, 3) if per_subdomain else None,
         "clocks": clock,
         "e2e": e2e,
         "gpu_launches": launches,
@@ -335,14 +356,15 @@ def run_ours(args, rank, world, device):
     return line
 
 
-def traffic_from_profiles(kernel, N, totals):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/traffic.json), scaled to this launch's particle count."""
+def traffic_from_profiles(workload, kernel, N):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary of
+    this workload (profiles/traffic.json), scaled to this launch's particle
+    count; None when no capture of this workload and kernel is committed."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
             data = json.load(f)
-        entry = data[kernel]
+        entry = data[workload][kernel]
         return int(entry["dram_bytes_per_particle"] * N)
     except Exception:
         return None

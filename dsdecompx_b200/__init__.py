@@ -117,6 +117,7 @@ def lib() -> C.CDLL:
             "dsx_grid_step": [vp, STEP_CALLBACK, vp, C.c_int, vp, C.POINTER(C.c_uint)],
             "dsx_grid_step_kernel_count": [vp],
             "dsx_grid_profile": [vp, C.c_int],
+            "dsx_grid_set_plain": [vp, C.c_int],
             "dsx_grid_kernel_times": [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)],
         }
         for name, args in sig.items():
@@ -416,6 +417,11 @@ class VirtualGrid:
         _check(self.L.dsx_grid_step(self.h, cb, None, 1 if capture else 0, _stream(stream),
                                     C.byref(st)))
         return st.value
+
+    def set_plain(self, plain: bool = True):
+        """Per-call operations launch their tile kernels once per subdomain
+        (comparison runs; results are unchanged)."""
+        _check(self.L.dsx_grid_set_plain(self.h, 1 if plain else 0))
 
     def profile(self, enable: bool = True):
         _check(self.L.dsx_grid_profile(self.h, 1 if enable else 0))

@@ -68,6 +68,10 @@ struct Grid {
     long long gcap = 0;             // ghost capacity
     int tile = 1024;
     int max_tiles = 1;              // ceil(ncap / tile) + P
+    // window of tiles one launch covers: [tile_first, tile_end), tile_end < 0
+    // meaning "to the layout's last tile" (plain mode launches per subdomain)
+    int tile_first = 0;
+    int tile_end = -1;
     int cut_offset[3] = {0, 0, 0};  // start of each axis in `cuts`
 
     // topology (static)

@@ -242,6 +242,10 @@ struct dsx_grid {
     signed char* d_dir = nullptr;
     unsigned* d_lut = nullptr;
     int* d_coord = nullptr;
+    // plain launches (per-call operations, one launch per subdomain)
+    bool plain = false;
+    std::vector<int> plain_tiles, plain_bounds;
+    dsx::PlainLaunch plain_launch;
 
     // host state
     bool plan_valid = false;
@@ -554,9 +558,33 @@ struct dsx_grid {
 
     // -------------------------------------------------------- operations
 
-    void enqueue_migrate(cudaStream_t stream, bool automatic_rebalance) {
+    void enqueue_migrate(cudaStream_t stream, bool automatic_rebalance,
+                         const dsx::PlainLaunch* pl = nullptr) {
         enqueue_rebalance(stream, automatic_rebalance);
-        dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream);
+        dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream, pl);
+    }
+
+    // Plain mode (per-call operations only): the current layout's tile starts
+    // on the host, read after the work queued so far.
+    const dsx::PlainLaunch* plain_layout(cudaStream_t stream) {
+        if (!plain) return nullptr;
+        plain_tiles = read_ints(layout[cur][2], P + 1, stream);
+        plain_launch.tile_start = plain_tiles.data();
+        plain_launch.boundary_start = nullptr;
+        return &plain_launch;
+    }
+
+    // Plain mode after a plan build: where each subdomain's boundary owners
+    // start (the reverse sum is then launched per subdomain).
+    void plain_boundaries(cudaStream_t stream) {
+        if (!plain) return;
+        const std::vector<int> cb = read_ints(S.cbase, P * dsx::kHaloCounters, stream);
+        const std::vector<int> info = read_ints(S.halo_info, 2, stream);
+        plain_bounds.assign(static_cast<std::size_t>(P) + 1, 0);
+        for (int r = 0; r < P; ++r)
+            plain_bounds[static_cast<std::size_t>(r)] =
+                cb[static_cast<std::size_t>(r) * dsx::kHaloCounters + dsx::kBoundaryCounter];
+        plain_bounds[static_cast<std::size_t>(P)] = info[1];
     }
 
     void enqueue_rebalance(cudaStream_t stream, bool automatic_rebalance) {
@@ -578,6 +606,7 @@ struct dsx_grid {
     }
 
     void commit_migrate() {
+        plain_bounds.clear();
         parity ^= 1;
         cur ^= 1;
         plan_valid = false;
@@ -585,14 +614,14 @@ struct dsx_grid {
         std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
     }
 
-    void enqueue_halo_build(cudaStream_t stream) {
-        dsx::launch_halo_build(params(), A, owned_off(), ghost_off(), S, stream);
+    void enqueue_halo_build(cudaStream_t stream, const dsx::PlainLaunch* pl = nullptr) {
+        dsx::launch_halo_build(params(), A, owned_off(), ghost_off(), S, stream, pl);
     }
 
-    void enqueue_reverse(cudaStream_t stream) {
+    void enqueue_reverse(cudaStream_t stream, const dsx::PlainLaunch* pl = nullptr) {
         const long long o = owned_off(), g = ghost_off();
         dsx::launch_reverse_sum3(params(), A.d[6] + o, A.d[7] + o, A.d[8] + o, A.d[6] + g, A.d[7] + g,
-                                 A.d[8] + g, S, stream);
+                                 A.d[8] + g, S, stream, pl);
     }
 
     unsigned read_status(cudaStream_t stream) {
@@ -617,7 +646,14 @@ struct dsx_grid {
 
     void migrate(cudaStream_t stream, long long* results, bool automatic_rebalance = true) {
         clear_status(stream);
-        enqueue_migrate(stream, automatic_rebalance);
+        if (plain) {
+            // the rebalance may move the cut planes but not the layout
+            enqueue_rebalance(stream, automatic_rebalance);
+            dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream,
+                                plain_layout(stream));
+        } else {
+            enqueue_migrate(stream, automatic_rebalance);
+        }
         commit_migrate();
         if (results) {
             cuda_check(cudaMemcpyAsync(results, S.mig_results, sizeof(long long) * 6 * P,
@@ -633,13 +669,14 @@ struct dsx_grid {
     void build_checked(cudaStream_t stream) {
         for (;;) {
             clear_status(stream);
-            enqueue_halo_build(stream);
+            enqueue_halo_build(stream, plain_layout(stream));
             const unsigned st = read_status(stream);
             if (!(st & dsx::kStatusGhostOverflow)) break;
             grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
         }
         plan_valid = true;
         ghosts_valid = true;
+        plain_boundaries(stream);
     }
 
     void exchange_halo(bool rebuild, bool positions_only, cudaStream_t stream, long long* results) {
@@ -657,6 +694,7 @@ struct dsx_grid {
         } else {
             clear_status(stream);
             enqueue_halo_build(stream);
+            plain_bounds.clear();
             plan_valid = true;
             ghosts_valid = true;
         }
@@ -679,7 +717,12 @@ struct dsx_grid {
 
     void reverse_halo(cudaStream_t stream) {
         if (P == 1 || !ghosts_valid) return;
-        enqueue_reverse(stream);
+        if (plain && static_cast<int>(plain_bounds.size()) == P + 1) {
+            plain_launch.boundary_start = plain_bounds.data();
+            enqueue_reverse(stream, &plain_launch);
+        } else {
+            enqueue_reverse(stream);
+        }
     }
 
     dsx::FieldOps field_ops(int nf, const int* ids, const int* ops, const char* what) {
@@ -1202,6 +1245,14 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
         if (grid->P == 1) fail(DSX_E_INVALID, "the batched step needs at least two subdomains");
         grid->step(callback, user, capture != 0, static_cast<cudaStream_t>(stream), status);
         cuda_check(cudaGetLastError(), "launch step");
+    });
+}
+
+int dsx_grid_set_plain(dsx_grid* grid, int plain) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        grid->plain = plain != 0;
+        grid->plain_bounds.clear();
     });
 }
 

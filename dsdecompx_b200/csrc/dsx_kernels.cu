@@ -132,6 +132,12 @@ __device__ __forceinline__ void move_record(const Arrays& A, long long src, long
     copy_fields(A.f, src, dst);
 }
 
+// End of the tile window of a launch: the window's own end in plain mode
+// (one launch per subdomain), else the tile count on the device.
+__device__ __forceinline__ int tile_limit(const Grid& G, const int* ntiles) {
+    return G.tile_end >= 0 ? G.tile_end : *ntiles;
+}
+
 // ------------------------------------------------------------------ layout
 
 // Writes the per-tile descriptors {s, begin, end, first tile of s} of a
@@ -220,9 +226,9 @@ __global__ void __launch_bounds__(NT, 4) k_mig_classify(Grid G, const double* __
                                                      const double* __restrict__ z, int* cnt,
                                                      int stride, int* imm_total) {
     __shared__ int ws[33];
-    const int g = blockIdx.x;
+    const int g = G.tile_first + blockIdx.x;
     const int P = G.P;
-    if (g >= G.tile_start[P]) return;
+    if (g >= tile_limit(G, G.tile_start + P)) return;
     const int4 td = G.tiles[g];
     const int s = td.x, begin = td.y, end = td.z;
     int stay = 0, emig = 0;
@@ -317,9 +323,9 @@ __global__ void __launch_bounds__(NT, 4) k_mig_move(Grid G, Arrays A, long long 
                                                  long long dst_off, const int* pre, int stride,
                                                  int* emig_src, int* emig_dst) {
     __shared__ int s_stay[NW], s_emig[NW];
-    const int g = blockIdx.x;
+    const int g = G.tile_first + blockIdx.x;
     const int P = G.P;
-    if (g >= G.tile_start[P]) return;
+    if (g >= tile_limit(G, G.tile_start + P)) return;
     const int4 td = G.tiles[g];
     const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -578,8 +584,8 @@ __global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const int4* __rest
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z,
                                                       unsigned* mask, int* cnt, int stride) {
-    const int nt = *ntiles;
-    for (int g = blockIdx.x; g < nt; g += gridDim.x) {
+    const int nt = tile_limit(G, ntiles);
+    for (int g = G.tile_first + blockIdx.x; g < nt; g += gridDim.x) {
         halo_classify_tile(g, G, tiles, x, y, z, mask, cnt, stride);
         __syncthreads();
     }
@@ -808,8 +814,8 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
                                                      int* ghost_entry, int* bowner, int* boff,
                                                      int* bslot) {
     if (*G.status & kStatusGhostOverflow) return;
-    const int nt = *ntiles;
-    for (int g = blockIdx.x; g < nt; g += gridDim.x) {
+    const int nt = tile_limit(G, ntiles);
+    for (int g = G.tile_first + blockIdx.x; g < nt; g += gridDim.x) {
         halo_scatter_tile(g, G, A, owned_off, ghost_off, tiles, mask, pre, stride, cbase,
                           ghost_owner, ghost_entry, bowner, boff, bslot);
         __syncthreads();
@@ -1637,10 +1643,11 @@ __global__ void __launch_bounds__(NT) k_reverse_sum3(const int* info, const int*
                                                      const double* __restrict__ gx,
                                                      const double* __restrict__ gy,
                                                      const double* __restrict__ gz,
-                                                     const unsigned* status) {
+                                                     const unsigned* status, int b_first,
+                                                     int b_end) {
     if (*status & kStatusGhostOverflow) return;
-    const int B = info[1];
-    for (int b = blockIdx.x * NT + threadIdx.x; b < B; b += gridDim.x * NT) {
+    const int B = b_end >= 0 ? b_end : info[1];
+    for (int b = b_first + blockIdx.x * NT + threadIdx.x; b < B; b += gridDim.x * NT) {
         const int i = bowner[b];
         const int k0 = boff[b], k1 = boff[b + 1];
         double fx = ox[i], fy = oy[i], fz = oz[i];
@@ -1936,19 +1943,41 @@ void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, int
     k_layout<<<1, 1024, 0, s>>>(G.P, G.tile, n, obase, tile_start, tiles);
 }
 
+// Runs launch(Gs, grid) once over all tiles, or, in plain mode, once per
+// subdomain with the tile window of that subdomain.
+template <class F>
+void per_subdomain(const Grid& G, const PlainLaunch* plain, F&& launch) {
+    if (!plain) {
+        launch(G, G.max_tiles);
+        return;
+    }
+    for (int r = 0; r < G.P; ++r) {
+        const int t0 = plain->tile_start[r], t1 = plain->tile_start[r + 1];
+        if (t1 <= t0) continue;
+        Grid Gs = G;
+        Gs.tile_first = t0;
+        Gs.tile_end = t1;
+        launch(Gs, t1 - t0);
+    }
+}
+
 void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
-                    const Scratch& S, cudaStream_t s) {
+                    const Scratch& S, cudaStream_t s, const PlainLaunch* plain) {
     cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P, s);
-    k_mig_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + src_off, A.d[1] + src_off,
-                                               A.d[2] + src_off, S.cnt, S.stride, S.imm_total);
+    per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
+        k_mig_classify<<<grid, NT, 0, s>>>(Gs, A.d[0] + src_off, A.d[1] + src_off,
+                                           A.d[2] + src_off, S.cnt, S.stride, S.imm_total);
+    });
     if (S.marks) S.marks->mark(s, "mig_classify");
     k_scan_counters<<<2, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
     if (S.marks) S.marks->mark(s, "mig_scan");
     k_mig_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.imm_total, S.imm_base, S.emig_info,
                                      S.mig_results);
     if (S.marks) S.marks->mark(s, "mig_layout");
-    k_mig_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, S.pre, S.stride, S.emig_src,
-                                          S.emig_dst);
+    per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
+        k_mig_move<<<grid, NT, 0, s>>>(Gs, A, src_off, dst_off, S.pre, S.stride, S.emig_src,
+                                       S.emig_dst);
+    });
     if (S.marks) S.marks->mark(s, "mig_move");
     const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
     const size_t smem = sizeof(int) * NW * G.P;
@@ -1963,20 +1992,24 @@ void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long
 }
 
 void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
-                       const Scratch& S, cudaStream_t s) {
-    k_halo_classify<<<G.max_tiles, NT, 0, s>>>(G, G.tiles, G.tile_start + G.P, A.d[0] + owned_off,
-                                                A.d[1] + owned_off, A.d[2] + owned_off, S.mask,
-                                                S.cnt, S.stride);
+                       const Scratch& S, cudaStream_t s, const PlainLaunch* plain) {
+    per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
+        k_halo_classify<<<grid, NT, 0, s>>>(Gs, G.tiles, G.tile_start + G.P, A.d[0] + owned_off,
+                                            A.d[1] + owned_off, A.d[2] + owned_off, S.mask,
+                                            S.cnt, S.stride);
+    });
     if (S.marks) S.marks->mark(s, "halo_classify");
     k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
     if (S.marks) S.marks->mark(s, "halo_scan");
     k_halo_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.list_len, S.send_base, S.g, S.gbase,
                                       S.boff, S.halo_info, S.cbase);
     if (S.marks) S.marks->mark(s, "halo_layout");
-    k_halo_scatter<<<G.max_tiles, NT, 0, s>>>(G, A, owned_off, ghost_off, G.tiles,
-                                              G.tile_start + G.P, S.mask, S.pre, S.stride,
-                                              S.cbase, S.ghost_owner, S.ghost_entry, S.bowner,
-                                              S.boff, S.bslot);
+    per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
+        k_halo_scatter<<<grid, NT, 0, s>>>(Gs, A, owned_off, ghost_off, G.tiles,
+                                           G.tile_start + G.P, S.mask, S.pre, S.stride, S.cbase,
+                                           S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
+                                           S.bslot);
+    });
     if (S.marks) S.marks->mark(s, "halo_scatter");
 }
 
@@ -2056,9 +2089,20 @@ void launch_forward_fields(const Grid& G, const Arrays& A, long long owned_off,
 }
 
 void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, const double* gx,
-                         const double* gy, const double* gz, const Scratch& S, cudaStream_t s) {
-    k_reverse_sum3<<<stream_grid(G.ncap), NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot, ox,
-                                                      oy, oz, gx, gy, gz, G.status);
+                         const double* gy, const double* gz, const Scratch& S, cudaStream_t s,
+                         const PlainLaunch* plain) {
+    if (plain && plain->boundary_start) {
+        for (int r = 0; r < G.P; ++r) {
+            const int b0 = plain->boundary_start[r], b1 = plain->boundary_start[r + 1];
+            if (b1 <= b0) continue;
+            k_reverse_sum3<<<stream_grid(b1 - b0), NT, 0, s>>>(S.halo_info, S.bowner, S.boff,
+                                                               S.bslot, ox, oy, oz, gx, gy, gz,
+                                                               G.status, b0, b1);
+        }
+    } else {
+        k_reverse_sum3<<<stream_grid(G.ncap), NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot,
+                                                          ox, oy, oz, gx, gy, gz, G.status, 0, -1);
+    }
     if (S.marks) S.marks->mark(s, "reverse_sum");
 }
 

@@ -67,11 +67,21 @@ struct Scratch {
 void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, int4* tiles,
                    cudaStream_t s);
 
+// Plain launches: host copies of the layout's tile starts and of the
+// boundary-owner starts per subdomain; with them every tile kernel of a
+// per-call operation is launched once per subdomain over its own tiles (the
+// way one process per subdomain would launch), instead of once for all.
+struct PlainLaunch {
+    const int* tile_start = nullptr;      // [P+1]
+    const int* boundary_start = nullptr;  // [P+1]
+};
+
 void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
-                    const Scratch& S, cudaStream_t s);
+                    const Scratch& S, cudaStream_t s, const PlainLaunch* plain = nullptr);
 
 void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off,
-                       long long ghost_off, const Scratch& S, cudaStream_t s);
+                       long long ghost_off, const Scratch& S, cudaStream_t s,
+                       const PlainLaunch* plain = nullptr);
 
 // migrate + plan build as one pipeline (the batched step); G: current layout,
 // Gn: the same grid with the next layout current.
@@ -98,7 +108,7 @@ void launch_forward_fields(const Grid& G, const Arrays& A, long long owned_off,
 // used for reverse_halo (forces) and for the halo adjoint.
 void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz,
                          const double* gx, const double* gy, const double* gz,
-                         const Scratch& S, cudaStream_t s);
+                         const Scratch& S, cudaStream_t s, const PlainLaunch* plain = nullptr);
 
 void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
                            long long ghost_off, const FieldOps& F, const Scratch& S,

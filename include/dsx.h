@@ -234,6 +234,15 @@ typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view*
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
                   void* stream, unsigned* status);
 
+/* Plain launches, for comparison runs: plain != 0 makes the per-call
+ * operations (dsx_grid_migrate, a rebuilding dsx_grid_exchange_halo,
+ * dsx_grid_reverse_halo) launch each of their tile kernels once per subdomain
+ * over that subdomain's tiles, reading the layout to the host first -- the
+ * launch pattern of one process per subdomain, as the reference runs P ranks.
+ * Results are identical to the default (one launch per phase for all
+ * subdomains); dsx_grid_step is not affected. */
+int dsx_grid_set_plain(dsx_grid* grid, int plain);
+
 /* Per-kernel timing of the batched step, for benchmarks: enable != 0 makes
  * the next steps record a CUDA event after every kernel (inside a captured
  * graph they are event-record nodes; captured graphs are rebuilt when the

@@ -15,11 +15,13 @@ pytestmark = pytest.mark.gpu
 
 def run_scenario(cuda, *, P, dims, L, halo, N, steps, seed, fields=ALL_FIELDS, sigma=0.3,
                  periodic=(True, True, True), edges=True, policy="manual", dynamic=None,
-                 lower=(0.0, 0.0, 0.0), ghost_capacity=0, data_fn=None):
+                 lower=(0.0, 0.0, 0.0), ghost_capacity=0, data_fn=None, plain=False):
     rng = np.random.default_rng(seed)
     upper = tuple(lo + l for lo, l in zip(lower, L))
     pair = Pair(P, dims, policy, lower, upper, periodic, halo, edges, dynamic, fields,
                 particles=N, ghost_capacity=ghost_capacity)
+    if plain:
+        pair.gpu.set_plain(True)
     try:
         data = data_fn(rng, N, lower, upper) if data_fn else uniform_particles(rng, N, lower, upper, fields)
         owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
@@ -244,6 +246,14 @@ def test_batched_step_matches_calls(cuda):
                 assert same(x[k], y[k]), (step, r, k)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("dims", [(2, 2, 2), (3, 2, 2)], ids=["2x2x2", "3x2x2"])
+def test_plain_launches_follow_the_reference(cuda, dims):
+    """One launch per subdomain (the comparison mode) gives the same arrays."""
+    P = int(np.prod(dims))
+    run_scenario(cuda, P=P, dims=dims, L=(12.0, 10.0, 9.0), halo=1.0, N=20000, steps=3,
+                 seed=31, fields=ALL_FIELDS[:3], plain=True).close()
 
 
 def test_halo_backward_is_reverse_halo(cuda):
