@@ -846,14 +846,18 @@ __device__ __forceinline__ double wrap_if(const Grid& G, int a, double v) {
 
 // F1: destination and new-owner halo mask of every owned particle; per-tile
 // counters; per-destination totals of the emigrants (atomics: only sums).
-__global__ void __launch_bounds__(NT, 4) k_step_classify(Grid G, const double* __restrict__ x,
+template <int CT, int MINB>
+__global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double* __restrict__ x,
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z, int* cnt,
                                                       int stride, int* imm_total, int* imm_list,
                                                       int* imm_bnd, int* imm_img,
                                                       unsigned short* __restrict__ dest_out,
                                                       unsigned* __restrict__ mask_out) {
-    __shared__ int s_cnt[NW][32];
+    constexpr int CI = TILE / CT;   // 32-particle groups per warp
+    constexpr int CW = CT / 32;
+    static_assert(CI * CT == TILE && CW >= 1, "tile split");
+    __shared__ int s_cnt[CW][32];
     const int g = blockIdx.x;
     // the descriptor is read together with the tile count (the table has a
     // row for every block of the launch)
@@ -861,10 +865,10 @@ __global__ void __launch_bounds__(NT, 4) k_step_classify(Grid G, const double* _
     if (g >= G.tile_start[G.P]) return;
     const int s = td.x, begin = td.y, end = td.z;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wbegin = begin + warp * 32 * ITEMS;
-    double px[ITEMS], py[ITEMS], pz[ITEMS];
+    const int wbegin = begin + warp * 32 * CI;
+    double px[CI], py[CI], pz[CI];
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
+    for (int j = 0; j < CI; ++j) {
         const int i = wbegin + j * 32 + lane;
         if (i < end) {
             px[j] = ro(x + i);
@@ -878,7 +882,7 @@ __global__ void __launch_bounds__(NT, 4) k_step_classify(Grid G, const double* _
     const int nn = G.nn[s];
     int acc = 0;
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
+    for (int j = 0; j < CI; ++j) {
         const int i = wbegin + j * 32 + lane;
         int d = -1;
         unsigned m = 0;
@@ -910,7 +914,7 @@ __global__ void __launch_bounds__(NT, 4) k_step_classify(Grid G, const double* _
     __syncthreads();
     if (threadIdx.x < kStepCounters) {
         int sum = 0;
-        for (int w = 0; w < NW; ++w) sum += s_cnt[w][threadIdx.x];
+        for (int w = 0; w < CW; ++w) sum += s_cnt[w][threadIdx.x];
         cnt[threadIdx.x * stride + g] = sum;
     }
 }
@@ -2013,6 +2017,11 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long
     if (S.marks) S.marks->mark(s, "halo_scatter");
 }
 
+// Threads per tile of the step's classify pass (each thread takes
+// TILE / kClassifyThreads particles) and its resident-CTA target.
+constexpr int kClassifyThreads = 128;
+constexpr int kClassifyBlocks = 8;
+
 // Shared memory the staged move needs for one tile of every array.
 int staged_bytes(const Arrays& A) {
     int bytes = 11 * (TILE * 8 + 32) + 2 * (TILE * 4 + 32);
@@ -2023,9 +2032,9 @@ int staged_bytes(const Arrays& A) {
 void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
                        long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
     cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P * (3 + kMaxNeighbors), s);
-    k_step_classify<<<G.max_tiles, NT, 0, s>>>(G, A.d[0] + src_off, A.d[1] + src_off,
-                                                A.d[2] + src_off, S.cnt, S.stride, S.imm_total,
-                                                S.imm_list, S.imm_bnd, S.imm_img, S.dest16, S.mask);
+    k_step_classify<kClassifyThreads, kClassifyBlocks><<<G.max_tiles, kClassifyThreads, 0, s>>>(
+        G, A.d[0] + src_off, A.d[1] + src_off, A.d[2] + src_off, S.cnt, S.stride, S.imm_total,
+        S.imm_list, S.imm_bnd, S.imm_img, S.dest16, S.mask);
     if (S.marks) S.marks->mark(s, "step_classify");
     k_scan_counters<<<kStepCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
     if (S.marks) S.marks->mark(s, "step_scan");
