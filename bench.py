@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes (no dsx_grid_autotune before timing)")
     ap.add_argument("--particles", type=int, default=0,
                     help="override the workload's particle count (small profiling cases)")
     return ap.parse_args()
@@ -194,10 +196,18 @@ def run_ours(args, rank, world, device):
         if world > 1:
             torch.distributed.barrier()
 
+    tune = None
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             status = grid.step(user_work, capture=True)
             assert status == 0, status
+        if not args.no_autotune:
+            # launch shapes picked on this workload's particles, then the
+            # step is re-captured with them
+            tune = grid.autotune(stream=stream)
+            for _ in range(2):
+                status = grid.step(user_work, capture=True)
+                assert status == 0, status
     stream.synchronize()
 
     # timed: the step calls alone (each returns its device status), no timing
@@ -337,7 +347,8 @@ def run_ours(args, rank, world, device):
                    "grid": list(dims), "particles": N, "record_bytes": S,
                    "step": "graph-captured batched step (dsx_grid_step)",
                    "l2": "inputs larger than L2 (%.2f GB of owned records)" % (N * S / 1e9),
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "autotune": tune},
         "roofline": roof,
         "step_roofline": {"algorithmic_bytes": int(step_bytes),
                           "kernels_ms": round(ours_ms, 4),

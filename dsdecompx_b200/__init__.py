@@ -60,6 +60,13 @@ class _FieldDesc(C.Structure):
     _fields_ = [("name", C.c_char_p), ("type", C.c_int), ("components", C.c_int)]
 
 
+class TuneReport(C.Structure):
+    _fields_ = [("classify_threads", C.c_int), ("move_staged", C.c_int),
+                ("reverse_ctas_per_sm", C.c_int), ("ghost_capacity", C.c_longlong),
+                ("classify_ms", C.c_float * 3), ("move_ms", C.c_float * 2),
+                ("reverse_ms", C.c_float * 4)]
+
+
 class GridView(C.Structure):
     _fields_ = [("base", C.c_void_p * 32), ("owned_offset", C.c_longlong),
                 ("ghost_offset", C.c_longlong), ("n", C.c_void_p), ("obase", C.c_void_p),
@@ -118,6 +125,7 @@ def lib() -> C.CDLL:
             "dsx_grid_step_kernel_count": [vp],
             "dsx_grid_profile": [vp, C.c_int],
             "dsx_grid_set_plain": [vp, C.c_int],
+            "dsx_grid_autotune": [vp, vp, vp],
             "dsx_grid_kernel_times": [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)],
         }
         for name, args in sig.items():
@@ -417,6 +425,20 @@ class VirtualGrid:
         _check(self.L.dsx_grid_step(self.h, cb, None, 1 if capture else 0, _stream(stream),
                                     C.byref(st)))
         return st.value
+
+    def autotune(self, stream=None) -> Dict[str, object]:
+        """Times the batched step's launch-shape candidates on the current
+        particles, keeps the fastest and sizes the ghost region; returns the
+        choices and the measured milliseconds per launch."""
+        r = TuneReport()
+        _check(self.L.dsx_grid_autotune(self.h, _stream(stream), C.byref(r)))
+        return {"classify_threads": r.classify_threads, "move_staged": bool(r.move_staged),
+                "reverse_ctas_per_sm": r.reverse_ctas_per_sm,
+                "ghost_capacity": int(r.ghost_capacity),
+                "classify_ms": {n: round(float(v), 4) for n, v in zip((64, 128, 256), r.classify_ms)},
+                "move_ms": {"staged": round(float(r.move_ms[0]), 4),
+                            "direct": round(float(r.move_ms[1]), 4)},
+                "reverse_ms": {n: round(float(v), 4) for n, v in zip((4, 8, 16, 32), r.reverse_ms)}}
 
     def set_plain(self, plain: bool = True):
         """Per-call operations launch their tile kernels once per subdomain

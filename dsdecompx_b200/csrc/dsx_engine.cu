@@ -846,6 +846,109 @@ struct dsx_grid {
         cur ^= 1;
     }
 
+    // Replays the step's idempotent parts on the current particles (the
+    // current owned half is only read) and keeps the fastest launch shapes.
+    void autotune(cudaStream_t stream, dsx_tune_report* out) {
+        dsx_tune_report r{};
+        for (float& v : r.classify_ms) v = -1.0f;
+        for (float& v : r.move_ms) v = -1.0f;
+        for (float& v : r.reverse_ms) v = -1.0f;
+        if (P > 1 && total > 0) {
+            cuda_check(cudaStreamSynchronize(stream), "synchronize before tuning");
+            destroy_graphs();
+            dsx::Marks* saved_marks = S.marks;
+            S.marks = nullptr;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+            cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+            auto time = [&](auto&& launch) {
+                constexpr int kReps = 5;
+                launch();
+                cuda_check(cudaEventRecord(e0, stream), "record");
+                for (int i = 0; i < kReps; ++i) launch();
+                cuda_check(cudaEventRecord(e1, stream), "record");
+                cuda_check(cudaEventSynchronize(e1), "synchronize");
+                float ms = 0.0f;
+                cuda_check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+                return ms / kReps;
+            };
+            auto pick = [](const float* ms, const int* value, int n, int fallback) {
+                int best = fallback;
+                float t = -1.0f;
+                for (int i = 0; i < n; ++i)
+                    if (ms[i] >= 0.0f && (t < 0.0f || ms[i] < t)) {
+                        t = ms[i];
+                        best = value[i];
+                    }
+                return best;
+            };
+            const long long src = owned_off(), dst = next_off();
+            auto grids = [&](dsx::Grid& G, dsx::Grid& Gn) {
+                G = params();
+                cur ^= 1;
+                Gn = params();
+                cur ^= 1;
+            };
+            dsx::Grid G, Gn;
+            grids(G, Gn);
+            clear_status(stream);
+            const int shapes[3] = {64, 128, 256};
+            for (int i = 0; i < 3; ++i) {
+                S.classify_threads = shapes[i];
+                r.classify_ms[i] = time([&] { dsx::launch_step_classify(G, A, src, S, stream); });
+            }
+            S.classify_threads = pick(r.classify_ms, shapes, 3, 128);
+            // the next layout's plan; the ghost region grows until it fits
+            for (;;) {
+                clear_status(stream);
+                dsx::launch_step_classify(G, A, src, S, stream);
+                dsx::launch_step_layout(G, S, stream);
+                const unsigned st = read_status(stream);
+                if (!(st & dsx::kStatusGhostOverflow)) break;
+                grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
+                grids(G, Gn);
+            }
+            const long long gho = ghost_off();
+            const int kinds[2] = {1, 0};
+            for (int i = 0; i < 2; ++i) {
+                if (kinds[i] == 1 && !dsx::staged_move_fits(A)) continue;
+                S.move_staged = kinds[i];
+                r.move_ms[i] = time([&] { dsx::launch_step_move(G, A, src, dst, gho, S, stream); });
+            }
+            S.move_staged = pick(r.move_ms, kinds, 2, 1);
+            dsx::launch_step_move(G, A, src, dst, gho, S, stream);
+            dsx::launch_step_finish(G, Gn, A, src, dst, gho, S, stream);
+            // the reverse sum into the next half's forces from the ghost
+            // region: both are rewritten by the next step
+            const int per_sm[4] = {4, 8, 16, 32};
+            for (int i = 0; i < 4; ++i) {
+                S.reverse_per_sm = per_sm[i];
+                r.reverse_ms[i] = time([&] {
+                    dsx::launch_reverse_sum3(Gn, A.d[6] + dst, A.d[7] + dst, A.d[8] + dst, A.d[6] + gho,
+                                             A.d[7] + gho, A.d[8] + gho, S, stream);
+                });
+            }
+            S.reverse_per_sm = pick(r.reverse_ms, per_sm, 4, 0);
+            const unsigned st = read_status(stream);
+            const long long ghosts = static_cast<int>(pinned_status[1]);
+            if (!(st & dsx::kStatusGhostOverflow) && gcap < ghosts + ghosts / 4)
+                grow_ghosts(ghosts + ghosts / 4, stream);
+            clear_status(stream);
+            cuda_check(cudaStreamSynchronize(stream), "synchronize after tuning");
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            S.marks = saved_marks;
+            plan_valid = false;
+            ghosts_valid = false;
+            destroy_graphs();
+        }
+        r.classify_threads = S.classify_threads;
+        r.move_staged = S.move_staged && dsx::staged_move_fits(A) ? 1 : 0;
+        r.reverse_ctas_per_sm = S.reverse_per_sm;
+        r.ghost_capacity = gcap;
+        if (out) *out = r;
+    }
+
     void step(dsx_step_callback cb, void* user, bool capture, cudaStream_t stream, unsigned* status_out) {
         if (capture && (graph_callback != cb || graph_user != user || graph_stream != stream)) {
             destroy_graphs();
@@ -1245,6 +1348,13 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
         if (grid->P == 1) fail(DSX_E_INVALID, "the batched step needs at least two subdomains");
         grid->step(callback, user, capture != 0, static_cast<cudaStream_t>(stream), status);
         cuda_check(cudaGetLastError(), "launch step");
+    });
+}
+
+int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        grid->autotune(static_cast<cudaStream_t>(stream), report);
     });
 }
 

@@ -2017,11 +2017,6 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long
     if (S.marks) S.marks->mark(s, "halo_scatter");
 }
 
-// Threads per tile of the step's classify pass (each thread takes
-// TILE / kClassifyThreads particles) and its resident-CTA target.
-constexpr int kClassifyThreads = 128;
-constexpr int kClassifyBlocks = 8;
-
 // Shared memory the staged move needs for one tile of every array.
 int staged_bytes(const Arrays& A) {
     int bytes = 11 * (TILE * 8 + 32) + 2 * (TILE * 4 + 32);
@@ -2029,22 +2024,45 @@ int staged_bytes(const Arrays& A) {
     return bytes;
 }
 
-void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
-                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
+void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, const Scratch& S,
+                          cudaStream_t s) {
     cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P * (3 + kMaxNeighbors), s);
-    k_step_classify<kClassifyThreads, kClassifyBlocks><<<G.max_tiles, kClassifyThreads, 0, s>>>(
-        G, A.d[0] + src_off, A.d[1] + src_off, A.d[2] + src_off, S.cnt, S.stride, S.imm_total,
-        S.imm_list, S.imm_bnd, S.imm_img, S.dest16, S.mask);
-    if (S.marks) S.marks->mark(s, "step_classify");
+    const double* x = A.d[0] + src_off;
+    const double* y = A.d[1] + src_off;
+    const double* z = A.d[2] + src_off;
+    switch (S.classify_threads) {
+    case 64:
+        k_step_classify<64, 12><<<G.max_tiles, 64, 0, s>>>(G, x, y, z, S.cnt, S.stride, S.imm_total,
+                                                            S.imm_list, S.imm_bnd, S.imm_img,
+                                                            S.dest16, S.mask);
+        break;
+    case 256:
+        k_step_classify<256, 4><<<G.max_tiles, 256, 0, s>>>(G, x, y, z, S.cnt, S.stride,
+                                                             S.imm_total, S.imm_list, S.imm_bnd,
+                                                             S.imm_img, S.dest16, S.mask);
+        break;
+    default:
+        k_step_classify<128, 8><<<G.max_tiles, 128, 0, s>>>(G, x, y, z, S.cnt, S.stride,
+                                                             S.imm_total, S.imm_list, S.imm_bnd,
+                                                             S.imm_img, S.dest16, S.mask);
+    }
+}
+
+void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s) {
     k_scan_counters<<<kStepCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
     if (S.marks) S.marks->mark(s, "step_scan");
     StepTables T{S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.imm_base, S.emig_info,
                  S.mig_results, S.list_ret, S.list_len, S.send_base, S.g, S.gbase, S.boff,
                  S.halo_info, S.cbase, S.cbase_imm, S.imm_tile_start, S.imm_tiles};
     k_step_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, T);
-    if (S.marks) S.marks->mark(s, "step_layout");
+}
+
+bool staged_move_fits(const Arrays& A) { return staged_bytes(A) <= kStagedMaxBytes; }
+
+void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
+                      long long ghost_off, const Scratch& S, cudaStream_t s) {
     const int staged = staged_bytes(A);
-    if (staged <= kStagedMaxBytes) {
+    if (S.move_staged && staged <= kStagedMaxBytes) {
         static bool attribute_set = false;   // once per process (one device per process)
         if (!attribute_set) {
             cudaFuncSetAttribute(k_step_move_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2060,7 +2078,10 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
                                                S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
                                                S.bslot);
     }
-    if (S.marks) S.marks->mark(s, "step_move");
+}
+
+void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
+                        long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
     const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
     const size_t smem = sizeof(int) * NW * G.P;
     k_emig_hist<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(G.P, S.emig_info, S.emig_dst,
@@ -2072,14 +2093,25 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
     // immigrants: masks, list ranks and ghost images over their segments
     const int imm_grid = G.max_tiles < sm_count() * 4 ? G.max_tiles : sm_count() * 4;
     k_halo_classify<<<imm_grid, NT, 0, s>>>(Gn, S.imm_tiles, S.imm_tile_start + G.P,
-                                                A.d[0] + dst_off, A.d[1] + dst_off,
-                                                A.d[2] + dst_off, S.mask, S.cnt2, S.stride);
+                                            A.d[0] + dst_off, A.d[1] + dst_off, A.d[2] + dst_off,
+                                            S.mask, S.cnt2, S.stride);
     k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt2, S.pre2, S.stride,
                                                    S.imm_tile_start + G.P);
     k_halo_scatter<<<imm_grid, NT, 0, s>>>(Gn, A, dst_off, ghost_off, S.imm_tiles,
-                                              S.imm_tile_start + G.P, S.mask, S.pre2, S.stride,
-                                              S.cbase_imm, S.ghost_owner, S.ghost_entry,
-                                              S.bowner, S.boff, S.bslot);
+                                           S.imm_tile_start + G.P, S.mask, S.pre2, S.stride,
+                                           S.cbase_imm, S.ghost_owner, S.ghost_entry, S.bowner,
+                                           S.boff, S.bslot);
+}
+
+void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
+                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
+    launch_step_classify(G, A, src_off, S, s);
+    if (S.marks) S.marks->mark(s, "step_classify");
+    launch_step_layout(G, S, s);
+    if (S.marks) S.marks->mark(s, "step_layout");
+    launch_step_move(G, A, src_off, dst_off, ghost_off, S, s);
+    if (S.marks) S.marks->mark(s, "step_move");
+    launch_step_finish(G, Gn, A, src_off, dst_off, ghost_off, S, s);
     if (S.marks) S.marks->mark(s, "immigrant_halo");
 }
 
@@ -2109,8 +2141,9 @@ void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, cons
                                                                G.status, b0, b1);
         }
     } else {
-        k_reverse_sum3<<<stream_grid(G.ncap), NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot,
-                                                          ox, oy, oz, gx, gy, gz, G.status, 0, -1);
+        const int grid = S.reverse_per_sm > 0 ? sm_count() * S.reverse_per_sm : stream_grid(G.ncap);
+        k_reverse_sum3<<<grid, NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot, ox, oy, oz, gx,
+                                           gy, gz, G.status, 0, -1);
     }
     if (S.marks) S.marks->mark(s, "reverse_sum");
 }

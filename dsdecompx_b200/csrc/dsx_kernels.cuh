@@ -62,6 +62,10 @@ struct Scratch {
     int* pre2 = nullptr;
     int max_chunks = 0;
     Marks* marks = nullptr;
+    // launch shapes the autotuner picks (these defaults are the untuned choice)
+    int classify_threads = 128;   // threads per 512-particle tile of the step classify: 64/128/256
+    int move_staged = 1;          // 1: tile records staged by bulk copies (if they fit), 0: direct reads
+    int reverse_per_sm = 0;       // CTAs per SM of the reverse sum; 0: one wave of the default shape
 };
 
 void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, int4* tiles,
@@ -87,6 +91,20 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off,
 // Gn: the same grid with the next layout current.
 void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
                        long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s);
+
+// The pipeline's parts, in order (the autotuner replays them one by one):
+// classify (destinations, masks, tile counters), the counter scan and the
+// next layout, the move (idempotent for a fixed current half), and the
+// emigrant placement plus the immigrants' ghost images.
+void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, const Scratch& S,
+                          cudaStream_t s);
+void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s);
+void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
+                      long long ghost_off, const Scratch& S, cudaStream_t s);
+void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
+                        long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s);
+// Whether the staged move can hold one tile of this record.
+bool staged_move_fits(const Arrays& A);
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off,
                          long long ghost_off, bool positions_only, const Scratch& S,

@@ -234,6 +234,29 @@ typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view*
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
                   void* stream, unsigned* status);
 
+/* Autotuning of the batched step's launch shapes on the grid's current
+ * particles: times each candidate by replaying the step's idempotent parts
+ * (nothing of the current owned half changes) and keeps the fastest --
+ * the classify pass's threads per 512-particle tile (64, 128, 256), the move
+ * with its tile records staged in shared memory by bulk copies or read
+ * directly, the reverse sum's CTAs per SM (4, 8, 16, 32) -- and sizes the
+ * ghost region to at least 1.25x the ghosts of the current particles (the
+ * per-neighbour send lists are slices of it).  Afterwards the halo plan is
+ * invalid (call exchange_halo or step next) and captured steps are
+ * re-captured.  report (optional) gets the choices and the measured times
+ * (milliseconds per launch; -1 where a candidate does not apply).  A grid of
+ * one subdomain has nothing to tune and keeps the defaults. */
+typedef struct dsx_tune_report {
+    int classify_threads;
+    int move_staged;
+    int reverse_ctas_per_sm;
+    long long ghost_capacity;
+    float classify_ms[3];    /* 64, 128, 256 threads per tile */
+    float move_ms[2];        /* staged, direct reads */
+    float reverse_ms[4];     /* 4, 8, 16, 32 CTAs per SM */
+} dsx_tune_report;
+int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report);
+
 /* Plain launches, for comparison runs: plain != 0 makes the per-call
  * operations (dsx_grid_migrate, a rebuilding dsx_grid_exchange_halo,
  * dsx_grid_reverse_halo) launch each of their tile kernels once per subdomain

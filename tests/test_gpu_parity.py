@@ -199,7 +199,8 @@ def ghost_force_filler(torch, capacity):
     return fill
 
 
-def test_batched_step_matches_calls(cuda):
+@pytest.mark.parametrize("tuned", [False, True], ids=["default", "autotuned"])
+def test_batched_step_matches_calls(cuda, tuned):
     import torch
 
     import dsdecompx_b200 as dsx
@@ -217,6 +218,13 @@ def test_batched_step_matches_calls(cuda):
     fill = ghost_force_filler(torch, 12000)
     side = torch.cuda.Stream()
     for step in range(4):
+        if tuned and step in (0, 2):
+            # tuning reads the particles and replaces the launch shapes
+            rep = b.autotune()
+            assert rep["classify_threads"] in (64, 128, 256)
+            assert rep["reverse_ctas_per_sm"] in (4, 8, 16, 32)
+            assert rep["ghost_capacity"] >= 12000
+            assert min(rep["classify_ms"].values()) > 0
         a.displace(rng, 0.3)
         for r in range(8):
             o = b.counts(r)[0]
