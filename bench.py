@@ -139,6 +139,18 @@ def algorithmic_bytes(S, N, E, G, B):
 
 # ------------------------------------------------------------------- our arm
 
+def max_over_ranks(value, world, device=None):
+    """The slowest rank's figure: an all-reduce MAX over the process group
+    (a CUDA tensor on `device` for NCCL, a CPU tensor for gloo)."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64,
+                     device=f"cuda:{device}" if device is not None else "cpu")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, device):
     import numpy as np
     import torch
@@ -228,10 +240,7 @@ def run_ours(args, rank, world, device):
     clock = clocks.summary()
     kernels_per_step = grid.step_kernel_count()
     launches = args.steps * (kernels_per_step + harness_kernels)
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=f"cuda:{device}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, world, device)
     ms_per_step = elapsed_ms / args.steps
     value = world * N / (ms_per_step / 1e3) / 1e6
 
@@ -293,10 +302,7 @@ def run_ours(args, rank, world, device):
             e1.record(stream)
         torch.cuda.synchronize(device)
         e_ms = e0.elapsed_time(e1) / args.e2e_steps
-        if world > 1:
-            t = torch.tensor([e_ms], device=f"cuda:{device}")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks(e_ms, world, device)
         e2e = {"value": round(world * N / (e_ms / 1e3) / 1e6, 3), "unit": "M particles/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(N * S + 8 * w.nranks),
                "ms_per_step": round(e_ms, 3),
@@ -406,6 +412,8 @@ def run_drop_in(args, w, wl, stream, rank, world):
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
+    if world > 1:
+        torch.distributed.barrier()
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clocks:
@@ -415,7 +423,9 @@ def run_drop_in(args, w, wl, stream, rank, world):
                 step()
             b.record(stream)
         torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / args.steps
+    if world > 1:
+        torch.distributed.barrier()
+    ms = max_over_ranks(a.elapsed_time(b), world, torch.cuda.current_device()) / args.steps
     return {"metric": METRIC, "value": round(world * N / (ms / 1e3) / 1e6, 3),
             "unit": "M particles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
