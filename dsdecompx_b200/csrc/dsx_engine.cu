@@ -491,8 +491,11 @@ struct dsx_grid {
         S.emig_info = device_alloc<int>(fixed_owned, 4);
         cuda_check(cudaMemset(S.emig_info, 0, 4 * sizeof(int)), "memset");
         S.mig_results = device_alloc<long long>(fixed_owned, static_cast<std::size_t>(P) * 6);
-        S.mask = device_alloc<unsigned>(fixed_owned, ncap);
-        S.dest16 = device_alloc<unsigned short>(fixed_owned, ncap);
+        // per particle (per-call halo build) and per tile slot (batched step)
+        const std::size_t slots = static_cast<std::size_t>(max_tiles) * dsx::kTile;
+        S.mask = device_alloc<unsigned>(fixed_owned, std::max<std::size_t>(slots, static_cast<std::size_t>(ncap)));
+        S.dest16 = device_alloc<unsigned short>(fixed_owned, slots);
+        S.tile_bases = device_alloc<int>(fixed_owned, static_cast<std::size_t>(max_tiles) * 32);
         S.list_len = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
         S.send_base = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
         S.g = device_alloc<int>(fixed_owned, P + 1);

@@ -189,30 +189,47 @@ __global__ void __launch_bounds__(1024) k_layout(int P, int tile, const int* n, 
 // cnt/pre are counter-major: [k * stride + tile]; pre[k*stride + ntiles] = total.
 __global__ void __launch_bounds__(1024) k_scan_counters(const int* cnt, int* pre, int stride,
                                                          const int* tile_start_end) {
-    __shared__ int ws[33];
     constexpr int PER = 8;
+    constexpr int CHUNK = 1024 * PER;
+    __shared__ int ws[33];
+    // a chunk of the counter, padded one word per 32 so that thread t's PER
+    // consecutive entries sit in distinct banks
+    __shared__ int buf[CHUNK + CHUNK / 32];
     const int k = blockIdx.x;
     const int ntiles = *tile_start_end;
     const int* src = cnt + static_cast<long long>(k) * stride;
     int* dst = pre + static_cast<long long>(k) * stride;
+    auto at = [](int i) { return i + (i >> 5); };
     int carry = 0;
-    for (int base = 0; base < ntiles; base += 1024 * PER) {
-        int v[PER];
-        int sum = 0;
-        const int first = base + threadIdx.x * PER;
+    for (int base = 0; base < ntiles; base += CHUNK) {
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
-            v[j] = first + j < ntiles ? src[first + j] : 0;
+            const int i = j * 1024 + threadIdx.x;
+            buf[at(i)] = base + i < ntiles ? src[base + i] : 0;
+        }
+        __syncthreads();
+        int v[PER];
+        int sum = 0;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            v[j] = buf[at(threadIdx.x * PER + j)];
             sum += v[j];
         }
         int total;
         int run = block_scan_excl<1024>(sum, total, ws) + carry;
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
-            if (first + j < ntiles) dst[first + j] = run;
+            buf[at(threadIdx.x * PER + j)] = run;
             run += v[j];
         }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int i = j * 1024 + threadIdx.x;
+            if (base + i < ntiles) dst[base + i] = buf[at(i)];
+        }
         carry += total;
+        __syncthreads();
     }
     if (threadIdx.x == 0) dst[ntiles] = carry;
 }
@@ -889,10 +906,10 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
         if (i < end) {
             double wx, wy, wz;
             d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
-            dest_out[i] = static_cast<unsigned short>(d);
+            dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(d);
             if (d == s) {
                 m = halo_mask(bs, lut, wx, wy, wz);
-                mask_out[i] = m;
+                mask_out[static_cast<long long>(g) * TILE + (i - begin)] = m;
             } else {
                 const unsigned me = halo_mask(halo_bounds(G, d), G.lut + d * 64, wx, wy, wz);
                 atomicAdd(&imm_total[d], 1);
@@ -948,6 +965,7 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
     __shared__ int ws[33];
     __shared__ int s_n[kMaxRanks + 1], s_ob[kMaxRanks + 1], s_ts[kMaxRanks + 1];
     __shared__ int s_in[kMaxRanks + 1], s_ib[kMaxRanks + 1], s_its[kMaxRanks + 1];
+    __shared__ int s_rcv[kMaxRanks + 1];
     const int P = G.P;
     const int t = threadIdx.x;
     const int ntiles = G.tile_start[P];
@@ -1013,26 +1031,36 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
     __syncthreads();
     fill_tiles(P, G.tile, s_n, s_ob, s_ts, G.tiles_next);
     fill_tiles(P, G.tile, s_in, s_ib, s_its, T.imm_tiles);
-    // receivers: blocks in the receiver's neighbor order
-    int mine = 0;
-    if (t < P) {
-        for (int m = 0; m < G.nn[t]; ++m) {
-            const int e = G.sender_of[t * kMaxNeighbors + m];
-            mine += e >= 0 ? T.list_len[e] : 0;
+    // receivers: blocks in the receiver's neighbor order, one warp per
+    // receiver (lane m reads the block of neighbor m)
+    const int warp = t >> 5, lane = t & 31, nwarps = blockDim.x >> 5;
+    for (int q = warp; q < P; q += nwarps) {
+        int len = 0;
+        if (lane < G.nn[q]) {
+            const int e = G.sender_of[q * kMaxNeighbors + lane];
+            len = e >= 0 ? T.list_len[e] : 0;
         }
+        const int sum = __reduce_add_sync(0xffffffffu, len);
+        if (lane == 0) s_rcv[q] = sum;
     }
+    __syncthreads();
+    const int mine = t < P ? s_rcv[t] : 0;
     int total_ghosts;
     const int gb = block_scan_excl<1024>(mine, total_ghosts, ws);
     if (t < P) {
         T.gq[t] = mine;
         T.gbase[t] = gb;
-        int run = gb;
-        for (int m = 0; m < G.nn[t]; ++m) {
-            const int e = G.sender_of[t * kMaxNeighbors + m];
-            if (e < 0) continue;
-            T.send_base[e] = run;
-            run += T.list_len[e];
+        s_rcv[t] = gb;
+    }
+    __syncthreads();
+    for (int q = warp; q < P; q += nwarps) {
+        int len = 0, e = -1;
+        if (lane < G.nn[q]) {
+            e = G.sender_of[q * kMaxNeighbors + lane];
+            len = e >= 0 ? T.list_len[e] : 0;
         }
+        const int incl = warp_inclusive_sum(len);
+        if (e >= 0) T.send_base[e] = s_rcv[q] + incl - len;
     }
     // boundary owners and images: retained part first, then the immigrants
     int bret = 0, bimm = 0, iret = 0, iimm = 0;
@@ -1045,15 +1073,15 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
     int total_b, total_i;
     const int bb = block_scan_excl<1024>(bret + bimm, total_b, ws);
     const int ib = block_scan_excl<1024>(iret + iimm, total_i, ws);   // syncs: send_base complete
+    for (int e = t; e < P * kMaxNeighbors; e += blockDim.x) {
+        const int r = e / kMaxNeighbors, n = e % kMaxNeighbors;
+        const bool active = n < G.nn[r] && G.nbr[e] >= 0;
+        T.cbase_ret[r * kHaloCounters + n] = active ? T.send_base[e] : 0;
+        T.cbase_imm[r * kHaloCounters + n] = active ? T.send_base[e] + T.list_ret[e] : 0;
+    }
     if (t < P) {
         int* cr = T.cbase_ret + t * kHaloCounters;
         int* ci = T.cbase_imm + t * kHaloCounters;
-        for (int n = 0; n < kMaxNeighbors; ++n) {
-            const int e = t * kMaxNeighbors + n;
-            const bool active = n < G.nn[t] && G.nbr[e] >= 0;
-            cr[n] = active ? T.send_base[e] : 0;
-            ci[n] = active ? T.send_base[e] + T.list_ret[e] : 0;
-        }
         cr[kBoundaryCounter] = bb;
         ci[kBoundaryCounter] = bb + bret;
         cr[kImageCounter] = ib;
@@ -1122,8 +1150,8 @@ __global__ void __launch_bounds__(NT, 4) k_step_move(Grid G, Arrays A, long long
         dest[j] = -1;
         msk[j] = 0;
         if (i < end) {
-            dest[j] = dest_in[i];
-            if (dest[j] == s) msk[j] = mask_in[i];
+            dest[j] = dest_in[static_cast<long long>(g) * TILE + (i - begin)];
+            if (dest[j] == s) msk[j] = mask_in[static_cast<long long>(g) * TILE + (i - begin)];
         }
         count_group(msk[j], nn, lane, acc);
         const int stays = __popc(__ballot_sync(0xffffffffu, dest[j] == s));
@@ -1410,14 +1438,26 @@ __device__ __forceinline__ int tile_base(const Grid& G, const int* pre, int stri
     return pre[k * stride + g];
 }
 
+// Counter bases of every tile of the layout (30 per tile, row stride 32), so
+// that the move reads them with one load per tile.
+__global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int stride,
+                                                   const int* cbase_ret, int* tile_bases) {
+    const int ntiles = G.tile_start[G.P];
+    for (long long idx = blockIdx.x * static_cast<long long>(NT) + threadIdx.x;
+         idx < static_cast<long long>(ntiles) * 32; idx += static_cast<long long>(gridDim.x) * NT) {
+        const int g = static_cast<int>(idx >> 5), k = static_cast<int>(idx & 31);
+        if (k < kStepCounters) tile_bases[idx] = tile_base(G, pre, stride, cbase_ret, g, G.tiles[g], k);
+    }
+}
+
 // F4 with the tile's records staged in shared memory (same output as
 // k_step_move).  Dynamic shared memory: sum over the arrays of TILE x element
 // bytes + 32.
 __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     Grid G, Arrays A, long long src_off, long long dst_off, long long ghost_off, const int* pre,
     int stride, const int* cbase_ret, const unsigned short* __restrict__ dest_in,
-    const unsigned* __restrict__ mask_in, int* emig_src, int* emig_dst, int* ghost_owner,
-    int* ghost_entry, int* bowner, int* boff, int* bslot) {
+    const unsigned* __restrict__ mask_in, const int* __restrict__ tile_bases, int* emig_src,
+    int* emig_dst, int* ghost_owner, int* ghost_entry, int* bowner, int* boff, int* bslot) {
     extern __shared__ __align__(16) unsigned char s_rec[];
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ int s_seg[kStagedArrays];
@@ -1427,28 +1467,24 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     __shared__ unsigned short s_own[kStageCap];
     __shared__ int s_ni[TILE];
     const int g = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // destinations, masks (per tile slot) and the counter bases (per tile)
+    // need only the tile index: they are read together with the descriptor
     const int4 td = G.tiles[g];
+    const long long slot0 = static_cast<long long>(g) * TILE + warp * 32 * ITEMS + lane;
+    unsigned short d16[ITEMS];
+    unsigned mraw[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        d16[j] = dest_in[slot0 + j * 32];
+        mraw[j] = mask_in[slot0 + j * 32];
+    }
+    const int base = threadIdx.x < kStepCounters ? tile_bases[static_cast<long long>(g) * 32 + threadIdx.x] : 0;
     if (g >= G.tile_start[G.P]) return;
     const int s = td.x, begin = td.y, end = td.z;
     const unsigned bar = smem_u32(&s_bar);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wbegin = begin + warp * 32 * ITEMS;
-    // what the tile needs first goes out first: destinations, masks (only
-    // meaningful for a stay) and the counter bases
-    int dest[ITEMS];
-    unsigned msk[ITEMS];
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const int i = wbegin + j * 32 + lane;
-        dest[j] = -1;
-        msk[j] = 0;
-        if (i < end) {
-            dest[j] = dest_in[i];
-            msk[j] = mask_in[i];
-        }
-    }
-    int base = 0;
-    if (threadIdx.x < kStepCounters) base = tile_base(G, pre, stride, cbase_ret, g, td, threadIdx.x);
+    // the tile's records go out as soon as the descriptor is known
     if (warp == 0) {
         if (lane == 0) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
@@ -1456,6 +1492,16 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         }
         __syncwarp();
         stage_issue(A, src_off, begin, end, s_rec, bar, s_seg, lane);
+    }
+    // (slots past the tile's end hold stale values: masked here; the mask
+    // is only meaningful for a stay)
+    int dest[ITEMS];
+    unsigned msk[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const bool in = wbegin + j * 32 + lane < end;
+        dest[j] = in ? static_cast<int>(d16[j]) : -1;
+        msk[j] = in ? mraw[j] : 0u;
     }
     const bool ghosts = !(*G.status & kStatusGhostOverflow);
     const int nn = G.nn[s];
@@ -2055,6 +2101,8 @@ void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s) {
                  S.mig_results, S.list_ret, S.list_len, S.send_base, S.g, S.gbase, S.boff,
                  S.halo_info, S.cbase, S.cbase_imm, S.imm_tile_start, S.imm_tiles};
     k_step_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, T);
+    k_tile_bases<<<stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s>>>(
+        G, S.pre, S.stride, S.cbase, S.tile_bases);
 }
 
 bool staged_move_fits(const Arrays& A) { return staged_bytes(A) <= kStagedMaxBytes; }
@@ -2071,7 +2119,8 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
         }
         k_step_move_staged<<<G.max_tiles, NT, staged, s>>>(
             G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
-            S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner, S.boff, S.bslot);
+            S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
+            S.bslot);
     } else {
         k_step_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
                                                S.cbase, S.dest16, S.mask, S.emig_src, S.emig_dst,

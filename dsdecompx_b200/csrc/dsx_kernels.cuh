@@ -38,7 +38,8 @@ struct Scratch {
     int* emig_info = nullptr;  // {E, nchunks}
     long long* mig_results = nullptr;  // [P][6]
     unsigned* mask = nullptr;  // [ncap] halo neighbor mask per owned particle
-    unsigned short* dest16 = nullptr;  // [ncap] destination of each owned particle (fused step)
+    unsigned short* dest16 = nullptr;  // [max_tiles * 512] destination per tile slot (fused step)
+    int* tile_bases = nullptr;         // [max_tiles * 32] step counter bases per tile
     int* list_len = nullptr;   // [P*26] send-list lengths
     int* send_base = nullptr;  // [P*26] first ghost slot of each send list
     int* g = nullptr;          // [P] ghosts per receiver
