@@ -1519,37 +1519,33 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     s_cnt[warp][lane] = acc;
     if (threadIdx.x < kStepCounters) s_base[threadIdx.x] = base;
     __syncthreads();
+    // staging offsets of the lists: lane n sums its list over the warps, then
+    // an exclusive scan over the lanes (every warp computes them; warp 0
+    // keeps them for the ghost pass)
+    int tot = 0;
+    if (lane < nn)
+        for (int w = 0; w < NW; ++w) tot += s_cnt[w][lane];
+    const int sincl = warp_inclusive_sum(tot);
+    const int Q = __shfl_sync(0xffffffffu, sincl, 31);
     if (warp == 0) {
-        int tot = 0;
-        if (lane < nn)
-            for (int w = 0; w < NW; ++w) tot += s_cnt[w][lane];
-        const int incl = warp_inclusive_sum(tot);
-        if (lane < nn) s_off[lane] = incl - tot;
-        if (lane == 31) s_off[nn] = incl;
+        if (lane < nn) s_off[lane] = sincl - tot;
+        if (lane == 31) s_off[nn] = sincl;
     }
-    // the records must have landed before anything reads them
-    const bool lost = !bulk_wait(bar);
-    if (__syncthreads_or(lost)) {
-        if (lost) bulk_wait(bar);   // copies still in flight get one more bounded wait
-        if (threadIdx.x == 0) atomicOr(G.status, kStatusCopyTimeout);
-        return;
-    }
-    const int Q = s_off[nn];
     const bool staged = Q <= kStageCap;
-    int sg[13];
-#pragma unroll
-    for (int a = 0; a < 13; ++a) sg[a] = s_seg[a];
-    const int* fseg = s_seg + 13;
     int run = 0, lrun = 0;
     if (lane < kStepCounters) {
         run = s_base[lane];
-        if (lane < nn) lrun = s_off[lane];
+        if (lane < nn) lrun = sincl - tot;
         for (int w = 0; w < warp; ++w) {
             run += s_cnt[w][lane];
             lrun += s_cnt[w][lane];
         }
     }
-    const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
+    const int run0 = run;
+    // the index work needs only destinations and masks, so it runs while the
+    // record copies are still landing: new slots, emigrant list, boundary
+    // owners and their image slots, and the ghost images staged by list
+    int nis[ITEMS];
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = wbegin + j * 32 + lane;
@@ -1560,8 +1556,8 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         const unsigned be = __ballot_sync(0xffffffffu, emig);
         const int ni = __shfl_sync(0xffffffffu, run, kStepStay) + __popc(bs_ & lt);
         const int eb = __shfl_sync(0xffffffffu, run, kStepEmig) + __popc(be & lt);
+        nis[j] = ni;
         if (stay) {
-            move_from_stage(G, A, s_rec, sg, fseg, l, dst_off + ni);
             s_ni[l] = ni;
         } else if (emig) {
             emig_src[eb] = i;
@@ -1587,16 +1583,9 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
                 const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
                 if ((mj >> n) & 1u) {
                     const int rank = __popc(hit & lt);
-                    const int slot = list_base + rank;
-                    bslot[img + k] = slot;
+                    bslot[img + k] = list_base + rank;
                     ++k;
-                    if (staged) {
-                        s_own[stage_base + rank] = static_cast<unsigned short>(l);
-                    } else {
-                        ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
-                        ghost_owner[slot] = ni;
-                        ghost_entry[slot] = s * kMaxNeighbors + n;
-                    }
+                    if (staged) s_own[stage_base + rank] = static_cast<unsigned short>(l);
                 }
                 if (lane == n) {
                     run += __popc(hit);
@@ -1610,21 +1599,61 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         if (lane == kStepStay) run += __popc(bs_);
         if (lane == kStepEmig) run += __popc(be);
     }
-    if (!ghosts || !staged) return;
-    __syncthreads();
-    for (int q = threadIdx.x; q < Q; q += NT) {
-        int lo = 0, hi = nn;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (s_off[mid] <= q) lo = mid;
-            else hi = mid;
+    // the records must have landed before anything reads them; after this
+    // barrier every warp's staging is visible too
+    const bool lost = !bulk_wait(bar);
+    if (__syncthreads_or(lost)) {
+        if (lost) bulk_wait(bar);   // copies still in flight get one more bounded wait
+        if (threadIdx.x == 0) atomicOr(G.status, kStatusCopyTimeout);
+        return;
+    }
+    int sg[13];
+#pragma unroll
+    for (int a = 0; a < 13; ++a) sg[a] = s_seg[a];
+    const int* fseg = s_seg + 13;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j)
+        if (dest[j] == s) move_from_stage(G, A, s_rec, sg, fseg, wbegin + j * 32 + lane - begin, dst_off + nis[j]);
+    if (!ghosts) return;
+    const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
+    if (staged) {
+        // list by list: consecutive threads write consecutive ghost slots
+        for (int q = threadIdx.x; q < Q; q += NT) {
+            int lo = 0, hi = nn;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (s_off[mid] <= q) lo = mid;
+                else hi = mid;
+            }
+            const int n = lo;
+            const int slot = s_base[n] + (q - s_off[n]);
+            const int l = s_own[q];
+            ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
+            ghost_owner[slot] = s_ni[l];
+            ghost_entry[slot] = s * kMaxNeighbors + n;
         }
-        const int n = lo;
-        const int slot = s_base[n] + (q - s_off[n]);
-        const int l = s_own[q];
-        ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
-        ghost_owner[slot] = s_ni[l];
-        ghost_entry[slot] = s * kMaxNeighbors + n;
+        return;
+    }
+    // a tile with more images than the staging holds (a halo wider than
+    // half a cell) writes them from the hitting lanes directly
+    run = run0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int l = wbegin + j * 32 + lane - begin;
+        const unsigned mj = msk[j];
+        const unsigned used = __reduce_or_sync(0xffffffffu, mj);
+        for (unsigned rest = used; rest; rest &= rest - 1) {
+            const int n = __ffs(rest) - 1;
+            const unsigned hit = __ballot_sync(0xffffffffu, (mj >> n) & 1u);
+            const int list_base = __shfl_sync(0xffffffffu, run, n);
+            if ((mj >> n) & 1u) {
+                const int slot = list_base + __popc(hit & lt);
+                ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
+                ghost_owner[slot] = nis[j];
+                ghost_entry[slot] = s * kMaxNeighbors + n;
+            }
+            if (lane == n) run += __popc(hit);
+        }
     }
 }
 

@@ -289,21 +289,25 @@ def test_halo_backward_is_reverse_halo(cuda):
     pair.close()
 
 
-@pytest.mark.parametrize("fields,particles", [(ALL_FIELDS[:2], 300_000), (ALL_FIELDS, 40_000)],
-                         ids=["staged-record", "wide-record"])
-def test_batched_step_many_tiles(cuda, fields, particles):
+@pytest.mark.parametrize("fields,particles,box,halo", [
+    (ALL_FIELDS[:2], 300_000, 12.0, 0.6),
+    (ALL_FIELDS, 40_000, 12.0, 0.6),
+    (ALL_FIELDS[:2], 20_000, 6.0, 1.1)], ids=["staged-record", "wide-record", "wide-halo"])
+def test_batched_step_many_tiles(cuda, fields, particles, box, halo):
     """The batched step against the per-call path and the oracle with far
     more 512-particle tiles than SMs, once with a record that the move stages
-    in shared memory and once with a record too wide to stage (the move then
-    reads HBM directly)."""
+    in shared memory, once with a record too wide to stage (the move then
+    reads HBM directly), and once with a halo wider than half a cell (every
+    particle has 26 images, more than a tile stages: they are written from
+    the hitting lanes)."""
     import torch
 
     import dsdecompx_b200 as dsx
     rng = np.random.default_rng(29)
-    capacity = 2 * particles
-    kw = dict(nranks=27, dims=(3, 3, 3), lower=(0, 0, 0), upper=(12, 12, 12), halo_width=0.6,
+    capacity = 2 * particles if halo < 1.0 else 30 * particles
+    kw = dict(nranks=27, dims=(3, 3, 3), lower=(0, 0, 0), upper=(box, box, box), halo_width=halo,
               fields=fields, particles=particles, ghost_capacity=capacity)
-    data = uniform_particles(rng, particles, (0, 0, 0), (12, 12, 12), fields)
+    data = uniform_particles(rng, particles, (0, 0, 0), (box, box, box), fields)
     a = Pair(**kw)
     owner = a.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
     per = split_by_owner(owner, data, 27)
