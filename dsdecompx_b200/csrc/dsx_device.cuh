@@ -115,7 +115,11 @@ struct Grid {
 // (of either sign) gives +0.  So the fast path is (t == 0 ? +0 : t) + lower:
 // the FP64 division, multiply and subtract are skipped without changing a bit
 // of the result.  Every other input (outside the box, NaN, inf) divides.
+//
+// With lower == 0 the fast path needs no arithmetic at all: t is v itself
+// and (t == 0 ? +0 : t) + 0 is v, or +0 for a zero of either sign.
 __device__ __forceinline__ double wrap_axis(double v, double lower, double extent) {
+    if (lower == 0.0 && v >= 0.0 && v < extent) return v == 0.0 ? 0.0 : v;
     const double t = __dsub_rn(v, lower);
     if (t >= 0.0 && t < extent) return __dadd_rn(t == 0.0 ? 0.0 : t, lower);
     const double q = floor(__ddiv_rn(t, extent));

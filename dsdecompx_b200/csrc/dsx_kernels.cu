@@ -524,7 +524,7 @@ __device__ __forceinline__ unsigned halo_mask(const TileBounds& b, const unsigne
     const unsigned flags = (px < b.lo[0] ? 1u : 0u) | (px > b.hi[0] ? 2u : 0u) |
                            (py < b.lo[1] ? 4u : 0u) | (py > b.hi[1] ? 8u : 0u) |
                            (pz < b.lo[2] ? 16u : 0u) | (pz > b.hi[2] ? 32u : 0u);
-    return flags ? __ldg(lut + flags) : 0u;
+    return flags ? lut[flags] : 0u;   // shared or global table
 }
 
 // Adds this warp's contribution of one 32-particle group to the per-lane
@@ -875,6 +875,7 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
     constexpr int CW = CT / 32;
     static_assert(CI * CT == TILE && CW >= 1, "tile split");
     __shared__ int s_cnt[CW][32];
+    __shared__ unsigned s_lut[64];   // the subdomain's halo flags -> neighbor mask
     const int g = blockIdx.x;
     // the descriptor is read together with the tile count (the table has a
     // row for every block of the launch)
@@ -895,7 +896,9 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
     }
     const TileBounds bs = halo_bounds(G, s);
     const Cell cell = cell_of(G, s);
-    const unsigned* lut = G.lut + s * 64;
+    for (int f = threadIdx.x; f < 64; f += CT) s_lut[f] = G.lut[s * 64 + f];
+    __syncthreads();
+    const unsigned* lut = s_lut;
     const int nn = G.nn[s];
     int acc = 0;
 #pragma unroll
