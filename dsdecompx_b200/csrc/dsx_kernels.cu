@@ -616,6 +616,7 @@ __global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, in
                                                        int* gbase, int* boff, int* info,
                                                        int* cbase) {
     __shared__ int ws[33];
+    __shared__ int s_rcv[kMaxRanks + 1];
     const int P = G.P;
     const int ntiles = G.tile_start[P];
     for (int idx = threadIdx.x; idx < P * kMaxNeighbors; idx += blockDim.x) {
@@ -626,26 +627,36 @@ __global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, in
         list_len[idx] = len;
     }
     __syncthreads();
-    const int q = threadIdx.x;
-    int mine = 0;
-    if (q < P) {
-        for (int m = 0; m < G.nn[q]; ++m) {
-            const int e = G.sender_of[q * kMaxNeighbors + m];
-            mine += e >= 0 ? list_len[e] : 0;
+    // receivers, one warp each: lane m reads the block of neighbor m
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int r = warp; r < P; r += nwarps) {
+        int len = 0;
+        if (lane < G.nn[r]) {
+            const int e = G.sender_of[r * kMaxNeighbors + lane];
+            len = e >= 0 ? list_len[e] : 0;
         }
+        const int sum = __reduce_add_sync(0xffffffffu, len);
+        if (lane == 0) s_rcv[r] = sum;
     }
+    __syncthreads();
+    const int q = threadIdx.x;
+    const int mine = q < P ? s_rcv[q] : 0;
     int total;
     const int excl = block_scan_excl<1024>(mine, total, ws);
     if (q < P) {
         gq[q] = mine;
         gbase[q] = excl;
-        int run = excl;
-        for (int m = 0; m < G.nn[q]; ++m) {
-            const int e = G.sender_of[q * kMaxNeighbors + m];
-            if (e < 0) continue;
-            send_base[e] = run;
-            run += list_len[e];
+        s_rcv[q] = excl;
+    }
+    __syncthreads();
+    for (int r = warp; r < P; r += nwarps) {
+        int len = 0, e = -1;
+        if (lane < G.nn[r]) {
+            e = G.sender_of[r * kMaxNeighbors + lane];
+            len = e >= 0 ? list_len[e] : 0;
         }
+        const int incl = warp_inclusive_sum(len);
+        if (e >= 0) send_base[e] = s_rcv[r] + incl - len;
     }
     if (q == 0) {
         gbase[P] = total;
@@ -1982,17 +1993,19 @@ __global__ void __launch_bounds__(NT) k_wrap_inplace(double* x, double* y, doubl
                                                      double3 lower, double3 extent, int3 periodic) {
     for (long long i = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i < n;
          i += static_cast<long long>(gridDim.x) * NT) {
+        // all three reads go out before any compare
+        const double vx = x[i], vy = y[i], vz = z[i];
         if (periodic.x) {
-            const double v = x[i], w = wrap_axis(v, lower.x, extent.x);
-            if (__double_as_longlong(w) != __double_as_longlong(v)) x[i] = w;
+            const double w = wrap_axis(vx, lower.x, extent.x);
+            if (__double_as_longlong(w) != __double_as_longlong(vx)) x[i] = w;
         }
         if (periodic.y) {
-            const double v = y[i], w = wrap_axis(v, lower.y, extent.y);
-            if (__double_as_longlong(w) != __double_as_longlong(v)) y[i] = w;
+            const double w = wrap_axis(vy, lower.y, extent.y);
+            if (__double_as_longlong(w) != __double_as_longlong(vy)) y[i] = w;
         }
         if (periodic.z) {
-            const double v = z[i], w = wrap_axis(v, lower.z, extent.z);
-            if (__double_as_longlong(w) != __double_as_longlong(v)) z[i] = w;
+            const double w = wrap_axis(vz, lower.z, extent.z);
+            if (__double_as_longlong(w) != __double_as_longlong(vz)) z[i] = w;
         }
     }
 }
@@ -2248,7 +2261,8 @@ void mark(const Scratch& S, cudaStream_t s, const char* what) {
 void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,
                          const double* extent, const int* periodic, cudaStream_t s) {
     if (n <= 0) return;
-    k_wrap_inplace<<<stream_grid(n), NT, 0, s>>>(
+    const long long blocks = (n + NT - 1) / NT;   // one particle per thread
+    k_wrap_inplace<<<static_cast<int>(blocks < 1 ? 1 : (blocks < (1 << 30) ? blocks : (1 << 30))), NT, 0, s>>>(
         x, y, z, n, make_double3(lower[0], lower[1], lower[2]),
         make_double3(extent[0], extent[1], extent[2]),
         make_int3(periodic[0], periodic[1], periodic[2]));

@@ -199,6 +199,81 @@ def ghost_force_filler(torch, capacity):
     return fill
 
 
+def growing_force_filler(torch, most):
+    """Like ghost_force_filler for a ghost region that may grow: slot k gets
+    sin((j + 1) k), written from tensors made up front for up to `most` slots."""
+    slots = torch.arange(most, device="cuda", dtype=torch.float64)
+    values = [torch.sin(slots * (j + 1)) for j in range(3)]
+
+    def fill(view, stream):
+        capacity = int(view.ghost_capacity)
+        assert capacity <= most
+        s = torch.cuda.ExternalStream(stream)
+        with torch.cuda.stream(s):
+            for j, k in enumerate((6, 7, 8)):
+                t = torch.as_tensor(DeviceArray(view.base[k] + 8 * int(view.ghost_offset), capacity),
+                                    device="cuda")
+                t.copy_(values[j][:capacity])
+    return fill
+
+
+def test_batched_step_ghost_overflow_redo(cuda):
+    """A step whose ghost region overflows (capacity 64) grows it and redoes
+    the halo build, the callback and the reverse sum; the result equals the
+    per-call path, which grows the same way."""
+    import torch
+
+    import dsdecompx_b200 as dsx
+    rng = np.random.default_rng(17)
+    fields = ALL_FIELDS[:2]
+    kw = dict(nranks=8, dims=(2, 2, 2), lower=(0, 0, 0), upper=(12, 12, 12), halo_width=0.6,
+              fields=fields, particles=8000, ghost_capacity=64)
+    data = uniform_particles(rng, 8000, (0, 0, 0), (12, 12, 12), fields)
+    a = Pair(**kw)
+    owner = a.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    per = split_by_owner(owner, data, 8)
+    a.upload(per)
+    b = dsx.VirtualGrid(**kw)
+    b.upload(per)
+    fill = growing_force_filler(torch, 1 << 18)
+    side = torch.cuda.Stream()
+    try:
+        for step in range(3):
+            a.displace(rng, 0.3)
+            for r in range(8):
+                o = b.counts(r)[0]
+                for name in "xyz":
+                    b.write(r, name, 0, a.gpu.read(r, name, 0, o))
+            a.gpu.migrate()
+            a.ref.migrate()
+            a.gpu.exchange_halo(rebuild=True)
+            a.ref.exchange_halo(rebuild=True)
+            fill(a.gpu.view(), torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            for r in range(8):
+                o, g = a.ref.counts(r)
+                for name in ("fx", "fy", "fz"):
+                    a.ref.write(r, name, o, a.gpu.read(r, name, o, g))
+            a.gpu.reverse_halo()
+            a.ref.reverse_halo()
+            a.compare(f"calls {step}")
+            torch.cuda.synchronize()
+            before = int(b.view().ghost_capacity)
+            with torch.cuda.stream(side):
+                st = b.step(fill, capture=step > 0)
+            side.synchronize()
+            assert st == 0
+            if step == 0:
+                assert int(b.view().ghost_capacity) > before == 64
+            for r in range(8):
+                x, y = a.gpu.snapshot(r), b.snapshot(r)
+                for k in x:
+                    assert same(x[k], y[k]), (step, r, k)
+    finally:
+        a.close()
+        b.close()
+
+
 @pytest.mark.parametrize("tuned", [False, True], ids=["default", "autotuned"])
 def test_batched_step_matches_calls(cuda, tuned):
     import torch
