@@ -1396,8 +1396,10 @@ int dsx_grid_kernel_times(dsx_grid* grid, int max, const char** names, float* ms
 }
 
 int dsx_grid_step_kernel_count(dsx_grid* grid) {
-    // rebalance (Dynamic only) + 7 migrate + 4 halo build + 1 reverse
-    return (grid->desc.policy == DSX_DYNAMIC ? 1 : 0) + 7 + 4 + 1;
+    // rebalance (Dynamic only); classify, counter scan, layout, tile bases,
+    // move; emigrant histogram, column scan, placement; immigrants' classify,
+    // scan, scatter; reverse sum
+    return (grid->desc.policy == DSX_DYNAMIC ? 1 : 0) + 5 + 3 + 3 + 1;
 }
 
 }  // extern "C"

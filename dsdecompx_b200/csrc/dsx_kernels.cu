@@ -2031,8 +2031,6 @@ int stream_grid(long long items) {
 
 }  // namespace
 
-int kernels_per_step() { return 0; }
-
 void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, int4* tiles,
                    cudaStream_t s) {
     k_layout<<<1, 1024, 0, s>>>(G.P, G.tile, n, obase, tile_start, tiles);

@@ -155,6 +155,4 @@ void launch_wrap_inplace(double* x, double* y, double* z, long long n, const dou
 // Records a named timing mark on `s` (no-op unless S.marks->on).
 void mark(const Scratch& S, cudaStream_t s, const char* what);
 
-int kernels_per_step();
-
 }  // namespace dsx
