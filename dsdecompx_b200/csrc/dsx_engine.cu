@@ -1349,6 +1349,9 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
                   unsigned* status) {
     return guarded([&] {
         if (grid->P == 1) fail(DSX_E_INVALID, "the batched step needs at least two subdomains");
+        if (capture && (stream == nullptr || static_cast<cudaStream_t>(stream) == cudaStreamLegacy ||
+                        static_cast<cudaStream_t>(stream) == cudaStreamPerThread))
+            fail(DSX_E_INVALID, "capturing the step in a CUDA graph needs a created stream, not the default stream");
         grid->step(callback, user, capture != 0, static_cast<cudaStream_t>(stream), status);
         cuda_check(cudaGetLastError(), "launch step");
     });

@@ -228,7 +228,8 @@ int dsx_grid_halo_backward(dsx_grid* grid, const double* ghost_cot_x,
  * half) on first use and replays them; the callback must then only enqueue
  * work on `stream` that reads counts from the view's device arrays.  The
  * callback must be idempotent: a step whose ghost build overflowed is redone
- * after the capacity grows.  status (optional) gets the step's device status
+ * after the capacity grows.  Capture needs a created stream (not the default
+ * stream; DSX_E_INVALID).  status (optional) gets the step's device status
  * bits (0 == ok). */
 typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view* view);
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,

@@ -423,3 +423,90 @@ def test_batched_step_many_tiles(cuda, fields, particles, box, halo):
     finally:
         a.close()
         b.close()
+
+
+def nan_equal(a, b) -> bool:
+    """Bitwise equality, except that every NaN counts as the same value (a
+    NaN made by inf - inf has the platform's own bits)."""
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    if a.dtype.kind == "f":
+        na, nb = np.isnan(a), np.isnan(b)
+        if not np.array_equal(na, nb):
+            return False
+        a, b = np.where(na, 0.0, a), np.where(nb, 0.0, b)
+    return same(a, b)
+
+
+def test_boundary_values_follow_the_reference(cuda):
+    """Positions on the cut planes, on the box faces, on the halo thresholds,
+    signed zeros, denormals, values far outside the box, infinities and NaN:
+    owners, wrapped positions, ghosts and sums as the reference's Host path
+    makes them."""
+    rng = np.random.default_rng(77)
+    L, h = 10.0, 1.0
+    special = np.array([0.0, -0.0, 5.0, 10.0, h, 5.0 - h, 5.0 + h, 10.0 - h, np.nextafter(5.0, 0),
+                        np.nextafter(5.0, 10), np.nextafter(10.0, 0), np.nextafter(h, 0),
+                        np.nextafter(10.0 - h, 10), -1e-300, 1e-320, 1e300, -1e300, 23.0, -7.5,
+                        np.inf, -np.inf, np.nan])
+    N = 3000
+    data = uniform_particles(rng, N, (0, 0, 0), (L, L, L))
+    for k in "xyz":
+        pick = rng.random(N) < 0.5
+        data[k][pick] = rng.choice(special, pick.sum())
+    empty = {k: v[:0] for k, v in data.items()}
+    pair = Pair(8, (2, 2, 2), "manual", (0, 0, 0), (L, L, L), (True, True, True), h, True, None,
+                (), particles=N)
+    try:
+        pair.upload([data] + [empty] * 7)
+        for step in range(2):
+            pair.gpu.migrate()
+            pair.ref.migrate()
+            pair.gpu.exchange_halo(rebuild=True)
+            pair.ref.exchange_halo(rebuild=True)
+            pair.set_ghost(rng, ["fx", "fy", "fz"])
+            pair.gpu.reverse_halo()
+            pair.ref.reverse_halo()
+            for r in range(8):
+                a, b = pair.gpu.snapshot(r), pair.ref.snapshot(r)
+                assert (a["owned"], a["ghosts"]) == (b["owned"], b["ghosts"]), (step, r)
+                for k in b:
+                    if k not in ("owned", "ghosts"):
+                        assert nan_equal(a[k], b[k]), (step, r, k)
+    finally:
+        pair.close()
+
+
+def test_empty_grid(cuda):
+    """No particles at all: every call and the batched step run and stay empty."""
+    import torch
+
+    import dsdecompx_b200 as dsx
+    kw = dict(nranks=8, dims=(2, 2, 2), lower=(0, 0, 0), upper=(10, 10, 10), halo_width=1.0,
+              particles=0)
+    pair = Pair(**kw)
+    g = dsx.VirtualGrid(**kw)
+    try:
+        empty = uniform_particles(np.random.default_rng(1), 0, (0, 0, 0), (10, 10, 10))
+        pair.upload([empty] * 8)
+        g.upload([empty] * 8)
+        assert (pair.gpu.migrate() == pair.ref.migrate()).all()
+        pair.gpu.exchange_halo(rebuild=True)
+        pair.ref.exchange_halo(rebuild=True)
+        pair.gpu.reverse_halo()
+        pair.ref.reverse_halo()
+        pair.compare("empty")
+        assert g.autotune()["ghost_capacity"] >= 0
+        side = torch.cuda.Stream()
+        for capture in (False, True, True):
+            with torch.cuda.stream(side):
+                assert g.step(None, capture=capture, stream=side.cuda_stream) == 0
+            side.synchronize()
+        with pytest.raises(ValueError, match="created stream"):
+            g.step(None, capture=True)
+        o, gh = g.all_counts()
+        assert o.sum() == 0 and gh.sum() == 0
+    finally:
+        pair.close()
+        g.close()

@@ -137,3 +137,71 @@ def test_port_matches_reference_rebalance():
         compare(a, b, 8, "rebalance")
     a.close()
     b.close()
+
+
+def boundary_data(rng, N, L, h):
+    """Uniform particles whose coordinates are, half of the time, one of the
+    delicate values: cut planes, box faces, halo thresholds and their
+    neighbours in FP64, signed zeros, denormals, far-away values, infinities
+    and NaN."""
+    special = np.array([0.0, -0.0, L / 2, L, h, L / 2 - h, L / 2 + h, L - h,
+                        np.nextafter(L / 2, 0), np.nextafter(L / 2, L), np.nextafter(L, 0),
+                        np.nextafter(h, 0), np.nextafter(L - h, L), -1e-300, 1e-320, 1e300,
+                        -1e300, 2.3 * L, -0.75 * L, np.inf, -np.inf, np.nan])
+    data = uniform_particles(rng, N, (0, 0, 0), (L, L, L))
+    for k in "xyz":
+        pick = rng.random(N) < 0.5
+        data[k][pick] = rng.choice(special, pick.sum())
+    return data
+
+
+def nan_equal(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    if a.dtype.kind == "f":
+        na, nb = np.isnan(a), np.isnan(b)
+        if not np.array_equal(na, nb):
+            return False
+        a, b = np.where(na, 0.0, a), np.where(nb, 0.0, b)
+    return same(a, b)
+
+
+@needs_ref
+def test_boundary_values_port_vs_reference():
+    """The restatement and the reference agree on the delicate inputs too
+    (the reference's release build: its debug invariants stop on particles
+    that belong to no subdomain, such as NaN positions)."""
+    rng = np.random.default_rng(77)
+    L, h, N, P = 10.0, 1.0, 3000, 8
+    a, b = make_pair("port", "ref", nranks=P, dims=(2, 2, 2), policy="manual", lower=(0, 0, 0),
+                     upper=(L, L, L), periodic=(True, True, True), halo_width=h,
+                     edges_and_corners=True, dynamic=None, fields=[], field_capacity=4 * N + 64)
+    try:
+        data = boundary_data(rng, N, L, h)
+        empty = {k: v[:0] for k, v in data.items()}
+        for g in (a, b):
+            g.set_owned(0, data)
+            for r in range(1, P):
+                g.set_owned(r, empty)
+        for step in range(2):
+            assert (a.migrate() == b.migrate()).all()
+            a.exchange_halo(rebuild=True)
+            b.exchange_halo(rebuild=True)
+            for r in range(P):
+                o, g_ = a.counts(r)
+                f = rng.normal(size=g_)
+                for name in ("fx", "fy", "fz"):
+                    a.write(r, name, o, f)
+                    b.write(r, name, o, f)
+            a.reverse_halo()
+            b.reverse_halo()
+            for r in range(P):
+                x, y = a.snapshot(r), b.snapshot(r)
+                assert (x["owned"], x["ghosts"]) == (y["owned"], y["ghosts"]), (step, r)
+                for k in x:
+                    if k not in ("owned", "ghosts"):
+                        assert nan_equal(x[k], y[k]), (step, r, k)
+    finally:
+        a.close()
+        b.close()
