@@ -63,7 +63,7 @@ class _FieldDesc(C.Structure):
 class TuneReport(C.Structure):
     _fields_ = [("classify_threads", C.c_int), ("move_staged", C.c_int),
                 ("reverse_ctas_per_sm", C.c_int), ("ghost_capacity", C.c_longlong),
-                ("classify_ms", C.c_float * 3), ("move_ms", C.c_float * 2),
+                ("classify_ms", C.c_float * 3), ("move_ms", C.c_float * 3),
                 ("reverse_ms", C.c_float * 4)]
 
 
@@ -432,12 +432,14 @@ class VirtualGrid:
         choices and the measured milliseconds per launch."""
         r = TuneReport()
         _check(self.L.dsx_grid_autotune(self.h, _stream(stream), C.byref(r)))
-        return {"classify_threads": r.classify_threads, "move_staged": bool(r.move_staged),
+        kinds = {0: "direct", 1: "staged", 2: "staged passes"}
+        return {"classify_threads": r.classify_threads, "move": kinds.get(r.move_staged, "?"),
                 "reverse_ctas_per_sm": r.reverse_ctas_per_sm,
                 "ghost_capacity": int(r.ghost_capacity),
                 "classify_ms": {n: round(float(v), 4) for n, v in zip((64, 128, 256), r.classify_ms)},
                 "move_ms": {"staged": round(float(r.move_ms[0]), 4),
-                            "direct": round(float(r.move_ms[1]), 4)},
+                            "direct": round(float(r.move_ms[1]), 4),
+                            "staged passes": round(float(r.move_ms[2]), 4)},
                 "reverse_ms": {n: round(float(v), 4) for n, v in zip((4, 8, 16, 32), r.reverse_ms)}}
 
     def set_plain(self, plain: bool = True):

@@ -912,13 +912,16 @@ struct dsx_grid {
                 grids(G, Gn);
             }
             const long long gho = ghost_off();
-            const int kinds[2] = {1, 0};
-            for (int i = 0; i < 2; ++i) {
-                if (kinds[i] == 1 && !dsx::staged_move_fits(A)) continue;
+            // staged, direct reads, staged in passes
+            const int kinds[3] = {1, 0, 2};
+            const int bits[3] = {2, 1, 4};
+            const int modes = dsx::staged_move_modes(A);
+            for (int i = 0; i < 3; ++i) {
+                if (!(modes & bits[i])) continue;
                 S.move_staged = kinds[i];
                 r.move_ms[i] = time([&] { dsx::launch_step_move(G, A, src, dst, gho, S, stream); });
             }
-            S.move_staged = pick(r.move_ms, kinds, 2, 1);
+            S.move_staged = pick(r.move_ms, kinds, 3, 1);
             dsx::launch_step_move(G, A, src, dst, gho, S, stream);
             dsx::launch_step_finish(G, Gn, A, src, dst, gho, S, stream);
             // the reverse sum into the next half's forces from the ghost
@@ -946,7 +949,7 @@ struct dsx_grid {
             destroy_graphs();
         }
         r.classify_threads = S.classify_threads;
-        r.move_staged = S.move_staged && dsx::staged_move_fits(A) ? 1 : 0;
+        r.move_staged = S.move_staged;
         r.reverse_ctas_per_sm = S.reverse_per_sm;
         r.ghost_capacity = gcap;
         if (out) *out = r;

@@ -1408,17 +1408,17 @@ __device__ __forceinline__ void ghost_from_stage(const Grid& G, const Arrays& A,
 }
 
 // Warp 0 issues the bulk copies of elements [first, last) of a tile into a
-// shared-memory buffer: lane k copies array k of the record and stores in
-// seg[k] where element 0 landed.  Lane 0 announces the byte total on the
+// shared-memory buffer: lane k copies array a0 + k of the record (arrays
+// [a0, a1)) and stores in seg[k] where element 0 landed.  Lane 0 announces the byte total on the
 // mbarrier before any copy starts.
 __device__ __forceinline__ void stage_issue(const Arrays& A, long long src_off, int first,
                                             int last, unsigned char* stage, unsigned bar,
-                                            int* seg, int lane) {
+                                            int* seg, int lane, int a0, int a1) {
     int b = 0;
     const unsigned char* base = nullptr;
-    if (lane < 13 + A.f.count) {
-        b = array_bytes(A, lane);
-        base = array_base(A, lane);
+    if (a0 + lane < a1) {
+        b = array_bytes(A, a0 + lane);
+        base = array_base(A, a0 + lane);
     }
     const int size = b ? TILE * b + 32 : 0;
     const int soff = warp_inclusive_sum(size) - size;
@@ -1452,6 +1452,38 @@ __device__ __forceinline__ int tile_base(const Grid& G, const int* pre, int stri
     return pre[k * stride + g];
 }
 
+// Array k of staged record l to owned slot dst (positions wrapped): the
+// per-array form of move_from_stage for a move split into several passes.
+__device__ __forceinline__ void move_array_from_stage(const Grid& G, const Arrays& A,
+                                                      const unsigned char* rec, int seg, int k,
+                                                      int l, long long dst) {
+    if (k < 11) {
+        const double v = srd(rec, seg, l);
+        A.d[k][dst] = k < 3 ? wrap_if(G, k, v) : v;
+    } else if (k < 13) {
+        (k == 11 ? A.type : A.gid)[dst] = sri(rec, seg, l);
+    } else {
+        const int b = A.f.bytes[k - 13];
+        const unsigned* src = reinterpret_cast<const unsigned*>(rec + seg + l * b);
+        unsigned* out = reinterpret_cast<unsigned*>(A.f.base[k - 13] + dst * b);
+        for (int w = 0; w < (b >> 2); ++w) out[w] = src[w];
+    }
+}
+
+// Array k of the ghost image of staged record l (position + shift, zero
+// force, the rest copied).
+__device__ __forceinline__ void ghost_array_from_stage(const Grid& G, const Arrays& A,
+                                                       const unsigned char* rec, int seg, int k,
+                                                       int l, long long gi, const double* sh) {
+    if (k < 3) {
+        A.d[k][gi] = __dadd_rn(wrap_if(G, k, srd(rec, seg, l)), sh[k]);
+    } else if (k >= 6 && k < 9) {
+        A.d[k][gi] = 0.0;
+    } else {
+        move_array_from_stage(G, A, rec, seg, k, l, gi);
+    }
+}
+
 // Counter bases of every tile of the layout (30 per tile, row stride 32), so
 // that the move reads them with one load per tile.
 __global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int stride,
@@ -1467,11 +1499,18 @@ __global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int s
 // F4 with the tile's records staged in shared memory (same output as
 // k_step_move).  Dynamic shared memory: sum over the arrays of TILE x element
 // bytes + 32.
+//
+// FULL: one pass over the whole record.  Otherwise the pass moves arrays
+// [a0, a1) only (a record too wide for three staged tiles per SM is moved in
+// several passes); every pass redoes the index work from the destinations
+// and masks, and only the pass with index_outputs writes its results.
+template <bool FULL>
 __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     Grid G, Arrays A, long long src_off, long long dst_off, long long ghost_off, const int* pre,
     int stride, const int* cbase_ret, const unsigned short* __restrict__ dest_in,
     const unsigned* __restrict__ mask_in, const int* __restrict__ tile_bases, int* emig_src,
-    int* emig_dst, int* ghost_owner, int* ghost_entry, int* bowner, int* boff, int* bslot) {
+    int* emig_dst, int* ghost_owner, int* ghost_entry, int* bowner, int* boff, int* bslot, int a0,
+    int a1, int index_outputs) {
     extern __shared__ __align__(16) unsigned char s_rec[];
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ int s_seg[kStagedArrays];
@@ -1505,7 +1544,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         __syncwarp();
-        stage_issue(A, src_off, begin, end, s_rec, bar, s_seg, lane);
+        stage_issue(A, src_off, begin, end, s_rec, bar, s_seg, lane, a0, a1);
     }
     // (slots past the tile's end hold stale values: masked here; the mask
     // is only meaningful for a stay)
@@ -1573,7 +1612,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         nis[j] = ni;
         if (stay) {
             s_ni[l] = ni;
-        } else if (emig) {
+        } else if (emig && index_outputs) {
             emig_src[eb] = i;
             emig_dst[eb] = dest[j];
         }
@@ -1584,7 +1623,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
             const int pm = __popc(mj);
             const int incl = warp_inclusive_sum(pm);
             const int img = __shfl_sync(0xffffffffu, run, kImageCounter) + incl - pm;
-            if (mj) {
+            if (mj && index_outputs) {
                 bowner[b] = ni;
                 boff[b] = img;
             }
@@ -1597,7 +1636,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
                 const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
                 if ((mj >> n) & 1u) {
                     const int rank = __popc(hit & lt);
-                    bslot[img + k] = list_base + rank;
+                    if (index_outputs) bslot[img + k] = list_base + rank;
                     ++k;
                     if (staged) s_own[stage_base + rank] = static_cast<unsigned short>(l);
                 }
@@ -1623,11 +1662,19 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     }
     int sg[13];
 #pragma unroll
-    for (int a = 0; a < 13; ++a) sg[a] = s_seg[a];
+    for (int a = 0; a < 13; ++a) sg[a] = FULL ? s_seg[a] : 0;
     const int* fseg = s_seg + 13;
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j)
-        if (dest[j] == s) move_from_stage(G, A, s_rec, sg, fseg, wbegin + j * 32 + lane - begin, dst_off + nis[j]);
+    for (int j = 0; j < ITEMS; ++j) {
+        if (dest[j] != s) continue;
+        const int l = wbegin + j * 32 + lane - begin;
+        if (FULL) {
+            move_from_stage(G, A, s_rec, sg, fseg, l, dst_off + nis[j]);
+        } else {
+            for (int c = a0; c < a1; ++c)
+                move_array_from_stage(G, A, s_rec, s_seg[c - a0], c, l, dst_off + nis[j]);
+        }
+    }
     if (!ghosts) return;
     const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
     if (staged) {
@@ -1642,9 +1689,17 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
             const int n = lo;
             const int slot = s_base[n] + (q - s_off[n]);
             const int l = s_own[q];
-            ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
-            ghost_owner[slot] = s_ni[l];
-            ghost_entry[slot] = s * kMaxNeighbors + n;
+            if (FULL) {
+                ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
+            } else {
+                for (int c = a0; c < a1; ++c)
+                    ghost_array_from_stage(G, A, s_rec, s_seg[c - a0], c, l, ghost_off + slot,
+                                           shift + 3 * n);
+            }
+            if (index_outputs) {
+                ghost_owner[slot] = s_ni[l];
+                ghost_entry[slot] = s * kMaxNeighbors + n;
+            }
         }
         return;
     }
@@ -1662,9 +1717,17 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
             const int list_base = __shfl_sync(0xffffffffu, run, n);
             if ((mj >> n) & 1u) {
                 const int slot = list_base + __popc(hit & lt);
-                ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
-                ghost_owner[slot] = nis[j];
-                ghost_entry[slot] = s * kMaxNeighbors + n;
+                if (FULL) {
+                    ghost_from_stage(G, A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
+                } else {
+                    for (int c = a0; c < a1; ++c)
+                        ghost_array_from_stage(G, A, s_rec, s_seg[c - a0], c, l, ghost_off + slot,
+                                               shift + 3 * n);
+                }
+                if (index_outputs) {
+                    ghost_owner[slot] = nis[j];
+                    ghost_entry[slot] = s * kMaxNeighbors + n;
+                }
             }
             if (lane == n) run += __popc(hit);
         }
@@ -2106,11 +2169,33 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long
     if (S.marks) S.marks->mark(s, "halo_scatter");
 }
 
-// Shared memory the staged move needs for one tile of every array.
-int staged_bytes(const Arrays& A) {
-    int bytes = 11 * (TILE * 8 + 32) + 2 * (TILE * 4 + 32);
-    for (int k = 0; k < A.f.count; ++k) bytes += TILE * A.f.bytes[k] + 32;
+// Shared memory the staged move needs for one tile of arrays [a0, a1).
+int staged_range_bytes(const Arrays& A, int a0, int a1) {
+    int bytes = 0;
+    for (int k = a0; k < a1; ++k) bytes += TILE * (k < 11 ? 8 : k < 13 ? 4 : A.f.bytes[k - 13]) + 32;
     return bytes;
+}
+
+int staged_bytes(const Arrays& A) { return staged_range_bytes(A, 0, 13 + A.f.count); }
+
+// A staged pass holds at most this much of the record, so that three CTAs
+// (their tiles in flight at once) fit an SM's shared memory.
+constexpr int kStagedPassBytes = 56 * 1024;
+
+// Consecutive array groups of at most kStagedPassBytes; false if one array
+// alone is wider.
+bool staged_passes(const Arrays& A, int* ends, int& passes) {
+    const int narrays = 13 + A.f.count;
+    passes = 0;
+    int start = 0;
+    while (start < narrays) {
+        int end = start;
+        while (end < narrays && staged_range_bytes(A, start, end + 1) <= kStagedPassBytes) ++end;
+        if (end == start || passes == kStagedArrays) return false;
+        ends[passes++] = end;
+        start = end;
+    }
+    return true;
 }
 
 void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, const Scratch& S,
@@ -2148,22 +2233,52 @@ void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s) {
         G, S.pre, S.stride, S.cbase, S.tile_bases);
 }
 
-bool staged_move_fits(const Arrays& A) { return staged_bytes(A) <= kStagedMaxBytes; }
+int staged_move_modes(const Arrays& A) {
+    int ends[kStagedArrays], passes = 0;
+    const bool split = staged_passes(A, ends, passes);
+    const bool one = staged_bytes(A) <= kStagedMaxBytes;
+    int modes = 1;   // direct reads always apply
+    if (one || split) modes |= 2;
+    if (one && split && passes > 1) modes |= 4;   // passes as an alternative to one pass
+    return modes;
+}
 
 void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
                       long long ghost_off, const Scratch& S, cudaStream_t s) {
-    const int staged = staged_bytes(A);
-    if (S.move_staged && staged <= kStagedMaxBytes) {
-        static bool attribute_set = false;   // once per process (one device per process)
-        if (!attribute_set) {
-            cudaFuncSetAttribute(k_step_move_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kStagedMaxBytes);
-            attribute_set = true;
+    static bool attribute_set = false;   // once per process (one device per process)
+    if (!attribute_set) {
+        cudaFuncSetAttribute(k_step_move_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kStagedMaxBytes);
+        cudaFuncSetAttribute(k_step_move_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kStagedMaxBytes);
+        attribute_set = true;
+    }
+    const int narrays = 13 + A.f.count;
+    const int whole = staged_bytes(A);
+    int ends[kStagedArrays], passes = 0;
+    const bool split = staged_passes(A, ends, passes);
+    auto staged = [&](bool full, int a0, int a1, int index_outputs) {
+        const int bytes = staged_range_bytes(A, a0, a1);
+        if (full)
+            k_step_move_staged<true><<<G.max_tiles, NT, bytes, s>>>(
+                G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
+                S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
+                S.boff, S.bslot, a0, a1, index_outputs);
+        else
+            k_step_move_staged<false><<<G.max_tiles, NT, bytes, s>>>(
+                G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
+                S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
+                S.boff, S.bslot, a0, a1, index_outputs);
+    };
+    if (S.move_staged == 1 && whole <= kStagedMaxBytes) {
+        staged(true, 0, narrays, 1);
+    } else if (S.move_staged != 0 && split) {
+        if (passes == 1) {
+            staged(true, 0, narrays, 1);
+        } else {
+            for (int p = 0, a0 = 0; p < passes; a0 = ends[p++])
+                staged(false, a0, ends[p], p == 0 ? 1 : 0);
         }
-        k_step_move_staged<<<G.max_tiles, NT, staged, s>>>(
-            G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
-            S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
-            S.bslot);
     } else {
         k_step_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
                                                S.cbase, S.dest16, S.mask, S.emig_src, S.emig_dst,

@@ -65,7 +65,7 @@ struct Scratch {
     Marks* marks = nullptr;
     // launch shapes the autotuner picks (these defaults are the untuned choice)
     int classify_threads = 128;   // threads per 512-particle tile of the step classify: 64/128/256
-    int move_staged = 1;          // 1: tile records staged by bulk copies (if they fit), 0: direct reads
+    int move_staged = 1;          // 1: staged (one pass if it fits), 2: staged in passes, 0: direct reads
     int reverse_per_sm = 0;       // CTAs per SM of the reverse sum; 0: one wave of the default shape
 };
 
@@ -104,8 +104,11 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
                       long long ghost_off, const Scratch& S, cudaStream_t s);
 void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
                         long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s);
-// Whether the staged move can hold one tile of this record.
-bool staged_move_fits(const Arrays& A);
+// Move kinds that apply to this record, as bits: 1 direct reads (kind 0),
+// 2 staged (kind 1: one pass when a tile of the record fits 100 KB of shared
+// memory, else passes of at most 56 KB), 4 staged in passes although one
+// pass fits (kind 2).
+int staged_move_modes(const Arrays& A);
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off,
                          long long ghost_off, bool positions_only, const Scratch& S,

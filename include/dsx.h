@@ -239,8 +239,9 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
  * particles: times each candidate by replaying the step's idempotent parts
  * (nothing of the current owned half changes) and keeps the fastest --
  * the classify pass's threads per 512-particle tile (64, 128, 256), the move
- * with its tile records staged in shared memory by bulk copies or read
- * directly, the reverse sum's CTAs per SM (4, 8, 16, 32) -- and sizes the
+ * with its tile records staged in shared memory by bulk copies (in one pass
+ * of up to 100 KB per tile, or in passes of at most 56 KB) or read directly, the
+ * reverse sum's CTAs per SM (4, 8, 16, 32) -- and sizes the
  * ghost region to at least 1.25x the ghosts of the current particles (the
  * per-neighbour send lists are slices of it).  Afterwards the halo plan is
  * invalid (call exchange_halo or step next) and captured steps are
@@ -249,11 +250,11 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
  * one subdomain has nothing to tune and keeps the defaults. */
 typedef struct dsx_tune_report {
     int classify_threads;
-    int move_staged;
+    int move_staged;         /* 1 staged (one pass if it fits), 2 staged in passes, 0 direct reads */
     int reverse_ctas_per_sm;
     long long ghost_capacity;
     float classify_ms[3];    /* 64, 128, 256 threads per tile */
-    float move_ms[2];        /* staged, direct reads */
+    float move_ms[3];        /* staged, direct reads, staged in passes */
     float reverse_ms[4];     /* 4, 8, 16, 32 CTAs per SM */
 } dsx_tune_report;
 int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report);

@@ -365,16 +365,18 @@ def test_halo_backward_is_reverse_halo(cuda):
 
 
 @pytest.mark.parametrize("fields,particles,box,halo", [
+    (ALL_FIELDS[:1], 300_000, 12.0, 0.6),
     (ALL_FIELDS[:2], 300_000, 12.0, 0.6),
     (ALL_FIELDS, 40_000, 12.0, 0.6),
-    (ALL_FIELDS[:2], 20_000, 6.0, 1.1)], ids=["staged-record", "wide-record", "wide-halo"])
+    (ALL_FIELDS[:2], 20_000, 6.0, 1.1)],
+    ids=["record-104B", "record-116B", "record-204B", "wide-halo"])
 def test_batched_step_many_tiles(cuda, fields, particles, box, halo):
     """The batched step against the per-call path and the oracle with far
-    more 512-particle tiles than SMs, once with a record that the move stages
-    in shared memory, once with a record too wide to stage (the move then
-    reads HBM directly), and once with a halo wider than half a cell (every
-    particle has 26 images, more than a tile stages: they are written from
-    the hitting lanes)."""
+    more 512-particle tiles than SMs: records the move stages in one pass
+    (104 B and 116 B per particle), a record too wide for one pass (204 B:
+    two passes of at most 56 KB per tile), and a halo wider than half a cell
+    (every particle has 26 images, more than a tile stages: they are written
+    from the hitting lanes)."""
     import torch
 
     import dsdecompx_b200 as dsx
