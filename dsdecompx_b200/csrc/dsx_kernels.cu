@@ -911,13 +911,33 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
     __syncthreads();
     const unsigned* lut = s_lut;
     const int nn = G.nn[s];
+    // with every periodic axis starting at 0, a coordinate inside its own
+    // cell needs no wrap arithmetic: both Host wraps return it (a -0 as +0)
+    const bool simple = (!G.periodic[0] || G.lower[0] == 0.0) &&
+                        (!G.periodic[1] || G.lower[1] == 0.0) &&
+                        (!G.periodic[2] || G.lower[2] == 0.0);
     int acc = 0;
 #pragma unroll
     for (int j = 0; j < CI; ++j) {
         const int i = wbegin + j * 32 + lane;
+        const bool valid = i < end;
+        const bool own = valid && simple && cell.lo[0] <= px[j] && px[j] < cell.hi[0] &&
+                         cell.lo[1] <= py[j] && py[j] < cell.hi[1] && cell.lo[2] <= pz[j] &&
+                         pz[j] < cell.hi[2];
         int d = -1;
         unsigned m = 0;
-        if (i < end) {
+        if (__all_sync(0xffffffffu, own || !valid)) {
+            // the whole group stays: destination s, mask of the own subdomain
+            if (valid) {
+                d = s;
+                const double wx = G.periodic[0] && px[j] == 0.0 ? 0.0 : px[j];
+                const double wy = G.periodic[1] && py[j] == 0.0 ? 0.0 : py[j];
+                const double wz = G.periodic[2] && pz[j] == 0.0 ? 0.0 : pz[j];
+                m = halo_mask(bs, lut, wx, wy, wz);
+                dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(d);
+                mask_out[static_cast<long long>(g) * TILE + (i - begin)] = m;
+            }
+        } else if (valid) {
             double wx, wy, wz;
             d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
             dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(d);
