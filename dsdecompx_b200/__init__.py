@@ -125,6 +125,8 @@ def lib() -> C.CDLL:
             "dsx_grid_step_kernel_count": [vp],
             "dsx_grid_profile": [vp, C.c_int],
             "dsx_grid_set_plain": [vp, C.c_int],
+            "dsx_grid_set_cuts": [vp, C.POINTER(C.c_double), vp],
+            "dsx_grid_rescale_domain": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, vp],
             "dsx_grid_autotune": [vp, vp, vp],
             "dsx_grid_kernel_times": [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)],
         }
@@ -441,6 +443,21 @@ class VirtualGrid:
                             "direct": round(float(r.move_ms[1]), 4),
                             "staged passes": round(float(r.move_ms[2]), 4)},
                 "reverse_ms": {n: round(float(v), 4) for n, v in zip((4, 8, 16, 32), r.reverse_ms)}}
+
+    def set_cuts(self, cuts: Sequence[Sequence[float]], stream=None):
+        """Replaces the cut planes (three increasing arrays spanning the box,
+        dims[a] + 1 values each); the halo plan becomes invalid."""
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(c, np.float64) for c in cuts]))
+        _check(self.L.dsx_grid_set_cuts(self.h, flat.ctypes.data_as(C.POINTER(C.c_double)),
+                                        _stream(stream)))
+
+    def rescale_domain(self, lower, upper, update: bool = False, stream=None):
+        """New box: cut planes keep their fractions, periodic shifts follow.
+        update=False (Decomp::rescale_domain) keeps the halo plan;
+        update=True (Decomp::update_domain) invalidates it."""
+        lo = (C.c_double * 3)(*lower)
+        hi = (C.c_double * 3)(*upper)
+        _check(self.L.dsx_grid_rescale_domain(self.h, lo, hi, 1 if update else 0, _stream(stream)))
 
     def set_plain(self, plain: bool = True):
         """Per-call operations launch their tile kernels once per subdomain

@@ -849,6 +849,68 @@ struct dsx_grid {
         cur ^= 1;
     }
 
+    // Decomposition::set_axis_cuts (dsDecompX src/decomp.cpp:146-163): the
+    // cuts must span the domain and increase strictly; the plan is invalid.
+    void set_cuts(const double* host, cudaStream_t stream) {
+        int total_cuts = 0;
+        for (int a = 0; a < 3; ++a) {
+            const double* c = host + total_cuts;
+            bool ok = c[0] == desc.lower[a] && c[dims[a]] == desc.upper[a];
+            for (int i = 0; i < dims[a]; ++i) ok = ok && c[i] < c[i + 1];
+            if (!ok) fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");
+            total_cuts += dims[a] + 1;
+        }
+        cuda_check(cudaStreamSynchronize(stream), "synchronize before new cuts");
+        cuda_check(cudaMemcpy(cuts, host, sizeof(double) * total_cuts, cudaMemcpyHostToDevice), "upload cuts");
+        plan_valid = false;
+        ghosts_valid = false;
+    }
+
+    // Decomposition::rescale_domain / update_domain (dsDecompX
+    // src/decomp.cpp:104-144): every cut keeps its fraction of the extent and
+    // the periodic shifts follow the new extent; rescale keeps the halo plan
+    // (same grid, same neighbours: a refresh uses the new shifts), update
+    // invalidates it.  Positions are the caller's.
+    void rescale_domain(const double* lower, const double* upper, bool invalidate,
+                        cudaStream_t stream) {
+        for (int a = 0; a < 3; ++a)
+            if (!(upper[a] > lower[a])) fail(DSX_E_INVALID, "global-domain extent must be positive");
+        const int total_cuts = dims[0] + dims[1] + dims[2] + 3;
+        std::vector<double> c(static_cast<std::size_t>(total_cuts));
+        cuda_check(cudaStreamSynchronize(stream), "synchronize before rescale");
+        cuda_check(cudaMemcpy(c.data(), cuts, sizeof(double) * total_cuts, cudaMemcpyDeviceToHost), "read cuts");
+        for (int a = 0, off = 0; a < 3; off += dims[a] + 1, ++a) {
+            const double old_extent = desc.upper[a] - desc.lower[a];
+            const double new_extent = upper[a] - lower[a];
+            for (int i = 0; i <= dims[a]; ++i) {
+                double& cut = c[static_cast<std::size_t>(off + i)];
+                const double fraction = (cut - desc.lower[a]) / old_extent;
+                cut = lower[a] + fraction * new_extent;
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            desc.lower[a] = lower[a];
+            desc.upper[a] = upper[a];
+        }
+        cuda_check(cudaMemcpy(cuts, c.data(), sizeof(double) * total_cuts, cudaMemcpyHostToDevice), "upload cuts");
+        build_topology();
+        const int E = dsx::kMaxNeighbors;
+        std::vector<double> shift(static_cast<std::size_t>(P) * E * 3, 0.0);
+        for (int s = 0; s < P; ++s) {
+            const auto& list = topo[static_cast<std::size_t>(s)];
+            for (std::size_t n = 0; n < list.size(); ++n)
+                for (int a = 0; a < 3; ++a)
+                    shift[3 * (static_cast<std::size_t>(s) * E + n) + a] = list[n].shift[a];
+        }
+        cuda_check(cudaMemcpy(d_shift, shift.data(), sizeof(double) * shift.size(), cudaMemcpyHostToDevice),
+                   "upload shifts");
+        destroy_graphs();   // captured kernels hold the old box
+        if (invalidate) {
+            plan_valid = false;
+            ghosts_valid = false;
+        }
+    }
+
     // Replays the step's idempotent parts on the current particles (the
     // current owned half is only read) and keeps the fastest launch shapes.
     void autotune(cudaStream_t stream, dsx_tune_report* out) {
@@ -1364,6 +1426,21 @@ int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report) {
     return guarded([&] {
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->autotune(static_cast<cudaStream_t>(stream), report);
+    });
+}
+
+int dsx_grid_set_cuts(dsx_grid* grid, const double* cuts, void* stream) {
+    return guarded([&] {
+        if (!grid || !cuts) fail(DSX_E_INVALID, "null argument");
+        grid->set_cuts(cuts, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_rescale_domain(dsx_grid* grid, const double* lower, const double* upper,
+                            int invalidate_plan, void* stream) {
+    return guarded([&] {
+        if (!grid || !lower || !upper) fail(DSX_E_INVALID, "null argument");
+        grid->rescale_domain(lower, upper, invalidate_plan != 0, static_cast<cudaStream_t>(stream));
     });
 }
 

@@ -235,6 +235,22 @@ typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view*
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
                   void* stream, unsigned* status);
 
+/* Cut planes (Decomposition::set_axis_cuts, dsDecompX src/decomp.cpp:146-163):
+ * cuts holds axis 0, 1, 2 concatenated, dims[a] + 1 values each, as
+ * dsx_grid_cuts returns them; they must span the domain and increase
+ * strictly (DSX_E_INVALID otherwise).  The halo plan becomes invalid. */
+int dsx_grid_set_cuts(dsx_grid* grid, const double* cuts, void* stream);
+
+/* New box (Decomp::rescale_domain and update_domain, dsDecompX
+ * src/decomp.cpp:104-144, src/runtime.cpp:843-849): every cut plane keeps
+ * its fraction of the extent and the periodic shifts follow the new extent.
+ * invalidate_plan == 0 (rescale_domain) keeps the halo plan, so a refreshing
+ * exchange_halo moves the ghosts with the new shifts; != 0 (update_domain)
+ * invalidates it.  Periodicity cannot change; particle positions are the
+ * caller's to rescale. */
+int dsx_grid_rescale_domain(dsx_grid* grid, const double* lower, const double* upper,
+                            int invalidate_plan, void* stream);
+
 /* Autotuning of the batched step's launch shapes on the grid's current
  * particles: times each candidate by replaying the step's idempotent parts
  * (nothing of the current owned half changes) and keeps the fastest --

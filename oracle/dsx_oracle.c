@@ -716,6 +716,54 @@ int orc_invalidate_halo(orc_grid* g) {
     return 0;
 }
 
+/* Decomposition::set_axis_cuts (dsDecompX src/decomp.cpp:146-163): the cuts
+   must span the domain and increase strictly; the geometry is refreshed and
+   the halo plan invalid. */
+int orc_set_cuts(orc_grid* g, const double* cuts) {
+    int off = 0;
+    for (int a = 0; a < 3; ++a) {
+        const double* c = cuts + off;
+        int ok = c[0] == g->lower[a] && c[g->dims[a]] == g->upper[a];
+        for (int i = 0; i < g->dims[a]; ++i) ok = ok && c[i] < c[i + 1];
+        if (!ok) return fail(g, "dynamic cuts must be strictly increasing and span the domain");
+        off += g->dims[a] + 1;
+    }
+    off = 0;
+    for (int a = 0; a < 3; ++a) {
+        for (int i = 0; i <= g->dims[a]; ++i) g->cuts[a][i] = cuts[off + i];
+        off += g->dims[a] + 1;
+    }
+    refresh_geometry(g);
+    return 0;
+}
+
+/* Decomposition::rescale_domain / update_domain (dsDecompX
+   src/decomp.cpp:104-144): every cut keeps its fraction of the extent, the
+   neighbours' periodic shifts follow the new extent; rescale keeps the halo
+   plan (same grid, same neighbours), update invalidates it.  Positions are
+   the caller's. */
+int orc_rescale_domain(orc_grid* g, const double* lower, const double* upper, int invalidate) {
+    for (int a = 0; a < 3; ++a) {
+        const double old_extent = g->upper[a] - g->lower[a];
+        const double new_extent = upper[a] - lower[a];
+        for (int i = 0; i <= g->dims[a]; ++i) {
+            const double fraction = (g->cuts[a][i] - g->lower[a]) / old_extent;
+            g->cuts[a][i] = lower[a] + fraction * new_extent;
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        g->lower[a] = lower[a];
+        g->upper[a] = upper[a];
+    }
+    int* valid = malloc(sizeof(int) * (size_t)g->P);
+    for (int s = 0; s < g->P; ++s) valid[s] = g->r[s].plan_valid;
+    refresh_geometry(g);
+    if (!invalidate)
+        for (int s = 0; s < g->P; ++s) g->r[s].plan_valid = valid[s];
+    free(valid);
+    return 0;
+}
+
 /* ---------------- halo (src/halo.cpp) ---------------- */
 
 static void plan_push(rank_t* r, int n, int index, const rec_t* rec) {

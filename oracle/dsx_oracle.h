@@ -68,6 +68,10 @@ int orc_rebalance(orc_grid* g, const double* local_work, int force,
                   long long* results, double* imbalance);
 int orc_set_halo_width(orc_grid* g, double width);
 int orc_invalidate_halo(orc_grid* g);
+/* cuts: axis 0, 1, 2 concatenated (dims[a] + 1 each) */
+int orc_set_cuts(orc_grid* g, const double* cuts);
+/* invalidate != 0: update_domain, else rescale_domain */
+int orc_rescale_domain(orc_grid* g, const double* lower, const double* upper, int invalidate);
 
 #ifdef __cplusplus
 }

@@ -68,11 +68,14 @@ def _lib(kind: str) -> C.CDLL:
             ("rebalance", [vp, dp, C.c_int, llp, dp]),
             ("set_halo_width", [vp, C.c_double]),
             ("invalidate_halo", [vp]),
+            ("rescale_domain", [vp, dp, dp, C.c_int]),
         ]:
             fn = getattr(lib, prefix + name)
             fn.restype = C.c_int
             fn.argtypes = args
         if kind == "port":
+            lib.orc_set_cuts.restype = C.c_int
+            lib.orc_set_cuts.argtypes = [vp, dp]
             lib.orc_reverse_exchange.argtypes = [vp, C.c_int, ip, ip]
             lib.orc_forward_exchange.argtypes = [vp, C.c_int, ip]
         else:
@@ -312,6 +315,22 @@ class Grid:
 
     def invalidate_halo(self):
         self._call("invalidate_halo")
+
+    def set_cuts(self, cuts: Sequence[Sequence[float]]):
+        """Replaces the cut planes (three increasing arrays spanning the
+        domain); the halo plan becomes invalid.  Port only: the reference has
+        no public call for it (it sets cuts inside its rebalance)."""
+        if self.kind != "port":
+            raise OracleError("set_cuts: the reference has no public call for it")
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(c, float) for c in cuts]))
+        self._call("set_cuts", flat.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def rescale_domain(self, lower, upper, update: bool = False):
+        """Decomp::rescale_domain (update=False: the halo plan is kept) or
+        Decomp::update_domain (update=True: the plan is invalidated)."""
+        lo = (C.c_double * 3)(*lower)
+        hi = (C.c_double * 3)(*upper)
+        self._call("rescale_domain", lo, hi, 1 if update else 0)
 
     def timed(self, op: str) -> float:
         """Slowest rank's wall time of one collective call (reference only)."""

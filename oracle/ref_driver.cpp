@@ -452,6 +452,21 @@ int ref_invalidate_halo(void* handle) {
     return run_all(s, [](int, RankState& state) { state.decomp->invalidate_halo(); });
 }
 
+// Decomp::rescale_domain (invalidate == 0) or Decomp::update_domain on every rank.
+int ref_rescale_domain(void* handle, const double* lower, const double* upper, int invalidate) {
+    auto* s = static_cast<Session*>(handle);
+    dsdecompx::GlobalDomain d = s->config.domain;   // periodicity as created
+    for (int a = 0; a < 3; ++a) {
+        d.lower[a] = lower[a];
+        d.upper[a] = upper[a];
+    }
+    s->config.domain = d;
+    return run_all(s, [d, invalidate](int, RankState& state) {
+        if (invalidate) state.decomp->update_domain(d);
+        else state.decomp->rescale_domain(d);
+    });
+}
+
 int ref_owner_rank(void* handle, long long n, const double* positions, int* out) {
     auto* s = static_cast<Session*>(handle);
     const auto& d = *s->ranks[0].decomp;

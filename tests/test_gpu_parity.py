@@ -512,3 +512,107 @@ def test_empty_grid(cuda):
     finally:
         pair.close()
         g.close()
+
+
+def test_set_cuts_follows_the_reference(cuda):
+    """Explicit cut planes (the cuts a Dynamic rebalance would set): owners,
+    ghosts and sums as the oracle makes them; bad cuts are refused."""
+    rng = np.random.default_rng(41)
+    L = (12.0, 10.0, 9.0)
+    pair = Pair(8, (2, 2, 2), "manual", (0, 0, 0), L, (True, True, True), 0.7, True, None,
+                ALL_FIELDS[:2], particles=6000)
+    try:
+        data = uniform_particles(rng, 6000, (0, 0, 0), L, ALL_FIELDS[:2])
+        owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+        pair.upload(split_by_owner(owner, data, 8))
+        for step, cuts in enumerate([([0, 4.5, 12.0], [0, 6.25, 10.0], [0, 3.0, 9.0]),
+                                     ([0, 7.5, 12.0], [0, 2.0, 10.0], [0, 5.5, 9.0])]):
+            pair.gpu.set_cuts(cuts)
+            pair.ref.set_cuts(cuts)
+            for a, b in zip(pair.gpu.cuts(), pair.ref.cuts()):
+                assert same(a, b)
+            pair.displace(rng, 0.2)
+            assert (pair.gpu.migrate() == pair.ref.migrate()).all()
+            pair.gpu.exchange_halo(rebuild=True)
+            pair.ref.exchange_halo(rebuild=True)
+            pair.set_ghost(rng, ["fx", "fy", "fz"])
+            pair.gpu.reverse_halo()
+            pair.ref.reverse_halo()
+            pair.compare(f"cuts {step}")
+        for bad in ([[0, 6.0, 11.0], [0, 5, 10], [0, 4, 9]],     # does not reach the upper face
+                    [[0, 12.0, 12.0], [0, 5, 10], [0, 4, 9]],    # not strictly increasing
+                    [[0.5, 6.0, 12.0], [0, 5, 10], [0, 4, 9]]):  # does not start at the lower face
+            with pytest.raises(ValueError):
+                pair.gpu.set_cuts(bad)
+    finally:
+        pair.close()
+
+
+def test_rescale_and_update_domain_follow_the_reference(cuda):
+    """A changing box (NPT-like): rescale_domain keeps the halo plan and a
+    refresh moves ghosts with the new periodic shifts, update_domain
+    invalidates the plan; cut planes keep their fractions.  The batched step
+    on a second grid (its captured graphs re-made for the new box) gives the
+    same arrays as the per-call path."""
+    import torch
+
+    import dsdecompx_b200 as dsx
+    rng = np.random.default_rng(6)
+    N = 8000
+    L = np.array([12.0, 10.0, 9.0])
+    kw = dict(nranks=27, dims=(3, 3, 3), lower=(0, 0, 0), upper=tuple(L), halo_width=0.8,
+              fields=ALL_FIELDS[:2], particles=N, ghost_capacity=4 * N)
+    pair = Pair(**kw)
+    twin = dsx.VirtualGrid(**kw)
+    fill = growing_force_filler(torch, 1 << 16)
+    side = torch.cuda.Stream()
+    try:
+        data = uniform_particles(rng, N, (0, 0, 0), tuple(L), ALL_FIELDS[:2])
+        owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+        per = split_by_owner(owner, data, 27)
+        pair.upload(per)
+        twin.upload(per)
+        box = L.copy()
+        for step, (factor, update) in enumerate([(1.02, False), (0.97, True), (1.01, False)]):
+            # per-call path and oracle
+            assert (pair.gpu.migrate() == pair.ref.migrate()).all()
+            pair.gpu.exchange_halo(rebuild=True)
+            pair.ref.exchange_halo(rebuild=True)
+            fill(pair.gpu.view(), torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            for r in range(27):
+                o, g = pair.ref.counts(r)
+                for name in ("fx", "fy", "fz"):
+                    pair.ref.write(r, name, o, pair.gpu.read(r, name, o, g))
+            pair.gpu.reverse_halo()
+            pair.ref.reverse_halo()
+            pair.compare(f"calls {step}")
+            # the same step batched on the twin
+            with torch.cuda.stream(side):
+                assert twin.step(fill, capture=True) == 0
+            side.synchronize()
+            for r in range(27):
+                x, y = pair.gpu.snapshot(r), twin.snapshot(r)
+                for k in x:
+                    assert same(x[k], y[k]), (step, r, k)
+            # new box on all three, positions scaled by the caller
+            new = box * factor
+            pair.gpu.rescale_domain((0, 0, 0), tuple(new), update=update)
+            pair.ref.rescale_domain((0, 0, 0), tuple(new), update=update)
+            twin.rescale_domain((0, 0, 0), tuple(new), update=update)
+            box = new
+            for g_ in (pair.gpu, pair.ref, twin):
+                for r in range(27):
+                    o = g_.counts(r)[0]
+                    for name in "xyz":
+                        g_.write(r, name, 0, g_.read(r, name, 0, o) * factor)
+            for a, b in zip(pair.gpu.cuts(), pair.ref.cuts()):
+                assert same(a, b), step
+            hg, hr = pair.gpu.exchange_halo(), pair.ref.exchange_halo()
+            assert (hg[:, 0] == hr[:, 0]).all()
+            # rescale kept the plan (refreshed in place), update rebuilt it
+            assert (hg[:, 3] == (0 if update else 1)).all()
+            pair.compare(f"{'update' if update else 'rescale'} {step}")
+    finally:
+        pair.close()
+        twin.close()

@@ -205,3 +205,47 @@ def test_boundary_values_port_vs_reference():
     finally:
         a.close()
         b.close()
+
+
+@needs_ref
+@pytest.mark.parametrize("policy,P,dims", [("manual", 8, (2, 2, 2)), ("dynamic", 27, (3, 3, 3))])
+def test_rescale_and_update_domain(policy, P, dims):
+    """Box changes (NPT-like): rescale_domain keeps the halo plan and refreshes
+    ghosts with the new periodic shifts, update_domain invalidates it; cut
+    planes keep their fractions of the extent.  Port vs reference."""
+    rng = np.random.default_rng(5)
+    N = 6000
+    L = (12.0, 10.0, 9.0)
+    dyn = (1.0, 1.01, 0.5, 0.1) if policy == "dynamic" else None
+    a, b = make_pair("port", "ref", nranks=P, dims=dims, policy=policy, lower=(0, 0, 0),
+                     upper=L, periodic=(True, True, True), halo_width=0.8,
+                     edges_and_corners=True, dynamic=dyn, fields=ALL_FIELDS[:2],
+                     field_capacity=4 * N + 64)
+    try:
+        data = uniform_particles(rng, N, (0, 0, 0), L, ALL_FIELDS[:2])
+        owner = b.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+        for r, d in enumerate(split_by_owner(owner, data, P)):
+            a.set_owned(r, d)
+            b.set_owned(r, d)
+        box = np.array(L)
+        for step, (factor, update) in enumerate([(1.02, False), (0.97, True), (1.01, False)]):
+            assert (a.migrate() == b.migrate()).all()
+            a.exchange_halo(rebuild=True)
+            b.exchange_halo(rebuild=True)
+            compare(a, b, P, f"build {step}")
+            new = box * factor
+            for g in (a, b):
+                g.rescale_domain((0.0, 0.0, 0.0), tuple(new), update=update)
+                for r in range(P):
+                    o, _ = g.counts(r)
+                    for k, name in enumerate("xyz"):
+                        g.write(r, name, 0, g.read(r, name, 0, o) * factor)
+            box = new
+            for x, y in zip(a.cuts(), b.cuts()):
+                assert same(x, y), step
+            ha, hb = a.exchange_halo(), b.exchange_halo()
+            assert (ha[:, 0] == hb[:, 0]).all()
+            compare(a, b, P, f"after {'update' if update else 'rescale'} {step}")
+    finally:
+        a.close()
+        b.close()
