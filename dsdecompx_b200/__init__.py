@@ -126,6 +126,8 @@ def lib() -> C.CDLL:
             "dsx_grid_profile": [vp, C.c_int],
             "dsx_grid_set_plain": [vp, C.c_int],
             "dsx_grid_set_cuts": [vp, C.POINTER(C.c_double), vp],
+            "dsx_grid_owner_rank": [vp, vp, vp, vp, C.c_longlong, vp, vp],
+            "dsx_grid_out_of_domain": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
             "dsx_grid_rescale_domain": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, vp],
             "dsx_grid_autotune": [vp, vp, vp],
             "dsx_grid_kernel_times": [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)],
@@ -443,6 +445,22 @@ class VirtualGrid:
                             "direct": round(float(r.move_ms[1]), 4),
                             "staged passes": round(float(r.move_ms[2]), 4)},
                 "reverse_ms": {n: round(float(v), 4) for n, v in zip((4, 8, 16, 32), r.reverse_ms)}}
+
+    def owner_rank(self, x, y, z, out, stream=None):
+        """Owning subdomain of device positions (torch tensors or pointers)
+        into the int32 device array `out`."""
+        ptr = lambda t: t if isinstance(t, int) else t.data_ptr()
+        n = x if isinstance(x, int) else x.numel()
+        _check(self.L.dsx_grid_owner_rank(self.h, ptr(x), ptr(y), ptr(z), n, ptr(out),
+                                          _stream(stream)))
+
+    def out_of_domain(self, stream=None):
+        """(per-subdomain flags, any): owned particles that belong elsewhere."""
+        flags = np.zeros(self.nranks, dtype=np.int32)
+        anyv = C.c_int()
+        _check(self.L.dsx_grid_out_of_domain(self.h, flags.ctypes.data_as(C.POINTER(C.c_int)),
+                                             C.byref(anyv), _stream(stream)))
+        return flags, bool(anyv.value)
 
     def set_cuts(self, cuts: Sequence[Sequence[float]], stream=None):
         """Replaces the cut planes (three increasing arrays spanning the box,

@@ -496,6 +496,7 @@ struct dsx_grid {
         S.mask = device_alloc<unsigned>(fixed_owned, std::max<std::size_t>(slots, static_cast<std::size_t>(ncap)));
         S.dest16 = device_alloc<unsigned short>(fixed_owned, slots);
         S.tile_bases = device_alloc<int>(fixed_owned, static_cast<std::size_t>(max_tiles) * 32);
+        S.out_flags = device_alloc<int>(fixed_owned, P);
         S.list_len = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
         S.send_base = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
         S.g = device_alloc<int>(fixed_owned, P + 1);
@@ -1426,6 +1427,30 @@ int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report) {
     return guarded([&] {
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->autotune(static_cast<cudaStream_t>(stream), report);
+    });
+}
+
+int dsx_grid_owner_rank(dsx_grid* grid, const double* x, const double* y, const double* z,
+                        long long n, int* out, void* stream) {
+    return guarded([&] {
+        if (!grid || n < 0 || (n > 0 && (!x || !y || !z || !out))) fail(DSX_E_INVALID, "null argument");
+        dsx::launch_owner_rank(grid->params(), x, y, z, n, out, static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch owner_rank");
+    });
+}
+
+int dsx_grid_out_of_domain(dsx_grid* grid, int* flags, int* any, void* stream) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const long long o = grid->owned_off();
+        dsx::launch_out_of_domain(grid->params(), grid->A.d[0] + o, grid->A.d[1] + o,
+                                  grid->A.d[2] + o, grid->S.out_flags, s);
+        std::vector<int> f = grid->read_ints(grid->S.out_flags, grid->P, s);
+        int hit = 0;
+        for (int v : f) hit |= v;
+        if (flags) std::copy(f.begin(), f.end(), flags);
+        if (any) *any = hit;
     });
 }
 

@@ -2069,6 +2069,41 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
     if (lane == 0) result[1] = 1.0;
 }
 
+// Decomposition::owner_rank (dsDecompX src/migration.cpp:74-98) of arbitrary
+// positions: one periodic wrap, then the cut bisection.
+__device__ __forceinline__ int owner_of(const Grid& G, double px, double py, double pz) {
+    const double p[3] = {px, py, pz};
+    int c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        c[a] = axis_coordinate(G.cuts + G.cut_offset[a], G.dims[a], wrap_if(G, a, p[a]));
+    return (c[0] * G.dims[1] + c[1]) * G.dims[2] + c[2];
+}
+
+__global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restrict__ x,
+                                                   const double* __restrict__ y,
+                                                   const double* __restrict__ z, long long n,
+                                                   int* out) {
+    for (long long i = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * NT)
+        out[i] = owner_of(G, x[i], y[i], z[i]);
+}
+
+// Decomp::has_out_of_domain_particles (dsDecompX src/runtime.cpp:828-840) for
+// every subdomain at once: flags[s] = 1 if an owned particle of s belongs to
+// another subdomain.
+__global__ void __launch_bounds__(NT) k_out_of_domain(Grid G, const double* __restrict__ x,
+                                                      const double* __restrict__ y,
+                                                      const double* __restrict__ z, int* flags) {
+    const int g = blockIdx.x;
+    const int4 td = G.tiles[g];
+    if (g >= G.tile_start[G.P]) return;
+    bool out = false;
+    for (int i = td.y + threadIdx.x; i < td.z; i += NT)
+        out = out || owner_of(G, x[i], y[i], z[i]) != td.x;
+    if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(&flags[td.x], 1);
+}
+
 // 1-rank migrate of the drop-in: every particle stays and keeps its slot; its
 // position is replaced by the once-wrapped value (dsDecompX
 // src/migration.cpp:106-116).  Only changed values are written back.
@@ -2385,6 +2420,17 @@ void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
 void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
                       long long* call_counter, double* result, cudaStream_t s) {
     k_rebalance<<<1, 32, 0, s>>>(G, work, params, call_counter, result);
+}
+
+void launch_owner_rank(const Grid& G, const double* x, const double* y, const double* z,
+                       long long n, int* out, cudaStream_t s) {
+    if (n > 0) k_owner_rank<<<stream_grid(n), NT, 0, s>>>(G, x, y, z, n, out);
+}
+
+void launch_out_of_domain(const Grid& G, const double* x, const double* y, const double* z,
+                          int* flags, cudaStream_t s) {
+    cudaMemsetAsync(flags, 0, sizeof(int) * G.P, s);
+    k_out_of_domain<<<G.max_tiles, NT, 0, s>>>(G, x, y, z, flags);
 }
 
 void mark(const Scratch& S, cudaStream_t s, const char* what) {

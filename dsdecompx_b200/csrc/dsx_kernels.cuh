@@ -40,6 +40,7 @@ struct Scratch {
     unsigned* mask = nullptr;  // [ncap] halo neighbor mask per owned particle
     unsigned short* dest16 = nullptr;  // [max_tiles * 512] destination per tile slot (fused step)
     int* tile_bases = nullptr;         // [max_tiles * 32] step counter bases per tile
+    int* out_flags = nullptr;          // [P] out-of-domain flags
     int* list_len = nullptr;   // [P*26] send-list lengths
     int* send_base = nullptr;  // [P*26] first ghost slot of each send list
     int* g = nullptr;          // [P] ghosts per receiver
@@ -154,6 +155,14 @@ void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
 // 1-rank drop-in migrate: wraps positions in place (every particle stays).
 void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,
                          const double* extent, const int* periodic, cudaStream_t s);
+
+// owner_rank of n positions (device arrays) into out[n].
+void launch_owner_rank(const Grid& G, const double* x, const double* y, const double* z,
+                       long long n, int* out, cudaStream_t s);
+// flags[s] = 1 if an owned particle of subdomain s (current layout) belongs
+// to another subdomain.
+void launch_out_of_domain(const Grid& G, const double* x, const double* y, const double* z,
+                          int* flags, cudaStream_t s);
 
 // Records a named timing mark on `s` (no-op unless S.marks->on).
 void mark(const Scratch& S, cudaStream_t s, const char* what);

@@ -235,6 +235,18 @@ typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view*
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
                   void* stream, unsigned* status);
 
+/* Owning subdomain of n positions (Decomposition::owner_rank, dsDecompX
+ * src/migration.cpp:74-98: one periodic wrap, then the cut planes): x, y, z
+ * and out are device arrays of n; enqueued on stream. */
+int dsx_grid_owner_rank(dsx_grid* grid, const double* x, const double* y, const double* z,
+                        long long n, int* out, void* stream);
+
+/* Decomp::has_out_of_domain_particles (dsDecompX src/runtime.cpp:828-840)
+ * for every subdomain: flags (optional, host, P ints) gets 1 where an owned
+ * particle belongs to another subdomain, any (optional) their OR -- the
+ * reference's all-rank answer.  Synchronizes stream. */
+int dsx_grid_out_of_domain(dsx_grid* grid, int* flags, int* any, void* stream);
+
 /* Cut planes (Decomposition::set_axis_cuts, dsDecompX src/decomp.cpp:146-163):
  * cuts holds axis 0, 1, 2 concatenated, dims[a] + 1 values each, as
  * dsx_grid_cuts returns them; they must span the domain and increase

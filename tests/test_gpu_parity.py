@@ -616,3 +616,44 @@ def test_rescale_and_update_domain_follow_the_reference(cuda):
     finally:
         pair.close()
         twin.close()
+
+
+def test_owner_rank_and_out_of_domain(cuda):
+    """owner_rank of arbitrary positions (faces, cut planes, far values,
+    infinities, NaN) and the per-subdomain out-of-domain flags, against the
+    oracle's owner rule, before and after a migrate."""
+    import torch
+    rng = np.random.default_rng(9)
+    L = (12.0, 10.0, 9.0)
+    pair = Pair(12, (3, 2, 2), "manual", (0, 0, 0), L, (True, True, False), 0.7, True, None,
+                (), particles=5000)
+    try:
+        data = uniform_particles(rng, 5000, (0, 0, 0), L)
+        owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+        pair.upload(split_by_owner(owner, data, 12))
+        flags, anyv = pair.gpu.out_of_domain()
+        assert not anyv and not flags.any()
+        pair.displace(rng, 0.5)
+        expect = np.zeros(12, dtype=np.int32)
+        for r in range(12):
+            o, _ = pair.ref.counts(r)
+            pos = np.stack([pair.ref.read(r, k, 0, o) for k in "xyz"], 1)
+            expect[r] = int((pair.ref.owner_rank(pos) != r).any()) if o else 0
+        flags, anyv = pair.gpu.out_of_domain()
+        assert (flags == expect).all() and anyv == bool(expect.any())
+        pair.gpu.migrate()
+        pair.ref.migrate()
+        flags, anyv = pair.gpu.out_of_domain()
+        assert not anyv
+        special = np.array([0.0, -0.0, 4.0, 8.0, 12.0, 5.0, 10.0, 9.0, np.nextafter(4.0, 0),
+                            -1e-300, 1e300, -37.5, np.inf, -np.inf, np.nan])
+        pos = rng.uniform(-20, 30, size=(4000, 3))
+        pick = rng.random(pos.shape) < 0.3
+        pos[pick] = rng.choice(special, pick.sum())
+        dev = [torch.as_tensor(np.ascontiguousarray(pos[:, a]), device="cuda") for a in range(3)]
+        out = torch.empty(len(pos), dtype=torch.int32, device="cuda")
+        pair.gpu.owner_rank(*dev, out)
+        torch.cuda.synchronize()
+        assert (out.cpu().numpy() == pair.ref.owner_rank(pos)).all()
+    finally:
+        pair.close()
