@@ -127,6 +127,8 @@ def lib() -> C.CDLL:
             "dsx_grid_set_plain": [vp, C.c_int],
             "dsx_grid_set_cuts": [vp, C.POINTER(C.c_double), vp],
             "dsx_grid_owner_rank": [vp, vp, vp, vp, C.c_longlong, vp, vp],
+            "dsx_grid_begin_halo_exchange": [vp, C.c_int, C.c_int, vp],
+            "dsx_grid_end_halo_exchange": [vp, vp, C.POINTER(C.c_longlong)],
             "dsx_grid_out_of_domain": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
             "dsx_grid_rescale_domain": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, vp],
             "dsx_grid_autotune": [vp, vp, vp],
@@ -445,6 +447,18 @@ class VirtualGrid:
                             "direct": round(float(r.move_ms[1]), 4),
                             "staged passes": round(float(r.move_ms[2]), 4)},
                 "reverse_ms": {n: round(float(v), 4) for n, v in zip((4, 8, 16, 32), r.reverse_ms)}}
+
+    def begin_halo_exchange(self, rebuild: bool = False, positions_only: bool = False, stream=None):
+        """Enqueues the halo refresh or build and returns at once."""
+        _check(self.L.dsx_grid_begin_halo_exchange(self.h, 1 if rebuild else 0,
+                                                   1 if positions_only else 0, _stream(stream)))
+
+    def end_halo_exchange(self, stream=None):
+        """Waits for the exchange begun before; results as exchange_halo's."""
+        res = np.zeros((self.nranks, 4), dtype=np.int64)
+        _check(self.L.dsx_grid_end_halo_exchange(self.h, _stream(stream),
+                                                 res.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return res
 
     def owner_rank(self, x, y, z, out, stream=None):
         """Owning subdomain of device positions (torch tensors or pointers)

@@ -649,6 +649,7 @@ struct dsx_grid {
     }
 
     void migrate(cudaStream_t stream, long long* results, bool automatic_rebalance = true) {
+        not_pending("migrate");
         clear_status(stream);
         if (plain) {
             // the rebalance may move the cut planes but not the layout
@@ -684,6 +685,7 @@ struct dsx_grid {
     }
 
     void exchange_halo(bool rebuild, bool positions_only, cudaStream_t stream, long long* results) {
+        not_pending("exchange_halo");
         if (rebuild) plan_valid = false;
         bool reused = false;
         if (P == 1) {
@@ -702,6 +704,11 @@ struct dsx_grid {
             plan_valid = true;
             ghosts_valid = true;
         }
+        report_halo(rebuild, reused, stream, results);
+    }
+
+    // Per subdomain {ghosts, layout changed, storage reallocated, plan reused}.
+    void report_halo(bool rebuild, bool reused, cudaStream_t stream, long long* results) {
         if (results) {
             std::vector<int> g(static_cast<std::size_t>(P), 0);
             if (ghosts_valid) g = read_ints(S.g, P, stream);
@@ -719,7 +726,58 @@ struct dsx_grid {
         }
     }
 
+    // Split-phase halo (Decomp::begin_halo_exchange / end_halo_exchange,
+    // dsDecompX src/halo.cpp:296-872): begin enqueues the refresh or one
+    // build attempt on the stream and returns; work on other streams can run
+    // meanwhile; end waits, grows the ghost region and rebuilds after an
+    // overflow, and returns the counts.  Nothing else may run on the grid in
+    // between (the reference's logic_error).
+    bool halo_pending = false, pending_rebuild = false, pending_reused = false, pending_build = false;
+
+    void not_pending(const char* what) {
+        if (halo_pending)
+            fail(DSX_E_LOGIC, std::string(what) + " while a split halo exchange is in progress");
+    }
+
+    void begin_halo(bool rebuild, bool positions_only, cudaStream_t stream) {
+        not_pending("begin_halo_exchange");
+        if (rebuild) plan_valid = false;
+        pending_rebuild = rebuild;
+        pending_reused = false;
+        pending_build = false;
+        if (P == 1) {
+            plan_valid = false;
+            ghosts_valid = false;
+        } else if (plan_valid) {
+            dsx::launch_halo_refresh(params(), A, owned_off(), ghost_off(), positions_only, S, stream);
+            pending_reused = true;
+        } else {
+            clear_status(stream);
+            enqueue_halo_build(stream, plain_layout(stream));
+            pending_build = true;
+        }
+        halo_pending = true;
+    }
+
+    void end_halo(cudaStream_t stream, long long* results) {
+        if (!halo_pending) fail(DSX_E_LOGIC, "end_halo_exchange without begin_halo_exchange");
+        halo_pending = false;
+        if (pending_build) {
+            const unsigned st = read_status(stream);
+            if (st & dsx::kStatusGhostOverflow) {
+                grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
+                build_checked(stream);
+            } else {
+                plan_valid = true;
+                ghosts_valid = true;
+                plain_boundaries(stream);
+            }
+        }
+        report_halo(pending_rebuild, pending_reused, stream, results);
+    }
+
     void reverse_halo(cudaStream_t stream) {
+        not_pending("reverse_halo");
         if (P == 1 || !ghosts_valid) return;
         if (plain && static_cast<int>(plain_bounds.size()) == P + 1) {
             plain_launch.boundary_start = plain_bounds.data();
@@ -1019,6 +1077,7 @@ struct dsx_grid {
     }
 
     void step(dsx_step_callback cb, void* user, bool capture, cudaStream_t stream, unsigned* status_out) {
+        not_pending("the batched step");
         if (capture && (graph_callback != cb || graph_user != user || graph_stream != stream)) {
             destroy_graphs();
             graph_callback = cb;
@@ -1427,6 +1486,21 @@ int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report) {
     return guarded([&] {
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->autotune(static_cast<cudaStream_t>(stream), report);
+    });
+}
+
+int dsx_grid_begin_halo_exchange(dsx_grid* grid, int rebuild, int positions_only, void* stream) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        grid->begin_halo(rebuild != 0, positions_only != 0, static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch halo exchange");
+    });
+}
+
+int dsx_grid_end_halo_exchange(dsx_grid* grid, void* stream, long long* results) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        grid->end_halo(static_cast<cudaStream_t>(stream), results);
     });
 }
 

@@ -235,6 +235,16 @@ typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view*
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
                   void* stream, unsigned* status);
 
+/* Split-phase halo exchange (Decomp::begin_halo_exchange /
+ * end_halo_exchange, dsDecompX src/halo.cpp:296-872): begin enqueues the
+ * refresh along the plan or the plan build on stream and returns at once, so
+ * interior work can run on other streams; end waits for it (growing the ghost
+ * region and rebuilding if it overflowed) and fills results like
+ * dsx_grid_exchange_halo.  Between the two, every other operation on the
+ * grid fails with DSX_E_LOGIC, as does end without begin or a second begin. */
+int dsx_grid_begin_halo_exchange(dsx_grid* grid, int rebuild, int positions_only, void* stream);
+int dsx_grid_end_halo_exchange(dsx_grid* grid, void* stream, long long* results);
+
 /* Owning subdomain of n positions (Decomposition::owner_rank, dsDecompX
  * src/migration.cpp:74-98: one periodic wrap, then the cut planes): x, y, z
  * and out are device arrays of n; enqueued on stream. */
