@@ -35,6 +35,18 @@ def test_cpp_dropin_sanity(cuda, tmp_path):
         assert same(data[3 + a], want[a]), a
 
 
+def test_cpp_grid_sanity(cuda):
+    """The virtual grid's C++ face (include/dsx_grid.hpp) in a C++ program:
+    id conservation, sum of reverse == #ghosts per call and per captured
+    step, split-phase misuse and bad cuts raise the reference's types."""
+    import dsdecompx_b200 as dsx
+    exe = os.path.join(os.path.dirname(dsx.library_path()), "grid_sanity")
+    assert os.path.exists(exe), "tests/cpp programs are built by __graft_entry__.build()"
+    proc = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert proc.returncode == 0, proc.stdout + proc.stderr
+    assert "grid_sanity: ok" in proc.stdout
+
+
 @pytest.mark.parametrize("lower,upper", [((0.0, 0.0, 0.0), (100.0, 100.0, 100.0)),
                                          ((-3.7, 1e-3, 1e6), (5.1, 0.3, 1e6 + 7.25))])
 def test_rank_migrate_matches_oracle(cuda, lower, upper):
