@@ -809,12 +809,14 @@ struct dsx_grid {
     }
 
     void reverse_exchange(int nf, const int* ids, const int* ops, cudaStream_t stream) {
+        not_pending("reverse_exchange");
         const dsx::FieldOps F = field_ops(nf, ids, ops, "reverse-exchanged");
         if (P == 1 || !ghosts_valid || nf == 0) return;
         dsx::launch_reverse_fields(params(), A, owned_off(), ghost_off(), F, S, stream);
     }
 
     void forward_exchange(int nf, const int* ids, cudaStream_t stream) {
+        not_pending("forward_exchange");
         const dsx::FieldOps F = field_ops(nf, ids, nullptr, "forward-exchanged");
         if (P == 1 || !ghosts_valid || nf == 0) return;
         dsx::launch_forward_fields(params(), A, owned_off(), ghost_off(), F, S, stream);
@@ -822,6 +824,7 @@ struct dsx_grid {
 
     void rebalance(const double* host_work, bool force, cudaStream_t stream, long long* results,
                    double* imbalance) {
+        not_pending("rebalance");
         if (host_work) {
             for (int s = 0; s < P; ++s)
                 if (!std::isfinite(host_work[s]) || host_work[s] < 0.0)
@@ -911,6 +914,7 @@ struct dsx_grid {
     // Decomposition::set_axis_cuts (dsDecompX src/decomp.cpp:146-163): the
     // cuts must span the domain and increase strictly; the plan is invalid.
     void set_cuts(const double* host, cudaStream_t stream) {
+        not_pending("set_cuts");
         int total_cuts = 0;
         for (int a = 0; a < 3; ++a) {
             const double* c = host + total_cuts;
@@ -932,6 +936,7 @@ struct dsx_grid {
     // invalidates it.  Positions are the caller's.
     void rescale_domain(const double* lower, const double* upper, bool invalidate,
                         cudaStream_t stream) {
+        not_pending("rescale_domain");
         for (int a = 0; a < 3; ++a)
             if (!(upper[a] > lower[a])) fail(DSX_E_INVALID, "global-domain extent must be positive");
         const int total_cuts = dims[0] + dims[1] + dims[2] + 3;
@@ -973,6 +978,7 @@ struct dsx_grid {
     // Replays the step's idempotent parts on the current particles (the
     // current owned half is only read) and keeps the fastest launch shapes.
     void autotune(cudaStream_t stream, dsx_tune_report* out) {
+        not_pending("autotune");
         dsx_tune_report r{};
         for (float& v : r.classify_ms) v = -1.0f;
         for (float& v : r.move_ms) v = -1.0f;

@@ -697,6 +697,10 @@ def test_split_phase_halo_exchange(cuda):
             pair.gpu.begin_halo_exchange()
         with pytest.raises(RuntimeError, match="in progress"):
             pair.gpu.migrate()
+        with pytest.raises(RuntimeError, match="in progress"):
+            pair.gpu.rescale_domain((0, 0, 0), L)
+        with pytest.raises(RuntimeError, match="in progress"):
+            pair.gpu.autotune()
         pair.gpu.end_halo_exchange()
         with pytest.raises(RuntimeError, match="without begin"):
             pair.gpu.end_halo_exchange()
