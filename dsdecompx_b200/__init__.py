@@ -60,10 +60,14 @@ class _FieldDesc(C.Structure):
     _fields_ = [("name", C.c_char_p), ("type", C.c_int), ("components", C.c_int)]
 
 
+# dsx_tune_report.move_staged values
+MOVE_KINDS = {0: "direct", 1: "staged", 2: "staged passes", 3: "staged direct forces"}
+
+
 class TuneReport(C.Structure):
     _fields_ = [("classify_threads", C.c_int), ("move_staged", C.c_int),
                 ("reverse_ctas_per_sm", C.c_int), ("ghost_capacity", C.c_longlong),
-                ("classify_ms", C.c_float * 3), ("move_ms", C.c_float * 3),
+                ("classify_ms", C.c_float * 3), ("move_ms", C.c_float * 4),
                 ("reverse_ms", C.c_float * 4)]
 
 
@@ -125,6 +129,7 @@ def lib() -> C.CDLL:
             "dsx_grid_step_kernel_count": [vp],
             "dsx_grid_profile": [vp, C.c_int],
             "dsx_grid_set_plain": [vp, C.c_int],
+            "dsx_grid_set_tuning": [vp, C.c_int, C.c_int, C.c_int],
             "dsx_grid_set_cuts": [vp, C.POINTER(C.c_double), vp],
             "dsx_grid_owner_rank": [vp, vp, vp, vp, C.c_longlong, vp, vp],
             "dsx_grid_begin_halo_exchange": [vp, C.c_int, C.c_int, vp],
@@ -438,14 +443,15 @@ class VirtualGrid:
         choices and the measured milliseconds per launch."""
         r = TuneReport()
         _check(self.L.dsx_grid_autotune(self.h, _stream(stream), C.byref(r)))
-        kinds = {0: "direct", 1: "staged", 2: "staged passes"}
+        kinds = MOVE_KINDS
         return {"classify_threads": r.classify_threads, "move": kinds.get(r.move_staged, "?"),
                 "reverse_ctas_per_sm": r.reverse_ctas_per_sm,
                 "ghost_capacity": int(r.ghost_capacity),
                 "classify_ms": {n: round(float(v), 4) for n, v in zip((64, 128, 256), r.classify_ms)},
                 "move_ms": {"staged": round(float(r.move_ms[0]), 4),
                             "direct": round(float(r.move_ms[1]), 4),
-                            "staged passes": round(float(r.move_ms[2]), 4)},
+                            "staged passes": round(float(r.move_ms[2]), 4),
+                            "staged direct forces": round(float(r.move_ms[3]), 4)},
                 "reverse_ms": {n: round(float(v), 4) for n, v in zip((4, 8, 16, 32), r.reverse_ms)}}
 
     def begin_halo_exchange(self, rebuild: bool = False, positions_only: bool = False, stream=None):
@@ -490,6 +496,12 @@ class VirtualGrid:
         lo = (C.c_double * 3)(*lower)
         hi = (C.c_double * 3)(*upper)
         _check(self.L.dsx_grid_rescale_domain(self.h, lo, hi, 1 if update else 0, _stream(stream)))
+
+    def set_tuning(self, classify_threads: int = 128, move: str = "staged",
+                   reverse_ctas_per_sm: int = 0):
+        """Sets the batched step's launch shapes (the choices autotune reports)."""
+        kind = {v: k for k, v in MOVE_KINDS.items()}[move]
+        _check(self.L.dsx_grid_set_tuning(self.h, classify_threads, kind, reverse_ctas_per_sm))
 
     def set_plain(self, plain: bool = True):
         """Per-call operations launch their tile kernels once per subdomain

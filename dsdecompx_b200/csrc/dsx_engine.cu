@@ -1039,16 +1039,16 @@ struct dsx_grid {
                 grids(G, Gn);
             }
             const long long gho = ghost_off();
-            // staged, direct reads, staged in passes
-            const int kinds[3] = {1, 0, 2};
-            const int bits[3] = {2, 1, 4};
+            // staged, direct reads, staged in passes, staged without forces
+            const int kinds[4] = {1, 0, 2, 3};
+            const int bits[4] = {2, 1, 4, 8};
             const int modes = dsx::staged_move_modes(A);
-            for (int i = 0; i < 3; ++i) {
+            for (int i = 0; i < 4; ++i) {
                 if (!(modes & bits[i])) continue;
                 S.move_staged = kinds[i];
                 r.move_ms[i] = time([&] { dsx::launch_step_move(G, A, src, dst, gho, S, stream); });
             }
-            S.move_staged = pick(r.move_ms, kinds, 3, 1);
+            S.move_staged = pick(r.move_ms, kinds, 4, 1);
             dsx::launch_step_move(G, A, src, dst, gho, S, stream);
             dsx::launch_step_finish(G, Gn, A, src, dst, gho, S, stream);
             // the reverse sum into the next half's forces from the ghost
@@ -1546,6 +1546,23 @@ int dsx_grid_rescale_domain(dsx_grid* grid, const double* lower, const double* u
     return guarded([&] {
         if (!grid || !lower || !upper) fail(DSX_E_INVALID, "null argument");
         grid->rescale_domain(lower, upper, invalidate_plan != 0, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
+                        int reverse_ctas_per_sm) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        if (classify_threads != 64 && classify_threads != 128 && classify_threads != 256)
+            fail(DSX_E_INVALID, "classify threads must be 64, 128 or 256");
+        if (move_kind < 0 || move_kind > 3) fail(DSX_E_INVALID, "move kind must be 0..3");
+        if (reverse_ctas_per_sm < 0 || reverse_ctas_per_sm > 32)
+            fail(DSX_E_INVALID, "reverse CTAs per SM must be 0..32");
+        grid->not_pending("set_tuning");
+        grid->S.classify_threads = classify_threads;
+        grid->S.move_staged = move_kind;
+        grid->S.reverse_per_sm = reverse_ctas_per_sm;
+        grid->destroy_graphs();   // captured steps hold the old launch shapes
     });
 }
 

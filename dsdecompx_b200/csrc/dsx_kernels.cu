@@ -1402,6 +1402,29 @@ __device__ __forceinline__ void move_from_stage(const Grid& G, const Arrays& A,
     fields_from_stage(A.f, rec, fseg, l, dst);
 }
 
+// move_from_stage for a tile staged without its force arrays: the owner's
+// forces come from HBM (fx, fy, fz), everything else from the stage.
+__device__ __forceinline__ void move_from_stage_forces(const Grid& G, const Arrays& A,
+                                                       const unsigned char* rec, const int* sg,
+                                                       const int* fseg, int l, long long dst,
+                                                       double fx, double fy, double fz) {
+    double v[11];
+#pragma unroll
+    for (int a = 0; a < 11; ++a)
+        if (a < 6 || a > 8) v[a] = srd(rec, sg[a], l);
+    v[6] = fx;
+    v[7] = fy;
+    v[8] = fz;
+    const int ty = sri(rec, sg[11], l), id = sri(rec, sg[12], l);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) A.d[a][dst] = wrap_if(G, a, v[a]);
+#pragma unroll
+    for (int a = 3; a < 11; ++a) A.d[a][dst] = v[a];
+    A.type[dst] = ty;
+    A.gid[dst] = id;
+    fields_from_stage(A.f, rec, fseg, l, dst);
+}
+
 // Ghost image of record l of the staged tile (plan-build semantics: wrapped
 // position + shift, velocities, zero force, mass, charge, type, id, fields).
 __device__ __forceinline__ void ghost_from_stage(const Grid& G, const Arrays& A,
@@ -1428,17 +1451,22 @@ __device__ __forceinline__ void ghost_from_stage(const Grid& G, const Arrays& A,
 }
 
 // Warp 0 issues the bulk copies of elements [first, last) of a tile into a
-// shared-memory buffer: lane k copies array a0 + k of the record (arrays
-// [a0, a1)) and stores in seg[k] where element 0 landed.  Lane 0 announces the byte total on the
+// shared-memory buffer: each lane copies one array k of [a0, a1) (skipping
+// the force arrays when asked) and stores in seg[k - a0] where element 0
+// landed.  Lane 0 announces the byte total on the
 // mbarrier before any copy starts.
 __device__ __forceinline__ void stage_issue(const Arrays& A, long long src_off, int first,
                                             int last, unsigned char* stage, unsigned bar,
-                                            int* seg, int lane, int a0, int a1) {
+                                            int* seg, int lane, int a0, int a1,
+                                            bool skip_forces = false) {
+    // lane -> array: a0 + lane, stepping over the force arrays (6..8) when
+    // they are read directly instead
+    const int k = a0 + lane + (skip_forces && a0 + lane >= 6 ? 3 : 0);
     int b = 0;
     const unsigned char* base = nullptr;
-    if (a0 + lane < a1) {
-        b = array_bytes(A, a0 + lane);
-        base = array_base(A, a0 + lane);
+    if (k < a1) {
+        b = array_bytes(A, k);
+        base = array_base(A, k);
     }
     const int size = b ? TILE * b + 32 : 0;
     const int soff = warp_inclusive_sum(size) - size;
@@ -1456,7 +1484,7 @@ __device__ __forceinline__ void stage_issue(const Arrays& A, long long src_off, 
     __syncwarp();
     if (b) {
         bulk_load(smem_u32(stage + soff), base + lo, bytes, bar);
-        seg[lane] = soff + static_cast<int>(gl - lo);
+        seg[k - a0] = soff + static_cast<int>(gl - lo);
     }
 }
 
@@ -1524,7 +1552,7 @@ __global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int s
 // [a0, a1) only (a record too wide for three staged tiles per SM is moved in
 // several passes); every pass redoes the index work from the destinations
 // and masks, and only the pass with index_outputs writes its results.
-template <bool FULL>
+template <bool FULL, bool DIRECT_FORCES>
 __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     Grid G, Arrays A, long long src_off, long long dst_off, long long ghost_off, const int* pre,
     int stride, const int* cbase_ret, const unsigned short* __restrict__ dest_in,
@@ -1564,7 +1592,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         __syncwarp();
-        stage_issue(A, src_off, begin, end, s_rec, bar, s_seg, lane, a0, a1);
+        stage_issue(A, src_off, begin, end, s_rec, bar, s_seg, lane, a0, a1, DIRECT_FORCES);
     }
     // (slots past the tile's end hold stale values: masked here; the mask
     // is only meaningful for a stay)
@@ -1672,6 +1700,18 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
         if (lane == kStepStay) run += __popc(bs_);
         if (lane == kStepEmig) run += __popc(be);
     }
+    // forces of the stays read from HBM (not staged), in flight with the copies
+    double fstay[ITEMS][3];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        fstay[j][0] = fstay[j][1] = fstay[j][2] = 0.0;
+        if (DIRECT_FORCES && dest[j] == s) {
+            const long long src = src_off + wbegin + j * 32 + lane;
+            fstay[j][0] = ro(A.d[6] + src);
+            fstay[j][1] = ro(A.d[7] + src);
+            fstay[j][2] = ro(A.d[8] + src);
+        }
+    }
     // the records must have landed before anything reads them; after this
     // barrier every warp's staging is visible too
     const bool lost = !bulk_wait(bar);
@@ -1688,7 +1728,10 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     for (int j = 0; j < ITEMS; ++j) {
         if (dest[j] != s) continue;
         const int l = wbegin + j * 32 + lane - begin;
-        if (FULL) {
+        if (FULL && DIRECT_FORCES) {
+            move_from_stage_forces(G, A, s_rec, sg, fseg, l, dst_off + nis[j], fstay[j][0],
+                                   fstay[j][1], fstay[j][2]);
+        } else if (FULL) {
             move_from_stage(G, A, s_rec, sg, fseg, l, dst_off + nis[j]);
         } else {
             for (int c = a0; c < a1; ++c)
@@ -2233,6 +2276,9 @@ int staged_range_bytes(const Arrays& A, int a0, int a1) {
 
 int staged_bytes(const Arrays& A) { return staged_range_bytes(A, 0, 13 + A.f.count); }
 
+// Shared memory of the three force arrays of one staged tile.
+constexpr int kForceStageBytes = 3 * (TILE * 8 + 32);
+
 // A staged pass holds at most this much of the record, so that three CTAs
 // (their tiles in flight at once) fit an SM's shared memory.
 constexpr int kStagedPassBytes = 56 * 1024;
@@ -2295,6 +2341,7 @@ int staged_move_modes(const Arrays& A) {
     int modes = 1;   // direct reads always apply
     if (one || split) modes |= 2;
     if (one && split && passes > 1) modes |= 4;   // passes as an alternative to one pass
+    if (staged_bytes(A) - kForceStageBytes <= kStagedMaxBytes) modes |= 8;
     return modes;
 }
 
@@ -2302,10 +2349,12 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
                       long long ghost_off, const Scratch& S, cudaStream_t s) {
     static bool attribute_set = false;   // once per process (one device per process)
     if (!attribute_set) {
-        cudaFuncSetAttribute(k_step_move_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kStagedMaxBytes);
-        cudaFuncSetAttribute(k_step_move_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kStagedMaxBytes);
+        cudaFuncSetAttribute(k_step_move_staged<true, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedMaxBytes);
+        cudaFuncSetAttribute(k_step_move_staged<true, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedMaxBytes);
+        cudaFuncSetAttribute(k_step_move_staged<false, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedMaxBytes);
         attribute_set = true;
     }
     const int narrays = 13 + A.f.count;
@@ -2315,17 +2364,22 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
     auto staged = [&](bool full, int a0, int a1, int index_outputs) {
         const int bytes = staged_range_bytes(A, a0, a1);
         if (full)
-            k_step_move_staged<true><<<G.max_tiles, NT, bytes, s>>>(
+            k_step_move_staged<true, false><<<G.max_tiles, NT, bytes, s>>>(
                 G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
                 S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
                 S.boff, S.bslot, a0, a1, index_outputs);
         else
-            k_step_move_staged<false><<<G.max_tiles, NT, bytes, s>>>(
+            k_step_move_staged<false, false><<<G.max_tiles, NT, bytes, s>>>(
                 G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
                 S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
                 S.boff, S.bslot, a0, a1, index_outputs);
     };
-    if (S.move_staged == 1 && whole <= kStagedMaxBytes) {
+    if (S.move_staged == 3 && whole - kForceStageBytes <= kStagedMaxBytes) {
+        k_step_move_staged<true, true><<<G.max_tiles, NT, whole - kForceStageBytes, s>>>(
+            G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
+            S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
+            S.bslot, 0, narrays, 1);
+    } else if (S.move_staged == 1 && whole <= kStagedMaxBytes) {
         staged(true, 0, narrays, 1);
     } else if (S.move_staged != 0 && split) {
         if (passes == 1) {

@@ -66,7 +66,8 @@ struct Scratch {
     Marks* marks = nullptr;
     // launch shapes the autotuner picks (these defaults are the untuned choice)
     int classify_threads = 128;   // threads per 512-particle tile of the step classify: 64/128/256
-    int move_staged = 1;          // 1: staged (one pass if it fits), 2: staged in passes, 0: direct reads
+    int move_staged = 1;          // 1: staged (one pass if it fits), 2: staged in passes,
+                                  // 3: staged without forces, 0: direct reads
     int reverse_per_sm = 0;       // CTAs per SM of the reverse sum; 0: one wave of the default shape
 };
 
@@ -108,7 +109,8 @@ void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long lon
 // Move kinds that apply to this record, as bits: 1 direct reads (kind 0),
 // 2 staged (kind 1: one pass when a tile of the record fits 100 KB of shared
 // memory, else passes of at most 56 KB), 4 staged in passes although one
-// pass fits (kind 2).
+// pass fits (kind 2), 8 staged in one pass without the force arrays, which
+// the stays read from HBM (kind 3: ghosts never need their owner's force).
 int staged_move_modes(const Arrays& A);
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off,

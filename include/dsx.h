@@ -288,14 +288,24 @@ int dsx_grid_rescale_domain(dsx_grid* grid, const double* lower, const double* u
  * one subdomain has nothing to tune and keeps the defaults. */
 typedef struct dsx_tune_report {
     int classify_threads;
-    int move_staged;         /* 1 staged (one pass if it fits), 2 staged in passes, 0 direct reads */
+    int move_staged;         /* move kind: 1 staged (one pass if it fits), 2 staged in passes,
+                                3 staged without the force arrays, 0 direct reads */
     int reverse_ctas_per_sm;
     long long ghost_capacity;
     float classify_ms[3];    /* 64, 128, 256 threads per tile */
-    float move_ms[3];        /* staged, direct reads, staged in passes */
+    float move_ms[4];        /* staged, direct reads, staged in passes, staged without forces */
     float reverse_ms[4];     /* 4, 8, 16, 32 CTAs per SM */
 } dsx_tune_report;
 int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report);
+
+/* Sets the batched step's launch shapes directly (as dsx_grid_autotune would
+ * choose them; for re-using a tuning, and for tests that force each kind):
+ * classify_threads 64, 128 or 256; move_kind as dsx_tune_report.move_staged
+ * (a kind that does not fit the record's shared-memory budget falls back to
+ * staged passes or direct reads); reverse_ctas_per_sm 0 (two waves of the
+ * grid's SMs) or 1..32.  Results are identical for every setting. */
+int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
+                        int reverse_ctas_per_sm);
 
 /* Plain launches, for comparison runs: plain != 0 makes the per-call
  * operations (dsx_grid_migrate, a rebuilding dsx_grid_exchange_halo,

@@ -210,6 +210,11 @@ public:
                             capture ? 1 : 0, stream, &status));
         return status;
     }
+    // classify_threads 64/128/256, move_kind as dsx_tune_report.move_staged,
+    // reverse_ctas_per_sm 0..32
+    void set_tuning(int classify_threads, int move_kind, int reverse_ctas_per_sm) {
+        check(dsx_grid_set_tuning(handle_, classify_threads, move_kind, reverse_ctas_per_sm));
+    }
     dsx_tune_report autotune(void* stream = nullptr) {
         dsx_tune_report r{};
         check(dsx_grid_autotune(handle_, stream, &r));

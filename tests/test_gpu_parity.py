@@ -427,6 +427,76 @@ def test_batched_step_many_tiles(cuda, fields, particles, box, halo):
         b.close()
 
 
+@pytest.mark.parametrize("fields,particles", [(ALL_FIELDS[:2], 200_000), (ALL_FIELDS, 60_000)],
+                         ids=["record-116B", "record-204B"])
+def test_every_tuning_gives_the_same_step(cuda, fields, particles):
+    """The batched step with each move kind forced (staged in one pass,
+    direct reads, staged in passes, staged without the force arrays) and each
+    classify shape and reverse grid: particles, ghosts and sums identical to
+    the per-call path (itself checked against the oracle here).  At 204 B per
+    particle one staged pass does not fit and kind 1 falls back to passes,
+    while the stage without forces (about 92 KB a tile) fits."""
+    import torch
+
+    import dsdecompx_b200 as dsx
+    rng = np.random.default_rng(31)
+    capacity = 2 * particles
+    kw = dict(nranks=27, dims=(3, 3, 3), lower=(0, 0, 0), upper=(12.0, 12.0, 12.0),
+              halo_width=0.6, fields=fields, particles=particles, ghost_capacity=capacity)
+    data = uniform_particles(rng, particles, (0, 0, 0), (12.0, 12.0, 12.0), fields)
+    a = Pair(**kw)
+    owner = a.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    per = split_by_owner(owner, data, 27)
+    a.upload(per)
+    tunings = [(128, "staged", 0), (64, "direct", 4), (256, "staged passes", 32),
+               (128, "staged direct forces", 8)]
+    grids = []
+    for t in tunings:
+        g = dsx.VirtualGrid(**kw)
+        g.upload(per)
+        g.set_tuning(*t)
+        grids.append(g)
+    with pytest.raises(ValueError):
+        grids[0].set_tuning(96, "staged", 0)
+    fill = ghost_force_filler(torch, capacity)
+    side = torch.cuda.Stream()
+    try:
+        for step in range(3):
+            a.displace(rng, 0.4)
+            for g in grids:
+                for r in range(27):
+                    o = g.counts(r)[0]
+                    for name in "xyz":
+                        g.write(r, name, 0, a.gpu.read(r, name, 0, o))
+            a.gpu.migrate()
+            a.ref.migrate()
+            a.gpu.exchange_halo(rebuild=True)
+            a.ref.exchange_halo(rebuild=True)
+            fill(a.gpu.view(), torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            for r in range(27):
+                o, gh = a.ref.counts(r)
+                for name in ("fx", "fy", "fz"):
+                    a.ref.write(r, name, o, a.gpu.read(r, name, o, gh))
+            a.gpu.reverse_halo()
+            a.ref.reverse_halo()
+            a.compare(f"calls {step}")
+            torch.cuda.synchronize()
+            for t, g in zip(tunings, grids):
+                with torch.cuda.stream(side):
+                    st = g.step(fill, capture=step > 0)
+                side.synchronize()
+                assert st == 0, t
+                for r in range(27):
+                    x, y = a.gpu.snapshot(r), g.snapshot(r)
+                    for k in x:
+                        assert same(x[k], y[k]), (t, step, r, k)
+    finally:
+        a.close()
+        for g in grids:
+            g.close()
+
+
 def nan_equal(a, b) -> bool:
     """Bitwise equality, except that every NaN counts as the same value (a
     NaN made by inf - inf has the platform's own bits)."""
