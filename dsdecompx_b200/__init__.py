@@ -137,6 +137,11 @@ def lib() -> C.CDLL:
             "dsx_grid_out_of_domain": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
             "dsx_grid_rescale_domain": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, vp],
             "dsx_grid_autotune": [vp, vp, vp],
+            "dsx_grid_migration_pairs": [vp, llp, vp],
+            "dsx_grid_send_lists": [vp, ip, ip, vp],
+            "dsx_grid_assemble": [vp, llp, C.c_int, C.POINTER(vp), C.c_longlong, vp, vp],
+            "dsx_grid_set_rebalance_work": [vp, dp],
+            "dsx_copy_segments": [vp, C.c_longlong, vp],
             "dsx_grid_kernel_times": [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)],
         }
         for name, args in sig.items():
@@ -145,6 +150,19 @@ def lib() -> C.CDLL:
             fn.restype = C.c_int
         _LIB = L
     return _LIB
+
+
+# dsx_segment and dsx_copy as numpy record types (C layout, natural alignment)
+SEGMENT_DTYPE = np.dtype([("source", np.int32), ("src_index", np.int64), ("dst_rank", np.int32),
+                          ("dst_index", np.int64), ("count", np.int64)], align=True)
+COPY_DTYPE = np.dtype([("src", np.uint64), ("dst", np.uint64), ("bytes", np.int64)], align=True)
+
+
+def copy_segments(copies: np.ndarray, stream=None):
+    """Device-to-device copies (a COPY_DTYPE array), all in one kernel."""
+    c = np.ascontiguousarray(copies, dtype=COPY_DTYPE)
+    if c.size:
+        _check(lib().dsx_copy_segments(c.ctypes.data, c.size, _stream(stream)))
 
 
 def _check(status: int):
@@ -502,6 +520,45 @@ class VirtualGrid:
         """Sets the batched step's launch shapes (the choices autotune reports)."""
         kind = {v: k for k, v in MOVE_KINDS.items()}[move]
         _check(self.L.dsx_grid_set_tuning(self.h, classify_threads, kind, reverse_ctas_per_sm))
+
+    # ----------------------------------------------- sharded grids
+    def migration_pairs(self, stream=None) -> np.ndarray:
+        """Emigrants of the last migration per (destination, source): (P, P)."""
+        out = np.zeros((self.nranks, self.nranks), dtype=np.int64)
+        _check(self.L.dsx_grid_migration_pairs(self.h, out.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                               _stream(stream)))
+        return out
+
+    def send_lists(self, stream=None):
+        """(length, first ghost slot) of every send list, 26 per sender."""
+        n = self.nranks * 26
+        length = np.zeros(n, dtype=np.int32)
+        first = np.zeros(n, dtype=np.int32)
+        _check(self.L.dsx_grid_send_lists(self.h, length.ctypes.data_as(C.POINTER(C.c_int)),
+                                          first.ctypes.data_as(C.POINTER(C.c_int)), _stream(stream)))
+        return length.astype(np.int64), first.astype(np.int64)
+
+    def assemble(self, counts, sources: Sequence[Sequence[int]], segments: np.ndarray, stream=None):
+        """New owned particles from segments (a SEGMENT_DTYPE array) of the
+        current ones (source -1) and of device buffers: sources[k][a] is the
+        address of array a's element 0 in buffer k."""
+        c = np.ascontiguousarray(counts, dtype=np.int64)
+        table = (C.c_void_p * max(32 * len(sources), 1))()
+        for k, ptrs in enumerate(sources):
+            for a, p in enumerate(ptrs):
+                table[32 * k + a] = p
+        seg = np.ascontiguousarray(segments, dtype=SEGMENT_DTYPE)
+        _check(self.L.dsx_grid_assemble(self.h, c.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                        len(sources), table, seg.size,
+                                        seg.ctypes.data if seg.size else None, _stream(stream)))
+
+    def set_rebalance_work(self, work=None):
+        """Work per subdomain for the next migrate's automatic rebalance."""
+        if work is None:
+            _check(self.L.dsx_grid_set_rebalance_work(self.h, None))
+            return
+        w = np.ascontiguousarray(work, dtype=np.float64)
+        _check(self.L.dsx_grid_set_rebalance_work(self.h, w.ctypes.data_as(C.POINTER(C.c_double))))
 
     def set_plain(self, plain: bool = True):
         """Per-call operations launch their tile kernels once per subdomain

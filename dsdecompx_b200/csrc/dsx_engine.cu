@@ -5,6 +5,7 @@
 #include "dsx_kernels.cuh"
 
 #include <algorithm>
+#include <climits>
 #include <array>
 #include <cmath>
 #include <cstdint>
@@ -233,6 +234,9 @@ struct dsx_grid {
     long long* call_counter = nullptr;
     double* rebalance_result = nullptr;   // [6]: automatic, explicit
     double* work = nullptr;               // [P]
+    int* pairs = nullptr;                 // [P*P] emigrants per (destination, source)
+    bool pairs_valid = false;             // the emigrant list belongs to the current layout
+    std::vector<double> next_work;        // work of the next per-call migrate's rebalance
     // static topology tables
     int* d_nn = nullptr;
     int* d_nbr = nullptr;
@@ -562,12 +566,6 @@ struct dsx_grid {
 
     // -------------------------------------------------------- operations
 
-    void enqueue_migrate(cudaStream_t stream, bool automatic_rebalance,
-                         const dsx::PlainLaunch* pl = nullptr) {
-        enqueue_rebalance(stream, automatic_rebalance);
-        dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream, pl);
-    }
-
     // Plain mode (per-call operations only): the current layout's tile starts
     // on the host, read after the work queued so far.
     const dsx::PlainLaunch* plain_layout(cudaStream_t stream) {
@@ -591,7 +589,8 @@ struct dsx_grid {
         plain_bounds[static_cast<std::size_t>(P)] = info[1];
     }
 
-    void enqueue_rebalance(cudaStream_t stream, bool automatic_rebalance) {
+    void enqueue_rebalance(cudaStream_t stream, bool automatic_rebalance,
+                           const double* work_in = nullptr) {
         const dsx::Grid G = params();
         if (desc.policy == DSX_DYNAMIC) {
             // Decomp::migrate: ++migration_calls, automatic rebalance every
@@ -604,12 +603,13 @@ struct dsx_grid {
             p.halo_width = halo_width;
             p.automatic = 1;
             p.interval = automatic_rebalance ? static_cast<long long>(desc.dyn_interval) : 0;
-            dsx::launch_rebalance(G, nullptr, p, call_counter, rebalance_result, stream);
+            dsx::launch_rebalance(G, work_in, p, call_counter, rebalance_result, stream);
             dsx::mark(S, stream, "rebalance");
         }
     }
 
     void commit_migrate() {
+        pairs_valid = true;
         plain_bounds.clear();
         parity ^= 1;
         cur ^= 1;
@@ -651,13 +651,23 @@ struct dsx_grid {
     void migrate(cudaStream_t stream, long long* results, bool automatic_rebalance = true) {
         not_pending("migrate");
         clear_status(stream);
+        // work supplied for this migrate's automatic rebalance (pageable
+        // source: the copy is staged before the call returns)
+        const double* work_in = nullptr;
+        if (!next_work.empty()) {
+            cuda_check(cudaMemcpyAsync(work, next_work.data(), sizeof(double) * P,
+                                       cudaMemcpyHostToDevice, stream), "upload work");
+            work_in = work;
+            next_work.clear();
+        }
         if (plain) {
             // the rebalance may move the cut planes but not the layout
-            enqueue_rebalance(stream, automatic_rebalance);
+            enqueue_rebalance(stream, automatic_rebalance, work_in);
             dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream,
                                 plain_layout(stream));
         } else {
-            enqueue_migrate(stream, automatic_rebalance);
+            enqueue_rebalance(stream, automatic_rebalance, work_in);
+            dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream);
         }
         commit_migrate();
         if (results) {
@@ -975,6 +985,115 @@ struct dsx_grid {
         }
     }
 
+    // ------------------------------------------------ sharded grids
+
+    // Emigrants of the last migration (per call or batched step) counted per
+    // (destination, source), dest-major.
+    void migration_pairs(long long* out, cudaStream_t stream) {
+        not_pending("migration_pairs");
+        if (!pairs_valid) fail(DSX_E_LOGIC, "no migration since the particles were last replaced");
+        if (!pairs) pairs = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * P);
+        dsx::launch_pair_counts(P, S, layout[cur ^ 1][1], ncap, pairs, stream);
+        const std::vector<int> h = read_ints(pairs, P * P, stream);
+        for (std::size_t i = 0; i < h.size(); ++i) out[i] = h[i];
+    }
+
+    // Length and first ghost slot of every send list (sender-major, 26 per
+    // sender) of the current plan.
+    void send_lists(int* len, int* base, cudaStream_t stream) {
+        not_pending("send_lists");
+        const std::size_t n = static_cast<std::size_t>(P) * dsx::kMaxNeighbors;
+        if (!ghosts_valid || P == 1) {
+            std::fill(len, len + n, 0);
+            std::fill(base, base + n, 0);
+            return;
+        }
+        cuda_check(cudaMemcpyAsync(len, S.list_len, sizeof(int) * n, cudaMemcpyDeviceToHost, stream), "read");
+        cuda_check(cudaMemcpyAsync(base, S.send_base, sizeof(int) * n, cudaMemcpyDeviceToHost, stream), "read");
+        cuda_check(cudaStreamSynchronize(stream), "synchronize");
+    }
+
+    // The next owned half from segments of the current half and of outside
+    // buffers, then the halves swap: counts[P] are the new owned counts; a
+    // segment copies `count` records of every array from source `source`
+    // (-1: the current owned half; k >= 0: sources[32 k + a] is array a's
+    // element 0) at src_index to subdomain dst_rank at dst_index.
+    void assemble(const long long* counts, int nsources, const void* const* sources, long long nseg,
+                  const dsx_segment* segs, cudaStream_t stream) {
+        not_pending("assemble");
+        std::vector<long long> ob(static_cast<std::size_t>(P) + 1, 0);
+        for (int s = 0; s < P; ++s) {
+            if (counts[s] < 0 || counts[s] > INT_MAX) fail(DSX_E_INVALID, "particle count out of range");
+            ob[static_cast<std::size_t>(s) + 1] = ob[static_cast<std::size_t>(s)] + counts[s];
+        }
+        const long long sum = ob[static_cast<std::size_t>(P)];
+        if (sum > ncap) fail(DSX_E_LENGTH, "particle storage is smaller than the assembled counts");
+        const int narrays = 13 + static_cast<int>(fields.size());
+        long long bytes[32];
+        unsigned char* dst_base[32];
+        const long long src_off = owned_off(), dst_off = next_off();
+        unsigned char* cur_base[32];
+        for (int a = 0; a < narrays; ++a) {
+            bytes[a] = a < 11 ? 8 : a < 13 ? 4 : fields[static_cast<std::size_t>(a - 13)].bytes;
+            unsigned char* b = static_cast<unsigned char*>(
+                a < 11 ? static_cast<void*>(A.d[a]) : a == 11 ? static_cast<void*>(A.type) :
+                a == 12 ? static_cast<void*>(A.gid) : static_cast<void*>(A.f.base[a - 13]));
+            dst_base[a] = b + dst_off * bytes[a];
+            cur_base[a] = b + src_off * bytes[a];
+        }
+        std::vector<dsx::CopyPiece> copies;
+        for (long long k = 0; k < nseg; ++k) {
+            const dsx_segment& g = segs[k];
+            if (g.count < 0 || g.src_index < 0 || g.dst_index < 0 || g.dst_rank < 0 || g.dst_rank >= P ||
+                g.source < -1 || g.source >= nsources)
+                fail(DSX_E_INVALID, "segment out of range");
+            if (g.dst_index + g.count > counts[g.dst_rank])
+                fail(DSX_E_INVALID, "segment past the end of its subdomain");
+            if (g.source == -1 && g.src_index + g.count > total)
+                fail(DSX_E_INVALID, "segment past the end of the owned particles");
+            if (!g.count) continue;
+            for (int a = 0; a < narrays; ++a) {
+                const unsigned char* src =
+                    g.source < 0 ? cur_base[a]
+                                 : static_cast<const unsigned char*>(sources[32 * g.source + a]);
+                if (!src) fail(DSX_E_INVALID, "null source array");
+                copies.push_back({src + g.src_index * bytes[a],
+                                  dst_base[a] + (ob[static_cast<std::size_t>(g.dst_rank)] + g.dst_index) * bytes[a],
+                                  g.count * bytes[a]});
+            }
+        }
+        cuda_check(dsx::launch_copies(copies, stream), "assemble copies");
+        std::vector<int> c(static_cast<std::size_t>(P) + 1, 0);
+        for (int s = 0; s < P; ++s) c[static_cast<std::size_t>(s)] = static_cast<int>(counts[s]);
+        const int next = cur ^ 1;
+        cuda_check(cudaMemcpyAsync(layout[next][0], c.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice,
+                                   stream), "assemble counts");
+        cur ^= 1;
+        dsx::launch_layout(params(), layout[cur][0], layout[cur][1], layout[cur][2], layout_tiles[cur], stream);
+        parity ^= 1;
+        total = sum;
+        plan_valid = false;
+        ghosts_valid = false;
+        pairs_valid = false;
+        plain_bounds.clear();
+        std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
+        cuda_check(cudaMemsetAsync(S.g, 0, sizeof(int) * (P + 1), stream), "memset");
+        cuda_check(cudaMemsetAsync(S.gbase, 0, sizeof(int) * (P + 1), stream), "memset");
+        cuda_check(cudaMemsetAsync(S.halo_info, 0, sizeof(int) * 4, stream), "memset");
+        cuda_check(cudaStreamSynchronize(stream), "assemble");
+    }
+
+    void set_rebalance_work(const double* host_work) {
+        if (!host_work) {
+            next_work.clear();
+            return;
+        }
+        for (int s = 0; s < P; ++s)
+            if (!std::isfinite(host_work[s]) || host_work[s] < 0.0)
+                fail(DSX_E_INVALID, "rebalance work must be finite and non-negative");
+        next_work.assign(host_work, host_work + P);
+    }
+
     // Replays the step's idempotent parts on the current particles (the
     // current owned half is only read) and keeps the fastest launch shapes.
     void autotune(cudaStream_t stream, dsx_tune_report* out) {
@@ -1137,6 +1256,7 @@ struct dsx_grid {
         total = sum;
         parity = 0;
         cur = 0;
+        pairs_valid = false;
         plan_valid = false;
         ghosts_valid = false;
         std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
@@ -1546,6 +1666,53 @@ int dsx_grid_rescale_domain(dsx_grid* grid, const double* lower, const double* u
     return guarded([&] {
         if (!grid || !lower || !upper) fail(DSX_E_INVALID, "null argument");
         grid->rescale_domain(lower, upper, invalidate_plan != 0, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_migration_pairs(dsx_grid* grid, long long* pairs, void* stream) {
+    return guarded([&] {
+        if (!grid || !pairs) fail(DSX_E_INVALID, "null argument");
+        grid->migration_pairs(pairs, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_send_lists(dsx_grid* grid, int* length, int* first_slot, void* stream) {
+    return guarded([&] {
+        if (!grid || !length || !first_slot) fail(DSX_E_INVALID, "null argument");
+        grid->send_lists(length, first_slot, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_assemble(dsx_grid* grid, const long long* counts, int nsources,
+                      const void* const* sources, long long nsegments, const dsx_segment* segments,
+                      void* stream) {
+    return guarded([&] {
+        if (!grid || !counts || (nsegments > 0 && !segments) || (nsources > 0 && !sources) ||
+            nsources < 0 || nsegments < 0)
+            fail(DSX_E_INVALID, "null argument");
+        grid->assemble(counts, nsources, sources, nsegments, segments, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int dsx_grid_set_rebalance_work(dsx_grid* grid, const double* work) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        grid->set_rebalance_work(work);
+    });
+}
+
+int dsx_copy_segments(const dsx_copy* copies, long long n, void* stream) {
+    return guarded([&] {
+        if (n < 0 || (n > 0 && !copies)) fail(DSX_E_INVALID, "null argument");
+        std::vector<dsx::CopyPiece> list;
+        list.reserve(static_cast<std::size_t>(n));
+        for (long long k = 0; k < n; ++k) {
+            if (copies[k].bytes < 0) fail(DSX_E_INVALID, "negative copy size");
+            if (copies[k].bytes && (!copies[k].src || !copies[k].dst)) fail(DSX_E_INVALID, "null copy address");
+            list.push_back({static_cast<const unsigned char*>(copies[k].src),
+                            static_cast<unsigned char*>(copies[k].dst), copies[k].bytes});
+        }
+        cuda_check(dsx::launch_copies(list, static_cast<cudaStream_t>(stream)), "copy segments");
     });
 }
 

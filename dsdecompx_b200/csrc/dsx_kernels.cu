@@ -2147,6 +2147,60 @@ __global__ void __launch_bounds__(NT) k_out_of_domain(Grid G, const double* __re
     if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(&flags[td.x], 1);
 }
 
+// Emigrants of the last migration counted per (destination, source):
+// pairs[t * P + q].  The source of emigrant e is the subdomain of the old
+// layout that held index emig_src[e] (obase_old: the old layout's P + 1
+// offsets; the largest q with obase_old[q] <= i, so empty subdomains are
+// stepped over).  E = info[0].
+__global__ void __launch_bounds__(NT) k_pair_counts(int P, const int* __restrict__ info,
+                                                    const int* __restrict__ emig_src,
+                                                    const int* __restrict__ emig_dst,
+                                                    const int* __restrict__ obase_old, int* pairs) {
+    const int E = info[0];
+    for (int e = blockIdx.x * NT + threadIdx.x; e < E; e += gridDim.x * NT) {
+        const int i = emig_src[e];
+        int lo = 0, hi = P;   // obase_old[lo] <= i < obase_old[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (obase_old[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        atomicAdd(&pairs[emig_dst[e] * P + lo], 1);
+    }
+}
+
+// Bytes [0, n) of src to dst by the threads of one CTA, in words of W bytes
+// between a byte-wise head (up to dst's W alignment) and tail; src and dst
+// have the same address modulo W.
+template <typename Word>
+__device__ __forceinline__ void copy_words(const unsigned char* __restrict__ src,
+                                           unsigned char* __restrict__ dst, long long n) {
+    constexpr int W = sizeof(Word);
+    long long head = static_cast<long long>((W - (reinterpret_cast<uintptr_t>(dst) & (W - 1))) & (W - 1));
+    if (head > n) head = n;
+    for (long long t = threadIdx.x; t < head; t += blockDim.x) dst[t] = src[t];
+    const long long words = (n - head) / W;
+    const Word* s = reinterpret_cast<const Word*>(src + head);
+    Word* d = reinterpret_cast<Word*>(dst + head);
+    for (long long t = threadIdx.x; t < words; t += blockDim.x) d[t] = s[t];
+    for (long long t = head + words * W + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+}
+
+// Device-to-device copies, one piece per CTA at a time (pieces of at most
+// kCopyPiece bytes, so that one long copy spreads over many CTAs): 16-byte
+// words when source and destination agree modulo 16, else 8, 4 or 1.
+__global__ void __launch_bounds__(NT) k_copy_pieces(const CopyPiece* __restrict__ pieces,
+                                                    long long n) {
+    for (long long j = blockIdx.x; j < n; j += gridDim.x) {
+        const CopyPiece c = pieces[j];
+        const uintptr_t mis = reinterpret_cast<uintptr_t>(c.src) ^ reinterpret_cast<uintptr_t>(c.dst);
+        if (!(mis & 15)) copy_words<uint4>(c.src, c.dst, c.bytes);
+        else if (!(mis & 7)) copy_words<unsigned long long>(c.src, c.dst, c.bytes);
+        else if (!(mis & 3)) copy_words<unsigned>(c.src, c.dst, c.bytes);
+        else copy_words<unsigned char>(c.src, c.dst, c.bytes);
+    }
+}
+
 // 1-rank migrate of the drop-in: every particle stays and keeps its slot; its
 // position is replaced by the once-wrapped value (dsDecompX
 // src/migration.cpp:106-116).  Only changed values are written back.
@@ -2489,6 +2543,39 @@ void launch_out_of_domain(const Grid& G, const double* x, const double* y, const
 
 void mark(const Scratch& S, cudaStream_t s, const char* what) {
     if (S.marks) S.marks->mark(s, what);
+}
+
+void launch_pair_counts(int P, const Scratch& S, const int* obase_old, long long ncap, int* pairs,
+                        cudaStream_t s) {
+    cudaMemsetAsync(pairs, 0, sizeof(int) * static_cast<std::size_t>(P) * P, s);
+    if (ncap > 0)
+        k_pair_counts<<<stream_grid(ncap), NT, 0, s>>>(P, S.emig_info, S.emig_src, S.emig_dst,
+                                                       obase_old, pairs);
+}
+
+cudaError_t launch_copies(const std::vector<CopyPiece>& copies, cudaStream_t s) {
+    std::vector<CopyPiece> pieces;
+    for (const CopyPiece& c : copies)
+        for (long long at = 0; at < c.bytes; at += kCopyPiece)
+            pieces.push_back({c.src + at, c.dst + at,
+                              c.bytes - at < kCopyPiece ? c.bytes - at : kCopyPiece});
+    if (pieces.empty()) return cudaSuccess;
+    // the descriptors live in stream-ordered memory: freed after the kernel
+    // on the same stream, so that calls on different streams never share them
+    CopyPiece* d = nullptr;
+    const std::size_t bytes = sizeof(CopyPiece) * pieces.size();
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&d), bytes, s);
+    if (e != cudaSuccess) return e;
+    // pageable source: the call returns once the descriptors are staged
+    e = cudaMemcpyAsync(d, pieces.data(), bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        const long long n = static_cast<long long>(pieces.size());
+        const long long cap = static_cast<long long>(sm_count()) * 8;
+        k_copy_pieces<<<static_cast<int>(n < cap ? n : cap), NT, 0, s>>>(d, n);
+        e = cudaGetLastError();
+    }
+    const cudaError_t f = cudaFreeAsync(d, s);
+    return e != cudaSuccess ? e : f;
 }
 
 void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,

@@ -4,6 +4,8 @@
 
 #include "dsx_device.cuh"
 
+#include <vector>
+
 namespace dsx {
 
 // Optional per-kernel timing: when `on`, every launch wrapper records an
@@ -165,6 +167,21 @@ void launch_owner_rank(const Grid& G, const double* x, const double* y, const do
 // to another subdomain.
 void launch_out_of_domain(const Grid& G, const double* x, const double* y, const double* z,
                           int* flags, cudaStream_t s);
+
+// Emigrants of the last migration per (destination, source), dest-major
+// P x P, from the emigrant list and the old layout's offsets.
+void launch_pair_counts(int P, const Scratch& S, const int* obase_old, long long ncap, int* pairs,
+                        cudaStream_t s);
+
+// One device-to-device copy; launch_copies splits them into pieces of at
+// most kCopyPiece bytes and runs them all in one kernel on `s`.
+struct CopyPiece {
+    const unsigned char* src;
+    unsigned char* dst;
+    long long bytes;
+};
+constexpr long long kCopyPiece = 256 * 1024;
+cudaError_t launch_copies(const std::vector<CopyPiece>& copies, cudaStream_t s);
 
 // Records a named timing mark on `s` (no-op unless S.marks->on).
 void mark(const Scratch& S, cudaStream_t s, const char* what);

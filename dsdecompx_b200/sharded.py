@@ -1,0 +1,750 @@
+"""Sharded virtual grid: the P subdomains of one box split over R processes.
+
+The reference runs one MPI rank per subdomain; here one process per GPU owns
+a block of subdomains (contiguous Cartesian blocks of the process grid, so
+that the surface between processes is small) and keeps a grid of all P
+subdomains that holds particles only in its own.  Every collective call runs
+the local call of that grid, then ONE exchange step with the processes that
+own the receiving subdomains, then assembles its own subdomains in the
+reference's order (dsDecompX src/migration.cpp:147-389, src/halo.cpp:609-649,
+src/halo.cpp:956-1040):
+
+* migrate: subdomain t holds its retained particles, then the immigrants of
+  every source subdomain q in ascending q, whichever process q lives on.  The
+  local migrate already places particles bound for another process's
+  subdomain t into the local copy of t, grouped by source in ascending order;
+  those groups are sent to t's owner.  The (destination, source) counts are
+  summed over all processes first, so every receiver knows where each group
+  goes and how many bytes each peer sends.
+* exchange_halo: receiver t's ghosts are its neighbors' send lists in t's
+  own neighbor-block order.  The local build writes the lists of local
+  senders (to every receiver); lists for another process's receiver are sent
+  there, and every process assembles its receivers' blocks into a separate
+  ghost region (the one its callers read and write).
+* reverse_halo: the forces of every assembled ghost go back to the process
+  that owns its sender, into the local grid's slot of the same list, and the
+  local reverse_halo sums each owner's images in the reference's order.
+* forward_exchange / reverse_exchange of registered fields follow the
+  refresh and the reverse.
+
+The protocol is written once, as generator steps that yield communication
+requests (:class:`AllReduce` of a small vector, :class:`Exchange` of byte
+buffers with peers).  :func:`run_distributed` serves them with
+torch.distributed (NCCL between GPUs, gloo on CPU: grouped point-to-point
+sends and receives per peer), :func:`run_lockstep` serves several shards of
+one process in lockstep (a received buffer is the sender's own).  Engines
+(the device engine here, or any object with the same methods) do the local
+work; a shard never reads another shard's memory except through a request.
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import ARRAYS, COPY_DTYPE, SEGMENT_DTYPE, VirtualGrid, copy_segments
+
+KMAX = 26           # neighbor entries per subdomain
+XYZ = [0, 1, 2]     # array ids of the positions
+FORCES = [6, 7, 8]  # array ids of the forces
+
+
+# ------------------------------------------------------------ requests
+
+class AllReduce:
+    """Sum of a numeric vector over all shards (every shard gets the sum)."""
+
+    def __init__(self, values: np.ndarray):
+        self.values = np.ascontiguousarray(values)
+
+
+class Exchange:
+    """Point-to-point exchange: sends[p] goes to shard p; recv_bytes[p] is the
+    size of what shard p sends here (both sides derive the sizes from the
+    same all-reduced counts; empty messages are not sent)."""
+
+    def __init__(self, sends: Dict[int, object], recv_bytes: Dict[int, int]):
+        self.sends = sends
+        self.recv_bytes = recv_bytes
+
+
+def run_distributed(gen, device="cuda", group=None):
+    """Runs one shard's protocol steps over torch.distributed (this process is
+    the shard with the process group's rank)."""
+    import torch
+    import torch.distributed as dist
+    reply = None
+    while True:
+        try:
+            req = gen.send(reply)
+        except StopIteration as stop:
+            return stop.value
+        if isinstance(req, AllReduce):
+            t = torch.from_numpy(req.values.copy()).to(device)
+            dist.all_reduce(t, group=group)
+            reply = t.cpu().numpy()
+        elif isinstance(req, Exchange):
+            ops, recv = [], {}
+            for p in sorted(req.recv_bytes):
+                n = int(req.recv_bytes[p])
+                if n:
+                    buf = torch.empty(n, dtype=torch.uint8, device=device)
+                    recv[p] = buf
+                    ops.append(dist.P2POp(dist.irecv, buf, p, group))
+            for p in sorted(req.sends):
+                buf = req.sends[p]
+                if buf is not None and buf.numel():
+                    ops.append(dist.P2POp(dist.isend, buf, p, group))
+            if ops:
+                for w in dist.batch_isend_irecv(ops):
+                    w.wait()
+            reply = recv
+        else:
+            raise TypeError(f"unknown request {req!r}")
+
+
+def run_lockstep(gens: Sequence):
+    """Runs the protocol steps of several shards of this process together:
+    shard i's generator is gens[i]; every shard must make the same requests in
+    the same order."""
+    R = len(gens)
+    replies: List[object] = [None] * R
+    while True:
+        reqs, done = [], []
+        for i, g in enumerate(gens):
+            try:
+                reqs.append(g.send(replies[i]))
+            except StopIteration as stop:
+                done.append(stop.value)
+        if done:
+            if len(done) != R:
+                raise RuntimeError("shards left the protocol at different steps")
+            return done
+        kinds = {type(r) for r in reqs}
+        if len(kinds) != 1:
+            raise RuntimeError("shards made different requests")
+        if isinstance(reqs[0], AllReduce):
+            total = reqs[0].values.copy()
+            for r in reqs[1:]:
+                total = total + r.values
+            replies = [total.copy() for _ in range(R)]
+        else:
+            replies = []
+            for i in range(R):
+                got = {}
+                for p, n in reqs[i].recv_bytes.items():
+                    if not n:
+                        continue
+                    buf = reqs[p].sends.get(i)
+                    if buf is None or int(buf.numel()) != int(n):
+                        raise RuntimeError(f"shard {p} sends {0 if buf is None else buf.numel()} "
+                                           f"bytes to shard {i}, which expects {n}")
+                    got[p] = buf
+                replies.append(got)
+
+
+# ------------------------------------------------------- host planning
+
+def subdomain_coords(rank: int, dims) -> Tuple[int, int, int]:
+    """Row-major process-grid coordinates (z fastest), as the reference's
+    Cartesian communicator numbers its ranks."""
+    return rank // (dims[1] * dims[2]), (rank // dims[2]) % dims[1], rank % dims[2]
+
+
+def block_owners(dims, nshards: int) -> np.ndarray:
+    """Shard of every subdomain: contiguous Cartesian blocks when some
+    (a, b, c), a * b * c = nshards, divides dims (the one with the least cut
+    area between blocks; ties: the first in (a, b, c) order), else
+    contiguous runs of subdomain ranks."""
+    P = int(np.prod(dims))
+    if nshards < 1 or nshards > P:
+        raise ValueError("shards must be in 1..P")
+    best = None
+    for a in range(1, nshards + 1):
+        if nshards % a or dims[0] % a:
+            continue
+        for b in range(1, nshards // a + 1):
+            if (nshards // a) % b or dims[1] % b:
+                continue
+            c = nshards // a // b
+            if dims[2] % c:
+                continue
+            cut = (a - 1) * dims[1] * dims[2] + (b - 1) * dims[0] * dims[2] + (c - 1) * dims[0] * dims[1]
+            if best is None or cut < best[0]:
+                best = (cut, a, b, c)
+    owners = np.zeros(P, dtype=np.int64)
+    if best is None:
+        for t in range(P):
+            owners[t] = t * nshards // P
+        return owners
+    _, a, b, c = best
+    bx, by, bz = dims[0] // a, dims[1] // b, dims[2] // c
+    for t in range(P):
+        x, y, z = subdomain_coords(t, dims)
+        owners[t] = ((x // bx) * b + y // by) * c + z // bz
+    return owners
+
+
+def halo_tables(topology):
+    """(nn[P], sender_of[P, 26]) from every subdomain's neighbor list:
+    receiver t's block m holds the list of its neighbor q toward -d_m, entry
+    q * 26 + n (-1: no sender), the matching rule of the reference's receives
+    (src/halo.cpp:609-649)."""
+    P = len(topology)
+    nn = np.array([len(t) for t in topology], dtype=np.int64)
+    sender_of = np.full((P, KMAX), -1, dtype=np.int64)
+    for t in range(P):
+        for m, nb in enumerate(topology[t]):
+            q = nb["rank"]
+            if q < 0:
+                continue
+            want = tuple(-d for d in nb["direction"])
+            for n, back in enumerate(topology[q]):
+                if tuple(back["direction"]) == want:
+                    sender_of[t, m] = q * KMAX + n
+                    break
+    return nn, sender_of
+
+
+def packed_bytes(n: int, elem_bytes: Sequence[int]) -> int:
+    """Size of a packed buffer of n records: one section per array, each
+    starting on a 16-byte boundary."""
+    return int(sum((n * b + 15) // 16 * 16 for b in elem_bytes))
+
+
+def section_offsets(n: int, elem_bytes: Sequence[int]) -> List[int]:
+    out, at = [], 0
+    for b in elem_bytes:
+        out.append(at)
+        at += (n * b + 15) // 16 * 16
+    return out
+
+
+class GhostPlan:
+    """Where every block of this shard's receivers comes from and where the
+    lists of its senders go (ranges are (source index, destination index,
+    count) rows)."""
+
+    def __init__(self, shard, owners, nn, sender_of, length, first):
+        P = len(owners)
+        mine = np.flatnonzero(owners == shard)
+        self.g = np.zeros(P, dtype=np.int64)          # assembled ghosts per receiver
+        self.gbase = np.zeros(P, dtype=np.int64)      # first assembled slot per receiver
+        self.local: List[Tuple[int, int, int]] = []   # engine ghost slot -> assembled slot
+        self.recv: Dict[int, List[Tuple[int, int, int]]] = {}   # buffer offset -> assembled slot
+        self.send: Dict[int, List[Tuple[int, int, int]]] = {}   # engine ghost slot -> buffer offset
+        at = 0
+        recv_at: Dict[int, int] = {}
+        for t in mine:
+            self.gbase[t] = at
+            for m in range(nn[t]):
+                e = sender_of[t, m]
+                if e < 0 or length[e] == 0:
+                    continue
+                p = int(owners[e // KMAX])
+                n = int(length[e])
+                if p == shard:
+                    self.local.append((int(first[e]), at, n))
+                else:
+                    off = recv_at.get(p, 0)
+                    self.recv.setdefault(p, []).append((off, at, n))
+                    recv_at[p] = off + n
+                at += n
+            self.g[t] = at - self.gbase[t]
+        self.total = at
+        send_at: Dict[int, int] = {}
+        for t in range(P):
+            p = int(owners[t])
+            if p == shard:
+                continue
+            for m in range(nn[t]):
+                e = sender_of[t, m]
+                if e < 0 or length[e] == 0 or owners[e // KMAX] != shard:
+                    continue
+                off = send_at.get(p, 0)
+                n = int(length[e])
+                self.send.setdefault(p, []).append((int(first[e]), off, n))
+                send_at[p] = off + n
+        self.recv_n = recv_at
+        self.send_n = send_at
+
+
+def _rows(ranges) -> np.ndarray:
+    return np.asarray(ranges, dtype=np.int64).reshape(-1, 3)
+
+
+def _swap(ranges) -> np.ndarray:
+    r = _rows(ranges)
+    return r[:, [1, 0, 2]]
+
+
+# --------------------------------------------------------- the grid
+
+class ShardedGrid:
+    """One shard of a sharded virtual grid.
+
+    engine: the local engine (a :class:`DeviceEngine` for the device path);
+    shard, nshards: this shard's index and the number of shards; owners:
+    shard of every subdomain (default :func:`block_owners`); run: how the
+    protocol's requests are served when a method is called directly
+    (default :func:`run_distributed`).  The ``*_steps`` methods return the
+    protocol generators themselves, for :func:`run_lockstep`.
+    """
+
+    def __init__(self, engine, shard: int, nshards: int, owners=None, run=None):
+        self.E = engine
+        self.P = engine.P
+        self.shard, self.nshards = int(shard), int(nshards)
+        self.owners = (np.asarray(owners, dtype=np.int64) if owners is not None
+                       else block_owners(engine.dims, nshards))
+        if self.owners.shape != (self.P,) or self.owners.min() < 0 or self.owners.max() >= nshards:
+            raise ValueError("owners must give a shard in 0..nshards-1 for every subdomain")
+        self.mine = np.flatnonzero(self.owners == self.shard)
+        self.nn, self.sender_of = halo_tables(engine.topology)
+        self.plan: Optional[GhostPlan] = None
+        self.run = run or (lambda gen: run_distributed(gen, device=engine.device))
+        self._prev_ids = None
+
+    # ---- particles
+    def upload(self, per_subdomain: Dict[int, Dict[str, np.ndarray]]):
+        """Particles of this shard's subdomains (dicts of host arrays keyed by
+        subdomain; missing subdomains are empty)."""
+        for t in per_subdomain:
+            if self.owners[t] != self.shard:
+                raise ValueError(f"subdomain {t} belongs to shard {self.owners[t]}")
+        self.E.upload(per_subdomain)
+        self.plan = None
+
+    def counts(self, t: int) -> Tuple[int, int]:
+        self._check_mine(t)
+        g = int(self.plan.g[t]) if self.plan is not None else 0
+        return int(self.E.owned_counts()[t]), g
+
+    def read(self, t: int, name: str) -> np.ndarray:
+        """Owned records then assembled ghosts of subdomain t (array `name`)."""
+        self._check_mine(t)
+        owned = self.E.read_owned(t, name)
+        if self.plan is None or not self.plan.g[t]:
+            return owned
+        ghosts = self.E.read_assembled(int(self.plan.gbase[t]), int(self.plan.g[t]), name)
+        return np.concatenate([owned, ghosts])
+
+    def write_ghosts(self, t: int, name: str, values):
+        """Values of the assembled ghosts of subdomain t (array `name`)."""
+        self._check_mine(t)
+        if self.plan is None:
+            raise RuntimeError("no halo plan: call exchange_halo first")
+        n = int(self.plan.g[t])
+        v = np.asarray(values)
+        if v.shape[0] != n:
+            raise ValueError(f"subdomain {t} has {n} ghosts")
+        self.E.write_assembled(int(self.plan.gbase[t]), name, v)
+
+    def write_owned(self, t: int, name: str, start: int, values):
+        self._check_mine(t)
+        self.E.write_owned(t, name, start, values)
+
+    def snapshot(self, t: int) -> Dict[str, np.ndarray]:
+        out = {name: self.read(t, name) for name in self.E.names}
+        out["owned"], out["ghosts"] = self.counts(t)
+        return out
+
+    def _check_mine(self, t: int):
+        if self.owners[t] != self.shard:
+            raise ValueError(f"subdomain {t} belongs to shard {self.owners[t]}")
+
+    # ---- collective calls (every shard calls them in the same order)
+    def migrate(self):
+        return self.run(self.migrate_steps())
+
+    def rebalance(self, work=None, force: bool = False):
+        return self.run(self.rebalance_steps(work, force))
+
+    def exchange_halo(self, rebuild: bool = False, positions_only: bool = False):
+        return self.run(self.exchange_halo_steps(rebuild, positions_only))
+
+    def reverse_halo(self):
+        return self.run(self.reverse_halo_steps())
+
+    def forward_exchange(self, names: Sequence[str]):
+        return self.run(self.forward_exchange_steps(names))
+
+    def reverse_exchange(self, fields: Sequence[Tuple[str, str]]):
+        return self.run(self.reverse_exchange_steps(fields))
+
+    def step(self, callback=None):
+        """migrate -> exchange_halo(rebuild) -> callback(self) -> reverse_halo."""
+        return self.run(self.step_steps(callback))
+
+    # ---- protocol steps
+    def step_steps(self, callback=None):
+        mig = yield from self.migrate_steps()
+        halo = yield from self.exchange_halo_steps(True, False)
+        if callback is not None:
+            callback(self)
+        yield from self.reverse_halo_steps()
+        return mig, halo
+
+    def migrate_steps(self):
+        E = self.E
+        if E.dynamic:
+            # the automatic rebalance sees every shard's counts
+            total = yield AllReduce(E.owned_counts().astype(np.float64))
+            E.set_rebalance_work(total)
+        res = E.migrate_local()
+        return (yield from self._redistribute(res))
+
+    def rebalance_steps(self, work=None, force: bool = False):
+        E = self.E
+        local = np.zeros(self.P, dtype=np.float64)
+        if work is None:
+            local[self.mine] = E.owned_counts()[self.mine]
+        else:
+            w = np.asarray(work, dtype=np.float64)
+            local[self.mine] = w[self.mine] if w.shape == (self.P,) else w
+        total = yield AllReduce(local)
+        flags, imbalance = E.rebalance_local(total, force)
+        res = E.last_migration()
+        mig = yield from self._redistribute(res)
+        out = {t: (int(flags[t, 0]), int(flags[t, 1]), int(mig[t][5])) for t in self.mine}
+        return out, float(imbalance)
+
+    def _redistribute(self, res):
+        """Sends every particle the local migrate placed into another shard's
+        subdomain to that shard and assembles this shard's subdomains."""
+        E, P, me, owners = self.E, self.P, self.shard, self.owners
+        M = E.migration_pairs()
+        Mg = (yield AllReduce(M.reshape(-1).astype(np.int64))).reshape(P, P)
+        local_n = res[:, 5].astype(np.int64)
+        obase = np.concatenate([[0], np.cumsum(local_n)])
+        allb = E.elem_bytes_all
+        sends = {}
+        for p in range(self.nshards):
+            if p == me:
+                continue
+            ts = [t for t in np.flatnonzero(owners == p) if local_n[t] > 0]
+            if not ts:
+                continue
+            n = int(sum(local_n[t] for t in ts))
+            rows, at = [], 0
+            for t in ts:
+                rows.append((int(obase[t]), at, int(local_n[t])))
+                at += int(local_n[t])
+            buf = E.new_buffer(packed_bytes(n, allb))
+            E.copy(("buffer", buf, n, E.all_arrays), ("owned",), _rows(rows), E.all_arrays)
+            sends[p] = buf
+        # what each peer sends: its sources' groups for my subdomains
+        per_peer = np.zeros((self.nshards, P), dtype=np.int64)   # [p, t]
+        for p in range(self.nshards):
+            if p != me:
+                per_peer[p] = Mg[:, owners == p].sum(axis=1)
+        recv_bytes = {p: packed_bytes(int(per_peer[p, self.mine].sum()), allb)
+                      for p in range(self.nshards) if p != me}
+        recv = yield Exchange(sends, recv_bytes)
+        # new layout: retained, then sources in ascending order
+        new_counts = np.zeros(P, dtype=np.int64)
+        peers = sorted(recv)
+        src_of = {p: k for k, p in enumerate(peers)}
+        peer_at = {p: 0 for p in peers}
+        segs = []
+        out = {}
+        for t in self.mine:
+            retained = int(res[t, 2])
+            received = int(Mg[t].sum())
+            new_counts[t] = retained + received
+            if retained:
+                segs.append((-1, int(obase[t]), int(t), 0, retained))
+            dst = retained
+            local_at = int(obase[t]) + retained
+            for q in np.flatnonzero(Mg[t]):
+                c = int(Mg[t, q])
+                p = int(owners[q])
+                if p == me:
+                    segs.append((-1, local_at, int(t), dst, c))
+                    local_at += c
+                else:
+                    segs.append((src_of[p], peer_at[p], int(t), dst, c))
+                    peer_at[p] += c
+                dst += c
+            sent = int(res[t, 3])
+            out[int(t)] = (int(sent != 0 or received != 0), int(res[t, 1]), retained, sent, received,
+                           int(new_counts[t]))
+        seg = np.zeros(len(segs), dtype=SEGMENT_DTYPE)
+        for i, s in enumerate(segs):
+            seg[i] = s
+        E.assemble_owned(new_counts, [(recv[p], int(per_peer[p, self.mine].sum())) for p in peers], seg)
+        self.plan = None
+        return out
+
+    def exchange_halo_steps(self, rebuild: bool = False, positions_only: bool = False):
+        E = self.E
+        build = rebuild or self.plan is None
+        E.halo_local(build, positions_only and not build)
+        if build:
+            length, first = E.send_lists()
+            total = yield AllReduce(length.astype(np.int64))
+            length = total.astype(np.int64)
+            prev = self.plan
+            self.plan = GhostPlan(self.shard, self.owners, self.nn, self.sender_of, length, first)
+            grew = E.ensure_assembled(self.plan.total)
+        else:
+            prev, grew = self.plan, False
+        arrays = XYZ if (positions_only and not build) else E.all_arrays
+        old_ids = E.assembled_ids(prev.total) if (build and prev is not None) else None
+        yield from self._ship_lists(arrays)
+        plan = self.plan
+        out = {}
+        for t in self.mine:
+            # layout_changed (src/runtime.cpp:966-980): a requested rebuild,
+            # another ghost count (none since a migrate) or other ghost ids
+            g = int(plan.g[t])
+            if rebuild:
+                changed = 1
+            elif prev is None:
+                changed = int(g != 0)
+            elif int(prev.g[t]) != g:
+                changed = 1
+            elif not build:
+                changed = 0
+            else:
+                changed = int(not E.same_ids(old_ids, int(prev.gbase[t]), int(plan.gbase[t]), g))
+            out[int(t)] = (g, changed, int(grew), int(not build))
+        return out
+
+    def _ship_lists(self, arrays):
+        """Lists of local senders: into the assembled region (own receivers)
+        or to the receivers' shards; lists of other shards' senders into the
+        assembled region."""
+        E, plan = self.E, self.plan
+        b = [E.elem_bytes[a] for a in arrays]
+        sends = {}
+        for p, rows in plan.send.items():
+            n = plan.send_n[p]
+            buf = E.new_buffer(packed_bytes(n, b))
+            E.copy(("buffer", buf, n, arrays), ("ghost",), _rows(rows), arrays)
+            sends[p] = buf
+        recv_bytes = {p: packed_bytes(n, b) for p, n in plan.recv_n.items()}
+        recv = yield Exchange(sends, recv_bytes)
+        if plan.local:
+            E.copy(("assembled",), ("ghost",), _rows(plan.local), arrays)
+        for p, rows in plan.recv.items():
+            E.copy(("assembled",), ("buffer", recv[p], plan.recv_n[p], arrays), _rows(rows), arrays)
+
+    def _return_lists(self, arrays):
+        """The inverse of _ship_lists: assembled values back into the local
+        engine's ghost slots of the same lists (own senders) or to the
+        senders' shards."""
+        E, plan = self.E, self.plan
+        b = [E.elem_bytes[a] for a in arrays]
+        if plan.local:
+            E.copy(("ghost",), ("assembled",), _swap(plan.local), arrays)
+        sends = {}
+        for p, rows in plan.recv.items():
+            n = plan.recv_n[p]
+            buf = E.new_buffer(packed_bytes(n, b))
+            E.copy(("buffer", buf, n, arrays), ("assembled",), _swap(rows), arrays)
+            sends[p] = buf
+        recv_bytes = {p: packed_bytes(n, b) for p, n in plan.send_n.items()}
+        recv = yield Exchange(sends, recv_bytes)
+        for p, rows in plan.send.items():
+            E.copy(("ghost",), ("buffer", recv[p], plan.send_n[p], arrays), _swap(rows), arrays)
+
+    def reverse_halo_steps(self):
+        if self.plan is None:
+            raise RuntimeError("reverse_halo without a halo plan")
+        yield from self._return_lists(FORCES)
+        self.E.reverse_local()
+
+    def forward_exchange_steps(self, names: Sequence[str]):
+        if self.plan is None:
+            raise RuntimeError("forward_exchange without a halo plan")
+        self.E.forward_local(list(names))
+        yield from self._ship_lists([self.E.array_id(n) for n in names])
+
+    def reverse_exchange_steps(self, fields: Sequence[Tuple[str, str]]):
+        if self.plan is None:
+            raise RuntimeError("reverse_exchange without a halo plan")
+        yield from self._return_lists([self.E.array_id(n) for n, _ in fields])
+        self.E.reverse_exchange_local(list(fields))
+
+
+# ----------------------------------------------------- device engine
+
+class DeviceEngine:
+    """The local engine of a shard on this process's GPU: a VirtualGrid of
+    all P subdomains, the assembled ghost region (device tensors), and the
+    copies between them as dsx_copy_segments calls on the current stream."""
+
+    device = "cuda"
+
+    def __init__(self, nranks: int, dims=(0, 0, 0), policy: str = "manual",
+                 lower=(0.0, 0.0, 0.0), upper=(1.0, 1.0, 1.0), periodic=(True, True, True),
+                 halo_width: float = 0.0, edges_and_corners: bool = True, dynamic=None,
+                 fields: Sequence[Tuple[str, object, int]] = (), particles: int = 0,
+                 ghost_capacity: int = 0):
+        import torch
+        self.torch = torch
+        self.grid = VirtualGrid(nranks, dims, policy, lower, upper, periodic, halo_width,
+                                edges_and_corners, dynamic, fields, particles, ghost_capacity)
+        self.P = nranks
+        self.dims = self.grid.topology(0)[0]
+        self.topology = [self.grid.neighbors(t) for t in range(nranks)]
+        self.dynamic = policy == "dynamic"
+        self.names = ARRAYS + [f[0] for f in self.grid.fields]
+        self.all_arrays = list(range(len(self.names)))
+        self.elem_bytes = [np.dtype(self.grid.dtype_of(n)).itemsize * self.grid.components(n)
+                           for n in self.names]
+        self.elem_bytes_all = list(self.elem_bytes)
+        self.asm_cap = 0
+        self.asm: List = []
+        self._last_migration = None
+
+    def close(self):
+        self.grid.close()
+
+    def array_id(self, name: str) -> int:
+        return self.names.index(name)
+
+    # ---- local calls
+    def owned_counts(self) -> np.ndarray:
+        return self.grid.all_counts()[0]
+
+    def set_rebalance_work(self, work):
+        self.grid.set_rebalance_work(work)
+
+    def migrate_local(self):
+        return self.grid.migrate()
+
+    def rebalance_local(self, work, force):
+        # Decomp::rebalance: explicit rebalance, then a migrate without the
+        # automatic one; its per-subdomain counts follow from the layout
+        before = self.owned_counts()
+        flags, imbalance = self.grid.rebalance(work, force)
+        self._last_migration = before
+        return flags, imbalance[0] if len(imbalance) else 1.0
+
+    def last_migration(self):
+        """Per-subdomain results of the migrate inside the last rebalance, in
+        migrate's format (previous from before, the rest from the pairs)."""
+        before = self._last_migration
+        pairs = self.grid.migration_pairs()
+        now = self.owned_counts()
+        sent = pairs.sum(axis=0)
+        received = pairs.sum(axis=1)
+        res = np.zeros((self.P, 6), dtype=np.int64)
+        res[:, 1] = before
+        res[:, 2] = before - sent
+        res[:, 3] = sent
+        res[:, 4] = received
+        res[:, 5] = now
+        res[:, 0] = (sent != 0) | (received != 0)
+        return res
+
+    def migration_pairs(self):
+        return self.grid.migration_pairs()
+
+    def halo_local(self, build: bool, positions_only: bool):
+        return self.grid.exchange_halo(rebuild=build, positions_only=positions_only)
+
+    def send_lists(self):
+        return self.grid.send_lists()
+
+    def reverse_local(self):
+        self.grid.reverse_halo()
+
+    def forward_local(self, names):
+        self.grid.forward_exchange(names)
+
+    def reverse_exchange_local(self, fields):
+        self.grid.reverse_exchange(fields)
+
+    def upload(self, per_subdomain):
+        empty = {n: np.zeros((0,) + ((self.grid.components(n),) if self.grid.components(n) > 1 else ()),
+                             dtype=self.grid.dtype_of(n)) for n in self.names}
+        self.grid.upload([per_subdomain.get(t, empty) for t in range(self.P)])
+
+    # ---- memory
+    def new_buffer(self, nbytes: int):
+        return self.torch.empty(int(nbytes), dtype=self.torch.uint8, device="cuda")
+
+    def ensure_assembled(self, n: int) -> bool:
+        if n <= self.asm_cap:
+            return False
+        cap = max(int(n * 1.25), 1024)
+        new = [self.torch.empty(cap * b, dtype=self.torch.uint8, device="cuda") for b in self.elem_bytes]
+        if self.asm:
+            for a, b in enumerate(self.elem_bytes):
+                new[a][:self.asm_cap * b].copy_(self.asm[a])
+        self.asm, self.asm_cap = new, cap
+        return True
+
+    def _bases(self, place, arrays):
+        kind = place[0]
+        v = self.grid.view()
+        if kind == "owned":
+            return [v.base[a] + int(v.owned_offset) * self.elem_bytes[a] for a in arrays]
+        if kind == "ghost":
+            return [v.base[a] + int(v.ghost_offset) * self.elem_bytes[a] for a in arrays]
+        if kind == "assembled":
+            return [self.asm[a].data_ptr() for a in arrays]
+        if kind == "buffer":
+            _, buf, n, sections = place
+            offs = section_offsets(n, [self.elem_bytes[a] for a in sections])
+            at = {a: o for a, o in zip(sections, offs)}
+            return [buf.data_ptr() + at[a] for a in arrays]
+        raise ValueError(kind)
+
+    def copy(self, dst, src, rows: np.ndarray, arrays):
+        """rows: (source index, destination index, count) per range; every
+        array of `arrays` is copied."""
+        if not len(rows):
+            return
+        sb, db = self._bases(src, arrays), self._bases(dst, arrays)
+        out = np.zeros(len(rows) * len(arrays), dtype=COPY_DTYPE)
+        for j, a in enumerate(arrays):
+            b = self.elem_bytes[a]
+            part = out[j * len(rows):(j + 1) * len(rows)]
+            part["src"] = (sb[j] + rows[:, 0] * b).astype(np.uint64)
+            part["dst"] = (db[j] + rows[:, 1] * b).astype(np.uint64)
+            part["bytes"] = rows[:, 2] * b
+        copy_segments(out[out["bytes"] > 0], self.torch.cuda.current_stream().cuda_stream)
+
+    def assemble_owned(self, counts, buffers, segments):
+        sources = []
+        for buf, n in buffers:
+            sources.append(self._bases(("buffer", buf, n, self.all_arrays), self.all_arrays))
+        self.grid.assemble(counts, sources, segments)
+
+    # ---- ids and host reads
+    def assembled_ids(self, n: int):
+        if not n:
+            return None
+        return self.asm[12][:n * 4].view(self.torch.int32).clone()
+
+    def same_ids(self, old, old_lo: int, new_lo: int, n: int) -> bool:
+        if n == 0:
+            return True
+        new = self.asm[12][new_lo * 4:(new_lo + n) * 4].view(self.torch.int32)
+        return bool(self.torch.equal(old[old_lo:old_lo + n], new))
+
+    def read_owned(self, t: int, name: str) -> np.ndarray:
+        return self.grid.read(t, name, 0, self.grid.counts(t)[0])
+
+    def write_owned(self, t: int, name: str, start: int, values):
+        self.grid.write(t, name, start, values)
+
+    def read_assembled(self, lo: int, n: int, name: str) -> np.ndarray:
+        a = self.array_id(name)
+        b = self.elem_bytes[a]
+        raw = self.asm[a][lo * b:(lo + n) * b].cpu().numpy()
+        dt = np.dtype(self.grid.dtype_of(name))
+        comps = self.grid.components(name)
+        out = raw.view(dt)
+        return out.reshape(n, comps) if comps > 1 else out
+
+    def write_assembled(self, lo: int, name: str, values):
+        a = self.array_id(name)
+        b = self.elem_bytes[a]
+        arr = np.ascontiguousarray(values, dtype=self.grid.dtype_of(name)).reshape(-1)
+        raw = self.torch.from_numpy(arr.view(np.uint8).copy())
+        self.asm[a][lo * b:lo * b + raw.numel()].copy_(raw)

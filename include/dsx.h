@@ -307,6 +307,60 @@ int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report);
 int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
                         int reverse_ctas_per_sm);
 
+/* ---- sharded grids: the P subdomains split over several processes ----
+ *
+ * Each process keeps a grid of all P subdomains that holds particles only in
+ * the subdomains it owns.  After a local migrate or halo build the particles
+ * and ghost lists that belong to another process's subdomains are sent there,
+ * and each process assembles its subdomains in the reference's order
+ * (retained, then immigrants by source rank; ghosts by the receiver's
+ * neighbor blocks).  These calls are the local pieces of that exchange. */
+
+/* Emigrants of the last migration (dsx_grid_migrate, dsx_grid_rebalance or a
+ * batched step) per (destination, source): pairs[t * P + q] (synchronizes).
+ * DSX_E_LOGIC when the particles were replaced since (upload, assemble). */
+int dsx_grid_migration_pairs(dsx_grid* grid, long long* pairs, void* stream);
+
+/* The current plan's send lists, 26 per sender (entry q * 26 + n: sender q's
+ * list toward its neighbor n): length and first ghost slot (relative to the
+ * view's ghost_offset).  All zero without a plan (synchronizes). */
+int dsx_grid_send_lists(dsx_grid* grid, int* length, int* first_slot, void* stream);
+
+/* One copy of `count` records of every particle array into the next owned
+ * layout: from source `source` (-1: the grid's current owned particles, index
+ * src_index in the view's owned numbering; k >= 0: outside buffer k) to
+ * subdomain dst_rank at position dst_index. */
+typedef struct dsx_segment {
+    int source;
+    long long src_index;
+    int dst_rank;
+    long long dst_index;
+    long long count;
+} dsx_segment;
+
+/* Replaces the owned particles: counts[P] are the new per-subdomain counts,
+ * sources[32 * k + a] the address of element 0 of array a (dsx_grid_view
+ * order: 13 core arrays, then the fields) in outside buffer k (device
+ * memory), segments fill the new layout (positions not covered are left
+ * undefined).  The halo plan becomes invalid (synchronizes). */
+int dsx_grid_assemble(dsx_grid* grid, const long long* counts, int nsources,
+                      const void* const* sources, long long nsegments, const dsx_segment* segments,
+                      void* stream);
+
+/* Work per subdomain (P values) for the automatic Dynamic rebalance of the
+ * next dsx_grid_migrate, instead of this grid's owned counts (a sharded grid
+ * passes the counts of all processes); null clears it. */
+int dsx_grid_set_rebalance_work(dsx_grid* grid, const double* work);
+
+/* Device-to-device copies, all in one kernel on `stream` (stream ordered;
+ * the list itself may be reused when the call returns). */
+typedef struct dsx_copy {
+    const void* src;
+    void* dst;
+    long long bytes;
+} dsx_copy;
+int dsx_copy_segments(const dsx_copy* copies, long long n, void* stream);
+
 /* Plain launches, for comparison runs: plain != 0 makes the per-call
  * operations (dsx_grid_migrate, a rebuilding dsx_grid_exchange_halo,
  * dsx_grid_reverse_halo) launch each of their tile kernels once per subdomain

@@ -58,6 +58,7 @@ struct orc_grid {
     double dyn_threshold, dyn_relax, dyn_minfrac;
     size_t dyn_interval, migration_calls;
     int in_rebalance;
+    double* next_work;   /* work of the next automatic rebalance (null: owned counts) */
     int ghosts_valid;
     int ftype[MAXF];
     size_t fcomp[MAXF], fbytes[MAXF];
@@ -381,7 +382,19 @@ void orc_destroy(orc_grid* g) {
     }
     free(g->r);
     for (int a = 0; a < 3; ++a) free(g->cuts[a]);
+    free(g->next_work);
     free(g);
+}
+
+/* Work per rank for the next migrate's automatic rebalance instead of the
+ * owned counts (a sharded run passes the counts of every shard). */
+int orc_set_rebalance_work(orc_grid* g, const double* work) {
+    free(g->next_work);
+    g->next_work = NULL;
+    if (!work) return 0;
+    g->next_work = malloc(sizeof(double) * (size_t)g->P);
+    memcpy(g->next_work, work, sizeof(double) * (size_t)g->P);
+    return 0;
 }
 
 const char* orc_last_error(orc_grid* g) { return g ? g->err : "null grid"; }
@@ -445,6 +458,15 @@ int orc_set_owned(orc_grid* g, int rank, long long n, const double* const* core,
     }
     p->owned = (size_t)n;
     p->ghosts = 0;
+    return 0;
+}
+
+/* Ghosts of rank `rank` per receive block m (its neighbor order), as the
+ * last exchange_halo laid them out: out[m] for m < *count. */
+int orc_halo_blocks(orc_grid* g, int rank, int* count, long long* out) {
+    const rank_t* r = &g->r[rank];
+    *count = r->nn;
+    for (int m = 0; m < r->nn; ++m) out[m] = g->ghosts_valid ? (long long)r->recv_n[m] : 0;
     return 0;
 }
 
@@ -597,16 +619,23 @@ static rec_t wrapped_record(const orc_grid* g, const parts_t* p, size_t i) {
 static int migrate_inner(orc_grid* g, long long* results) {
     /* Decomp::migrate (src/runtime.cpp:983-1019): automatic Dynamic rebalance */
     ++g->migration_calls;
+    double* supplied = g->next_work;   /* one migrate only */
+    g->next_work = NULL;
     if (!g->in_rebalance && g->policy == 3 && g->dyn_interval != 0 &&
         g->migration_calls % g->dyn_interval == 0) {
         double* work = malloc(sizeof(double) * (size_t)g->P);
-        for (int s = 0; s < g->P; ++s) work[s] = (double)g->r[s].p.owned;
+        for (int s = 0; s < g->P; ++s)
+            work[s] = supplied ? supplied[s] : (double)g->r[s].p.owned;
         int attempted, changed;
         double imbalance;
         int status = rebalance_geometry(g, work, 0, &attempted, &changed, &imbalance);
         free(work);
-        if (status) return status;
+        if (status) {
+            free(supplied);
+            return status;
+        }
     }
+    free(supplied);
     int P = g->P;
     /* classify (src/migration.cpp:437-445) */
     int** dest = malloc(sizeof(int*) * (size_t)P);

@@ -47,6 +47,8 @@ int orc_set_owned(orc_grid* g, int rank, long long n,
                   const double* const* core, const int* type,
                   const int* global_id, const void* const* fields);
 int orc_counts(orc_grid* g, int rank, long long* owned, long long* ghosts);
+int orc_halo_blocks(orc_grid* g, int rank, int* count, long long* out);
+int orc_set_rebalance_work(orc_grid* g, const double* work);
 /* array ids: 0..10 x y z vx vy vz fx fy fz mass charge, 11 type,
  * 12 global_id, 13+f registered field f */
 int orc_read(orc_grid* g, int rank, int array, long long start,

@@ -242,6 +242,22 @@ class Grid:
                 fptrs[f] = arr.ctypes.data
         self._call("set_owned", rank, n, core, _ptr(typ), _ptr(gid), fptrs)
 
+    def set_rebalance_work(self, work=None):
+        """Work per rank for the next migrate's automatic rebalance."""
+        if self.kind != "port":
+            raise OracleError("set_rebalance_work is a call of the restatement")
+        w = None if work is None else np.ascontiguousarray(work, dtype=np.float64)
+        self._call("set_rebalance_work", None if w is None else w.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def halo_blocks(self, rank: int) -> np.ndarray:
+        """Ghosts of `rank` per receive block (its neighbor order)."""
+        if self.kind != "port":
+            raise OracleError("halo_blocks is a query of the restatement")
+        n = C.c_int()
+        out = np.zeros(26, dtype=np.int64)
+        self._call("halo_blocks", rank, C.byref(n), out.ctypes.data_as(C.POINTER(C.c_longlong)))
+        return out[:n.value]
+
     def counts(self, rank: int) -> Tuple[int, int]:
         o, g = C.c_longlong(), C.c_longlong()
         self._call("counts", rank, C.byref(o), C.byref(g))

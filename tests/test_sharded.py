@@ -1,0 +1,223 @@
+"""Sharded virtual grid: the host side on CPU.
+
+The planning helpers are checked directly; the protocol (migrate, halo build
+and refresh, reverse_halo, field exchanges, Dynamic rebalance) runs with
+shard engines over the oracle, R shards in lockstep in one process and two
+shards as gloo ranks, and every array of every subdomain is compared bit for
+bit with one oracle grid holding all subdomains.
+"""
+import datetime
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from helpers import ALL_FIELDS
+from oracle import Grid
+from shard_oracle import OracleEngine
+from shard_scenario import Scenario, distributed_drive, initial, lockstep_drive
+
+from dsdecompx_b200 import sharded as shd
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FIELDS3 = [(n, t, c) for n, t, c in ALL_FIELDS[:3]]
+TYPE_INDEX = {"int32": 0, "int64": 1, "uint32": 2, "uint64": 3, "float32": 4, "float64": 5}
+
+
+def oracle_fields(fields):
+    return [(n, TYPE_INDEX[t], c) for n, t, c in fields]
+
+
+# ------------------------------------------------------------ planning
+
+@pytest.mark.parametrize("dims,R", [((4, 4, 4), 8), ((4, 4, 4), 2), ((2, 2, 2), 4), ((3, 1, 4), 2),
+                                    ((3, 3, 3), 4), ((8, 8, 4), 8)])
+def test_block_owners(dims, R):
+    owners = shd.block_owners(dims, R)
+    P = int(np.prod(dims))
+    assert owners.shape == (P,) and set(owners) == set(range(R))
+    counts = np.bincount(owners, minlength=R)
+    assert counts.max() - counts.min() <= 1
+    if dims == (3, 3, 3):
+        # no exact block split: contiguous runs of ranks
+        assert (np.diff(owners) >= 0).all()
+    else:
+        # blocks: each shard's subdomains form a box of the process grid
+        for s in range(R):
+            c = np.array([shd.subdomain_coords(t, dims) for t in np.flatnonzero(owners == s)])
+            span = c.max(axis=0) - c.min(axis=0) + 1
+            assert np.prod(span) == len(c)
+
+
+def test_block_owners_prefers_the_smallest_cut():
+    # 8 x 8 x 4 over 4 shards: 2 x 2 x 1 cuts 2 * 32 faces, 4 x 1 x 1 cuts 3 * 32
+    owners = shd.block_owners((8, 8, 4), 4)
+    coords = np.array([shd.subdomain_coords(t, (8, 8, 4)) for t in range(256)])
+    assert len({tuple(c) for c in coords[owners == 0][:, :2] // 4}) == 1
+    assert set(coords[owners == 0][:, 2]) == {0, 1, 2, 3}
+
+
+@pytest.mark.parametrize("dims", [(2, 2, 2), (3, 1, 4), (4, 4, 4)])
+def test_halo_tables_point_back(dims):
+    from dsdecompx_b200 import plan_topology
+    P = int(np.prod(dims))
+    topo = [plan_topology(P, t, dims, "manual", (0, 0, 0), (1, 1, 1), (True, False, True))[1]
+            for t in range(P)]
+    nn, sender_of = shd.halo_tables(topo)
+    for t in range(P):
+        for m in range(nn[t]):
+            e = sender_of[t, m]
+            if topo[t][m]["rank"] < 0:
+                assert e == -1
+                continue
+            q, n = divmod(int(e), 26)
+            assert q == topo[t][m]["rank"]
+            assert topo[q][n]["rank"] == t
+            assert tuple(topo[q][n]["direction"]) == tuple(-d for d in topo[t][m]["direction"])
+
+
+def test_ghost_plans_agree_between_shards():
+    """What shard a sends shard b (lists and their order) is what b expects."""
+    from dsdecompx_b200 import plan_topology
+    dims, R = (4, 2, 3), 3
+    P = int(np.prod(dims))
+    topo = [plan_topology(P, t, dims)[1] for t in range(P)]
+    nn, sender_of = shd.halo_tables(topo)
+    owners = shd.block_owners(dims, R)
+    rng = np.random.default_rng(5)
+    length = np.zeros(P * 26, np.int64)
+    for t in range(P):
+        for n in range(nn[t]):
+            length[t * 26 + n] = rng.integers(0, 9)
+    first = np.concatenate([[0], np.cumsum(length)])[:-1]   # any local layout
+    plans = [shd.GhostPlan(s, owners, nn, sender_of, length, first) for s in range(R)]
+    for a in range(R):
+        for b in range(R):
+            if a == b:
+                continue
+            sent = [r[2] for r in plans[a].send.get(b, [])]
+            got = [r[2] for r in plans[b].recv.get(a, [])]
+            assert sent == got
+            assert plans[a].send_n.get(b, 0) == plans[b].recv_n.get(a, 0)
+    # every block of every receiver lands exactly once
+    for s in range(R):
+        p = plans[s]
+        covered = sorted([(r[1], r[2]) for r in p.local] +
+                         [(r[1], r[2]) for rows in p.recv.values() for r in rows])
+        at = 0
+        for lo, n in covered:
+            assert lo == at
+            at += n
+        assert at == p.total
+
+
+def test_packed_sections_are_aligned():
+    b = [8, 4, 12, 1]
+    offs = shd.section_offsets(5, b)
+    assert offs == [0, 48, 80, 144] and all(o % 16 == 0 for o in offs)
+    assert shd.packed_bytes(5, b) == 160
+
+
+# ------------------------------------------------------------ protocol
+
+def make_ref(kw, fields):
+    return Grid("port", kw["nranks"], kw["dims"], kw["policy"], (0, 0, 0), kw["upper"],
+                kw.get("periodic", (True, True, True)), kw["halo_width"], True, kw.get("dynamic"),
+                oracle_fields(fields))
+
+
+def make_shards(kw, fields, R, run=None):
+    shards = []
+    for s in range(R):
+        e = OracleEngine(kw["nranks"], kw["dims"], kw["policy"], (0, 0, 0), kw["upper"],
+                         kw.get("periodic", (True, True, True)), kw["halo_width"], True,
+                         kw.get("dynamic"), oracle_fields(fields))
+        shards.append(shd.ShardedGrid(e, s, R, run=run))
+    return shards
+
+
+CASES = {
+    "2x2x2-R2": dict(nranks=8, dims=(2, 2, 2), policy="manual", upper=(10.0, 10.0, 10.0),
+                     halo_width=1.0, N=3000),
+    "3x1x4-R3-open": dict(nranks=12, dims=(3, 1, 4), policy="manual", upper=(9.0, 5.0, 12.0),
+                          periodic=(True, False, False), halo_width=0.8, N=3000),
+    "dynamic-R4": dict(nranks=8, dims=(2, 2, 2), policy="dynamic", upper=(12.0, 12.0, 12.0),
+                       halo_width=0.9, dynamic=(1.0, 1.05, 0.5, 0.1), N=3000),
+}
+
+
+@pytest.mark.parametrize("case,R", [("2x2x2-R2", 2), ("3x1x4-R3-open", 3), ("dynamic-R4", 4)])
+def test_lockstep_shards_match_one_grid(case, R):
+    kw = CASES[case]
+    fields = FIELDS3
+    ref = make_ref(kw, fields)
+    shards = make_shards(kw, fields, R)
+    per = initial(ref, kw["nranks"], kw["upper"], kw["N"], 17, fields)
+    for t in range(kw["nranks"]):
+        ref.set_owned(t, per[t])
+    for sh in shards:
+        sh.upload({t: per[t] for t in sh.mine})
+    Scenario(shards, lockstep_drive(shards), ref, kw["nranks"], fields).run(steps=3, sigma=0.8)
+    if kw["policy"] == "dynamic":
+        assert not np.allclose(ref.cuts()[0], np.linspace(0, 12, 3))
+
+
+def test_lockstep_rebalance_with_work():
+    kw = CASES["dynamic-R4"]
+    fields = []
+    ref = make_ref(kw, fields)
+    shards = make_shards(kw, fields, 2)
+    per = initial(ref, 8, kw["upper"], kw["N"], 3, fields)
+    for t in range(8):
+        ref.set_owned(t, per[t])
+    for sh in shards:
+        sh.upload({t: per[t] for t in sh.mine})
+    work = np.linspace(1.0, 4.0, 8) * 100.0
+    flags, imb = ref.rebalance(work, force=True)
+    outs = shd.run_lockstep([sh.rebalance_steps(work, True) for sh in shards])
+    for sh, (out, imbalance) in zip(shards, outs):
+        assert imbalance == imb[0]
+        for t, row in out.items():
+            assert row == tuple(int(v) for v in flags[t])
+    for a, b in zip(ref.cuts(), shards[0].E.g.cuts()):
+        assert np.array_equal(a, b)
+    Scenario(shards, lockstep_drive(shards), ref, 8, fields).compare("after rebalance")
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def gloo_rank(rank, world, port, case):
+    import torch
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world,
+                                         timeout=datetime.timedelta(seconds=60))
+    try:
+        kw = CASES[case]
+        fields = FIELDS3
+        ref = make_ref(kw, fields)
+        e = OracleEngine(kw["nranks"], kw["dims"], kw["policy"], (0, 0, 0), kw["upper"],
+                         kw.get("periodic", (True, True, True)), kw["halo_width"], True,
+                         kw.get("dynamic"), oracle_fields(fields))
+        sh = shd.ShardedGrid(e, rank, world, run=lambda g: shd.run_distributed(g, device="cpu"))
+        per = initial(ref, kw["nranks"], kw["upper"], kw["N"], 23, fields)
+        for t in range(kw["nranks"]):
+            ref.set_owned(t, per[t])
+        sh.upload({t: per[t] for t in sh.mine})
+        Scenario([sh], distributed_drive(sh), ref, kw["nranks"], fields).run(steps=2, sigma=0.8)
+    finally:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+@pytest.mark.parametrize("case", ["2x2x2-R2", "dynamic-R4"])
+def test_two_gloo_ranks_match_one_grid(case):
+    mp.start_processes(gloo_rank, args=(2, free_port(), case), nprocs=2, start_method="spawn")
