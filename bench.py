@@ -10,9 +10,13 @@ reverse_halo, run as the batched, CUDA-graph-captured step of the virtual grid
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
                   [--impl ours|reference]
 
-Multi-GPU (torchrun): every rank runs its own replica of the workload; there
-is no data-path collective (the path does not shard across GPUs in this
-build), only a barrier and the max-over-ranks of the timed region.
+Multi-GPU (torchrun, one process per GPU): the sharded virtual grid.  The
+global grid is N copies of the workload's block (the box and the particle
+count grow with N: weak scaling); each rank owns one block of subdomains and
+every step exchanges migrants, ghost lists and ghost forces with the ranks
+that own the neighboring blocks over NCCL (grouped send/recv per peer).  The
+timed region is the max over ranks.  --sharded runs the same path on one GPU
+(one shard).
 """
 from __future__ import annotations
 
@@ -49,6 +53,8 @@ def parse():
                     help="keep the default launch shapes (no dsx_grid_autotune before timing)")
     ap.add_argument("--particles", type=int, default=0,
                     help="override the workload's particle count (small profiling cases)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="the sharded grid's step (the multi-GPU path) also at one GPU")
     return ap.parse_args()
 
 
@@ -373,6 +379,171 @@ def run_ours(args, rank, world, device):
     return line
 
 
+def shard_factors(world):
+    """(a, b, c), a * b * c = world: the block counts along x, y, z (prime
+    factors go to the axis with the fewest blocks so far)."""
+    f, n, p = [1, 1, 1], world, 2
+    while n > 1:
+        while n % p == 0:
+            f[f.index(min(f))] *= p
+            n //= p
+        p += 1
+    return tuple(f)
+
+
+def run_sharded(args, rank, world, device):
+    """The step of the sharded grid: migrate -> halo build -> ghost forces and
+    drift -> reverse_halo, every call one exchange step with the neighboring
+    blocks' ranks."""
+    import numpy as np
+    import torch
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import sharded as shd
+    from dsdecompx_b200 import workloads as W
+
+    w = W.WORKLOADS[args.workload]
+    if args.particles:
+        import dataclasses
+        w = dataclasses.replace(w, particles=args.particles)
+    if w.nranks == 1:
+        raise SystemExit("the sharded grid needs a workload of several subdomains")
+    wl = W.harness()
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream(device)
+    fa = shard_factors(world)
+    bdims, _ = dsx.plan_topology(w.nranks, 0, w.dims, w.policy, w.lower, w.upper)
+    upper = tuple(u * k for u, k in zip(w.upper, fa))
+    P = w.nranks * world
+    dims, _ = dsx.plan_topology(P, 0, w.dims if w.policy == "manual" else (0, 0, 0), w.policy,
+                                w.lower, upper) if w.policy != "manual" else \
+        (tuple(d * k for d, k in zip(bdims, fa)), None)
+    if tuple(dims) != tuple(d * k for d, k in zip(bdims, fa)):
+        raise SystemExit(f"process grid {dims} is not {fa} blocks of {bdims}")
+    # rank (bx, by, bz) owns the block of subdomains at those block coordinates
+    bx, by, bz = rank // (fa[1] * fa[2]), (rank // fa[2]) % fa[1], rank % fa[2]
+    coords = np.array([shd.subdomain_coords(t, dims) for t in range(P)])
+    owners = ((coords[:, 0] // bdims[0]) * fa[1] + coords[:, 1] // bdims[1]) * fa[2] + coords[:, 2] // bdims[2]
+    # this block's particles: the workload's distribution in the block's box
+    data = W.generate(w, seed=args.seed + 7919 * rank)
+    n = len(data["x"])
+    for a, (name, k) in enumerate(zip("xyz", (bx, by, bz))):
+        data[name] = data[name] + k * w.upper[a]
+    data["global_id"] = (data["global_id"] + rank * n).astype(np.int32)
+    if "id64" in data:
+        data["id64"] = data["id64"] + rank * n
+    cell = []
+    for a, (name, k) in enumerate(zip("xyz", (bx, by, bz))):
+        rel = np.floor((data[name] - w.lower[a]) / (upper[a] - w.lower[a]) * dims[a]).astype(np.int64)
+        cell.append(np.clip(rel, k * bdims[a], (k + 1) * bdims[a] - 1))
+    owner = (cell[0] * dims[1] + cell[1]) * dims[2] + cell[2]
+    counts, grouped = W.group_by_owner(data, owner, P)
+    del data, owner, cell
+    N = int(counts.sum())
+    S = w.record_bytes()
+    names = dsx.ARRAYS + [f[0] for f in w.fields]
+    pinned = []
+    for name in names:
+        if name in grouped:
+            t = torch.from_numpy(np.ascontiguousarray(grouped[name])).pin_memory()
+        else:
+            t = torch.zeros(N, dtype=torch.float64).pin_memory()
+        pinned.append(t)
+    del grouped
+    ptrs = [t.data_ptr() for t in pinned]
+    engine = shd.DeviceEngine(P, dims if w.policy == "manual" else (0, 0, 0), w.policy, w.lower,
+                              upper, halo_width=w.halo, fields=w.fields,
+                              particles=int(1.5 * N) + 65536, ghost_capacity=int(0.9 * N))
+    sh = shd.ShardedGrid(engine, rank, world, owners=owners,
+                         run=lambda g: shd.run_distributed(g, device=f"cuda:{device}"))
+    totals = torch.zeros(4, dtype=torch.int32, device=device)
+    seed = args.seed + 1000 * rank
+
+    def user_work(shard):
+        s = stream.cuda_stream
+        gv = shard.ghost_view(totals)
+        wl.dsxw_ghost_forces(C.byref(gv), seed, 0, s)
+        v = shard.E.grid.view()
+        wl.dsxw_drift(C.byref(v), seed, 0, w.drift, s)
+        wl.dsxw_advance(s)
+
+    with torch.cuda.stream(stream):
+        sh.upload_flat(counts, ptrs)
+        for _ in range(args.warmup):
+            sh.step(user_work)
+    stream.synchronize()
+    torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = engine.launches
+    with ClockSampler(device) as clocks:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for _ in range(args.steps):
+                sh.step(user_work)
+            end.record(stream)
+        torch.cuda.synchronize(device)
+    launches = engine.launches - launches0 + 3 * args.steps
+    elapsed_ms = max_over_ranks(start.elapsed_time(end), world, device)
+    torch.distributed.barrier()
+    clock = clocks.summary()
+    ms_per_step = elapsed_ms / args.steps
+    everyone = torch.tensor([float(N)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(everyone)
+    Ntot = int(everyone.item())
+    value = Ntot / (ms_per_step / 1e3) / 1e6
+    # the step's least traffic (this rank): what the fused step's kernels move
+    tot = engine.grid.totals(stream=stream)
+    alg = algorithmic_bytes(S, tot["particles"], tot["emigrants"], tot["ghosts"], tot["boundary"])
+    step_bytes = sum(alg[k] for k in ("step_classify", "step_move", "emig_place", "immigrant_halo",
+                                      "reverse_sum"))
+    peak, peak_kind = peaks()
+    achieved = step_bytes / (ms_per_step / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": "whole sharded step (per-call path + exchanges)",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6.65 TB/s",
+            "algorithmic_bytes_per_launch": int(step_bytes), "avg_launch_ms": round(ms_per_step, 4),
+            "traffic": None}
+    e2e = None
+    if args.e2e_steps > 0:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            cnt = sh.download_flat(ptrs)
+            torch.distributed.barrier()
+            e0.record(stream)
+            for _ in range(args.e2e_steps):
+                sh.upload_flat(cnt, ptrs)
+                sh.step(user_work)
+                cnt = sh.download_flat(ptrs)
+            e1.record(stream)
+        torch.cuda.synchronize(device)
+        e_ms = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, world, device)
+        nb = int(cnt.sum()) * S + 8 * P
+        e2e = {"value": round(Ntot / (e_ms / 1e3) / 1e6, 3), "unit": "M particles/s",
+               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "ms_per_step": round(e_ms, 3),
+               "path": "ShardedGrid.upload_flat (pinned host) -> ShardedGrid.step -> download_flat"}
+    engine.close()
+    return {
+        "metric": METRIC, "value": round(value, 3), "unit": "M particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded numpy PCG64 + counter-based device deviates)",
+        "config": {"workload": w.name, "description": w.description + f"; one block per GPU, "
+                   f"{fa[0]}x{fa[1]}x{fa[2]} blocks", "subdomains": P, "grid": list(dims),
+                   "particles": Ntot, "record_bytes": S,
+                   "step": "sharded grid (ShardedGrid.step: per-call operations, one NCCL "
+                           "exchange step per call)",
+                   "l2": "inputs larger than L2 (%.2f GB of owned records per GPU)" % (N * S / 1e9),
+                   "parallelism": f"subdomain blocks x{world}"},
+        "roofline": roof,
+        "clocks": clock,
+        "e2e": e2e,
+        "gpu_launches": launches,
+    }
+
+
 def traffic_from_profiles(workload, kernel, N):
     """DRAM bytes per launch of `kernel` from the committed ncu summary of
     this workload (profiles/traffic.json), scaled to this launch's particle
@@ -578,14 +749,20 @@ def main():
         return
 
     import torch
-    if world > 1:
+    sharded = world > 1 or args.sharded
+    if sharded:
         import datetime
         torch.cuda.set_device(local)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = run_ours(args, rank, world, local)
-    if world > 1:
+        if world == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", str(29500 + os.getpid() % 1000))
+        torch.distributed.init_process_group("nccl", rank=rank, world_size=world,
+                                             timeout=datetime.timedelta(seconds=120))
+        line = run_sharded(args, rank, world, local)
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+    else:
+        line = run_ours(args, rank, world, local)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             from dsdecompx_b200 import workloads as W

@@ -315,6 +315,38 @@ class ShardedGrid:
         self.E.upload(per_subdomain)
         self.plan = None
 
+    def upload_flat(self, counts, arrays: List[Optional[int]]):
+        """Particles from raw host or device pointers (arrays[13 + nfields],
+        subdomains concatenated in rank order; counts[P] zero outside this
+        shard's subdomains)."""
+        c = np.asarray(counts, dtype=np.int64)
+        if c.shape != (self.P,) or (c[self.owners != self.shard] != 0).any():
+            raise ValueError("particles outside this shard's subdomains")
+        self.E.grid.upload_flat(c, arrays)
+        self.plan = None
+
+    def download_flat(self, arrays: List[Optional[int]]) -> np.ndarray:
+        return self.E.grid.download_flat(arrays)
+
+    def ghost_view(self, totals):
+        """A dsx_grid_view whose ghost region is this shard's assembled ghosts
+        (for device code written against the grid view): totals is a device
+        int32 tensor whose element 0 this call sets to the ghost count."""
+        from . import GridView
+        plan = self.plan
+        v = self.E.grid.view()
+        g = GridView()
+        for a in range(len(self.E.names)):
+            g.base[a] = self.E.asm[a].data_ptr() if self.E.asm else None
+        g.owned_offset = 0
+        g.ghost_offset = 0
+        g.particles = 0
+        g.ghost_capacity = self.E.asm_cap
+        g.nranks = self.P
+        totals.fill_(int(plan.total) if plan is not None else 0)
+        g.halo_totals = totals.data_ptr()
+        return g
+
     def counts(self, t: int) -> Tuple[int, int]:
         self._check_mine(t)
         g = int(self.plan.g[t]) if self.plan is not None else 0
@@ -598,6 +630,7 @@ class DeviceEngine:
         self.asm_cap = 0
         self.asm: List = []
         self._last_migration = None
+        self.launches = 0   # kernels of this library launched through this engine
 
     def close(self):
         self.grid.close()
@@ -613,6 +646,9 @@ class DeviceEngine:
         self.grid.set_rebalance_work(work)
 
     def migrate_local(self):
+        # classify, scan, layout, move, emigrant histogram / column scan /
+        # placement, and the rebalance kernel of a Dynamic grid
+        self.launches += 7 + (1 if self.dynamic else 0)
         return self.grid.migrate()
 
     def rebalance_local(self, work, force):
@@ -641,15 +677,19 @@ class DeviceEngine:
         return res
 
     def migration_pairs(self):
+        self.launches += 1
         return self.grid.migration_pairs()
 
     def halo_local(self, build: bool, positions_only: bool):
+        # build: classify, scan, layout, scatter; refresh: one kernel
+        self.launches += 4 if build else 1
         return self.grid.exchange_halo(rebuild=build, positions_only=positions_only)
 
     def send_lists(self):
         return self.grid.send_lists()
 
     def reverse_local(self):
+        self.launches += 1
         self.grid.reverse_halo()
 
     def forward_local(self, names):
@@ -707,12 +747,16 @@ class DeviceEngine:
             part["src"] = (sb[j] + rows[:, 0] * b).astype(np.uint64)
             part["dst"] = (db[j] + rows[:, 1] * b).astype(np.uint64)
             part["bytes"] = rows[:, 2] * b
-        copy_segments(out[out["bytes"] > 0], self.torch.cuda.current_stream().cuda_stream)
+        out = out[out["bytes"] > 0]
+        if out.size:
+            self.launches += 1
+            copy_segments(out, self.torch.cuda.current_stream().cuda_stream)
 
     def assemble_owned(self, counts, buffers, segments):
         sources = []
         for buf, n in buffers:
             sources.append(self._bases(("buffer", buf, n, self.all_arrays), self.all_arrays))
+        self.launches += 2   # the copies and the new layout
         self.grid.assemble(counts, sources, segments)
 
     # ---- ids and host reads

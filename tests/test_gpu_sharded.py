@@ -129,3 +129,40 @@ def test_assemble_checks_its_segments(cuda):
             g.assemble(counts * 10, [], seg[:0])
     finally:
         g.close()
+
+
+def test_one_shard_over_nccl(cuda):
+    """The distributed driver over a one-rank NCCL group (its all-reduces on
+    device tensors; a single shard has no peers): the sharded step of one
+    shard equals the grid's own calls."""
+    import datetime
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import sharded as shd
+    from shard_scenario import distributed_drive
+    kw = CASES["dynamic-4x4x2-R4"]
+    P, N = kw["nranks"], 30_000
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    owner = Grid("port", P, kw["dims"], kw["policy"], (0, 0, 0), kw["upper"], (True, True, True),
+                 kw["halo_width"], True, kw["dynamic"], [(n, TYPE_INDEX[t], c) for n, t, c in kw["fields"]])
+    per = initial(owner, P, kw["upper"], N, 43, kw["fields"])
+    owner.close()
+    ref = dsx.VirtualGrid(**grid_kw(kw), particles=N, ghost_capacity=2 * N)
+    ref.upload(per)
+    e = shd.DeviceEngine(**grid_kw(kw), particles=N + 4096, ghost_capacity=N)
+    sh = shd.ShardedGrid(e, 0, 1)
+    try:
+        sh.upload({t: per[t] for t in range(P)})
+        Scenario([sh], distributed_drive(sh), ref, P, kw["fields"]).run(steps=2, sigma=0.8)
+    finally:
+        ref.close()
+        e.close()
+        dist.destroy_process_group()
