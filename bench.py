@@ -82,6 +82,12 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.file = None
+        self.skip = 0
+
+    def _lines(self):
+        self.file.flush()
+        with open(self.file.name) as f:
+            return sum(1 for line in f if line.count(",") >= 8)
 
     def __enter__(self):
         try:
@@ -90,6 +96,12 @@ class ClockSampler:
                 ["nvidia-smi", f"--query-gpu={CLOCK_QUERY}", "--format=csv,noheader,nounits",
                  "-i", str(self.device), "-lms", "20"], stdout=self.file,
                 stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a moment to start: the timed region begins
+            # once it samples, and only the samples after that count
+            t0 = time.time()
+            while self._lines() == 0 and time.time() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.skip = self._lines()
         except Exception:
             self.proc = None
         return self
@@ -113,6 +125,10 @@ class ClockSampler:
                 if len(parts) >= 9:
                     rows.append(parts)
         os.unlink(self.file.name)
+        if len(rows) > self.skip:
+            rows = rows[self.skip:]
+        elif rows:
+            rows = rows[-1:]   # the region ended before the next sample: the last one before it
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -752,6 +768,9 @@ def main():
     sharded = world > 1 or args.sharded
     if sharded:
         import datetime
+        # NCCL's own log lines (its version banner) go to stderr: stdout
+        # carries only the JSON line
+        os.environ.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
         torch.cuda.set_device(local)
         if world == 1:
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")

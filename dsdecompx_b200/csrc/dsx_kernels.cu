@@ -12,6 +12,7 @@
 #include "dsx_kernels.cuh"
 
 #include <cstdio>
+#include <mutex>
 
 namespace dsx {
 namespace {
@@ -2182,7 +2183,17 @@ __device__ __forceinline__ void copy_words(const unsigned char* __restrict__ src
     const long long words = (n - head) / W;
     const Word* s = reinterpret_cast<const Word*>(src + head);
     Word* d = reinterpret_cast<Word*>(dst + head);
-    for (long long t = threadIdx.x; t < words; t += blockDim.x) d[t] = s[t];
+    // four loads in flight per thread before their stores
+    constexpr int U = 4;
+    for (long long t = threadIdx.x; t < words; t += U * blockDim.x) {
+        Word v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (t + u * blockDim.x < words) v[u] = s[t + u * blockDim.x];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (t + u * blockDim.x < words) d[t + u * blockDim.x] = v[u];
+    }
     for (long long t = head + words * W + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
 }
 
@@ -2553,29 +2564,51 @@ void launch_pair_counts(int P, const Scratch& S, const int* obase_old, long long
                                                        obase_old, pairs);
 }
 
+namespace {
+// Descriptor staging of launch_copies, reused from call to call: pinned host
+// and device buffers, and an event after the kernel that last read them
+// (the next call waits for it before it overwrites them).
+struct CopyStage {
+    std::mutex lock;
+    CopyPiece* host = nullptr;
+    CopyPiece* device = nullptr;
+    std::size_t capacity = 0;
+    cudaEvent_t done = nullptr;
+};
+CopyStage g_copy_stage;
+}  // namespace
+
 cudaError_t launch_copies(const std::vector<CopyPiece>& copies, cudaStream_t s) {
-    std::vector<CopyPiece> pieces;
+    std::size_t n = 0;
+    for (const CopyPiece& c : copies) n += static_cast<std::size_t>((c.bytes + kCopyPiece - 1) / kCopyPiece);
+    if (!n) return cudaSuccess;
+    CopyStage& st = g_copy_stage;
+    std::lock_guard<std::mutex> hold(st.lock);
+    cudaError_t e = cudaSuccess;
+    if (!st.done && (e = cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(st.done)) != cudaSuccess) return e;
+    if (n > st.capacity) {
+        const std::size_t cap = n + n / 2 + 1024;
+        cudaFreeHost(st.host);
+        cudaFree(st.device);
+        st.host = nullptr;
+        st.device = nullptr;
+        st.capacity = 0;
+        if ((e = cudaMallocHost(reinterpret_cast<void**>(&st.host), sizeof(CopyPiece) * cap)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(reinterpret_cast<void**>(&st.device), sizeof(CopyPiece) * cap)) != cudaSuccess) return e;
+        st.capacity = cap;
+    }
+    std::size_t k = 0;
     for (const CopyPiece& c : copies)
         for (long long at = 0; at < c.bytes; at += kCopyPiece)
-            pieces.push_back({c.src + at, c.dst + at,
-                              c.bytes - at < kCopyPiece ? c.bytes - at : kCopyPiece});
-    if (pieces.empty()) return cudaSuccess;
-    // the descriptors live in stream-ordered memory: freed after the kernel
-    // on the same stream, so that calls on different streams never share them
-    CopyPiece* d = nullptr;
-    const std::size_t bytes = sizeof(CopyPiece) * pieces.size();
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&d), bytes, s);
+            st.host[k++] = {c.src + at, c.dst + at, c.bytes - at < kCopyPiece ? c.bytes - at : kCopyPiece};
+    e = cudaMemcpyAsync(st.device, st.host, sizeof(CopyPiece) * n, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return e;
-    // pageable source: the call returns once the descriptors are staged
-    e = cudaMemcpyAsync(d, pieces.data(), bytes, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) {
-        const long long n = static_cast<long long>(pieces.size());
-        const long long cap = static_cast<long long>(sm_count()) * 8;
-        k_copy_pieces<<<static_cast<int>(n < cap ? n : cap), NT, 0, s>>>(d, n);
-        e = cudaGetLastError();
-    }
-    const cudaError_t f = cudaFreeAsync(d, s);
-    return e != cudaSuccess ? e : f;
+    const long long cap = static_cast<long long>(sm_count()) * 8;
+    const long long count = static_cast<long long>(n);
+    k_copy_pieces<<<static_cast<int>(count < cap ? count : cap), NT, 0, s>>>(st.device, count);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaEventRecord(st.done, s);
 }
 
 void launch_wrap_inplace(double* x, double* y, double* z, long long n, const double* lower,

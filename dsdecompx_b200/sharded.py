@@ -220,53 +220,97 @@ def section_offsets(n: int, elem_bytes: Sequence[int]) -> List[int]:
     return out
 
 
+def group_exclusive(keys: np.ndarray, values: np.ndarray) -> np.ndarray:
+    """Exclusive running sum of values within runs of equal consecutive keys."""
+    if not len(values):
+        return values.copy()
+    before = np.cumsum(values) - values
+    start = np.ones(len(keys), dtype=bool)
+    start[1:] = keys[1:] != keys[:-1]
+    first = np.maximum.accumulate(np.where(start, np.arange(len(keys)), 0))
+    return before - before[first]
+
+
+def merge_rows(rows: np.ndarray) -> np.ndarray:
+    """(source, destination, count) rows with the runs that continue each
+    other in both source and destination merged into one row."""
+    rows = np.asarray(rows, dtype=np.int64).reshape(-1, 3)
+    if len(rows) < 2:
+        return rows
+    s, d, n = rows[:, 0], rows[:, 1], rows[:, 2]
+    start = np.ones(len(rows), dtype=bool)
+    start[1:] = (s[1:] != s[:-1] + n[:-1]) | (d[1:] != d[:-1] + n[:-1])
+    at = np.flatnonzero(start)
+    return np.stack([s[at], d[at], np.add.reduceat(n, at)], axis=1)
+
+
 class GhostPlan:
     """Where every block of this shard's receivers comes from and where the
-    lists of its senders go (ranges are (source index, destination index,
-    count) rows)."""
+    lists of its senders go: (k, 3) rows of (source index, destination index,
+    count) -- local: engine ghost slot -> assembled slot; recv[p]: offset in
+    shard p's buffer -> assembled slot; send[p]: engine ghost slot -> offset
+    in the buffer for shard p."""
 
     def __init__(self, shard, owners, nn, sender_of, length, first):
         P = len(owners)
-        mine = np.flatnonzero(owners == shard)
-        self.g = np.zeros(P, dtype=np.int64)          # assembled ghosts per receiver
-        self.gbase = np.zeros(P, dtype=np.int64)      # first assembled slot per receiver
-        self.local: List[Tuple[int, int, int]] = []   # engine ghost slot -> assembled slot
-        self.recv: Dict[int, List[Tuple[int, int, int]]] = {}   # buffer offset -> assembled slot
-        self.send: Dict[int, List[Tuple[int, int, int]]] = {}   # engine ghost slot -> buffer offset
-        at = 0
-        recv_at: Dict[int, int] = {}
-        for t in mine:
-            self.gbase[t] = at
-            for m in range(nn[t]):
-                e = sender_of[t, m]
-                if e < 0 or length[e] == 0:
-                    continue
-                p = int(owners[e // KMAX])
-                n = int(length[e])
-                if p == shard:
-                    self.local.append((int(first[e]), at, n))
-                else:
-                    off = recv_at.get(p, 0)
-                    self.recv.setdefault(p, []).append((off, at, n))
-                    recv_at[p] = off + n
-                at += n
-            self.g[t] = at - self.gbase[t]
-        self.total = at
-        send_at: Dict[int, int] = {}
-        for t in range(P):
-            p = int(owners[t])
-            if p == shard:
-                continue
-            for m in range(nn[t]):
-                e = sender_of[t, m]
-                if e < 0 or length[e] == 0 or owners[e // KMAX] != shard:
-                    continue
-                off = send_at.get(p, 0)
-                n = int(length[e])
-                self.send.setdefault(p, []).append((int(first[e]), off, n))
-                send_at[p] = off + n
-        self.recv_n = recv_at
-        self.send_n = send_at
+        owners = np.asarray(owners)
+        length = np.asarray(length, dtype=np.int64)
+        first = np.asarray(first, dtype=np.int64)
+        blocks = np.arange(KMAX)[None, :] < np.asarray(nn)[:, None]      # [P, 26]
+        sender_shard = np.where(sender_of >= 0, owners[np.maximum(sender_of, 0) // KMAX], -1)
+        live = blocks & (sender_of >= 0)
+        live &= np.where(live, length[np.maximum(sender_of, 0)], 0) > 0
+        # receivers of this shard, blocks in (t, m) order
+        mine = owners == shard
+        t_idx, m_idx = np.nonzero(live & mine[:, None])
+        e = sender_of[t_idx, m_idx]
+        n = length[e]
+        at = np.cumsum(n) - n
+        self.total = int(n.sum())
+        self.g = np.bincount(t_idx, weights=n, minlength=P).astype(np.int64)
+        self.gbase = np.zeros(P, dtype=np.int64)
+        order = np.flatnonzero(mine)
+        self.gbase[order] = np.cumsum(self.g[order]) - self.g[order]
+        p = sender_shard[t_idx, m_idx]
+        loc = p == shard
+        self.local = merge_rows(np.stack([first[e[loc]], at[loc], n[loc]], axis=1))
+        self.recv: Dict[int, np.ndarray] = {}
+        self.recv_n: Dict[int, int] = {}
+        for q in np.unique(p[~loc]):
+            sel = p == q
+            off = np.cumsum(n[sel]) - n[sel]
+            self.recv[int(q)] = merge_rows(np.stack([off, at[sel], n[sel]], axis=1))
+            self.recv_n[int(q)] = int(n[sel].sum())
+        # lists of this shard's senders to other shards' receivers, in the
+        # receivers' (t, m) order
+        t_idx, m_idx = np.nonzero(live & ~mine[:, None] & (sender_shard == shard))
+        e = sender_of[t_idx, m_idx]
+        n = length[e]
+        p = owners[t_idx]
+        self.send: Dict[int, np.ndarray] = {}
+        self.send_n: Dict[int, int] = {}
+        for q in np.unique(p):
+            sel = p == q
+            off = np.cumsum(n[sel]) - n[sel]
+            self.send[int(q)] = merge_rows(np.stack([first[e[sel]], off, n[sel]], axis=1))
+            self.send_n[int(q)] = int(n[sel].sum())
+
+
+def merge_segments(seg: np.ndarray) -> np.ndarray:
+    """Assembly segments in (destination subdomain, position) order, with
+    the ones that continue each other (same source and subdomain, contiguous
+    source and destination) merged."""
+    seg = seg[np.lexsort((seg["dst_index"], seg["dst_rank"]))]
+    if len(seg) < 2:
+        return seg
+    cont = np.zeros(len(seg), dtype=bool)
+    cont[1:] = ((seg["source"][1:] == seg["source"][:-1]) & (seg["dst_rank"][1:] == seg["dst_rank"][:-1]) &
+                (seg["src_index"][1:] == seg["src_index"][:-1] + seg["count"][:-1]) &
+                (seg["dst_index"][1:] == seg["dst_index"][:-1] + seg["count"][:-1]))
+    at = np.flatnonzero(~cont)
+    out = seg[at].copy()
+    out["count"] = np.add.reduceat(seg["count"], at)
+    return out
 
 
 def _rows(ranges) -> np.ndarray:
@@ -452,60 +496,61 @@ class ShardedGrid:
         allb = E.elem_bytes_all
         sends = {}
         for p in range(self.nshards):
-            if p == me:
+            ts = np.flatnonzero((owners == p) & (local_n > 0))
+            if p == me or not len(ts):
                 continue
-            ts = [t for t in np.flatnonzero(owners == p) if local_n[t] > 0]
-            if not ts:
-                continue
-            n = int(sum(local_n[t] for t in ts))
-            rows, at = [], 0
-            for t in ts:
-                rows.append((int(obase[t]), at, int(local_n[t])))
-                at += int(local_n[t])
+            cnt = local_n[ts]
+            n = int(cnt.sum())
+            rows = np.stack([obase[ts], np.cumsum(cnt) - cnt, cnt], axis=1)
             buf = E.new_buffer(packed_bytes(n, allb))
-            E.copy(("buffer", buf, n, E.all_arrays), ("owned",), _rows(rows), E.all_arrays)
+            E.copy(("buffer", buf, n, E.all_arrays), ("owned",), rows, E.all_arrays)
             sends[p] = buf
         # what each peer sends: its sources' groups for my subdomains
-        per_peer = np.zeros((self.nshards, P), dtype=np.int64)   # [p, t]
-        for p in range(self.nshards):
-            if p != me:
-                per_peer[p] = Mg[:, owners == p].sum(axis=1)
-        recv_bytes = {p: packed_bytes(int(per_peer[p, self.mine].sum()), allb)
-                      for p in range(self.nshards) if p != me}
-        recv = yield Exchange(sends, recv_bytes)
-        # new layout: retained, then sources in ascending order
-        new_counts = np.zeros(P, dtype=np.int64)
+        mine = self.mine
+        sub = Mg[mine]                                               # [my subdomains, sources]
+        from_peer = {p: int(sub[:, owners == p].sum()) for p in range(self.nshards) if p != me}
+        recv = yield Exchange(sends, {p: packed_bytes(n, allb) for p, n in from_peer.items()})
+        # new layout of t: retained, then the groups of its sources in
+        # ascending source order, from this shard or from the source's shard
         peers = sorted(recv)
-        src_of = {p: k for k, p in enumerate(peers)}
-        peer_at = {p: 0 for p in peers}
-        segs = []
-        out = {}
-        for t in self.mine:
-            retained = int(res[t, 2])
-            received = int(Mg[t].sum())
-            new_counts[t] = retained + received
-            if retained:
-                segs.append((-1, int(obase[t]), int(t), 0, retained))
-            dst = retained
-            local_at = int(obase[t]) + retained
-            for q in np.flatnonzero(Mg[t]):
-                c = int(Mg[t, q])
-                p = int(owners[q])
-                if p == me:
-                    segs.append((-1, local_at, int(t), dst, c))
-                    local_at += c
-                else:
-                    segs.append((src_of[p], peer_at[p], int(t), dst, c))
-                    peer_at[p] += c
-                dst += c
-            sent = int(res[t, 3])
-            out[int(t)] = (int(sent != 0 or received != 0), int(res[t, 1]), retained, sent, received,
-                           int(new_counts[t]))
-        seg = np.zeros(len(segs), dtype=SEGMENT_DTYPE)
-        for i, s in enumerate(segs):
-            seg[i] = s
-        E.assemble_owned(new_counts, [(recv[p], int(per_peer[p, self.mine].sum())) for p in peers], seg)
+        retained = res[mine, 2].astype(np.int64)
+        received = sub.sum(axis=1)
+        new_counts = np.zeros(P, dtype=np.int64)
+        new_counts[mine] = retained + received
+        ti, q = np.nonzero(sub)
+        c = sub[ti, q]
+        p = owners[q]
+        source = np.full(len(c), -1, dtype=np.int64)
+        src = np.zeros(len(c), dtype=np.int64)
+        loc = p == me
+        src[loc] = obase[mine[ti[loc]]] + retained[ti[loc]] + group_exclusive(ti[loc], c[loc])
+        for k, pp in enumerate(peers):
+            sel = p == pp
+            src[sel] = np.cumsum(c[sel]) - c[sel]
+            source[sel] = k
+        sent = res[mine, 3].astype(np.int64)
+        out = {int(t): (int(sent[i] != 0 or received[i] != 0), int(res[t, 1]), int(retained[i]),
+                        int(sent[i]), int(received[i]), int(new_counts[t]))
+               for i, t in enumerate(mine)}
         self.plan = None
+        if not peers and not local_n[owners != me].any():
+            # nothing came in and nothing left: the local layout is final
+            return out
+        keep = retained > 0
+        nk = int(keep.sum())
+        seg = np.zeros(nk + len(c), dtype=SEGMENT_DTYPE)
+        seg["source"][:nk] = -1
+        seg["src_index"][:nk] = obase[mine[keep]]
+        seg["dst_rank"][:nk] = mine[keep]
+        seg["dst_index"][:nk] = 0
+        seg["count"][:nk] = retained[keep]
+        seg["source"][nk:] = source
+        seg["src_index"][nk:] = src
+        seg["dst_rank"][nk:] = mine[ti]
+        seg["dst_index"][nk:] = retained[ti] + group_exclusive(ti, c)
+        seg["count"][nk:] = c
+        seg = merge_segments(seg)
+        E.assemble_owned(new_counts, [(recv[pp], from_peer[pp]) for pp in peers], seg)
         return out
 
     def exchange_halo_steps(self, rebuild: bool = False, positions_only: bool = False):
@@ -557,7 +602,7 @@ class ShardedGrid:
             sends[p] = buf
         recv_bytes = {p: packed_bytes(n, b) for p, n in plan.recv_n.items()}
         recv = yield Exchange(sends, recv_bytes)
-        if plan.local:
+        if len(plan.local):
             E.copy(("assembled",), ("ghost",), _rows(plan.local), arrays)
         for p, rows in plan.recv.items():
             E.copy(("assembled",), ("buffer", recv[p], plan.recv_n[p], arrays), _rows(rows), arrays)
@@ -568,7 +613,7 @@ class ShardedGrid:
         senders' shards."""
         E, plan = self.E, self.plan
         b = [E.elem_bytes[a] for a in arrays]
-        if plan.local:
+        if len(plan.local):
             E.copy(("ghost",), ("assembled",), _swap(plan.local), arrays)
         sends = {}
         for p, rows in plan.recv.items():

@@ -94,24 +94,40 @@ def test_ghost_plans_agree_between_shards():
             length[t * 26 + n] = rng.integers(0, 9)
     first = np.concatenate([[0], np.cumsum(length)])[:-1]   # any local layout
     plans = [shd.GhostPlan(s, owners, nn, sender_of, length, first) for s in range(R)]
-    for a in range(R):
-        for b in range(R):
-            if a == b:
-                continue
-            sent = [r[2] for r in plans[a].send.get(b, [])]
-            got = [r[2] for r in plans[b].recv.get(a, [])]
-            assert sent == got
-            assert plans[a].send_n.get(b, 0) == plans[b].recv_n.get(a, 0)
-    # every block of every receiver lands exactly once
+    # identity of every local ghost slot: (list e, position k in the list)
+    ident = np.full(int(length.sum()), -1, np.int64)
+    for e in range(P * 26):
+        ident[first[e]:first[e] + length[e]] = e * 10_000 + np.arange(length[e])
+
+    def expand(rows):
+        if not len(rows):
+            return np.zeros(0, np.int64), np.zeros(0, np.int64)
+        src = np.concatenate([np.arange(r[0], r[0] + r[2]) for r in rows])
+        dst = np.concatenate([np.arange(r[1], r[1] + r[2]) for r in rows])
+        return src, dst
+
     for s in range(R):
         p = plans[s]
-        covered = sorted([(r[1], r[2]) for r in p.local] +
-                         [(r[1], r[2]) for rows in p.recv.values() for r in rows])
-        at = 0
-        for lo, n in covered:
-            assert lo == at
-            at += n
-        assert at == p.total
+        # what each assembled slot must hold: blocks in (receiver, neighbor) order
+        want = []
+        for t in np.flatnonzero(owners == s):
+            for m in range(nn[t]):
+                e = sender_of[t, m]
+                if e >= 0:
+                    want.extend(e * 10_000 + np.arange(length[e]))
+        got = np.full(p.total, -1, np.int64)
+        src, dst = expand(p.local)
+        got[dst] = ident[src]
+        for q, rows in p.recv.items():
+            # shard q's buffer for s: its engine slots in q's send rows
+            bsrc, boff = expand(plans[q].send[s])
+            buf = np.full(plans[q].send_n[s], -1, np.int64)
+            buf[boff] = ident[bsrc]
+            off, dst = expand(rows)
+            got[dst] = buf[off]
+            assert p.recv_n[q] == plans[q].send_n[s]
+        assert p.total == len(want) and np.array_equal(got, np.array(want, np.int64))
+        assert p.g.sum() == p.total
 
 
 def test_packed_sections_are_aligned():
@@ -221,3 +237,29 @@ def gloo_rank(rank, world, port, case):
 @pytest.mark.parametrize("case", ["2x2x2-R2", "dynamic-R4"])
 def test_two_gloo_ranks_match_one_grid(case):
     mp.start_processes(gloo_rank, args=(2, free_port(), case), nprocs=2, start_method="spawn")
+
+
+def test_row_and_segment_merging():
+    assert list(shd.group_exclusive(np.array([0, 0, 1, 1, 1]), np.array([1, 2, 3, 4, 5]))) == [0, 1, 0, 3, 7]
+    rows = np.array([(0, 10, 5), (5, 15, 3), (9, 18, 1), (10, 19, 2)])
+    assert shd.merge_rows(rows).tolist() == [[0, 10, 8], [9, 18, 3]]
+    rng = np.random.default_rng(3)
+    from dsdecompx_b200 import SEGMENT_DTYPE
+    for _ in range(20):
+        k = 40
+        seg = np.zeros(k, dtype=SEGMENT_DTYPE)
+        seg["source"] = rng.integers(-1, 2, k)
+        seg["dst_rank"] = rng.integers(0, 3, k)
+        seg["count"] = rng.integers(1, 4, k)
+        # contiguous destinations per subdomain, sources often continuing
+        for r in range(3):
+            sel = np.flatnonzero(seg["dst_rank"] == r)
+            seg["dst_index"][sel] = np.cumsum(seg["count"][sel]) - seg["count"][sel]
+            seg["src_index"][sel] = seg["dst_index"][sel] + 100 * r + rng.integers(0, 2, len(sel))
+        merged = shd.merge_segments(seg)
+        assert len(merged) <= len(seg)
+
+        def expand(s):
+            return sorted((int(x["dst_rank"]), int(x["dst_index"]) + i, int(x["source"]),
+                           int(x["src_index"]) + i) for x in s for i in range(int(x["count"])))
+        assert expand(seg) == expand(merged)
