@@ -2158,15 +2158,24 @@ __global__ void __launch_bounds__(NT) k_pair_counts(int P, const int* __restrict
                                                     const int* __restrict__ emig_dst,
                                                     const int* __restrict__ obase_old, int* pairs) {
     const int E = info[0];
-    for (int e = blockIdx.x * NT + threadIdx.x; e < E; e += gridDim.x * NT) {
-        const int i = emig_src[e];
-        int lo = 0, hi = P;   // obase_old[lo] <= i < obase_old[hi]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (obase_old[mid] <= i) lo = mid;
-            else hi = mid;
+    const int lane = threadIdx.x & 31;
+    // whole warps walk the list; lanes with the same (destination, source)
+    // add once per warp (consecutive emigrants mostly share both)
+    for (int base = blockIdx.x * NT + (threadIdx.x & ~31); base < E; base += gridDim.x * NT) {
+        const int e = base + lane;
+        int key = -1;
+        if (e < E) {
+            const int i = emig_src[e];
+            int lo = 0, hi = P;   // obase_old[lo] <= i < obase_old[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (obase_old[mid] <= i) lo = mid;
+                else hi = mid;
+            }
+            key = emig_dst[e] * P + lo;
         }
-        atomicAdd(&pairs[emig_dst[e] * P + lo], 1);
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        if (key >= 0 && lane == __ffs(same) - 1) atomicAdd(&pairs[key], __popc(same));
     }
 }
 
@@ -2559,9 +2568,11 @@ void mark(const Scratch& S, cudaStream_t s, const char* what) {
 void launch_pair_counts(int P, const Scratch& S, const int* obase_old, long long ncap, int* pairs,
                         cudaStream_t s) {
     cudaMemsetAsync(pairs, 0, sizeof(int) * static_cast<std::size_t>(P) * P, s);
-    if (ncap > 0)
-        k_pair_counts<<<stream_grid(ncap), NT, 0, s>>>(P, S.emig_info, S.emig_src, S.emig_dst,
-                                                       obase_old, pairs);
+    if (ncap > 0) {
+        const long long want = (ncap + NT - 1) / NT, cap = static_cast<long long>(sm_count()) * 4;
+        k_pair_counts<<<static_cast<int>(want < cap ? want : cap), NT, 0, s>>>(
+            P, S.emig_info, S.emig_src, S.emig_dst, obase_old, pairs);
+    }
 }
 
 namespace {
