@@ -123,6 +123,14 @@ class Scenario:
                 for t, row in out.items():
                     assert (int(hr[t][0]), int(hr[t][1])) == row[:2], (step, t, hr[t], row)
             self.compare(f"refresh {step}")
+            # positions-only refresh: the ghosts' positions follow, the rest
+            # of their records stays (compared on the positions)
+            self.displace(step + 2000, sigma * 0.1)
+            self.ref.exchange_halo()
+            for out in self.drive("exchange_halo", False, True):
+                for t, row in out.items():
+                    assert row[0] == int(self.ref.counts(t)[1]) and row[3] == 1, (step, t, row)
+            self.compare(f"positions refresh {step}", names=["x", "y", "z", "global_id"])
 
 
 def lockstep_drive(shards):

@@ -162,10 +162,13 @@ CASES = {
                           periodic=(True, False, False), halo_width=0.8, N=3000),
     "dynamic-R4": dict(nranks=8, dims=(2, 2, 2), policy="dynamic", upper=(12.0, 12.0, 12.0),
                        halo_width=0.9, dynamic=(1.0, 1.05, 0.5, 0.1), N=3000),
+    "3x3x3-R4-runs": dict(nranks=27, dims=(3, 3, 3), policy="manual", upper=(9.0, 9.0, 9.0),
+                          halo_width=0.7, N=4000),
 }
 
 
-@pytest.mark.parametrize("case,R", [("2x2x2-R2", 2), ("3x1x4-R3-open", 3), ("dynamic-R4", 4)])
+@pytest.mark.parametrize("case,R", [("2x2x2-R2", 2), ("3x1x4-R3-open", 3), ("dynamic-R4", 4),
+                                    ("3x3x3-R4-runs", 4)])
 def test_lockstep_shards_match_one_grid(case, R):
     kw = CASES[case]
     fields = FIELDS3
