@@ -53,6 +53,9 @@ def parse():
                     help="keep the default launch shapes (no dsx_grid_autotune before timing)")
     ap.add_argument("--particles", type=int, default=0,
                     help="override the workload's particle count (small profiling cases)")
+    ap.add_argument("--no-aux", action="store_true",
+                    help="skip the timings of the calls around the step (owner queries, "
+                         "refreshes, split-phase overlap, rebalance, box changes)")
     ap.add_argument("--sharded", action="store_true",
                     help="the sharded grid's step (the multi-GPU path) also at one GPU")
     return ap.parse_args()
@@ -366,6 +369,13 @@ def run_ours(args, rank, world, device):
         grid.set_plain(False)
         per_subdomain = round(q0.elapsed_time(q1) / args.plain_steps, 3)
 
+    aux = None
+    if not args.no_aux:
+        try:
+            aux = measure_calls(grid, w, N, S, stream, device)
+        except Exception as exc:   # reported, not fatal: the step's line stands
+            aux = {"error": f"{type(exc).__name__}: {exc}"}
+
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "M particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -391,8 +401,110 @@ def run_ours(args, rank, world, device):
         "clocks": clock,
         "e2e": e2e,
         "gpu_launches": launches,
+        "aux": aux,
     }
     return line
+
+
+def measure_calls(grid, w, N, S, stream, device, reps=10):
+    """CUDA-event timings of the calls around the step, on the step's
+    particles: owner queries and the out-of-domain check over every owned
+    particle, halo refreshes (positions only, full) along the current plan,
+    the split-phase refresh with independent work on another stream between
+    begin and end, an explicit rebalance (with its migrate), and box / cut
+    changes.  Bytes are each call's least traffic; fractions are of the
+    measured copy bandwidth."""
+    import numpy as np
+    import torch
+    peak, _ = peaks()
+
+    def timed(fn, n=reps):
+        fn()
+        torch.cuda.synchronize(device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        return a.elapsed_time(b) / n
+
+    def row(ms, nbytes):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        return {"ms": round(ms, 4), "bytes": int(nbytes), "achieved_gbs": round(gbs, 1),
+                "frac": round(gbs / peak, 4)}
+
+    out = {}
+    with torch.cuda.stream(stream):
+        grid.exchange_halo(rebuild=True, stream=stream, results=False)
+        v = grid.view()
+        G = int(grid.totals(stream=stream)["ghosts"])
+        o = int(v.owned_offset)
+        pos = [v.base[a] + 8 * o for a in range(3)]
+        owner = torch.empty(N, dtype=torch.int32, device=device)
+        out["owner_rank"] = row(timed(lambda: grid.owner_rank(
+            pos[0], pos[1], pos[2], owner.data_ptr(), n=N, stream=stream)), 28 * N)
+        out["out_of_domain"] = row(timed(lambda: grid.out_of_domain(stream=stream)), 24 * N)
+        # per ghost: owner index and list entry, the owner's positions in,
+        # positions and zeroed forces out (full: velocities and fields too)
+        fb = S - 96
+        out["refresh_positions"] = row(timed(lambda: grid.exchange_halo(
+            positions_only=True, stream=stream, results=False)), 80 * G)
+        out["refresh_full"] = row(timed(lambda: grid.exchange_halo(
+            stream=stream, results=False)), (128 + 2 * fb) * G)
+        # split phase: begin returns before the refresh has run; interior
+        # work that computes (an FP64 matrix product on another stream) runs
+        # beside it until end
+        side = torch.cuda.Stream(device)
+        m = torch.rand(1024, 1024, dtype=torch.float64, device=device)
+
+        def interior():
+            side.wait_stream(stream)
+            with torch.cuda.stream(side):
+                torch.mm(m, m)
+            stream.wait_stream(side)
+
+        def split():
+            side.wait_stream(stream)   # before begin: the two then run side by side
+            grid.begin_halo_exchange(positions_only=True, stream=stream)
+            with torch.cuda.stream(side):
+                torch.mm(m, m)
+            grid.end_halo_exchange(stream=stream)
+            stream.wait_stream(side)
+
+        t_refresh = out["refresh_positions"]["ms"]
+        t_work = timed(interior)
+        t_split = timed(split)
+        torch.cuda.synchronize(device)
+        h0 = time.perf_counter()
+        grid.begin_halo_exchange(positions_only=True, stream=stream)
+        h1 = time.perf_counter()
+        grid.end_halo_exchange(stream=stream)
+        h2 = time.perf_counter()
+        grid.exchange_halo(positions_only=True, stream=stream, results=True)
+        h3 = time.perf_counter()
+        out["split_phase"] = {"refresh_ms": t_refresh, "interior_ms": round(t_work, 4),
+                              "begin_work_end_ms": round(t_split, 4),
+                              "hidden_fraction": round((t_refresh + t_work - t_split) /
+                                                       min(t_refresh, t_work), 3),
+                              "interior": "1024 x 1024 FP64 matrix product on another stream",
+                              "begin_host_us": round((h1 - h0) * 1e6, 1),
+                              "end_host_us": round((h2 - h1) * 1e6, 1),
+                              "blocking_call_host_us": round((h3 - h2) * 1e6, 1)}
+        counts = grid.all_counts(stream=stream)[0].astype(np.float64)
+        out["rebalance_with_work_ms"] = round(timed(lambda: grid.rebalance(
+            counts, force=True, stream=stream), 3), 3)
+        lo, up = w.lower, w.upper
+        bigger = tuple(u * 1.0001 for u in up)
+
+        def rescale():
+            grid.rescale_domain(lo, bigger, stream=stream)
+            grid.rescale_domain(lo, up, stream=stream)
+        out["rescale_domain_pair_ms"] = round(timed(rescale, 3), 3)
+        out["set_cuts_ms"] = round(timed(lambda: grid.set_cuts(grid.cuts(stream=stream),
+                                                               stream=stream), 3), 3)
+    out["particles"], out["ghosts"] = N, G
+    return out
 
 
 def shard_factors(world):

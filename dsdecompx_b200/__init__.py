@@ -484,12 +484,26 @@ class VirtualGrid:
                                                  res.ctypes.data_as(C.POINTER(C.c_longlong))))
         return res
 
-    def owner_rank(self, x, y, z, out, stream=None):
-        """Owning subdomain of device positions (torch tensors or pointers)
-        into the int32 device array `out`."""
-        ptr = lambda t: t if isinstance(t, int) else t.data_ptr()
-        n = x if isinstance(x, int) else x.numel()
-        _check(self.L.dsx_grid_owner_rank(self.h, ptr(x), ptr(y), ptr(z), n, ptr(out),
+    def owner_rank(self, x, y, z, out, n: Optional[int] = None, stream=None):
+        """Owning subdomain of n device positions into the int32 device array
+        `out`: torch tensors (n defaults to their common length, which every
+        one must have), or raw device addresses with n given."""
+        arrays = (x, y, z, out)
+        if all(isinstance(t, int) for t in arrays):
+            if n is None:
+                raise ValueError("owner_rank on raw addresses needs the particle count n")
+            ptrs = arrays
+        elif any(isinstance(t, int) for t in arrays):
+            raise ValueError("owner_rank takes four tensors or four addresses")
+        else:
+            sizes = {int(t.numel()) for t in arrays}
+            if len(sizes) != 1 or (n is not None and n > min(sizes)):
+                raise ValueError("owner_rank: x, y, z and out must hold n elements each")
+            n = min(sizes) if n is None else n
+            if x.dtype != y.dtype or str(x.dtype) != "torch.float64" or str(out.dtype) != "torch.int32":
+                raise ValueError("owner_rank: float64 positions, int32 out")
+            ptrs = tuple(t.data_ptr() for t in arrays)
+        _check(self.L.dsx_grid_owner_rank(self.h, ptrs[0], ptrs[1], ptrs[2], int(n), ptrs[3],
                                           _stream(stream)))
 
     def out_of_domain(self, stream=None):

@@ -1809,19 +1809,44 @@ __global__ void __launch_bounds__(NT) k_halo_refresh(Grid G, Arrays A, long long
                                                      const int* __restrict__ ghost_entry) {
     if (*G.status & kStatusGhostOverflow) return;
     const int total = info[0];
-    for (int slot = blockIdx.x * NT + threadIdx.x; slot < total; slot += gridDim.x * NT) {
-        const long long src = owned_off + ghost_owner[slot];
-        const double* sh = G.shift + 3ll * ghost_entry[slot];
-        const long long gi = ghost_off + slot;
-        A.d[0][gi] = __dadd_rn(A.d[0][src], sh[0]);
-        A.d[1][gi] = __dadd_rn(A.d[1][src], sh[1]);
-        A.d[2][gi] = __dadd_rn(A.d[2][src], sh[2]);
-        A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
-        if (!positions_only) {
-            A.d[3][gi] = A.d[3][src];
-            A.d[4][gi] = A.d[4][src];
-            A.d[5][gi] = A.d[5][src];
-            copy_fields(A.f, src, gi);
+    // four ghosts per thread and pass: their owner indices, then their
+    // owners' positions, are all in flight before the first store
+    constexpr int U = 4;
+    const int step = gridDim.x * NT;
+    for (int s0 = blockIdx.x * NT + threadIdx.x; s0 < total; s0 += U * step) {
+        int own[U], ent[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int slot = s0 + u * step;
+            own[u] = slot < total ? ro(ghost_owner + slot) : 0;
+            ent[u] = slot < total ? ro(ghost_entry + slot) : 0;
+        }
+        double p[U][3];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (s0 + u * step < total) {
+                const long long src = owned_off + own[u];
+                p[u][0] = A.d[0][src];
+                p[u][1] = A.d[1][src];
+                p[u][2] = A.d[2][src];
+            }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int slot = s0 + u * step;
+            if (slot >= total) continue;
+            const long long src = owned_off + own[u];
+            const double* sh = G.shift + 3ll * ent[u];
+            const long long gi = ghost_off + slot;
+            A.d[0][gi] = __dadd_rn(p[u][0], sh[0]);
+            A.d[1][gi] = __dadd_rn(p[u][1], sh[1]);
+            A.d[2][gi] = __dadd_rn(p[u][2], sh[2]);
+            A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+            if (!positions_only) {
+                A.d[3][gi] = A.d[3][src];
+                A.d[4][gi] = A.d[4][src];
+                A.d[5][gi] = A.d[5][src];
+                copy_fields(A.f, src, gi);
+            }
         }
     }
 }
@@ -2113,24 +2138,73 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
     if (lane == 0) result[1] = 1.0;
 }
 
+
+// upper_bound(cuts, cuts + dims + 1, v) - cuts - 1 clamped to [0, dims - 1],
+// as a count of the cuts that v is not below: the cuts increase strictly, so
+// !(v < cut) holds on a prefix of them (on all of them for a NaN, where the
+// bisection of axis_coordinate also ends past the last cut).
+// Axes of at most kCountedCells cells; the loop is unrolled and predicated
+// (no branches).
+constexpr int kCountedCells = 8;
+__device__ __forceinline__ int axis_coordinate_count(const double* cuts, int dims, double v) {
+    int c = -1;
+#pragma unroll
+    for (int k = 0; k <= kCountedCells; ++k)
+        if (k <= dims) c += !(v < cuts[k]);
+    c = c > dims - 1 ? dims - 1 : c;
+    return c < 0 ? 0 : c;
+}
+
 // Decomposition::owner_rank (dsDecompX src/migration.cpp:74-98) of arbitrary
-// positions: one periodic wrap, then the cut bisection.
-__device__ __forceinline__ int owner_of(const Grid& G, double px, double py, double pz) {
+// positions: one periodic wrap, then the cut search, with the cut planes in
+// shared memory (s_cuts: G.cuts staged, the axes at G.cut_offset): counted on
+// small axes, bisected on long ones.
+__device__ __forceinline__ int owner_of_staged(const Grid& G, const double* s_cuts, double px,
+                                               double py, double pz) {
     const double p[3] = {px, py, pz};
     int c[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-        c[a] = axis_coordinate(G.cuts + G.cut_offset[a], G.dims[a], wrap_if(G, a, p[a]));
+    for (int a = 0; a < 3; ++a) {
+        const double v = wrap_if(G, a, p[a]);
+        const double* cuts = s_cuts + G.cut_offset[a];
+        c[a] = G.dims[a] <= kCountedCells ? axis_coordinate_count(cuts, G.dims[a], v)
+                                          : axis_coordinate(cuts, G.dims[a], v);
+    }
     return (c[0] * G.dims[1] + c[1]) * G.dims[2] + c[2];
 }
 
+__device__ __forceinline__ void stage_cuts(const Grid& G, double* s_cuts) {
+    const int total = G.dims[0] + G.dims[1] + G.dims[2] + 3;
+    for (int k = threadIdx.x; k < total; k += blockDim.x) s_cuts[k] = G.cuts[k];
+    __syncthreads();
+}
+
+// Four positions per thread and pass, all loaded before any search.
 __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restrict__ x,
                                                    const double* __restrict__ y,
                                                    const double* __restrict__ z, long long n,
                                                    int* out) {
-    for (long long i = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i < n;
-         i += static_cast<long long>(gridDim.x) * NT)
-        out[i] = owner_of(G, x[i], y[i], z[i]);
+    __shared__ double s_cuts[kMaxRanks + 16];   // cut_offset[a] + kCountedCells <= 1036
+    stage_cuts(G, s_cuts);
+    constexpr int U = 4;
+    const long long step = static_cast<long long>(gridDim.x) * NT;
+    for (long long i0 = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i0 < n; i0 += U * step) {
+        double px[U], py[U], pz[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long i = i0 + u * step;
+            if (i < n) {
+                px[u] = ro(x + i);
+                py[u] = ro(y + i);
+                pz[u] = ro(z + i);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long i = i0 + u * step;
+            if (i < n) out[i] = owner_of_staged(G, s_cuts, px[u], py[u], pz[u]);
+        }
+    }
 }
 
 // Decomp::has_out_of_domain_particles (dsDecompX src/runtime.cpp:828-840) for
@@ -2139,12 +2213,22 @@ __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restr
 __global__ void __launch_bounds__(NT) k_out_of_domain(Grid G, const double* __restrict__ x,
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z, int* flags) {
+    __shared__ double s_cuts[kMaxRanks + 16];   // cut_offset[a] + kCountedCells <= 1036
     const int g = blockIdx.x;
     const int4 td = G.tiles[g];
     if (g >= G.tile_start[G.P]) return;
+    stage_cuts(G, s_cuts);
+    // a position inside the subdomain's own cut planes is owned there (the
+    // wrap leaves a position inside the box as it is, -0 aside, which lies
+    // in the same cell); only the others are searched
+    const Cell cell = cell_of(G, td.x);
     bool out = false;
-    for (int i = td.y + threadIdx.x; i < td.z; i += NT)
-        out = out || owner_of(G, x[i], y[i], z[i]) != td.x;
+    for (int i = td.y + threadIdx.x; i < td.z; i += NT) {
+        const double px = ro(x + i), py = ro(y + i), pz = ro(z + i);
+        const bool inside = cell.lo[0] <= px && px < cell.hi[0] && cell.lo[1] <= py &&
+                            py < cell.hi[1] && cell.lo[2] <= pz && pz < cell.hi[2];
+        if (!inside) out = out || owner_of_staged(G, s_cuts, px, py, pz) != td.x;
+    }
     if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(&flags[td.x], 1);
 }
 
@@ -2261,6 +2345,29 @@ int stream_grid(long long items) {
     const long long want = (items + NT - 1) / NT;
     const long long cap = static_cast<long long>(sm_count()) * 8;
     long long g = want < cap ? want : cap;
+    return static_cast<int>(g < 1 ? 1 : g);
+}
+
+// Grid of a grid-stride kernel of NT threads: the CTAs that fit on the GPU at
+// once (one wave, from the kernel's own occupancy), fewer for small work.
+int resident_grid(const void* kernel, long long items) {
+    static std::mutex lock;
+    static std::vector<std::pair<const void*, int>> cache;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> hold(lock);
+        for (const auto& k : cache)
+            if (k.first == kernel) per_sm = k.second;
+        if (!per_sm) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, 0) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+            cache.emplace_back(kernel, per_sm);
+        }
+    }
+    const long long want = (items + NT - 1) / NT;
+    const long long cap = static_cast<long long>(sm_count()) * per_sm;
+    const long long g = want < cap ? want : cap;
     return static_cast<int>(g < 1 ? 1 : g);
 }
 
@@ -2507,7 +2614,7 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                          bool positions_only, const Scratch& S, cudaStream_t s) {
-    k_halo_refresh<<<stream_grid(G.gcap), NT, 0, s>>>(G, A, owned_off, ghost_off,
+    k_halo_refresh<<<resident_grid(reinterpret_cast<const void*>(k_halo_refresh), G.gcap), NT, 0, s>>>(G, A, owned_off, ghost_off,
                                                       positions_only ? 1 : 0, S.halo_info,
                                                       S.ghost_owner, S.ghost_entry);
 }
@@ -2515,7 +2622,7 @@ void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, lo
 void launch_forward_fields(const Grid& G, const Arrays& A, long long owned_off,
                            long long ghost_off, const FieldOps& F, const Scratch& S,
                            cudaStream_t s) {
-    k_forward_fields<<<stream_grid(G.gcap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
+    k_forward_fields<<<resident_grid(reinterpret_cast<const void*>(k_forward_fields), G.gcap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
                                                         S.ghost_owner, G.status);
 }
 
@@ -2541,7 +2648,7 @@ void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, cons
 void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
                            long long ghost_off, const FieldOps& F, const Scratch& S,
                            cudaStream_t s) {
-    k_reverse_fields<<<stream_grid(G.ncap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
+    k_reverse_fields<<<resident_grid(reinterpret_cast<const void*>(k_reverse_fields), G.ncap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
                                                         S.bowner, S.boff, S.bslot, G.status);
 }
 
@@ -2552,7 +2659,7 @@ void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
 
 void launch_owner_rank(const Grid& G, const double* x, const double* y, const double* z,
                        long long n, int* out, cudaStream_t s) {
-    if (n > 0) k_owner_rank<<<stream_grid(n), NT, 0, s>>>(G, x, y, z, n, out);
+    if (n > 0) k_owner_rank<<<resident_grid(reinterpret_cast<const void*>(k_owner_rank), n), NT, 0, s>>>(G, x, y, z, n, out);
 }
 
 void launch_out_of_domain(const Grid& G, const double* x, const double* y, const double* z,

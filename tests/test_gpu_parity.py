@@ -725,6 +725,15 @@ def test_owner_rank_and_out_of_domain(cuda):
         pair.gpu.owner_rank(*dev, out)
         torch.cuda.synchronize()
         assert (out.cpu().numpy() == pair.ref.owner_rank(pos)).all()
+        # raw addresses need the count; lengths must agree (checked on the host)
+        out.zero_()
+        pair.gpu.owner_rank(*[t.data_ptr() for t in dev], out.data_ptr(), n=len(pos))
+        torch.cuda.synchronize()
+        assert (out.cpu().numpy() == pair.ref.owner_rank(pos)).all()
+        with pytest.raises(ValueError):
+            pair.gpu.owner_rank(*[t.data_ptr() for t in dev], out.data_ptr())
+        with pytest.raises(ValueError):
+            pair.gpu.owner_rank(dev[0], dev[1], dev[2][:10], out)
     finally:
         pair.close()
 
