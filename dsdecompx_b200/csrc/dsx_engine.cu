@@ -2,6 +2,7 @@
 // the kernels in dsx_kernels.cu, CUDA-graph capture of the batched step, and
 // the extern "C" entry points declared in include/dsx.h.
 #include "dsx.h"
+#include "dsx_errors.h"
 #include "dsx_kernels.cuh"
 
 #include <algorithm>
@@ -200,6 +201,8 @@ T* device_alloc(std::vector<void*>& owned, std::size_t count) {
 }
 
 }  // namespace
+
+void dsx::set_last_error(const char* message) { g_error = message ? message : ""; }
 
 struct dsx_grid {
     dsx_grid_desc desc{};

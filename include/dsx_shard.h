@@ -1,0 +1,109 @@
+/* Sharded virtual grid, native: the P subdomains of one box split over
+ * several processes (one GPU each), every collective call one exchange step
+ * with the processes that own neighboring blocks.
+ *
+ * The reference runs one MPI rank per subdomain (dsDecompX
+ * include/dsdecompx.hpp:70-248, src/runtime.cpp:862-1041).  Here a process
+ * owns a block of subdomains and keeps a grid of all P (dsx_grid_*) that
+ * holds particles only in its own; after each local call the particles and
+ * ghost lists that belong to another process's subdomains are sent there,
+ * and every process assembles its subdomains in the reference's order
+ * (retained, then immigrants by source rank; ghosts in the receiver's
+ * neighbor-block order), so each subdomain's arrays equal the reference's.
+ *
+ * The two communication steps come from the caller as a transport: a sum
+ * over all shards of a small vector, and point-to-point byte messages
+ * between device buffers (an MPI host: MPI_Allreduce and CUDA-aware
+ * MPI_Isend / MPI_Irecv; a NCCL host: ncclAllReduce and grouped
+ * ncclSend / ncclRecv).  Every shard makes the same transport calls in the
+ * same order.  Errors follow dsx.h (DSX_OK or a negative DSX_E_* code,
+ * message in dsx_last_error). */
+#ifndef DSX_SHARD_H
+#define DSX_SHARD_H
+
+#include "dsx.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dsx_transport {
+    void* user;
+    /* values[0..n) := their sum over all shards (every shard gets it). */
+    int (*allreduce_i64)(void* user, long long* values, long long n);
+    int (*allreduce_f64)(void* user, double* values, long long n);
+    /* Sends send[k] (send_bytes[k] device bytes) to shard send_to[k] and
+     * receives recv_bytes[k] bytes from shard recv_from[k] into recv[k]
+     * (device).  The send buffers are ready when `stream`'s work so far is
+     * done; the call returns once the received bytes are in place for later
+     * work on `stream`.  Peers appear once each, ascending; zero-byte
+     * messages are left out on both sides. */
+    int (*exchange)(void* user, int nsend, const int* send_to, const void* const* send,
+                    const long long* send_bytes, int nrecv, const int* recv_from,
+                    void* const* recv, const long long* recv_bytes, void* stream);
+} dsx_transport;
+
+typedef struct dsx_shard dsx_shard;
+
+/* desc and fields as dsx_grid_create (desc->nranks = P subdomains in all);
+ * particles: this shard's owned-particle capacity; owners: the shard of
+ * every subdomain (P values), or null for contiguous Cartesian blocks (the
+ * factorisation of nshards that divides the process grid with the least cut
+ * area, else contiguous runs of subdomain ranks).  The transport is copied. */
+int dsx_shard_create(const dsx_grid_desc* desc, const dsx_field_desc* fields, int nfields,
+                     long long particles, long long ghost_capacity, int shard, int nshards,
+                     const int* owners, const dsx_transport* transport, dsx_shard** out);
+int dsx_shard_destroy(dsx_shard* shard);
+
+/* The shard of every subdomain (P values). */
+int dsx_shard_owners(dsx_shard* shard, int* owners);
+
+/* This shard's particles: counts[P] (zero outside its subdomains) and host
+ * or device arrays as dsx_grid_upload. */
+int dsx_shard_upload(dsx_shard* shard, const long long* counts, const void* const* arrays,
+                     void* stream);
+
+/* Decomp::migrate on every shard (with the Dynamic rebalance over all
+ * shards' counts).  results: null, or P x {changed, previous, retained, sent,
+ * received, new_owned}, filled for this shard's subdomains. */
+int dsx_shard_migrate(dsx_shard* shard, void* stream, long long* results);
+
+/* Decomp::rebalance with work per subdomain (P values, this shard's entries
+ * used; null: owned counts).  results: null, or P x {attempted, changed,
+ * new_owned} for this shard's subdomains; imbalance: null or one value. */
+int dsx_shard_rebalance(dsx_shard* shard, const double* work, int force, void* stream,
+                        long long* results, double* imbalance);
+
+/* Decomp::exchange_halo: builds (rebuild != 0, or no plan) or refreshes
+ * (positions_only: x, y, z) this shard's receivers' ghosts.  results: null,
+ * or P x {ghost_count, layout_changed, storage_reallocated, plan_reused} for
+ * this shard's subdomains. */
+int dsx_shard_exchange_halo(dsx_shard* shard, int rebuild, int positions_only, void* stream,
+                            long long* results);
+
+/* Decomp::reverse_halo: every ghost's force (in the assembled ghost region)
+ * added to its owner, in the reference's order. */
+int dsx_shard_reverse_halo(dsx_shard* shard, void* stream);
+
+/* Field exchanges as dsx_grid_forward_exchange / dsx_grid_reverse_exchange,
+ * on the assembled ghosts. */
+int dsx_shard_forward_exchange(dsx_shard* shard, int nfields, const int* field_ids, void* stream);
+int dsx_shard_reverse_exchange(dsx_shard* shard, int nfields, const int* field_ids,
+                               const int* ops, void* stream);
+
+/* Owned particles: the local grid's view (owned half, per-subdomain counts).
+ * Ghosts: the assembled region -- base[a] its arrays, ghost_offset 0,
+ * ghost_capacity its capacity, g / gbase (device, P and P + 1 values) and
+ * halo_totals (device {ghosts, 0}) this shard's receivers' blocks. */
+int dsx_shard_owned_view(dsx_shard* shard, dsx_grid_view* out);
+int dsx_shard_ghost_view(dsx_shard* shard, dsx_grid_view* out);
+
+/* Host counts per subdomain (zero outside this shard's subdomains), read
+ * after the work queued on `stream`. */
+int dsx_shard_counts(dsx_shard* shard, long long* owned, long long* ghosts, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DSX_SHARD_H */

@@ -1,5 +1,6 @@
-"""The C-ABI library loads, exports every entry point include/dsx.h declares,
+"""The C-ABI library loads, exports every entry point the C headers under include/ declare,
 and its host-side topology planning matches the oracle (no GPU needed)."""
+import glob
 import os
 import re
 
@@ -13,9 +14,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "dsx.h")).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(dsx_[a-z_0-9]+)\s*\(", text)) - {"dsx_step_callback"})
+    """Entry points of every C header under include/ (dsx.h, dsx_shard.h, ...)."""
+    names = set()
+    for h in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))):
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names |= set(re.findall(r"\b(dsx_[a-z_0-9]+)\s*\(", text))
+    return sorted(names - {"dsx_step_callback"})
 
 
 def test_library_exports_every_declared_symbol():

@@ -47,6 +47,20 @@ def test_cpp_grid_sanity(cuda):
     assert "grid_sanity: ok" in proc.stdout
 
 
+@pytest.mark.gpu
+def test_cpp_shard_sanity(cuda):
+    """The native sharded grid (include/dsx_shard.h) in a C++ program: shards
+    as threads on one GPU with a barrier-and-copy transport, every array of
+    every subdomain equal to one grid's after migrate, halo build, reverse
+    sums, field exchanges and refresh (Manual over 4 shards, Dynamic over 2)."""
+    import dsdecompx_b200 as dsx
+    exe = os.path.join(os.path.dirname(dsx.library_path()), "shard_sanity")
+    assert os.path.exists(exe), "tests/cpp programs are built by __graft_entry__.build()"
+    proc = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert proc.returncode == 0, proc.stdout + proc.stderr
+    assert "shard_sanity: ok" in proc.stdout
+
+
 @pytest.mark.parametrize("lower,upper", [((0.0, 0.0, 0.0), (100.0, 100.0, 100.0)),
                                          ((-3.7, 1e-3, 1e6), (5.1, 0.3, 1e6 + 7.25))])
 def test_rank_migrate_matches_oracle(cuda, lower, upper):
