@@ -58,6 +58,8 @@ def parse():
                          "refreshes, split-phase overlap, rebalance, box changes)")
     ap.add_argument("--sharded", action="store_true",
                     help="the sharded grid's step (the multi-GPU path) also at one GPU")
+    ap.add_argument("--sharded-impl", default="native", choices=["native", "python"],
+                    help="the library's sharded protocol (dsx_shard_*) or the Python one")
     return ap.parse_args()
 
 
@@ -579,21 +581,31 @@ def run_sharded(args, rank, world, device):
         pinned.append(t)
     del grouped
     ptrs = [t.data_ptr() for t in pinned]
-    engine = shd.DeviceEngine(P, dims if w.policy == "manual" else (0, 0, 0), w.policy, w.lower,
-                              upper, halo_width=w.halo, fields=w.fields,
-                              particles=int(1.5 * N) + 65536, ghost_capacity=int(0.9 * N))
-    sh = shd.ShardedGrid(engine, rank, world, owners=owners,
-                         run=lambda g: shd.run_distributed(g, device=f"cuda:{device}"))
+    native = args.sharded_impl == "native"
+    grid_args = (P, dims if w.policy == "manual" else (0, 0, 0), w.policy, w.lower, upper)
+    grid_kw = dict(halo_width=w.halo, fields=w.fields, particles=int(1.5 * N) + 65536,
+                   ghost_capacity=int(0.9 * N))
+    if native:
+        sh = shd.NativeShardedGrid(*grid_args, **grid_kw, shard=rank, nshards=world, owners=owners,
+                                   device=f"cuda:{device}")
+        engine = None
+    else:
+        engine = shd.DeviceEngine(*grid_args, **grid_kw)
+        sh = shd.ShardedGrid(engine, rank, world, owners=owners,
+                             run=lambda g: shd.run_distributed(g, device=f"cuda:{device}"))
     totals = torch.zeros(4, dtype=torch.int32, device=device)
     seed = args.seed + 1000 * rank
 
     def user_work(shard):
         s = stream.cuda_stream
-        gv = shard.ghost_view(totals)
+        gv = shard.ghost_view() if native else shard.ghost_view(totals)
         wl.dsxw_ghost_forces(C.byref(gv), seed, 0, s)
-        v = shard.E.grid.view()
+        v = shard.owned_view() if native else shard.E.grid.view()
         wl.dsxw_drift(C.byref(v), seed, 0, w.drift, s)
         wl.dsxw_advance(s)
+
+    def launched():
+        return sh.launches if native else engine.launches
 
     with torch.cuda.stream(stream):
         sh.upload_flat(counts, ptrs)
@@ -603,7 +615,7 @@ def run_sharded(args, rank, world, device):
     torch.distributed.barrier()
     torch.cuda.synchronize(device)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = engine.launches
+    launches0 = launched()
     with ClockSampler(device) as clocks:
         with torch.cuda.stream(stream):
             start.record(stream)
@@ -611,7 +623,7 @@ def run_sharded(args, rank, world, device):
                 sh.step(user_work)
             end.record(stream)
         torch.cuda.synchronize(device)
-    launches = engine.launches - launches0 + 3 * args.steps
+    launches = launched() - launches0 + 3 * args.steps
     elapsed_ms = max_over_ranks(start.elapsed_time(end), world, device)
     torch.distributed.barrier()
     clock = clocks.summary()
@@ -621,7 +633,7 @@ def run_sharded(args, rank, world, device):
     Ntot = int(everyone.item())
     value = Ntot / (ms_per_step / 1e3) / 1e6
     # the step's least traffic (this rank): what the fused step's kernels move
-    tot = engine.grid.totals(stream=stream)
+    tot = sh.totals(stream=stream) if native else engine.grid.totals(stream=stream)
     alg = algorithmic_bytes(S, tot["particles"], tot["emigrants"], tot["ghosts"], tot["boundary"])
     step_bytes = sum(alg[k] for k in ("step_classify", "step_move", "emig_place", "immigrant_halo",
                                       "reverse_sum"))
@@ -651,8 +663,8 @@ def run_sharded(args, rank, world, device):
         nb = int(cnt.sum()) * S + 8 * P
         e2e = {"value": round(Ntot / (e_ms / 1e3) / 1e6, 3), "unit": "M particles/s",
                "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "ms_per_step": round(e_ms, 3),
-               "path": "ShardedGrid.upload_flat (pinned host) -> ShardedGrid.step -> download_flat"}
-    engine.close()
+               "path": f"{type(sh).__name__}.upload_flat (pinned host) -> step -> download_flat"}
+    (sh if native else engine).close()
     return {
         "metric": METRIC, "value": round(value, 3), "unit": "M particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -661,7 +673,8 @@ def run_sharded(args, rank, world, device):
         "config": {"workload": w.name, "description": w.description + f"; one block per GPU, "
                    f"{fa[0]}x{fa[1]}x{fa[2]} blocks", "subdomains": P, "grid": list(dims),
                    "particles": Ntot, "record_bytes": S,
-                   "step": "sharded grid (ShardedGrid.step: per-call operations, one NCCL "
+                   "step": ("native sharded grid (dsx_shard_*" if native else
+                            "sharded grid (ShardedGrid") + ": per-call operations, one NCCL "
                            "exchange step per call)",
                    "l2": "inputs larger than L2 (%.2f GB of owned records per GPU)" % (N * S / 1e9),
                    "parallelism": f"subdomain blocks x{world}"},

@@ -142,6 +142,23 @@ def lib() -> C.CDLL:
             "dsx_grid_assemble": [vp, llp, C.c_int, C.POINTER(vp), C.c_longlong, vp, vp],
             "dsx_grid_set_rebalance_work": [vp, dp],
             "dsx_copy_segments": [vp, C.c_longlong, vp],
+            "dsx_shard_create": [C.POINTER(_GridDesc), C.POINTER(_FieldDesc), C.c_int, C.c_longlong,
+                                 C.c_longlong, C.c_int, C.c_int, ip, vp, C.POINTER(vp)],
+            "dsx_shard_destroy": [vp],
+            "dsx_shard_owners": [vp, ip],
+            "dsx_shard_upload": [vp, llp, C.POINTER(vp), vp],
+            "dsx_shard_download": [vp, llp, C.POINTER(vp), vp],
+            "dsx_shard_migrate": [vp, vp, llp],
+            "dsx_shard_rebalance": [vp, dp, C.c_int, vp, llp, dp],
+            "dsx_shard_exchange_halo": [vp, C.c_int, C.c_int, vp, llp],
+            "dsx_shard_reverse_halo": [vp, vp],
+            "dsx_shard_forward_exchange": [vp, C.c_int, ip, vp],
+            "dsx_shard_reverse_exchange": [vp, C.c_int, ip, ip, vp],
+            "dsx_shard_owned_view": [vp, C.POINTER(GridView)],
+            "dsx_shard_ghost_view": [vp, C.POINTER(GridView)],
+            "dsx_shard_counts": [vp, llp, llp, vp],
+            "dsx_shard_launches": [vp, llp],
+            "dsx_shard_totals": [vp, llp, vp],
             "dsx_grid_kernel_times": [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float)],
         }
         for name, args in sig.items():

@@ -134,6 +134,7 @@ struct dsx_shard {
     int* d_totals = nullptr;   // {ghosts, 0}
 
     std::map<int, std::unique_ptr<DeviceBuffer>> sendbuf, recvbuf;
+    long long launches = 0;   // kernels of this library launched for this shard
 
     ~dsx_shard() {
         for (void* p : assembled) cudaFree(p);
@@ -209,7 +210,9 @@ struct dsx_shard {
                 list.push_back({src[j] + si * b, dst[j] + di * b, rows.n[r] * b});
             }
         }
-        if (!list.empty()) check(dsx_copy_segments(list.data(), static_cast<long long>(list.size()), s));
+        if (list.empty()) return;
+        check(dsx_copy_segments(list.data(), static_cast<long long>(list.size()), s));
+        ++const_cast<dsx_shard*>(this)->launches;
     }
 
     // one message per peer each way through the transport
@@ -261,6 +264,7 @@ struct dsx_shard {
     void redistribute(const std::vector<long long>& res, cudaStream_t s, long long* results) {
         std::vector<long long> pairs(static_cast<std::size_t>(P) * P);
         check(dsx_grid_migration_pairs(grid, pairs.data(), s));
+        ++launches;
         allreduce(pairs);
         const auto M = [&](int t, int q) { return pairs[static_cast<std::size_t>(t) * P + q]; };
         std::vector<long long> local_n(static_cast<std::size_t>(P)), obase(static_cast<std::size_t>(P) + 1, 0);
@@ -358,6 +362,7 @@ struct dsx_shard {
             const std::vector<unsigned char*> sec = sections(in.at(peers[k]), from_peer.at(peers[k]), all);
             for (std::size_t a = 0; a < sec.size(); ++a) sources[k * kArraySlots + a] = sec[a];
         }
+        launches += 2;   // the copies and the new layout
         check(dsx_grid_assemble(grid, counts.data(), static_cast<int>(peers.size()),
                                 sources.empty() ? nullptr : sources.data(),
                                 static_cast<long long>(segs.size()), segs.empty() ? nullptr : segs.data(), s));
@@ -372,6 +377,9 @@ struct dsx_shard {
         }
         std::vector<long long> res(static_cast<std::size_t>(6) * P);
         check(dsx_grid_migrate(grid, s, res.data()));
+        // classify, scan, layout, move, emigrant histogram / scan / placement
+        // (and the rebalance kernel of a Dynamic grid)
+        launches += 7 + (dynamic ? 1 : 0);
         redistribute(res, s, results);
     }
 
@@ -383,6 +391,7 @@ struct dsx_shard {
         std::vector<long long> flags(static_cast<std::size_t>(3) * P);
         std::vector<double> imb(static_cast<std::size_t>(P), 1.0);
         check(dsx_grid_rebalance(grid, w.data(), force ? 1 : 0, s, flags.data(), imb.data()));
+        launches += 8 + 1;   // the rebalance, its migrate, the pair counts
         // the migrate inside the rebalance, in migrate's result format
         std::vector<long long> pairs(static_cast<std::size_t>(P) * P);
         check(dsx_grid_migration_pairs(grid, pairs.data(), s));
@@ -544,6 +553,7 @@ struct dsx_shard {
         const std::vector<long long> prev_g = g;
         std::vector<long long> hres(static_cast<std::size_t>(4) * P);
         check(dsx_grid_exchange_halo(grid, build ? 1 : 0, (positions_only && !build) ? 1 : 0, s, hres.data()));
+        launches += build ? 4 : 1;   // classify, scan, layout, scatter; or the refresh
         bool grew = false;
         if (build) {
             std::vector<int> len(static_cast<std::size_t>(P) * kNeighbors), first(len.size());
@@ -577,6 +587,7 @@ struct dsx_shard {
         if (!planned) fail(DSX_E_LOGIC, "reverse_halo without a halo plan");
         give_back({6, 7, 8}, s);
         check(dsx_grid_reverse_halo(grid, s));
+        ++launches;
     }
 
     std::vector<int> field_arrays(int nfields, const int* ids) const {
@@ -729,6 +740,13 @@ int dsx_shard_upload(dsx_shard* shard, const long long* counts, const void* cons
     });
 }
 
+int dsx_shard_download(dsx_shard* shard, long long* counts, void* const* arrays, void* stream) {
+    return guarded([&] {
+        if (!shard || !counts) fail(DSX_E_INVALID, "null argument");
+        check(dsx_grid_download(shard->grid, counts, arrays, stream));
+    });
+}
+
 int dsx_shard_migrate(dsx_shard* shard, void* stream, long long* results) {
     return guarded([&] {
         if (!shard) fail(DSX_E_INVALID, "null shard");
@@ -765,6 +783,7 @@ int dsx_shard_forward_exchange(dsx_shard* shard, int nfields, const int* field_i
         if (!shard->planned) fail(DSX_E_LOGIC, "forward_exchange without a halo plan");
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
         check(dsx_grid_forward_exchange(shard->grid, nfields, field_ids, s));
+        ++shard->launches;
         shard->ship(shard->field_arrays(nfields, field_ids), s);
     });
 }
@@ -777,6 +796,7 @@ int dsx_shard_reverse_exchange(dsx_shard* shard, int nfields, const int* field_i
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
         shard->give_back(shard->field_arrays(nfields, field_ids), s);
         check(dsx_grid_reverse_exchange(shard->grid, nfields, field_ids, ops, s));
+        ++shard->launches;
     });
 }
 
@@ -805,6 +825,20 @@ int dsx_shard_ghost_view(dsx_shard* shard, dsx_grid_view* out) {
         g.ghost_capacity = shard->assembled_cap;
         g.nranks = shard->P;
         *out = g;
+    });
+}
+
+int dsx_shard_totals(dsx_shard* shard, long long* out4, void* stream) {
+    return guarded([&] {
+        if (!shard || !out4) fail(DSX_E_INVALID, "null argument");
+        check(dsx_grid_totals(shard->grid, out4, stream));
+    });
+}
+
+int dsx_shard_launches(dsx_shard* shard, long long* count) {
+    return guarded([&] {
+        if (!shard || !count) fail(DSX_E_INVALID, "null argument");
+        *count = shard->launches;
     });
 }
 

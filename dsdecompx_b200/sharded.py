@@ -405,6 +405,10 @@ class ShardedGrid:
         ghosts = self.E.read_assembled(int(self.plan.gbase[t]), int(self.plan.g[t]), name)
         return np.concatenate([owned, ghosts])
 
+    def read_owned(self, t: int, name: str) -> np.ndarray:
+        self._check_mine(t)
+        return self.E.read_owned(t, name)
+
     def write_ghosts(self, t: int, name: str, values):
         """Values of the assembled ghosts of subdomain t (array `name`)."""
         self._check_mine(t)
@@ -837,3 +841,301 @@ class DeviceEngine:
         arr = np.ascontiguousarray(values, dtype=self.grid.dtype_of(name)).reshape(-1)
         raw = self.torch.from_numpy(arr.view(np.uint8).copy())
         self.asm[a][lo * b:lo * b + raw.numel()].copy_(raw)
+
+
+# ------------------------------------------------- the native protocol
+
+import ctypes as _C
+
+_ALLREDUCE_I64 = _C.CFUNCTYPE(_C.c_int, _C.c_void_p, _C.POINTER(_C.c_longlong), _C.c_longlong)
+_ALLREDUCE_F64 = _C.CFUNCTYPE(_C.c_int, _C.c_void_p, _C.POINTER(_C.c_double), _C.c_longlong)
+_EXCHANGE = _C.CFUNCTYPE(_C.c_int, _C.c_void_p, _C.c_int, _C.POINTER(_C.c_int),
+                         _C.POINTER(_C.c_void_p), _C.POINTER(_C.c_longlong), _C.c_int,
+                         _C.POINTER(_C.c_int), _C.POINTER(_C.c_void_p), _C.POINTER(_C.c_longlong),
+                         _C.c_void_p)
+
+
+class _Transport(_C.Structure):
+    _fields_ = [("user", _C.c_void_p), ("allreduce_i64", _ALLREDUCE_I64),
+                ("allreduce_f64", _ALLREDUCE_F64), ("exchange", _EXCHANGE)]
+
+
+class _DeviceBytes:
+    """n device bytes at a raw address, as a CUDA-array-interface object."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = dict(shape=(int(n),), typestr="|u1", data=(int(ptr), False),
+                                             version=3, strides=None)
+
+
+class TorchTransport:
+    """The native shard's transport over torch.distributed (NCCL between
+    GPUs): sums through all_reduce, messages through grouped isend / irecv
+    per peer on the caller's stream.  Exceptions become DSX_E_RUNTIME."""
+
+    def __init__(self, device="cuda", group=None):
+        self.device, self.group = device, group
+        self.error: Optional[BaseException] = None
+        self._i64 = _ALLREDUCE_I64(self._allreduce_i64)
+        self._f64 = _ALLREDUCE_F64(self._allreduce_f64)
+        self._ex = _EXCHANGE(self._exchange)
+        self.struct = _Transport(None, self._i64, self._f64, self._ex)
+
+    def _allreduce(self, ptr, n, dtype):
+        import torch
+        import torch.distributed as dist
+        host = np.ctypeslib.as_array(ptr, shape=(int(n),))
+        t = torch.from_numpy(host.astype(dtype)).to(self.device)
+        dist.all_reduce(t, group=self.group)
+        host[:] = t.cpu().numpy()
+
+    def _allreduce_i64(self, user, ptr, n):
+        try:
+            self._allreduce(ptr, n, np.int64)
+            return 0
+        except BaseException as exc:   # never through the C frames
+            self.error = exc
+            return -3
+
+    def _allreduce_f64(self, user, ptr, n):
+        try:
+            self._allreduce(ptr, n, np.float64)
+            return 0
+        except BaseException as exc:
+            self.error = exc
+            return -3
+
+    def _exchange(self, user, nsend, to, send, send_bytes, nrecv, frm, recv, recv_bytes, stream):
+        try:
+            import torch
+            import torch.distributed as dist
+            ops = []
+            as_tensor = lambda p, n: torch.as_tensor(_DeviceBytes(p, n), device=self.device)
+            for k in range(nrecv):
+                ops.append(dist.P2POp(dist.irecv, as_tensor(recv[k], recv_bytes[k]), int(frm[k]), self.group))
+            for k in range(nsend):
+                ops.append(dist.P2POp(dist.isend, as_tensor(send[k], send_bytes[k]), int(to[k]), self.group))
+            if ops:
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream or 0)):
+                    for w in dist.batch_isend_irecv(ops):
+                        w.wait()
+            return 0
+        except BaseException as exc:
+            self.error = exc
+            return -3
+
+
+class NativeShardedGrid:
+    """One shard of the native sharded grid (dsx_shard_*): the same protocol
+    as ShardedGrid, run by the library, with a transport (default: this
+    process's torch.distributed group)."""
+
+    def __init__(self, nranks: int, dims=(0, 0, 0), policy: str = "manual", lower=(0.0, 0.0, 0.0),
+                 upper=(1.0, 1.0, 1.0), periodic=(True, True, True), halo_width: float = 0.0,
+                 edges_and_corners: bool = True, dynamic=None,
+                 fields: Sequence[Tuple[str, object, int]] = (), particles: int = 0,
+                 ghost_capacity: int = 0, shard: Optional[int] = None, nshards: Optional[int] = None,
+                 owners=None, transport: Optional[TorchTransport] = None, device="cuda"):
+        from . import FIELD_TYPES, _check, _FieldDesc, _grid_desc, lib
+        import torch.distributed as dist
+        self.L = lib()
+        self._check = _check
+        self.P = nranks
+        self.shard = dist.get_rank() if shard is None else int(shard)
+        self.nshards = dist.get_world_size() if nshards is None else int(nshards)
+        self.transport = transport or TorchTransport(device)
+        d = _grid_desc(nranks, dims, policy, lower, upper, periodic, halo_width, edges_and_corners, dynamic)
+        self.fields = [(str(n), FIELD_TYPES[t] if isinstance(t, str) else int(t), int(c))
+                       for n, t, c in fields]
+        self._names = [n.encode() for n, _, _ in self.fields]
+        fd = (_FieldDesc * max(len(self.fields), 1))(
+            *[_FieldDesc(self._names[i], t, c) for i, (_, t, c) in enumerate(self.fields)])
+        own = None
+        if owners is not None:
+            self._owners_arg = np.ascontiguousarray(owners, dtype=np.int32)
+            own = self._owners_arg.ctypes.data_as(_C.POINTER(_C.c_int))
+        h = _C.c_void_p()
+        self._call(self.L.dsx_shard_create(_C.byref(d), fd, len(self.fields), int(particles),
+                                           int(ghost_capacity), self.shard, self.nshards, own,
+                                           _C.byref(self.transport.struct), _C.byref(h)))
+        self.h = h
+        out = np.zeros(nranks, dtype=np.int32)
+        self._call(self.L.dsx_shard_owners(self.h, out.ctypes.data_as(_C.POINTER(_C.c_int))))
+        self.owners = out.astype(np.int64)
+        self.mine = np.flatnonzero(self.owners == self.shard)
+
+    def _call(self, status):
+        err, self.transport.error = self.transport.error, None
+        if status != 0 and err is not None:
+            raise RuntimeError(f"transport failed: {err!r}") from err
+        self._check(status)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.dsx_shard_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _stream(self, stream):
+        from . import _stream
+        return _stream(stream)
+
+    def upload_flat(self, counts, arrays: List[Optional[int]], stream=None):
+        c = np.ascontiguousarray(counts, dtype=np.int64)
+        ptrs = (_C.c_void_p * (13 + len(self.fields)))(*[a or None for a in arrays])
+        self._call(self.L.dsx_shard_upload(self.h, c.ctypes.data_as(_C.POINTER(_C.c_longlong)), ptrs,
+                                           self._stream(stream)))
+
+    def migrate(self, stream=None):
+        res = np.zeros((self.P, 6), dtype=np.int64)
+        self._call(self.L.dsx_shard_migrate(self.h, self._stream(stream),
+                                            res.ctypes.data_as(_C.POINTER(_C.c_longlong))))
+        return {int(t): tuple(int(v) for v in res[t]) for t in self.mine}
+
+    def rebalance(self, work=None, force: bool = False, stream=None):
+        res = np.zeros((self.P, 3), dtype=np.int64)
+        imb = _C.c_double()
+        w = None if work is None else np.ascontiguousarray(work, dtype=np.float64)
+        self._call(self.L.dsx_shard_rebalance(
+            self.h, None if w is None else w.ctypes.data_as(_C.POINTER(_C.c_double)), 1 if force else 0,
+            self._stream(stream), res.ctypes.data_as(_C.POINTER(_C.c_longlong)), _C.byref(imb)))
+        return {int(t): tuple(int(v) for v in res[t]) for t in self.mine}, imb.value
+
+    def exchange_halo(self, rebuild: bool = False, positions_only: bool = False, stream=None):
+        res = np.zeros((self.P, 4), dtype=np.int64)
+        self._call(self.L.dsx_shard_exchange_halo(self.h, 1 if rebuild else 0, 1 if positions_only else 0,
+                                                  self._stream(stream),
+                                                  res.ctypes.data_as(_C.POINTER(_C.c_longlong))))
+        return {int(t): tuple(int(v) for v in res[t]) for t in self.mine}
+
+    def reverse_halo(self, stream=None):
+        self._call(self.L.dsx_shard_reverse_halo(self.h, self._stream(stream)))
+
+    def _field_ids(self, names):
+        index = {n: i for i, (n, _, _) in enumerate(self.fields)}
+        return (_C.c_int * max(len(names), 1))(*[index[n] for n in names])
+
+    def forward_exchange(self, names: Sequence[str], stream=None):
+        self._call(self.L.dsx_shard_forward_exchange(self.h, len(names), self._field_ids(names),
+                                                     self._stream(stream)))
+
+    def reverse_exchange(self, fields: Sequence[Tuple[str, str]], stream=None):
+        from . import OPS
+        ops = (_C.c_int * max(len(fields), 1))(*[OPS[o] for _, o in fields])
+        self._call(self.L.dsx_shard_reverse_exchange(self.h, len(fields),
+                                                     self._field_ids([n for n, _ in fields]), ops,
+                                                     self._stream(stream)))
+
+    def step(self, callback=None, stream=None):
+        """migrate -> exchange_halo(rebuild) -> callback(self) -> reverse_halo."""
+        mig = self.migrate(stream)
+        halo = self.exchange_halo(True, False, stream)
+        if callback is not None:
+            callback(self)
+        self.reverse_halo(stream)
+        return mig, halo
+
+    def owned_view(self):
+        from . import GridView
+        v = GridView()
+        self._call(self.L.dsx_shard_owned_view(self.h, _C.byref(v)))
+        return v
+
+    def totals(self, stream=None) -> Dict[str, int]:
+        """The local grid's totals (owned, emigrants of the last migrate,
+        ghosts of its own lists, boundary owners)."""
+        out = np.zeros(4, dtype=np.int64)
+        self._call(self.L.dsx_shard_totals(self.h, out.ctypes.data_as(_C.POINTER(_C.c_longlong)),
+                                           self._stream(stream)))
+        return dict(particles=int(out[0]), emigrants=int(out[1]), ghosts=int(out[2]),
+                    boundary=int(out[3]))
+
+    @property
+    def launches(self) -> int:
+        n = _C.c_longlong()
+        self._call(self.L.dsx_shard_launches(self.h, _C.byref(n)))
+        return n.value
+
+    def ghost_view(self):
+        from . import GridView
+        v = GridView()
+        self._call(self.L.dsx_shard_ghost_view(self.h, _C.byref(v)))
+        return v
+
+    def all_counts(self, stream=None):
+        o = np.zeros(self.P, dtype=np.int64)
+        g = np.zeros(self.P, dtype=np.int64)
+        self._call(self.L.dsx_shard_counts(self.h, o.ctypes.data_as(_C.POINTER(_C.c_longlong)),
+                                           g.ctypes.data_as(_C.POINTER(_C.c_longlong)),
+                                           self._stream(stream)))
+        return o, g
+
+    def download_flat(self, arrays: List[Optional[int]], stream=None):
+        """This shard's owned particles into host or device arrays (the
+        subdomains concatenated in rank order); returns the counts."""
+        c = np.zeros(self.P, dtype=np.int64)
+        ptrs = (_C.c_void_p * (13 + len(self.fields)))(*[a or None for a in arrays])
+        self._call(self.L.dsx_shard_download(self.h, c.ctypes.data_as(_C.POINTER(_C.c_longlong)), ptrs,
+                                             self._stream(stream)))
+        return c
+
+    def counts(self, t: int) -> Tuple[int, int]:
+        o, g = self.all_counts()
+        return int(o[t]), int(g[t])
+
+    def read_owned(self, t: int, name: str) -> np.ndarray:
+        return self.read(t, name)[:self.counts(t)[0]]
+
+    def _array(self, name: str):
+        """(array id, element dtype, components) of a core array or field."""
+        from . import ARRAYS, CORE_DTYPES, FIELD_DTYPES
+        if name in ARRAYS:
+            return ARRAYS.index(name), np.dtype(CORE_DTYPES[ARRAYS.index(name)]), 1
+        k = [f[0] for f in self.fields].index(name)
+        return 13 + k, np.dtype(FIELD_DTYPES[self.fields[k][1]]), self.fields[k][2]
+
+    def read(self, t: int, name: str) -> np.ndarray:
+        """Owned records then assembled ghosts of subdomain t (host)."""
+        o, g = self.all_counts()
+        a, dt, comps = self._array(name)
+        b = dt.itemsize * comps
+        out = np.zeros((int(o[t]) + int(g[t])) * b, dtype=np.uint8)
+        v = self.owned_view()
+        _device_to_host(out[:int(o[t]) * b], v.base[a] + b * (int(v.owned_offset) + int(o[:t].sum())))
+        if g[t]:
+            _device_to_host(out[int(o[t]) * b:], self.ghost_view().base[a] + b * int(g[:t].sum()))
+        arr = out.view(dt)
+        return arr.reshape(-1, comps) if comps > 1 else arr
+
+    def write_owned(self, t: int, name: str, start: int, values):
+        o, _ = self.all_counts()
+        a, dt, comps = self._array(name)
+        raw = np.ascontiguousarray(values, dtype=dt).reshape(-1).view(np.uint8)
+        v = self.owned_view()
+        b = dt.itemsize * comps
+        _host_to_device(v.base[a] + b * (int(v.owned_offset) + int(o[:t].sum()) + int(start)), raw)
+
+    def write_ghosts(self, t: int, name: str, values):
+        _, g = self.all_counts()
+        a, dt, comps = self._array(name)
+        raw = np.ascontiguousarray(values, dtype=dt).reshape(-1).view(np.uint8)
+        if raw.size != int(g[t]) * dt.itemsize * comps:
+            raise ValueError(f"subdomain {t} has {int(g[t])} ghosts")
+        _host_to_device(self.ghost_view().base[a] + dt.itemsize * comps * int(g[:t].sum()), raw)
+
+
+def _device_to_host(dst: np.ndarray, src_ptr: int):
+    if dst.size:
+        import torch
+        dst[:] = torch.as_tensor(_DeviceBytes(src_ptr, dst.size), device="cuda").cpu().numpy()
+
+
+def _host_to_device(dst_ptr: int, src: np.ndarray):
+    if src.size:
+        import torch
+        torch.as_tensor(_DeviceBytes(dst_ptr, src.size), device="cuda").copy_(torch.from_numpy(src.copy()))

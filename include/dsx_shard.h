@@ -63,6 +63,10 @@ int dsx_shard_owners(dsx_shard* shard, int* owners);
 int dsx_shard_upload(dsx_shard* shard, const long long* counts, const void* const* arrays,
                      void* stream);
 
+/* This shard's owned particles into host or device arrays (as
+ * dsx_grid_download: counts[P] out, subdomains in rank order). */
+int dsx_shard_download(dsx_shard* shard, long long* counts, void* const* arrays, void* stream);
+
 /* Decomp::migrate on every shard (with the Dynamic rebalance over all
  * shards' counts).  results: null, or P x {changed, previous, retained, sent,
  * received, new_owned}, filled for this shard's subdomains. */
@@ -97,6 +101,13 @@ int dsx_shard_reverse_exchange(dsx_shard* shard, int nfields, const int* field_i
  * halo_totals (device {ghosts, 0}) this shard's receivers' blocks. */
 int dsx_shard_owned_view(dsx_shard* shard, dsx_grid_view* out);
 int dsx_shard_ghost_view(dsx_shard* shard, dsx_grid_view* out);
+
+/* The local grid's totals as dsx_grid_totals ({owned particles, emigrants
+ * of the last migrate, ghosts of its own lists, boundary owners}). */
+int dsx_shard_totals(dsx_shard* shard, long long* out4, void* stream);
+
+/* Kernels of this library launched for this shard so far (benchmarks). */
+int dsx_shard_launches(dsx_shard* shard, long long* count);
 
 /* Host counts per subdomain (zero outside this shard's subdomains), read
  * after the work queued on `stream`. */

@@ -61,7 +61,7 @@ class Scenario:
                 o = sh.counts(t)[0]
                 d = displacement(step, t, o, sigma)
                 for a, name in enumerate("xyz"):
-                    sh.write_owned(t, name, 0, sh.E.read_owned(t, name) + d[:, a])
+                    sh.write_owned(t, name, 0, sh.read_owned(t, name) + d[:, a])
 
     def compare(self, what, names=None, ghosts=True):
         for sh in self.shards:
@@ -73,7 +73,7 @@ class Scenario:
                     assert sg == g, (what, t, sg, g)
                 for name in names or self.names:
                     want = self.ref.read(t, name, 0, o + (g if ghosts else 0))
-                    got = sh.read(t, name) if ghosts else sh.E.read_owned(t, name)
+                    got = sh.read(t, name) if ghosts else sh.read_owned(t, name)
                     assert same(want, got), (what, t, name)
 
     def set_ghosts(self, names):

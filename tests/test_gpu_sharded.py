@@ -166,3 +166,45 @@ def test_one_shard_over_nccl(cuda):
         ref.close()
         e.close()
         dist.destroy_process_group()
+
+
+def test_native_shard_over_nccl(cuda):
+    """The native sharded grid (dsx_shard_*) through its torch.distributed
+    transport on a one-rank NCCL group: every call equals the grid's own."""
+    import datetime
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import sharded as shd
+    from shard_scenario import distributed_drive
+    kw = CASES["dynamic-4x4x2-R4"]
+    P, N = kw["nranks"], 30_000
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    owner = Grid("port", P, kw["dims"], kw["policy"], (0, 0, 0), kw["upper"], (True, True, True),
+                 kw["halo_width"], True, kw["dynamic"], [(n, TYPE_INDEX[t], c) for n, t, c in kw["fields"]])
+    per = initial(owner, P, kw["upper"], N, 47, kw["fields"])
+    owner.close()
+    ref = dsx.VirtualGrid(**grid_kw(kw), particles=N, ghost_capacity=2 * N)
+    ref.upload(per)
+    sh = shd.NativeShardedGrid(**grid_kw(kw), particles=N + 4096, ghost_capacity=N)
+    try:
+        names = dsx.ARRAYS + [f[0] for f in kw["fields"]]
+        counts = np.array([len(d["x"]) for d in per], dtype=np.int64)
+        host = []
+        for name in names:
+            dt = np.dtype(ref.dtype_of(name))
+            host.append(np.ascontiguousarray(np.concatenate([np.asarray(d[name], dtype=dt).reshape(-1)
+                                                             for d in per])))
+        sh.upload_flat(counts, [h.ctypes.data for h in host])
+        Scenario([sh], distributed_drive(sh), ref, P, kw["fields"]).run(steps=2, sigma=0.8)
+    finally:
+        ref.close()
+        sh.close()
+        dist.destroy_process_group()
