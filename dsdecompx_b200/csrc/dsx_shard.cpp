@@ -135,6 +135,7 @@ struct dsx_shard {
 
     std::map<int, std::unique_ptr<DeviceBuffer>> sendbuf, recvbuf;
     long long launches = 0;   // kernels of this library launched for this shard
+    long long capacity = 0;   // owned particles the local grid can hold
 
     ~dsx_shard() {
         for (void* p : assembled) cudaFree(p);
@@ -262,11 +263,33 @@ struct dsx_shard {
     // After a local migrate (res: P x 6): the particles placed into other
     // shards' subdomains go there; this shard's subdomains are assembled.
     void redistribute(const std::vector<long long>& res, cudaStream_t s, long long* results) {
-        std::vector<long long> pairs(static_cast<std::size_t>(P) * P);
+        // one all-reduce carries the (destination, source) counts, every
+        // subdomain's retained particles and every shard's storage, so that
+        // all shards see any shard's shortfall before data moves and fail
+        // together (the reference agrees on errors the same way,
+        // src/runtime.cpp:214-230)
+        const std::size_t PP = static_cast<std::size_t>(P) * P;
+        std::vector<long long> pairs(PP + static_cast<std::size_t>(P) + static_cast<std::size_t>(nshards), 0);
         check(dsx_grid_migration_pairs(grid, pairs.data(), s));
         ++launches;
+        for (int t : mine) pairs[PP + t] = res[static_cast<std::size_t>(6 * t + 2)];
+        pairs[PP + P + shard] = capacity;
         allreduce(pairs);
         const auto M = [&](int t, int q) { return pairs[static_cast<std::size_t>(t) * P + q]; };
+        {
+            std::vector<long long> need(static_cast<std::size_t>(nshards), 0);
+            for (int t = 0; t < P; ++t) {
+                long long n = pairs[PP + t];
+                for (int q = 0; q < P; ++q) n += M(t, q);
+                need[static_cast<std::size_t>(owners[t])] += n;
+            }
+            for (int r = 0; r < nshards; ++r)
+                if (need[r] > pairs[PP + P + r]) {
+                    planned = false;
+                    fail(DSX_E_LENGTH, "particle storage of shard " + std::to_string(r) +
+                                           " is smaller than its subdomains' particles after migration");
+                }
+        }
         std::vector<long long> local_n(static_cast<std::size_t>(P)), obase(static_cast<std::size_t>(P) + 1, 0);
         for (int t = 0; t < P; ++t) {
             local_n[t] = res[static_cast<std::size_t>(6 * t + 5)];
@@ -663,6 +686,7 @@ int dsx_shard_create(const dsx_grid_desc* desc, const dsx_field_desc* fields, in
         sh->nshards = nshards;
         sh->tr = *transport;
         sh->dynamic = desc->policy == DSX_DYNAMIC;
+        sh->capacity = particles;
         if (nshards > sh->P) fail(DSX_E_INVALID, "more shards than subdomains");
         int coords[3];
         double local[6];

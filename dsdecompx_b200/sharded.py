@@ -494,7 +494,25 @@ class ShardedGrid:
         subdomain to that shard and assembles this shard's subdomains."""
         E, P, me, owners = self.E, self.P, self.shard, self.owners
         M = E.migration_pairs()
-        Mg = (yield AllReduce(M.reshape(-1).astype(np.int64))).reshape(P, P)
+        # one all-reduce carries the (destination, source) counts, every
+        # subdomain's retained particles and every shard's storage, so that
+        # all shards see any shard's shortfall before data moves and fail
+        # together (the reference agrees on errors the same way,
+        # src/runtime.cpp:214-230)
+        retained_mine = np.zeros(P, dtype=np.int64)
+        retained_mine[self.mine] = res[self.mine, 2]
+        capacity = np.zeros(self.nshards, dtype=np.int64)
+        capacity[me] = E.capacity
+        red = yield AllReduce(np.concatenate([M.reshape(-1).astype(np.int64), retained_mine, capacity]))
+        Mg = red[:P * P].reshape(P, P)
+        need = np.bincount(owners, weights=red[P * P:P * P + P] + Mg.sum(axis=1),
+                           minlength=self.nshards).astype(np.int64)
+        short = np.flatnonzero(need > red[P * P + P:])
+        if len(short):
+            self.plan = None
+            raise MemoryError(f"dsDecompX: particle storage of shard(s) {short.tolist()} is smaller "
+                              f"than their subdomains' particles after migration "
+                              f"({need[short].tolist()} > {red[P * P + P:][short].tolist()})")
         local_n = res[:, 5].astype(np.int64)
         obase = np.concatenate([[0], np.cumsum(local_n)])
         allb = E.elem_bytes_all
@@ -679,6 +697,7 @@ class DeviceEngine:
         self.asm_cap = 0
         self.asm: List = []
         self._last_migration = None
+        self.capacity = int(particles)   # owned particles this shard can hold
         self.launches = 0   # kernels of this library launched through this engine
 
     def close(self):

@@ -387,6 +387,51 @@ void run(const Case& cs) {
     std::printf("%s: %s\n", cs.name, failures ? "FAILED" : "ok");
 }
 
+dsx_grid_desc desc(int P, int d0, int d1, int d2, int policy, double L);
+
+// Shard 1 can hold 10 particles; migration would give it about half of
+// them: both shards' migrate calls fail with DSX_E_LENGTH at the same
+// collective, before any particle moves (neither waits in an exchange).
+void shortfall() {
+    const dsx_grid_desc d = desc(8, 2, 2, 2, DSX_MANUAL, 10.0);
+    const long long N = 4000;
+    Hub hub(2);
+    std::vector<Ctx> ctx(2);
+    std::vector<dsx_shard*> shards(2, nullptr);
+    for (int r = 0; r < 2; ++r) {
+        ctx[r] = {&hub, r};
+        dsx_transport tr{&ctx[r], allreduce_i64, allreduce_f64, exchange};
+        must(dsx_shard_create(&d, nullptr, 0, r == 0 ? N : 10, 0, r, 2, nullptr, &tr, &shards[r]), "create");
+    }
+    std::vector<int> owners(8);
+    must(dsx_shard_owners(shards[0], owners.data()), "owners");
+    int first = 0;
+    while (owners[first] != 0) ++first;
+    std::vector<double> x(N), y(N), z(N);
+    std::vector<int> id(N);
+    for (long long i = 0; i < N; ++i) {
+        x[i] = 10.0 * unit(7 * i);
+        y[i] = 10.0 * unit(7 * i + 1);
+        z[i] = 10.0 * unit(7 * i + 2);
+        id[i] = static_cast<int>(i);
+    }
+    std::vector<const void*> ptrs(13, nullptr);
+    ptrs[0] = x.data();
+    ptrs[1] = y.data();
+    ptrs[2] = z.data();
+    ptrs[12] = id.data();
+    std::vector<long long> counts(8, 0);
+    counts[first] = N;   // every particle in one subdomain of shard 0
+    must(dsx_shard_upload(shards[0], counts.data(), ptrs.data(), nullptr), "upload");
+    counts[first] = 0;
+    must(dsx_shard_upload(shards[1], counts.data(), ptrs.data(), nullptr), "upload");
+    std::vector<int> status(2, DSX_OK);
+    on_shards(2, [&](int r) { status[r] = dsx_shard_migrate(shards[r], nullptr, nullptr); });
+    expect(status[0] == DSX_E_LENGTH && status[1] == DSX_E_LENGTH, "both shards refuse a shortfall", 0);
+    for (dsx_shard* s : shards) dsx_shard_destroy(s);
+    std::printf("storage shortfall: %s\n", (status[0] == DSX_E_LENGTH && status[1] == DSX_E_LENGTH) ? "ok" : "FAILED");
+}
+
 dsx_grid_desc desc(int P, int d0, int d1, int d2, int policy, double L) {
     dsx_grid_desc d{};
     d.nranks = P;
@@ -413,6 +458,7 @@ dsx_grid_desc desc(int P, int d0, int d1, int d2, int policy, double L) {
 int main() {
     run({"manual 4x4x2 over 4 shards", desc(32, 4, 4, 2, DSX_MANUAL, 16.0), 4, 60000});
     run({"dynamic 2x2x2 over 2 shards", desc(8, 0, 0, 0, DSX_DYNAMIC, 12.0), 2, 30000});
+    shortfall();
     if (failures) return 1;
     std::printf("shard_sanity: ok\n");
     return 0;

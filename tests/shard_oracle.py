@@ -43,6 +43,7 @@ class OracleEngine:
                            for n in self.names]
         self.elem_bytes_all = list(self.elem_bytes)
         self.asm = [np.zeros(0, np.uint8) for _ in self.names]
+        self.capacity = 1 << 40   # owned particles this shard can hold (the oracle grows)
         self.asm_cap = 0
         self._before = None
         self._last_res = None

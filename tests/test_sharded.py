@@ -266,3 +266,96 @@ def test_row_and_segment_merging():
             return sorted((int(x["dst_rank"]), int(x["dst_index"]) + i, int(x["source"]),
                            int(x["src_index"]) + i) for x in s for i in range(int(x["count"])))
         assert expand(seg) == expand(merged)
+
+
+# ------------------------------------------------------- failures
+
+def drive_until_failure(gens):
+    """Serves the shards' requests (all-reduces only) until they stop;
+    returns what each raised (None: it finished)."""
+    replies = [None] * len(gens)
+    outcome = [None] * len(gens)
+    live = list(range(len(gens)))
+    while live:
+        reqs = {}
+        for i in list(live):
+            try:
+                reqs[i] = gens[i].send(replies[i])
+            except StopIteration:
+                live.remove(i)
+            except Exception as exc:   # noqa: BLE001 - recorded for the assertions
+                outcome[i] = exc
+                live.remove(i)
+        if not reqs:
+            break
+        assert len(reqs) == len(gens), "a shard stopped while another waits in a collective"
+        assert all(isinstance(r, shd.AllReduce) for r in reqs.values())
+        total = sum(r.values for r in reqs.values())
+        replies = [total.copy() for _ in gens]
+    return outcome
+
+
+@pytest.mark.parametrize("case", ["2x2x2-R2", "dynamic-R4"])
+def test_shards_agree_on_a_storage_shortfall(case):
+    """One shard's storage is too small for its subdomains after migration:
+    every shard raises the same error at the same collective (the reference's
+    error agreement), before any particle moves between shards."""
+    kw = CASES[case]
+    ref = make_ref(kw, [])
+    shards = make_shards(kw, [], 2)
+    per = initial(ref, kw["nranks"], kw["upper"], kw["N"], 19, [])
+    for sh in shards:
+        sh.upload({t: per[t] for t in sh.mine})
+    shards[1].E.capacity = 10
+    outcome = drive_until_failure([sh.migrate_steps() for sh in shards])
+    assert all(isinstance(e, MemoryError) for e in outcome), outcome
+    assert all("shard(s) [1]" in str(e) for e in outcome)
+
+
+def gloo_failure_rank(rank, world, port, out_dir, mode):
+    import torch
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world,
+                                         timeout=datetime.timedelta(seconds=20))
+    kw = CASES["2x2x2-R2"]
+    ref = make_ref(kw, [])
+    e = OracleEngine(kw["nranks"], kw["dims"], kw["policy"], (0, 0, 0), kw["upper"],
+                     (True, True, True), kw["halo_width"], True, None, [])
+    sh = shd.ShardedGrid(e, rank, world, run=lambda g: shd.run_distributed(g, device="cpu"))
+    per = initial(ref, kw["nranks"], kw["upper"], kw["N"], 29, [])
+    sh.upload({t: per[t] for t in sh.mine})
+    if mode == "storage" and rank == 0:
+        e.capacity = 10
+    result = "finished"
+    try:
+        sh.migrate()
+        sh.exchange_halo(rebuild=True)
+        if mode == "peer_leaves":
+            if rank == 1:
+                os._exit(0)   # leaves between steps, none of its work in flight
+            sh.migrate()      # the next collective must fail, not wait for ever
+    except MemoryError as exc:
+        result = "MemoryError: " + str(exc)
+    except RuntimeError as exc:
+        result = "RuntimeError: " + str(exc)
+    with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as f:
+        f.write(result)
+    if mode == "storage":
+        torch.distributed.destroy_process_group()
+
+
+def test_two_gloo_ranks_agree_on_a_storage_shortfall(tmp_path):
+    mp.start_processes(gloo_failure_rank, args=(2, free_port(), str(tmp_path), "storage"), nprocs=2,
+                       start_method="spawn")
+    for r in range(2):
+        got = open(tmp_path / f"rank{r}.txt").read()
+        assert got.startswith("MemoryError") and "shard(s) [0]" in got, (r, got)
+
+
+def test_a_rank_that_leaves_is_detected_by_the_next_collective(tmp_path):
+    mp.start_processes(gloo_failure_rank, args=(2, free_port(), str(tmp_path), "peer_leaves"),
+                       nprocs=2, start_method="spawn")
+    got = open(tmp_path / "rank0.txt").read()
+    assert got.startswith("RuntimeError"), got
