@@ -589,24 +589,21 @@ class ShardedGrid:
         else:
             prev, grew = self.plan, False
         arrays = XYZ if (positions_only and not build) else E.all_arrays
-        old_ids = E.assembled_ids(prev.total) if (build and prev is not None) else None
         yield from self._ship_lists(arrays)
         plan = self.plan
         out = {}
         for t in self.mine:
             # layout_changed (src/runtime.cpp:966-980): a requested rebuild,
-            # another ghost count (none since a migrate) or other ghost ids
+            # or another ghost count than before (none since a migrate); a
+            # build is only ever forced by a missing plan, so the ghost ids of
+            # an unrequested rebuild never need comparing
             g = int(plan.g[t])
             if rebuild:
                 changed = 1
             elif prev is None:
                 changed = int(g != 0)
-            elif int(prev.g[t]) != g:
-                changed = 1
-            elif not build:
-                changed = 0
             else:
-                changed = int(not E.same_ids(old_ids, int(prev.gbase[t]), int(plan.gbase[t]), g))
+                changed = int(int(prev.g[t]) != g)
             out[int(t)] = (g, changed, int(grew), int(not build))
         return out
 
@@ -827,18 +824,7 @@ class DeviceEngine:
         self.launches += 2   # the copies and the new layout
         self.grid.assemble(counts, sources, segments)
 
-    # ---- ids and host reads
-    def assembled_ids(self, n: int):
-        if not n:
-            return None
-        return self.asm[12][:n * 4].view(self.torch.int32).clone()
-
-    def same_ids(self, old, old_lo: int, new_lo: int, n: int) -> bool:
-        if n == 0:
-            return True
-        new = self.asm[12][new_lo * 4:(new_lo + n) * 4].view(self.torch.int32)
-        return bool(self.torch.equal(old[old_lo:old_lo + n], new))
-
+    # ---- host reads
     def read_owned(self, t: int, name: str) -> np.ndarray:
         return self.grid.read(t, name, 0, self.grid.counts(t)[0])
 

@@ -231,15 +231,6 @@ class OracleEngine:
         for t in range(self.P):
             self.g.set_owned(t, data[t])
 
-    def assembled_ids(self, n):
-        return self.asm[12][:n * 4].view(np.int32).copy() if n else None
-
-    def same_ids(self, old, old_lo, new_lo, n):
-        if n == 0:
-            return True
-        new = self.asm[12][new_lo * 4:(new_lo + n) * 4].view(np.int32)
-        return bool(np.array_equal(old[old_lo:old_lo + n], new))
-
     def read_owned(self, t, name):
         return self.g.read(t, name, 0, self.g.counts(t)[0])
 
