@@ -379,6 +379,31 @@ void run(const Case& cs) {
         on_shards(R, [&](int r) { must(dsx_shard_exchange_halo(shards[r], 0, 0, streams[r], nullptr), "shard refresh"); });
         compare("ghosts after the refresh", true);
     }
+    // a positions-only refresh (the ghosts' positions follow, the rest stays
+    // as both grids left it), then Decomp::rebalance with work per subdomain
+    displace(500, 0.05);
+    must(dsx_grid_exchange_halo(ref, 0, 1, nullptr, nullptr), "positions refresh");
+    on_shards(R, [&](int r) { must(dsx_shard_exchange_halo(shards[r], 0, 1, streams[r], nullptr), "shard positions"); });
+    compare("ghosts after the positions refresh", true);
+    {
+        std::vector<double> work(P);
+        for (int t = 0; t < P; ++t) work[t] = 100.0 + 37.0 * ((t * 7) % P);
+        std::vector<long long> fr(3 * P);
+        std::vector<double> imb(P);
+        must(dsx_grid_rebalance(ref, work.data(), 1, nullptr, fr.data(), imb.data()), "rebalance");
+        std::vector<std::vector<long long>> fs(R, std::vector<long long>(3 * P));
+        std::vector<double> is(R);
+        on_shards(R, [&](int r) {
+            must(dsx_shard_rebalance(shards[r], work.data(), 1, streams[r], fs[r].data(), &is[r]), "shard rebalance");
+        });
+        for (int t = 0; t < P; ++t)
+            for (int k = 0; k < 3; ++k) expect(fs[owners[t]][3 * t + k] == fr[3 * t + k], "rebalance results", t);
+        for (int r = 0; r < R; ++r) expect(is[r] == imb[0], "rebalance imbalance", r);
+        compare("owned after the rebalance", false);
+        must(dsx_grid_exchange_halo(ref, 1, 0, nullptr, nullptr), "halo");
+        on_shards(R, [&](int r) { must(dsx_shard_exchange_halo(shards[r], 1, 0, streams[r], nullptr), "shard halo"); });
+        compare("ghosts after the rebalance", true);
+    }
     for (int r = 0; r < R; ++r) {
         dsx_shard_destroy(shards[r]);
         cudaStreamDestroy(streams[r]);
