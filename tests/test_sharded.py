@@ -359,3 +359,29 @@ def test_a_rank_that_leaves_is_detected_by_the_next_collective(tmp_path):
                        nprocs=2, start_method="spawn")
     got = open(tmp_path / "rank0.txt").read()
     assert got.startswith("RuntimeError"), got
+
+
+@pytest.mark.parametrize("case,R,start", [
+    ("2x2x2-R2", 2, "one-subdomain"),
+    ("wide-halo-R3", 3, "placed"),
+])
+def test_lockstep_edge_cases(case, R, start):
+    """Every particle starting in subdomain 0 (the other shards start
+    empty, the first migrate sends almost everything across shards); a halo
+    wider than half a cell (every particle has many images)."""
+    kw = dict(CASES.get(case, {}))
+    if case == "wide-halo-R3":
+        kw = dict(nranks=27, dims=(3, 3, 3), policy="manual", upper=(6.0, 6.0, 6.0),
+                  halo_width=1.1, N=1500)
+    fields = FIELDS3[:2]
+    ref = make_ref(kw, fields)
+    shards = make_shards(kw, fields, R)
+    per = initial(ref, kw["nranks"], kw["upper"], kw["N"], 71, fields)
+    if start == "one-subdomain":
+        everything = {k: np.concatenate([p[k] for p in per]) for k in per[0]}
+        per = [everything] + [{k: v[:0] for k, v in everything.items()} for _ in per[1:]]
+    for t in range(kw["nranks"]):
+        ref.set_owned(t, per[t])
+    for sh in shards:
+        sh.upload({t: per[t] for t in sh.mine})
+    Scenario(shards, lockstep_drive(shards), ref, kw["nranks"], fields).run(steps=2, sigma=0.5)
