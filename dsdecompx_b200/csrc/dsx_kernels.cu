@@ -70,6 +70,18 @@ struct Cell {
     double lo[3], hi[3];
 };
 
+__device__ __forceinline__ bool inside_cell(const Cell& cell, double px, double py, double pz) {
+    return cell.lo[0] <= px && px < cell.hi[0] && cell.lo[1] <= py && py < cell.hi[1] &&
+           cell.lo[2] <= pz && pz < cell.hi[2];
+}
+
+// With every periodic axis starting at 0, a coordinate inside its own cell
+// needs no wrap arithmetic: both Host wraps return it (a -0 as +0).
+__device__ __forceinline__ bool simple_wrap(const Grid& G) {
+    return (!G.periodic[0] || G.lower[0] == 0.0) && (!G.periodic[1] || G.lower[1] == 0.0) &&
+           (!G.periodic[2] || G.lower[2] == 0.0);
+}
+
 __device__ __forceinline__ Cell cell_of(const Grid& G, int s) {
     Cell cell;
     const int packed = G.coord[s];
@@ -261,10 +273,17 @@ __global__ void __launch_bounds__(NT, 4) k_mig_classify(Grid G, const double* __
             pz[j] = ro(z + i);
         }
     }
+    const bool simple = simple_wrap(G);
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = begin + threadIdx.x + j * NT;
-        if (i >= end) continue;
+        const bool valid = i < end;
+        // a group that stays inside its cell needs no wrap arithmetic
+        if (__all_sync(0xffffffffu, !valid || (simple && inside_cell(cell, px[j], py[j], pz[j])))) {
+            stay += valid ? 1 : 0;
+            continue;
+        }
+        if (!valid) continue;
         double wx, wy, wz;
         const int d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
         if (d == s) {
@@ -354,14 +373,29 @@ __global__ void __launch_bounds__(NT, 4) k_mig_move(Grid G, Arrays A, long long 
     double wx[ITEMS], wy[ITEMS], wz[ITEMS];
     int nstay = 0, nemig = 0;
     const Cell cell = cell_of(G, s);
+    const bool simple = simple_wrap(G);
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = wbegin + j * 32 + lane;
+        const bool valid = i < end;
         dest[j] = -1;
-        if (i < end) {
+        double px = 0.0, py = 0.0, pz = 0.0;
+        if (valid) {
             const long long src = src_off + i;
-            dest[j] = destination_near(G, cell, ro(A.d[0] + src), ro(A.d[1] + src), ro(A.d[2] + src),
-                                       wx[j], wy[j], wz[j]);
+            px = ro(A.d[0] + src);
+            py = ro(A.d[1] + src);
+            pz = ro(A.d[2] + src);
+        }
+        if (__all_sync(0xffffffffu, !valid || (simple && inside_cell(cell, px, py, pz)))) {
+            // the whole group stays: both Host wraps return the coordinate (a -0 as +0)
+            if (valid) {
+                dest[j] = s;
+                wx[j] = G.periodic[0] && px == 0.0 ? 0.0 : px;
+                wy[j] = G.periodic[1] && py == 0.0 ? 0.0 : py;
+                wz[j] = G.periodic[2] && pz == 0.0 ? 0.0 : pz;
+            }
+        } else if (valid) {
+            dest[j] = destination_near(G, cell, px, py, pz, wx[j], wy[j], wz[j]);
         }
         nstay += __popc(__ballot_sync(0xffffffffu, dest[j] == s));
         nemig += __popc(__ballot_sync(0xffffffffu, dest[j] >= 0 && dest[j] != s));
