@@ -498,13 +498,18 @@ struct dsx_shard {
         if (n <= assembled_cap && !assembled.empty()) return false;
         const long long cap = std::max<long long>(n + n / 4, 1024);
         std::vector<void*> next(bytes.size(), nullptr);
-        for (std::size_t a = 0; a < bytes.size(); ++a) {
-            cuda(cudaMalloc(&next[a], static_cast<std::size_t>(cap * bytes[a])), "cudaMalloc ghost region");
-            if (assembled_cap)
-                cuda(cudaMemcpyAsync(next[a], assembled[a], static_cast<std::size_t>(assembled_cap * bytes[a]),
-                                     cudaMemcpyDeviceToDevice, s), "copy ghost region");
+        cudaError_t e = cudaSuccess;
+        for (std::size_t a = 0; a < bytes.size() && e == cudaSuccess; ++a) {
+            e = cudaMalloc(&next[a], static_cast<std::size_t>(cap * bytes[a]));
+            if (e == cudaSuccess && assembled_cap)
+                e = cudaMemcpyAsync(next[a], assembled[a], static_cast<std::size_t>(assembled_cap * bytes[a]),
+                                    cudaMemcpyDeviceToDevice, s);
         }
-        cuda(cudaStreamSynchronize(s), "grow ghost region");
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            for (void* p : next) cudaFree(p);   // the old region stays in use
+            cuda(e, "grow ghost region");
+        }
         for (void* p : assembled) cudaFree(p);
         assembled = next;
         assembled_cap = cap;
