@@ -572,18 +572,20 @@ def run_sharded(args, rank, world, device):
     N = int(counts.sum())
     S = w.record_bytes()
     names = dsx.ARRAYS + [f[0] for f in w.fields]
+    # pinned host copies sized for the shard's storage: after migration a
+    # rank may hold more particles than it started with
+    capacity = int(1.5 * N) + 65536
     pinned = []
     for name in names:
-        if name in grouped:
-            t = torch.from_numpy(np.ascontiguousarray(grouped[name])).pin_memory()
-        else:
-            t = torch.zeros(N, dtype=torch.float64).pin_memory()
+        src = np.ascontiguousarray(grouped[name]) if name in grouped else np.zeros(N)
+        t = torch.zeros((capacity,) + src.shape[1:], dtype=torch.from_numpy(src[:0]).dtype).pin_memory()
+        t[:N].copy_(torch.from_numpy(src))
         pinned.append(t)
     del grouped
     ptrs = [t.data_ptr() for t in pinned]
     native = args.sharded_impl == "native"
     grid_args = (P, dims if w.policy == "manual" else (0, 0, 0), w.policy, w.lower, upper)
-    grid_kw = dict(halo_width=w.halo, fields=w.fields, particles=int(1.5 * N) + 65536,
+    grid_kw = dict(halo_width=w.halo, fields=w.fields, particles=capacity,
                    ghost_capacity=int(0.9 * N))
     if native:
         sh = shd.NativeShardedGrid(*grid_args, **grid_kw, shard=rank, nshards=world, owners=owners,
