@@ -58,6 +58,9 @@ def parse():
                          "refreshes, split-phase overlap, rebalance, box changes)")
     ap.add_argument("--sharded", action="store_true",
                     help="the sharded grid's step (the multi-GPU path) also at one GPU")
+    ap.add_argument("--exchange-volume", type=int, default=0, metavar="R",
+                    help="bytes the sharded protocol sends per step with R shards (R = a^3 blocks "
+                         "of the workload), the shards run in lockstep on one GPU")
     ap.add_argument("--sharded-impl", default="native", choices=["native", "python"],
                     help="the library's sharded protocol (dsx_shard_*) or the Python one")
     return ap.parse_args()
@@ -509,6 +512,74 @@ def measure_calls(grid, w, N, S, stream, device, reps=10):
     return out
 
 
+def exchange_volume(args):
+    """Bytes each shard sends per step (migrants, ghost lists, returned
+    forces) with R shards, each one block of the workload: R instances of
+    the Python protocol run in lockstep on one GPU and count what they send.
+    With the measured peer bandwidth this is the NVLink part of a step."""
+    import ctypes as Cc
+
+    import numpy as np
+    import torch
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import sharded as shd
+    from dsdecompx_b200 import workloads as W
+    R = args.exchange_volume
+    w = W.WORKLOADS[args.workload]
+    per = args.particles or w.particles
+    fa = shard_factors(R)
+    bdims, _ = dsx.plan_topology(w.nranks, 0, w.dims, w.policy, w.lower, w.upper)
+    dims = tuple(d * k for d, k in zip(bdims, fa))
+    P = int(np.prod(dims))
+    upper = tuple(u * k for u, k in zip(w.upper, fa))
+    coords = np.array([shd.subdomain_coords(t, dims) for t in range(P)])
+    owners = ((coords[:, 0] // bdims[0]) * fa[1] + coords[:, 1] // bdims[1]) * fa[2] + coords[:, 2] // bdims[2]
+    shards = []
+    for r in range(R):
+        b = (r // (fa[1] * fa[2]), (r // fa[2]) % fa[1], r % fa[2])
+        d = W.generate(w, seed=args.seed + 7919 * r, particles=per)
+        for a, name in enumerate("xyz"):
+            d[name] = d[name] + b[a] * w.upper[a]
+        d["global_id"] = (d["global_id"] + r * per).astype(np.int32)
+        if "id64" in d:
+            d["id64"] = d["id64"] + r * per
+        cell = []
+        for a, name in enumerate("xyz"):
+            rel = np.floor((d[name] - w.lower[a]) / (upper[a] - w.lower[a]) * dims[a]).astype(np.int64)
+            cell.append(np.clip(rel, b[a] * bdims[a], (b[a] + 1) * bdims[a] - 1))
+        own = (cell[0] * dims[1] + cell[1]) * dims[2] + cell[2]
+        engine = shd.DeviceEngine(P, dims if w.policy == "manual" else (0, 0, 0), w.policy, w.lower, upper,
+                                  halo_width=w.halo, fields=w.fields, particles=int(1.5 * per) + 65536,
+                                  ghost_capacity=per)
+        sh = shd.ShardedGrid(engine, r, R, owners=owners)
+        sh.upload({int(t): {k: v[own == t] for k, v in d.items()} for t in np.flatnonzero(owners == r)})
+        shards.append(sh)
+    wl = W.harness()
+    steps = max(args.steps, 1)
+    for step in range(args.warmup + steps):
+        if step == args.warmup:
+            for sh in shards:
+                sh.sent_bytes = {k: 0 for k in sh.sent_bytes}
+        for r, sh in enumerate(shards):
+            v = sh.E.grid.view()
+            wl.dsxw_drift(Cc.byref(v), args.seed + r, step, w.drift, torch.cuda.current_stream().cuda_stream)
+        shd.run_lockstep([sh.step_steps() for sh in shards])
+    torch.cuda.synchronize()
+    sent = [{k: v / steps for k, v in sh.sent_bytes.items()} for sh in shards]
+    most = max(sum(s.values()) for s in sent)
+    link = 770.0   # measured NVLink peer copy, GB/s per direction
+    return {"metric": "bytes sent per shard per step", "value": int(most), "unit": "B",
+            "higher_is_better": False, "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "emulated_shards": R, "data": "synthetic",
+            "config": {"workload": w.name, "particles_per_shard": per, "blocks": list(fa),
+                       "subdomains": P, "grid": list(dims)},
+            "per_kind_max_bytes": {k: int(max(s[k] for s in sent)) for k in sent[0]},
+            "per_kind_mean_bytes": {k: int(np.mean([s[k] for s in sent])) for k in sent[0]},
+            "nvlink_us_per_step_at_770_gbs": round(most / (link * 1e9) * 1e6, 1),
+            "assembled_ghosts_per_shard": [int(sh.plan.total) for sh in shards]}
+
+
 def shard_factors(world):
     """(a, b, c), a * b * c = world: the block counts along x, y, z (prime
     factors go to the axis with the fewest blocks so far)."""
@@ -892,6 +963,9 @@ def main():
         return
 
     import torch
+    if args.exchange_volume:
+        print(json.dumps(exchange_volume(args)))
+        return
     sharded = world > 1 or args.sharded
     if sharded:
         import datetime

@@ -347,7 +347,8 @@ class ShardedGrid:
         self.nn, self.sender_of = halo_tables(engine.topology)
         self.plan: Optional[GhostPlan] = None
         self.run = run or (lambda gen: run_distributed(gen, device=engine.device))
-        self._prev_ids = None
+        # bytes this shard sent to other shards, per kind of message
+        self.sent_bytes = {"migrants": 0, "ghost lists": 0, "returned values": 0}
 
     # ---- particles
     def upload(self, per_subdomain: Dict[int, Dict[str, np.ndarray]]):
@@ -527,6 +528,7 @@ class ShardedGrid:
             buf = E.new_buffer(packed_bytes(n, allb))
             E.copy(("buffer", buf, n, E.all_arrays), ("owned",), rows, E.all_arrays)
             sends[p] = buf
+            self.sent_bytes["migrants"] += packed_bytes(n, allb)
         # what each peer sends: its sources' groups for my subdomains
         mine = self.mine
         sub = Mg[mine]                                               # [my subdomains, sources]
@@ -619,6 +621,7 @@ class ShardedGrid:
             buf = E.new_buffer(packed_bytes(n, b))
             E.copy(("buffer", buf, n, arrays), ("ghost",), _rows(rows), arrays)
             sends[p] = buf
+            self.sent_bytes["ghost lists"] += packed_bytes(n, b)
         recv_bytes = {p: packed_bytes(n, b) for p, n in plan.recv_n.items()}
         recv = yield Exchange(sends, recv_bytes)
         if len(plan.local):
@@ -640,6 +643,7 @@ class ShardedGrid:
             buf = E.new_buffer(packed_bytes(n, b))
             E.copy(("buffer", buf, n, arrays), ("assembled",), _swap(rows), arrays)
             sends[p] = buf
+            self.sent_bytes["returned values"] += packed_bytes(n, b)
         recv_bytes = {p: packed_bytes(n, b) for p, n in plan.send_n.items()}
         recv = yield Exchange(sends, recv_bytes)
         for p, rows in plan.send.items():

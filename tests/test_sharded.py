@@ -182,6 +182,8 @@ def test_lockstep_shards_match_one_grid(case, R):
     Scenario(shards, lockstep_drive(shards), ref, kw["nranks"], fields).run(steps=3, sigma=0.8)
     if kw["policy"] == "dynamic":
         assert not np.allclose(ref.cuts()[0], np.linspace(0, 12, 3))
+    sent = {k: sum(sh.sent_bytes[k] for sh in shards) for k in shards[0].sent_bytes}
+    assert sent["migrants"] > 0 and sent["ghost lists"] > 0 and sent["returned values"] > 0, sent
 
 
 def test_lockstep_rebalance_with_work():
