@@ -11,6 +11,10 @@ importing :func:`lib` raises.
   ``exchange_halo``, ``reverse_halo``, ``reverse_exchange``,
   ``forward_exchange``, ``rebalance``, ``halo_backward`` and the batched,
   graph-captured ``step``.
+* :mod:`dsdecompx_b200.sharded` -- the P subdomains split over several
+  processes (one GPU each): ``NativeShardedGrid`` (the library's
+  ``dsx_shard_*`` with a torch.distributed transport) and ``ShardedGrid``
+  (the same protocol in Python, with engines that can be swapped).
 """
 from __future__ import annotations
 
