@@ -150,8 +150,9 @@ std::uint64_t mix(std::uint64_t z) {
 
 double unit(std::uint64_t k) { return static_cast<double>(mix(k) >> 11) * (1.0 / 9007199254740992.0); }
 
-constexpr int kArrays = 15;   // 13 core + "tag" (int64) + "vec" (float32 x 3)
-const int kBytes[kArrays] = {8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 4, 4, 8, 12};
+// 13 core arrays + "tag" (int64), "vec" (float32 x 3), "u" (uint32), "wide" (float64 x 7)
+constexpr int kArrays = 17;
+const int kBytes[kArrays] = {8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 4, 4, 8, 12, 4, 56};
 
 struct Case {
     const char* name;
@@ -207,9 +208,10 @@ void write_shard(dsx_shard* sh, int P, int t, bool ghosts, int a, const void* da
 
 void run(const Case& cs) {
     const int P = cs.desc.nranks, R = cs.R;
-    const dsx_field_desc fields[2] = {{"tag", DSX_INT64, 1}, {"vec", DSX_FLOAT32, 3}};
+    const dsx_field_desc fields[4] = {{"tag", DSX_INT64, 1}, {"vec", DSX_FLOAT32, 3},
+                                      {"u", DSX_UINT32, 1}, {"wide", DSX_FLOAT64, 7}};
     dsx_grid* ref = nullptr;
-    must(dsx_grid_create(&cs.desc, fields, 2, cs.N, 0, &ref), "create grid");
+    must(dsx_grid_create(&cs.desc, fields, 4, cs.N, 0, &ref), "create grid");
     // every particle starts in subdomain 0 of a Manual grid with the same
     // process grid, whose migrate places them (so that the grids under test
     // start with the same cuts and no migrate behind them)
@@ -221,7 +223,7 @@ void run(const Case& cs) {
         place.policy = DSX_MANUAL;
     }
     dsx_grid* placer = nullptr;
-    must(dsx_grid_create(&place, fields, 2, cs.N, 0, &placer), "create placer");
+    must(dsx_grid_create(&place, fields, 4, cs.N, 0, &placer), "create placer");
     {
         std::vector<std::vector<unsigned char>> host(kArrays);
         for (int a = 0; a < kArrays; ++a) host[a].resize(static_cast<std::size_t>(cs.N * kBytes[a]));
@@ -241,6 +243,12 @@ void run(const Case& cs) {
             std::memcpy(&host[12][i * 4], &id, 4);
             std::memcpy(&host[13][i * 8], &tag, 8);
             std::memcpy(&host[14][i * 12], vec, 12);
+            const unsigned u = static_cast<unsigned>(i) * 2654435761u;
+            std::memcpy(&host[15][i * 4], &u, 4);
+            for (int k = 0; k < 7; ++k) {
+                const double wv = std::sin(0.01 * static_cast<double>(i) + k);
+                std::memcpy(&host[16][i * 56 + 8 * k], &wv, 8);
+            }
         }
         std::vector<long long> counts(P, 0);
         counts[0] = cs.N;
@@ -266,7 +274,7 @@ void run(const Case& cs) {
     for (int r = 0; r < R; ++r) {
         ctx[r] = {&hub, r};
         dsx_transport tr{&ctx[r], allreduce_i64, allreduce_f64, exchange};
-        must(dsx_shard_create(&cs.desc, fields, 2, cs.N, 0, r, R, nullptr, &tr, &shards[r]), "create shard");
+        must(dsx_shard_create(&cs.desc, fields, 4, cs.N, 0, r, R, nullptr, &tr, &shards[r]), "create shard");
         cuda(cudaStreamCreate(&streams[r]), "stream");
     }
     std::vector<int> owners(P);
@@ -359,19 +367,31 @@ void run(const Case& cs) {
                 }
                 if (g[t]) must(dsx_grid_write(ref, t, 13, o[t], g[t], tag.data(), nullptr), "write");
                 write_shard(shards[owners[t]], P, t, true, 13, tag.data());
+                std::vector<unsigned> u(g[t]);
+                std::vector<double> wide(7 * g[t]);
+                for (long long i = 0; i < g[t]; ++i) {
+                    int id;
+                    std::memcpy(&id, &gh[12][i * 4], 4);
+                    u[i] = static_cast<unsigned>(31 * id + t);
+                    for (int k = 0; k < 7; ++k) wide[7 * i + k] = std::sin(0.1 * id + t + k);
+                }
+                if (g[t]) must(dsx_grid_write(ref, t, 15, o[t], g[t], u.data(), nullptr), "write");
+                write_shard(shards[owners[t]], P, t, true, 15, u.data());
+                if (g[t]) must(dsx_grid_write(ref, t, 16, o[t], g[t], wide.data(), nullptr), "write");
+                write_shard(shards[owners[t]], P, t, true, 16, wide.data());
             }
         }
         must(dsx_grid_reverse_halo(ref, nullptr), "reverse");
         on_shards(R, [&](int r) { must(dsx_shard_reverse_halo(shards[r], streams[r]), "shard reverse"); });
-        const int ids[1] = {0}, ops[1] = {step % 4};
-        must(dsx_grid_reverse_exchange(ref, 1, ids, ops, nullptr), "reverse fields");
+        const int ids[3] = {0, 2, 3}, ops[3] = {step % 4, (step + 1) % 4, (step + 2) % 4};
+        must(dsx_grid_reverse_exchange(ref, 3, ids, ops, nullptr), "reverse fields");
         on_shards(R, [&](int r) {
-            must(dsx_shard_reverse_exchange(shards[r], 1, ids, ops, streams[r]), "shard reverse fields");
+            must(dsx_shard_reverse_exchange(shards[r], 3, ids, ops, streams[r]), "shard reverse fields");
         });
         compare("owned after the reverse sums", false);
-        const int both[2] = {1, 0};
-        must(dsx_grid_forward_exchange(ref, 2, both, nullptr), "forward fields");
-        on_shards(R, [&](int r) { must(dsx_shard_forward_exchange(shards[r], 2, both, streams[r]), "shard forward"); });
+        const int all[4] = {3, 2, 1, 0};
+        must(dsx_grid_forward_exchange(ref, 4, all, nullptr), "forward fields");
+        on_shards(R, [&](int r) { must(dsx_shard_forward_exchange(shards[r], 4, all, streams[r]), "shard forward"); });
         compare("ghosts after the forward exchange", true);
 
         displace(step + 100, 0.05);
