@@ -34,10 +34,13 @@ typedef struct dsx_transport {
     int (*allreduce_f64)(void* user, double* values, long long n);
     /* Sends send[k] (send_bytes[k] device bytes) to shard send_to[k] and
      * receives recv_bytes[k] bytes from shard recv_from[k] into recv[k]
-     * (device).  The send buffers are ready when `stream`'s work so far is
-     * done; the call returns once the received bytes are in place for later
-     * work on `stream`.  Peers appear once each, ascending; zero-byte
-     * messages are left out on both sides. */
+     * (device).  Both kinds of buffer are in use by the work queued on
+     * `stream` so far (the sends are being filled, the receive buffers of
+     * an earlier call may still be read): a transport whose transfers are
+     * not ordered on `stream` (MPI) synchronizes it before touching them.
+     * The call returns once the received bytes are in place for later work
+     * on `stream` and the send buffers may be refilled by it.  Peers appear
+     * once each, ascending; zero-byte messages are left out on both sides. */
     int (*exchange)(void* user, int nsend, const int* send_to, const void* const* send,
                     const long long* send_bytes, int nrecv, const int* recv_from,
                     void* const* recv, const long long* recv_bytes, void* stream);
