@@ -8,7 +8,7 @@
 //
 // usage: shard_sanity   (exits 0 and prints "shard_sanity: ok" when every
 //                        check passed)
-#include <dsx_shard.h>
+#include <dsx_shard.hpp>
 
 #include <cuda_runtime_api.h>
 
@@ -19,6 +19,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <memory>
+#include <stdexcept>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -435,21 +437,45 @@ void run(const Case& cs) {
 dsx_grid_desc desc(int P, int d0, int d1, int d2, int policy, double L);
 
 // Shard 1 can hold 10 particles; migration would give it about half of
-// them: both shards' migrate calls fail with DSX_E_LENGTH at the same
-// collective, before any particle moves (neither waits in an exchange).
+// them: both shards' migrate calls fail at the same collective, before any
+// particle moves (neither waits in an exchange), and the C++ face
+// (dsx_shard.hpp) raises std::length_error on both.
 void shortfall() {
     const dsx_grid_desc d = desc(8, 2, 2, 2, DSX_MANUAL, 10.0);
     const long long N = 4000;
     Hub hub(2);
     std::vector<Ctx> ctx(2);
-    std::vector<dsx_shard*> shards(2, nullptr);
+    std::vector<std::unique_ptr<dsx::ShardedGrid>> shards;
     for (int r = 0; r < 2; ++r) {
         ctx[r] = {&hub, r};
-        dsx_transport tr{&ctx[r], allreduce_i64, allreduce_f64, exchange};
-        must(dsx_shard_create(&d, nullptr, 0, r == 0 ? N : 10, 0, r, 2, nullptr, &tr, &shards[r]), "create");
+        Ctx* c = &ctx[r];
+        dsx::Transport tr;
+        tr.sum_i64 = [c](long long* v, long long n) { allreduce(c, c->hub->li, v, n); };
+        tr.sum_f64 = [c](double* v, long long n) { allreduce(c, c->hub->ld, v, n); };
+        tr.messages = [c](const std::vector<dsx::Message>& out, const std::vector<dsx::Message>& in,
+                          void* stream) {
+            std::vector<int> to, from;
+            std::vector<const void*> sb;
+            std::vector<void*> rb;
+            std::vector<long long> sn, rn;
+            for (const auto& m : out) {
+                to.push_back(m.peer);
+                sb.push_back(m.data);
+                sn.push_back(m.bytes);
+            }
+            for (const auto& m : in) {
+                from.push_back(m.peer);
+                rb.push_back(m.data);
+                rn.push_back(m.bytes);
+            }
+            if (exchange(c, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
+                         static_cast<int>(from.size()), from.data(), rb.data(), rn.data(), stream) != DSX_OK)
+                throw std::runtime_error("exchange");
+        };
+        shards.push_back(std::make_unique<dsx::ShardedGrid>(d, std::vector<dsx::FieldSpec>{},
+                                                            r == 0 ? N : 10, r, 2, tr));
     }
-    std::vector<int> owners(8);
-    must(dsx_shard_owners(shards[0], owners.data()), "owners");
+    const std::vector<int> owners = shards[0]->owners();
     int first = 0;
     while (owners[first] != 0) ++first;
     std::vector<double> x(N), y(N), z(N);
@@ -467,14 +493,22 @@ void shortfall() {
     ptrs[12] = id.data();
     std::vector<long long> counts(8, 0);
     counts[first] = N;   // every particle in one subdomain of shard 0
-    must(dsx_shard_upload(shards[0], counts.data(), ptrs.data(), nullptr), "upload");
+    shards[0]->upload(counts, ptrs);
     counts[first] = 0;
-    must(dsx_shard_upload(shards[1], counts.data(), ptrs.data(), nullptr), "upload");
-    std::vector<int> status(2, DSX_OK);
-    on_shards(2, [&](int r) { status[r] = dsx_shard_migrate(shards[r], nullptr, nullptr); });
-    expect(status[0] == DSX_E_LENGTH && status[1] == DSX_E_LENGTH, "both shards refuse a shortfall", 0);
-    for (dsx_shard* s : shards) dsx_shard_destroy(s);
-    std::printf("storage shortfall: %s\n", (status[0] == DSX_E_LENGTH && status[1] == DSX_E_LENGTH) ? "ok" : "FAILED");
+    shards[1]->upload(counts, ptrs);
+    std::vector<int> caught(2, 0);
+    on_shards(2, [&](int r) {
+        try {
+            shards[r]->migrate();
+        } catch (const std::length_error&) {
+            caught[r] = 1;
+        } catch (...) {
+            caught[r] = 2;
+        }
+    });
+    const bool ok = caught[0] == 1 && caught[1] == 1;
+    expect(ok, "both shards raise length_error on a shortfall", 0);
+    std::printf("storage shortfall: %s\n", ok ? "ok" : "FAILED");
 }
 
 dsx_grid_desc desc(int P, int d0, int d1, int d2, int policy, double L) {
