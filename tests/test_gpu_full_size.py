@@ -105,3 +105,102 @@ def test_full_size_step_properties(cuda, workload):
                                want.view(torch.int32) if t == "<i4" else want.view(torch.int64)), a
     finally:
         grid.close()
+
+
+def test_full_size_two_shards_match_one_grid(cuda):
+    """clustered_64 (16M particles, Dynamic cuts) split over two shards in
+    lockstep on one GPU against one grid holding all 64 subdomains: after
+    each drifted migrate, halo build and reverse sum every owned and every
+    ghost array of every subdomain is bit-identical (compared on the
+    device)."""
+    import torch
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import sharded as shd
+    from dsdecompx_b200 import workloads as W
+    w = W.WORKLOADS["clustered_64"]
+    dims, _ = dsx.plan_topology(w.nranks, 0, w.dims, w.policy, w.lower, w.upper)
+    data = W.generate(w, seed=13)
+    owner = W.initial_owner(w, dims, data["x"], data["y"], data["z"])
+    counts, grouped = W.group_by_owner(data, owner, w.nranks)
+    del data, owner
+    N, P = int(counts.sum()), w.nranks
+    names = dsx.ARRAYS + [f[0] for f in w.fields]
+    ob = np.concatenate([[0], np.cumsum(counts)])
+    kw = dict(halo_width=w.halo, fields=w.fields)
+    ref = dsx.VirtualGrid(P, w.dims, w.policy, w.lower, w.upper, particles=N,
+                          ghost_capacity=int(0.9 * N), **kw)
+    host = [np.ascontiguousarray(grouped[n]) if n in grouped else None for n in names]
+    ref.upload_flat(counts, [h.ctypes.data if h is not None else None for h in host])
+    shards = []
+    for r in range(2):
+        e = shd.DeviceEngine(P, w.dims, w.policy, w.lower, w.upper, particles=N, ghost_capacity=N // 2, **kw)
+        sh = shd.ShardedGrid(e, r, 2)
+        c = np.where(sh.owners == r, counts, 0)
+        part = [np.ascontiguousarray(np.concatenate([h[ob[t]:ob[t + 1]] for t in sh.mine]))
+                if h is not None else None for h in host]
+        sh.upload_flat(c, [p.ctypes.data if p is not None else None for p in part])
+        shards.append(sh)
+    del host, grouped
+    wl = W.harness()
+    sizes = [8] * 11 + [4, 4] + [8]   # bytes per record of every array (one int64 field)
+
+    def region(base, offset, start, n, a):
+        t = "<i4" if sizes[a] == 4 else "<i8"
+        return torch.as_tensor(DeviceArray(base + sizes[a] * (offset + start), n, t), device="cuda")
+
+    def compare(what, ghosts):
+        rv = ref.view()
+        ro_, rg = ref.all_counts()
+        rob = np.concatenate([[0], np.cumsum(ro_)])
+        rgb = np.concatenate([[0], np.cumsum(rg)])
+        for sh in shards:
+            sv = sh.E.grid.view()
+            so = sh.E.owned_counts()
+            sob = np.concatenate([[0], np.cumsum(so)])
+            for t in sh.mine:
+                assert so[t] == ro_[t], (what, t)
+                for a in range(len(sizes)):
+                    assert torch.equal(region(rv.base[a], int(rv.owned_offset), int(rob[t]), int(ro_[t]), a),
+                                       region(sv.base[a], int(sv.owned_offset), int(sob[t]), int(so[t]), a)), \
+                        (what, t, a)
+                if ghosts:
+                    g = int(sh.plan.g[t])
+                    assert g == rg[t], (what, t)
+                    for a in range(len(sizes)):
+                        mine_g = region(sh.E.asm[a].data_ptr(), 0, int(sh.plan.gbase[t]), g, a)
+                        want = region(rv.base[a], int(rv.ghost_offset), int(rgb[t]), g, a)
+                        assert torch.equal(want, mine_g), (what, t, a)
+
+    def ghost_forces(base, offset, gid_base, gid_offset, n):
+        gid = torch.as_tensor(DeviceArray(gid_base + 4 * gid_offset, n, "<i4"), device="cuda")
+        for k, a in enumerate((6, 7, 8)):
+            f = torch.as_tensor(DeviceArray(base[a] + 8 * offset, n, "<f8"), device="cuda")
+            f.copy_(torch.sin(gid.double() * 0.37 + k))
+
+    try:
+        for step in range(2):
+            for g in [ref] + [sh.E.grid for sh in shards]:
+                v = g.view()
+                wl.dsxw_drift(C.byref(v), 9, step, 0.3, torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            ref.migrate()
+            shd.run_lockstep([sh.migrate_steps() for sh in shards])
+            compare(f"migrate {step}", False)
+            ref.exchange_halo(rebuild=True)
+            shd.run_lockstep([sh.exchange_halo_steps(True, False) for sh in shards])
+            compare(f"halo {step}", True)
+            rv = ref.view()
+            G = int(ref.totals()["ghosts"])
+            ghost_forces(list(rv.base), int(rv.ghost_offset), rv.base[12], int(rv.ghost_offset), G)
+            for sh in shards:
+                asm = [t.data_ptr() for t in sh.E.asm]
+                ghost_forces(asm, 0, asm[12], 0, int(sh.plan.total))
+            torch.cuda.synchronize()
+            ref.reverse_halo()
+            shd.run_lockstep([sh.reverse_halo_steps() for sh in shards])
+            compare(f"reverse {step}", False)
+    finally:
+        ref.close()
+        for sh in shards:
+            sh.E.close()
