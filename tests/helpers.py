@@ -3,11 +3,11 @@ the same sequence of calls go to the CUDA grid and to the oracle, and every
 array of every subdomain is compared bit for bit."""
 from __future__ import annotations
 
-from typing import Dict, List, Optional, Sequence, Tuple
+from typing import Dict, List, Sequence
 
 import numpy as np
 
-from oracle import ARRAYS, FIELD_DTYPES, Grid
+from oracle import FIELD_DTYPES, Grid
 
 FIELD_TYPE_NAMES = ["int32", "int64", "uint32", "uint64", "float32", "float64"]
 

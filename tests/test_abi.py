@@ -4,7 +4,6 @@ import glob
 import os
 import re
 
-import numpy as np
 import pytest
 
 import dsdecompx_b200 as dsx
