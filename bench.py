@@ -390,7 +390,7 @@ def run_ours(args, rank, world, device):
                    "grid": list(dims), "particles": N, "record_bytes": S,
                    "step": "graph-captured batched step (dsx_grid_step)",
                    "l2": "inputs larger than L2 (%.2f GB of owned records)" % (N * S / 1e9),
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "parallelism": "1 GPU",
                    "autotune": tune},
         "roofline": roof,
         "step_roofline": {"algorithmic_bytes": int(step_bytes),

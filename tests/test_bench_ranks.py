@@ -1,9 +1,9 @@
 """Host logic of bench.py's multi-process path, on CPU with gloo.
 
-bench.py --gpus N runs one process per GPU (replicas of the workload, weak
-scaling): every rank times its own steps and the job reports the slowest
-rank's time; the reference arm runs on rank 0 only.  Both are checked here
-with two gloo ranks and no GPU.
+bench.py --gpus N runs one process per GPU (the sharded grid, one block of
+subdomains per rank, weak scaling): every rank times its own steps and the
+job reports the slowest rank's time; the reference arm runs on rank 0 only.
+Both are checked here with two gloo ranks and no GPU.
 """
 import json
 import os
