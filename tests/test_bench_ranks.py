@@ -59,3 +59,34 @@ def test_reference_arm_runs_on_rank_zero_only():
                        env=env, capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr
     assert p.stdout.strip() == ""
+
+
+def test_shard_factors_cover_the_rank_count():
+    """bench.py's weak-scaling layout: N ranks as (a, b, c) blocks of the
+    workload, a * b * c = N, the prime factors spread over the axes."""
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.shard_factors(1) == (1, 1, 1)
+    assert bench.shard_factors(2) == (2, 1, 1)
+    assert bench.shard_factors(4) == (2, 2, 1)
+    assert bench.shard_factors(8) == (2, 2, 2)
+    for n in range(1, 33):
+        a, b, c = bench.shard_factors(n)
+        assert a * b * c == n and max(a, b, c) <= n
+
+
+def test_sharded_process_grids_are_blocks_of_the_workload():
+    """For the default workload at 2, 3, 4 and 8 ranks the planner's process
+    grid of the grown box is the workload's grid times the block counts, so
+    every rank owns exactly one block (bench.py refuses to run otherwise)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import workloads as W
+    w = W.WORKLOADS["clustered_64"]
+    block, _ = dsx.plan_topology(w.nranks, 0, w.dims, w.policy, w.lower, w.upper)
+    for n in (2, 3, 4, 8):
+        fa = bench.shard_factors(n)
+        upper = tuple(u * k for u, k in zip(w.upper, fa))
+        dims, _ = dsx.plan_topology(w.nranks * n, 0, (0, 0, 0), w.policy, w.lower, upper)
+        assert tuple(dims) == tuple(d * k for d, k in zip(block, fa)), (n, dims)
