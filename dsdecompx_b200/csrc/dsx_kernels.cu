@@ -581,6 +581,34 @@ __device__ __forceinline__ void count_group(unsigned m, int nn, int lane, int& a
     if (lane == kImageCounter) acc += total_images;
 }
 
+// count_group over K groups at once (lane holds one particle of each): the
+// same sums, one warp reduction per neighbor instead of one ballot per group.
+template <int K>
+__device__ __forceinline__ void count_groups(const unsigned (&m)[K], int lane, int& acc) {
+    unsigned all = 0;
+    int boundary = 0, images = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        all |= m[j];
+        boundary += m[j] != 0u;
+        images += __popc(m[j]);
+    }
+    const unsigned used = __reduce_or_sync(0xffffffffu, all);
+    if (!used) return;
+    for (unsigned rest = used; rest; rest &= rest - 1) {
+        const int n = __ffs(rest) - 1;
+        unsigned c = 0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) c += (m[j] >> n) & 1u;
+        const int total = static_cast<int>(__reduce_add_sync(0xffffffffu, c));
+        if (lane == n) acc += total;
+    }
+    const int total_boundary = __reduce_add_sync(0xffffffffu, boundary);
+    const int total_images = __reduce_add_sync(0xffffffffu, images);
+    if (lane == kBoundaryCounter) acc += total_boundary;
+    if (lane == kImageCounter) acc += total_images;
+}
+
 // H1: neighbor mask of every owned particle and per-tile list counts.
 // `tiles`/`ntiles`: the tiles to classify (all owned particles of a layout,
 // or the immigrant segments of a fused step).
@@ -952,6 +980,9 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                         (!G.periodic[1] || G.lower[1] == 0.0) &&
                         (!G.periodic[2] || G.lower[2] == 0.0);
     int acc = 0;
+    unsigned m[CI];
+    int fast = 0;         // this lane's particles that took the warp-uniform path
+    unsigned slow = 0;    // groups left to the general path (the same in every lane)
 #pragma unroll
     for (int j = 0; j < CI; ++j) {
         const int i = wbegin + j * 32 + lane;
@@ -959,26 +990,40 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
         const bool own = valid && simple && cell.lo[0] <= px[j] && px[j] < cell.hi[0] &&
                          cell.lo[1] <= py[j] && py[j] < cell.hi[1] && cell.lo[2] <= pz[j] &&
                          pz[j] < cell.hi[2];
-        int d = -1;
-        unsigned m = 0;
+        m[j] = 0;
         if (__all_sync(0xffffffffu, own || !valid)) {
             // the whole group stays: destination s, mask of the own subdomain
             if (valid) {
-                d = s;
                 const double wx = G.periodic[0] && px[j] == 0.0 ? 0.0 : px[j];
                 const double wy = G.periodic[1] && py[j] == 0.0 ? 0.0 : py[j];
                 const double wz = G.periodic[2] && pz[j] == 0.0 ? 0.0 : pz[j];
-                m = halo_mask(bs, lut, wx, wy, wz);
-                dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(d);
-                mask_out[static_cast<long long>(g) * TILE + (i - begin)] = m;
+                m[j] = halo_mask(bs, lut, wx, wy, wz);
+                dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(s);
+                mask_out[static_cast<long long>(g) * TILE + (i - begin)] = m[j];
+                ++fast;
             }
-        } else if (valid) {
+        } else {
+            slow |= 1u << j;
+        }
+    }
+    count_groups<CI>(m, lane, acc);
+    const int fast_stays = __reduce_add_sync(0xffffffffu, fast);
+    if (lane == kStepStay) acc += fast_stays;
+    // The general path, one group per pass: its code appears once (the
+    // unrolled path above stays small enough for the instruction cache) and
+    // re-reads the group's positions, still in L1.
+#pragma unroll 1
+    for (; slow; slow &= slow - 1) {
+        const int i = wbegin + (__ffs(slow) - 1) * 32 + lane;
+        int d = -1;
+        unsigned mg = 0;
+        if (i < end) {
             double wx, wy, wz;
-            d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
+            d = destination_near(G, cell, ro(x + i), ro(y + i), ro(z + i), wx, wy, wz);
             dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(d);
             if (d == s) {
-                m = halo_mask(bs, lut, wx, wy, wz);
-                mask_out[static_cast<long long>(g) * TILE + (i - begin)] = m;
+                mg = halo_mask(bs, lut, wx, wy, wz);
+                mask_out[static_cast<long long>(g) * TILE + (i - begin)] = mg;
             } else {
                 const unsigned me = halo_mask(halo_bounds(G, d), G.lut + d * 64, wx, wy, wz);
                 atomicAdd(&imm_total[d], 1);
@@ -990,7 +1035,7 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                 }
             }
         }
-        count_group(m, nn, lane, acc);
+        count_group(mg, nn, lane, acc);
         const int stays = __popc(__ballot_sync(0xffffffffu, d == s));
         const int emigs = __popc(__ballot_sync(0xffffffffu, d >= 0 && d != s));
         if (lane == kStepStay) acc += stays;
