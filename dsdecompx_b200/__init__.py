@@ -72,7 +72,8 @@ class TuneReport(C.Structure):
     _fields_ = [("classify_threads", C.c_int), ("move_staged", C.c_int),
                 ("reverse_ctas_per_sm", C.c_int), ("ghost_capacity", C.c_longlong),
                 ("classify_ms", C.c_float * 3), ("move_ms", C.c_float * 4),
-                ("reverse_ms", C.c_float * 4)]
+                ("reverse_ms", C.c_float * 4), ("classify_combine", C.c_int),
+                ("classify_combined_ms", C.c_float * 3)]
 
 
 class GridView(C.Structure):
@@ -133,7 +134,7 @@ def lib() -> C.CDLL:
             "dsx_grid_step_kernel_count": [vp],
             "dsx_grid_profile": [vp, C.c_int],
             "dsx_grid_set_plain": [vp, C.c_int],
-            "dsx_grid_set_tuning": [vp, C.c_int, C.c_int, C.c_int],
+            "dsx_grid_set_tuning": [vp, C.c_int, C.c_int, C.c_int, C.c_int],
             "dsx_grid_set_cuts": [vp, C.POINTER(C.c_double), vp],
             "dsx_grid_owner_rank": [vp, vp, vp, vp, C.c_longlong, vp, vp],
             "dsx_grid_begin_halo_exchange": [vp, C.c_int, C.c_int, vp],
@@ -483,10 +484,14 @@ class VirtualGrid:
         r = TuneReport()
         _check(self.L.dsx_grid_autotune(self.h, _stream(stream), C.byref(r)))
         kinds = MOVE_KINDS
-        return {"classify_threads": r.classify_threads, "move": kinds.get(r.move_staged, "?"),
+        return {"classify_threads": r.classify_threads,
+                "classify_combine": bool(r.classify_combine),
+                "move": kinds.get(r.move_staged, "?"),
                 "reverse_ctas_per_sm": r.reverse_ctas_per_sm,
                 "ghost_capacity": int(r.ghost_capacity),
                 "classify_ms": {n: round(float(v), 4) for n, v in zip((64, 128, 256), r.classify_ms)},
+                "classify_combined_ms": {n: round(float(v), 4)
+                                         for n, v in zip((64, 128, 256), r.classify_combined_ms)},
                 "move_ms": {"staged": round(float(r.move_ms[0]), 4),
                             "direct": round(float(r.move_ms[1]), 4),
                             "staged passes": round(float(r.move_ms[2]), 4),
@@ -551,10 +556,11 @@ class VirtualGrid:
         _check(self.L.dsx_grid_rescale_domain(self.h, lo, hi, 1 if update else 0, _stream(stream)))
 
     def set_tuning(self, classify_threads: int = 128, move: str = "staged",
-                   reverse_ctas_per_sm: int = 0):
+                   reverse_ctas_per_sm: int = 0, classify_combine: bool = False):
         """Sets the batched step's launch shapes (the choices autotune reports)."""
         kind = {v: k for k, v in MOVE_KINDS.items()}[move]
-        _check(self.L.dsx_grid_set_tuning(self.h, classify_threads, kind, reverse_ctas_per_sm))
+        _check(self.L.dsx_grid_set_tuning(self.h, classify_threads, kind, reverse_ctas_per_sm,
+                                          1 if classify_combine else 0))
 
     # ----------------------------------------------- sharded grids
     def migration_pairs(self, stream=None) -> np.ndarray:

@@ -1103,6 +1103,7 @@ struct dsx_grid {
         not_pending("autotune");
         dsx_tune_report r{};
         for (float& v : r.classify_ms) v = -1.0f;
+        for (float& v : r.classify_combined_ms) v = -1.0f;
         for (float& v : r.move_ms) v = -1.0f;
         for (float& v : r.reverse_ms) v = -1.0f;
         if (P > 1 && total > 0) {
@@ -1145,11 +1146,22 @@ struct dsx_grid {
             grids(G, Gn);
             clear_status(stream);
             const int shapes[3] = {64, 128, 256};
-            for (int i = 0; i < 3; ++i) {
-                S.classify_threads = shapes[i];
-                r.classify_ms[i] = time([&] { dsx::launch_step_classify(G, A, src, S, stream); });
-            }
-            S.classify_threads = pick(r.classify_ms, shapes, 3, 128);
+            float best_classify = -1.0f;
+            int best_threads = 128, best_combine = 0;
+            for (int c = 0; c < 2; ++c)
+                for (int i = 0; i < 3; ++i) {
+                    S.classify_threads = shapes[i];
+                    S.classify_combine = c;
+                    const float ms = time([&] { dsx::launch_step_classify(G, A, src, S, stream); });
+                    (c ? r.classify_combined_ms : r.classify_ms)[i] = ms;
+                    if (best_classify < 0.0f || ms < best_classify) {
+                        best_classify = ms;
+                        best_threads = shapes[i];
+                        best_combine = c;
+                    }
+                }
+            S.classify_threads = best_threads;
+            S.classify_combine = best_combine;
             // the next layout's plan; the ghost region grows until it fits
             for (;;) {
                 clear_status(stream);
@@ -1198,6 +1210,7 @@ struct dsx_grid {
             destroy_graphs();
         }
         r.classify_threads = S.classify_threads;
+        r.classify_combine = S.classify_combine;
         r.move_staged = S.move_staged;
         r.reverse_ctas_per_sm = S.reverse_per_sm;
         r.ghost_capacity = gcap;
@@ -1720,7 +1733,7 @@ int dsx_copy_segments(const dsx_copy* copies, long long n, void* stream) {
 }
 
 int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
-                        int reverse_ctas_per_sm) {
+                        int reverse_ctas_per_sm, int classify_combine) {
     return guarded([&] {
         if (!grid) fail(DSX_E_INVALID, "null grid");
         if (classify_threads != 64 && classify_threads != 128 && classify_threads != 256)
@@ -1730,6 +1743,7 @@ int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
             fail(DSX_E_INVALID, "reverse CTAs per SM must be 0..32");
         grid->not_pending("set_tuning");
         grid->S.classify_threads = classify_threads;
+        grid->S.classify_combine = classify_combine != 0;
         grid->S.move_staged = move_kind;
         grid->S.reverse_per_sm = reverse_ctas_per_sm;
         grid->destroy_graphs();   // captured steps hold the old launch shapes

@@ -609,6 +609,35 @@ __device__ __forceinline__ void count_groups(const unsigned (&m)[K], int lane, i
     if (lane == kImageCounter) acc += total_images;
 }
 
+// Immigrant totals of one 32-particle group: a lane with key >= 0 holds an
+// emigrant bound for subdomain `key` (-1: none) with the new owner's
+// neighbor mask `me`, counted into the owner's total, boundary, image and
+// per-list counters with one atomic per distinct destination of the warp.
+// Every lane of the warp calls it.  It pays where the emigrants of a step are
+// many and share few destinations (per-lane atomics on the same counters
+// serialise); with a few emigrants per warp the match costs more than it
+// saves, and the autotuner chooses.
+__device__ __forceinline__ void add_immigrants(int key, unsigned me, int lane, int* total,
+                                               int* bnd, int* img, int* list) {
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (key < 0) return;
+    const bool leader = lane == __ffs(peers) - 1;
+    const int boundary = __reduce_add_sync(peers, me != 0u ? 1 : 0);
+    const int images = __reduce_add_sync(peers, __popc(me));
+    if (leader) {
+        atomicAdd(&total[key], __popc(peers));
+        if (boundary) {
+            atomicAdd(&bnd[key], boundary);
+            atomicAdd(&img[key], images);
+        }
+    }
+    for (unsigned r = __reduce_or_sync(peers, me); r; r &= r - 1) {
+        const int n = __ffs(r) - 1;
+        const int c = __popc(__ballot_sync(peers, (me >> n) & 1u));
+        if (leader) atomicAdd(&list[key * kMaxNeighbors + n], c);
+    }
+}
+
 // H1: neighbor mask of every owned particle and per-tile list counts.
 // `tiles`/`ntiles`: the tiles to classify (all owned particles of a layout,
 // or the immigrant segments of a fused step).
@@ -936,8 +965,9 @@ __device__ __forceinline__ double wrap_if(const Grid& G, int a, double v) {
 }
 
 // F1: destination and new-owner halo mask of every owned particle; per-tile
-// counters; per-destination totals of the emigrants (atomics: only sums).
-template <int CT, int MINB>
+// counters; per-destination totals of the emigrants (atomics: only sums;
+// COMBINE: one per destination and warp, add_immigrants).
+template <int CT, int MINB, bool COMBINE>
 __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double* __restrict__ x,
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z, int* cnt,
@@ -1016,7 +1046,7 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
     for (; slow; slow &= slow - 1) {
         const int i = wbegin + (__ffs(slow) - 1) * 32 + lane;
         int d = -1;
-        unsigned mg = 0;
+        unsigned mg = 0, me = 0;
         if (i < end) {
             double wx, wy, wz;
             d = destination_near(G, cell, ro(x + i), ro(y + i), ro(z + i), wx, wy, wz);
@@ -1025,16 +1055,20 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                 mg = halo_mask(bs, lut, wx, wy, wz);
                 mask_out[static_cast<long long>(g) * TILE + (i - begin)] = mg;
             } else {
-                const unsigned me = halo_mask(halo_bounds(G, d), G.lut + d * 64, wx, wy, wz);
-                atomicAdd(&imm_total[d], 1);
-                if (me) {
-                    atomicAdd(&imm_bnd[d], 1);
-                    atomicAdd(&imm_img[d], __popc(me));
-                    for (unsigned r = me; r; r &= r - 1)
-                        atomicAdd(&imm_list[d * kMaxNeighbors + __ffs(r) - 1], 1);
+                me = halo_mask(halo_bounds(G, d), G.lut + d * 64, wx, wy, wz);
+                if constexpr (!COMBINE) {
+                    atomicAdd(&imm_total[d], 1);
+                    if (me) {
+                        atomicAdd(&imm_bnd[d], 1);
+                        atomicAdd(&imm_img[d], __popc(me));
+                        for (unsigned r = me; r; r &= r - 1)
+                            atomicAdd(&imm_list[d * kMaxNeighbors + __ffs(r) - 1], 1);
+                    }
                 }
             }
         }
+        if constexpr (COMBINE)
+            add_immigrants(d >= 0 && d != s ? d : -1, me, lane, imm_total, imm_bnd, imm_img, imm_list);
         count_group(mg, nn, lane, acc);
         const int stays = __popc(__ballot_sync(0xffffffffu, d == s));
         const int emigs = __popc(__ballot_sync(0xffffffffu, d >= 0 && d != s));
@@ -2565,21 +2599,23 @@ void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, con
     const double* x = A.d[0] + src_off;
     const double* y = A.d[1] + src_off;
     const double* z = A.d[2] + src_off;
+    // the two forms of each shape have one signature
+    auto pick = [&](auto plain, auto combined) { return S.classify_combine ? combined : plain; };
     switch (S.classify_threads) {
     case 64:
-        k_step_classify<64, 12><<<G.max_tiles, 64, 0, s>>>(G, x, y, z, S.cnt, S.stride, S.imm_total,
-                                                            S.imm_list, S.imm_bnd, S.imm_img,
-                                                            S.dest16, S.mask);
+        pick(k_step_classify<64, 12, false>, k_step_classify<64, 12, true>)<<<G.max_tiles, 64, 0, s>>>(
+            G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
+            S.mask);
         break;
     case 256:
-        k_step_classify<256, 4><<<G.max_tiles, 256, 0, s>>>(G, x, y, z, S.cnt, S.stride,
-                                                             S.imm_total, S.imm_list, S.imm_bnd,
-                                                             S.imm_img, S.dest16, S.mask);
+        pick(k_step_classify<256, 4, false>, k_step_classify<256, 4, true>)<<<G.max_tiles, 256, 0, s>>>(
+            G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
+            S.mask);
         break;
     default:
-        k_step_classify<128, 8><<<G.max_tiles, 128, 0, s>>>(G, x, y, z, S.cnt, S.stride,
-                                                             S.imm_total, S.imm_list, S.imm_bnd,
-                                                             S.imm_img, S.dest16, S.mask);
+        pick(k_step_classify<128, 8, false>, k_step_classify<128, 8, true>)<<<G.max_tiles, 128, 0, s>>>(
+            G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
+            S.mask);
     }
 }
 

@@ -68,6 +68,7 @@ struct Scratch {
     Marks* marks = nullptr;
     // launch shapes the autotuner picks (these defaults are the untuned choice)
     int classify_threads = 128;   // threads per 512-particle tile of the step classify: 64/128/256
+    int classify_combine = 0;     // immigrant counters combined per warp before the atomics
     int move_staged = 1;          // 1: staged (one pass if it fits), 2: staged in passes,
                                   // 3: staged without forces, 0: direct reads
     int reverse_per_sm = 0;       // CTAs per SM of the reverse sum; 0: one wave of the default shape

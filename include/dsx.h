@@ -295,6 +295,10 @@ typedef struct dsx_tune_report {
     float classify_ms[3];    /* 64, 128, 256 threads per tile */
     float move_ms[4];        /* staged, direct reads, staged in passes, staged without forces */
     float reverse_ms[4];     /* 4, 8, 16, 32 CTAs per SM */
+    int classify_combine;    /* 1: a warp's immigrant counters combined per destination
+                                before one atomic each (pays when many emigrants share
+                                few destinations) */
+    float classify_combined_ms[3];   /* the combined form at 64, 128, 256 threads */
 } dsx_tune_report;
 int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report);
 
@@ -303,9 +307,10 @@ int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report);
  * classify_threads 64, 128 or 256; move_kind as dsx_tune_report.move_staged
  * (a kind that does not fit the record's shared-memory budget falls back to
  * staged passes or direct reads); reverse_ctas_per_sm 0 (two waves of the
- * grid's SMs) or 1..32.  Results are identical for every setting. */
+ * grid's SMs) or 1..32; classify_combine as dsx_tune_report.classify_combine.
+ * Results are identical for every setting. */
 int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
-                        int reverse_ctas_per_sm);
+                        int reverse_ctas_per_sm, int classify_combine);
 
 /* ---- sharded grids: the P subdomains split over several processes ----
  *

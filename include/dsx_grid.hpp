@@ -211,9 +211,11 @@ public:
         return status;
     }
     // classify_threads 64/128/256, move_kind as dsx_tune_report.move_staged,
-    // reverse_ctas_per_sm 0..32
-    void set_tuning(int classify_threads, int move_kind, int reverse_ctas_per_sm) {
-        check(dsx_grid_set_tuning(handle_, classify_threads, move_kind, reverse_ctas_per_sm));
+    // reverse_ctas_per_sm 0..32, classify_combine as dsx_tune_report's
+    void set_tuning(int classify_threads, int move_kind, int reverse_ctas_per_sm,
+                    bool classify_combine = false) {
+        check(dsx_grid_set_tuning(handle_, classify_threads, move_kind, reverse_ctas_per_sm,
+                                  classify_combine ? 1 : 0));
     }
     dsx_tune_report autotune(void* stream = nullptr) {
         dsx_tune_report r{};

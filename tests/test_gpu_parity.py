@@ -300,6 +300,7 @@ def test_batched_step_matches_calls(cuda, tuned):
             assert rep["reverse_ctas_per_sm"] in (4, 8, 16, 32)
             assert rep["ghost_capacity"] >= 12000
             assert min(rep["classify_ms"].values()) > 0
+            assert min(rep["classify_combined_ms"].values()) > 0
         a.displace(rng, 0.3)
         for r in range(8):
             o = b.counts(r)[0]
@@ -432,7 +433,8 @@ def test_batched_step_many_tiles(cuda, fields, particles, box, halo):
 def test_every_tuning_gives_the_same_step(cuda, fields, particles):
     """The batched step with each move kind forced (staged in one pass,
     direct reads, staged in passes, staged without the force arrays) and each
-    classify shape and reverse grid: particles, ghosts and sums identical to
+    classify shape, with and without the immigrant counters combined per
+    warp, and reverse grid: particles, ghosts and sums identical to
     the per-call path (itself checked against the oracle here).  At 204 B per
     particle one staged pass does not fit and kind 1 falls back to passes,
     while the stage without forces (about 92 KB a tile) fits."""
@@ -449,7 +451,8 @@ def test_every_tuning_gives_the_same_step(cuda, fields, particles):
     per = split_by_owner(owner, data, 27)
     a.upload(per)
     tunings = [(128, "staged", 0), (64, "direct", 4), (256, "staged passes", 32),
-               (128, "staged direct forces", 8)]
+               (128, "staged direct forces", 8), (128, "staged", 0, True), (64, "staged", 8, True),
+               (256, "direct", 4, True)]
     grids = []
     for t in tunings:
         g = dsx.VirtualGrid(**kw)
