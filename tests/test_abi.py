@@ -67,3 +67,57 @@ def test_topology_matches_oracle(case):
         dims, nbrs = dsx.plan_topology(P, r, **kw)
         assert dims == g.topology(r)[0]
         assert nbrs == g.neighbors(r)
+
+
+def _mirrors():
+    """(C struct name, Python mirror) of every struct that crosses the ABI."""
+    import ctypes as C
+
+    from dsdecompx_b200 import sharded
+    return [("dsx_domain", dsx._Domain), ("dsx_migration_result", dsx._MigrationResult),
+            ("dsx_grid_desc", dsx._GridDesc), ("dsx_field_desc", dsx._FieldDesc),
+            ("dsx_grid_view", dsx.GridView), ("dsx_tune_report", dsx.TuneReport),
+            ("dsx_segment", dsx.SEGMENT_DTYPE), ("dsx_copy", dsx.COPY_DTYPE),
+            ("dsx_transport", sharded._Transport)], C
+
+
+def test_struct_layouts_match_headers(tmp_path):
+    """The ctypes structures and numpy record types of the Python front end
+    have the size and field offsets that a C compiler gives the header
+    structs (a field added on one side only would shift every later one)."""
+    import shutil
+    import subprocess
+    mirrors, C = _mirrors()
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    layout = {}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "dsx.h"', '#include "dsx_shard.h"',
+             "int main(void) {"]
+    for name, mirror in mirrors:
+        fields = list(mirror.names) if hasattr(mirror, "names") else [f[0] for f in mirror._fields_]
+        layout[name] = fields
+        lines.append(f'    printf("{name} size %zu\\n", sizeof({name}));')
+        for f in fields:
+            lines.append(f'    printf("{name} {f} %zu\\n", offsetof({name}, {f}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    want = {}
+    for line in filter(None, out):
+        name, what, value = line.split()
+        want[(name, what)] = int(value)
+    for name, mirror in mirrors:
+        if hasattr(mirror, "names"):
+            size = mirror.itemsize
+            offsets = {f: mirror.fields[f][1] for f in mirror.names}
+        else:
+            size = C.sizeof(mirror)
+            offsets = {f[0]: getattr(mirror, f[0]).offset for f in mirror._fields_}
+        assert size == want[(name, "size")], (name, size, want[(name, "size")])
+        for f, off in offsets.items():
+            assert off == want[(name, f)], (name, f, off, want[(name, f)])
