@@ -104,6 +104,12 @@ def scenario(P, dims, L, halo, N, steps, seed, fields=ALL_FIELDS, sigma=0.3, pol
      dict(periodic=(True, False, False), edges=False, lower=(-4.5, 1.0, 100.0))),
     (27, (3, 3, 3), (9.0, 9.0, 9.0), 0.9, dict(sigma=2.5, fields=ALL_FIELDS[:3])),
     (6, (0, 0, 0), (12.0, 8.0, 4.0), 0.5, dict(policy="balanced")),
+    # a halo wider than half a cell: one particle reaches the same receiver
+    # as its -x and its +x image (two blocks of one sender)
+    (2, (2, 1, 1), (10.0, 10.0, 10.0), 3.0, dict(sigma=1.0)),
+    (3, (3, 1, 1), (9.0, 4.0, 4.0), 2.5, dict(fields=ALL_FIELDS[:2])),
+    # every axis periodic with the box off the origin: no shortcut wrap
+    (8, (2, 2, 2), (10.0, 10.0, 10.0), 1.0, dict(lower=(-5.0, -5.0, -5.0), sigma=2.0)),
 ])
 def test_port_matches_reference(P, dims, L, halo, kw):
     scenario(P, dims, L, halo, N=1500 * max(1, P // 4), steps=3, seed=P, **kw)
