@@ -67,9 +67,11 @@ static inline int MPI_Reduce(const void* send, void* receive, int count, MPI_Dat
     (void)root;
     return MPI_Allreduce(send, receive, count, type, op, comm);
 }
+/* wall-clock seconds, as MPI_Wtime is defined (timespec_get: ISO C11 and
+ * C++17, no POSIX feature macro needed) */
 static inline double MPI_Wtime(void) {
     struct timespec t;
-    clock_gettime(CLOCK_MONOTONIC, &t);
+    timespec_get(&t, TIME_UTC);
     return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
 }
 
