@@ -33,15 +33,20 @@ def oracle_fields(fields):
 
 # ------------------------------------------------------------ planning
 
-@pytest.mark.parametrize("dims,R", [((4, 4, 4), 8), ((4, 4, 4), 2), ((2, 2, 2), 4), ((3, 1, 4), 2),
-                                    ((3, 3, 3), 4), ((8, 8, 4), 8)])
-def test_block_owners(dims, R):
+@pytest.mark.parametrize("dims,R,blocks", [
+    ((4, 4, 4), 8, True), ((4, 4, 4), 2, True), ((2, 2, 2), 4, True), ((3, 1, 4), 2, True),
+    ((3, 3, 3), 4, False), ((8, 8, 4), 8, True),
+    # shard counts with no factorisation that divides the grid: runs of ranks
+    ((4, 4, 4), 5, False), ((8, 8, 4), 7, False), ((4, 4, 4), 3, False),
+    # prime or composite counts that still divide one or two axes
+    ((5, 2, 2), 5, True), ((6, 4, 4), 6, True), ((3, 3, 3), 9, True)])
+def test_block_owners(dims, R, blocks):
     owners = shd.block_owners(dims, R)
     P = int(np.prod(dims))
     assert owners.shape == (P,) and set(owners) == set(range(R))
     counts = np.bincount(owners, minlength=R)
     assert counts.max() - counts.min() <= 1
-    if dims == (3, 3, 3):
+    if not blocks:
         # no exact block split: contiguous runs of ranks
         assert (np.diff(owners) >= 0).all()
     else:
