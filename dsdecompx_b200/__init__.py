@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
                                  C.c_longlong, C.c_int, C.c_int, ip, vp, C.POINTER(vp)],
             "dsx_shard_destroy": [vp],
             "dsx_shard_owners": [vp, ip],
+            "dsx_shard_plan_owners": [ip, C.c_int, ip],
             "dsx_shard_upload": [vp, llp, C.POINTER(vp), vp],
             "dsx_shard_download": [vp, llp, C.POINTER(vp), vp],
             "dsx_shard_migrate": [vp, vp, llp],

@@ -751,6 +751,21 @@ int dsx_shard_destroy(dsx_shard* shard) {
     return DSX_OK;
 }
 
+int dsx_shard_plan_owners(const int* dims, int nshards, int* owners) {
+    return guarded([&] {
+        if (!dims || !owners) fail(DSX_E_INVALID, "null argument");
+        long long P = 1;
+        for (int a = 0; a < 3; ++a) {
+            if (dims[a] < 1) fail(DSX_E_INVALID, "process grid dims must be positive");
+            P *= dims[a];
+            if (P > (1 << 20)) fail(DSX_E_INVALID, "process grid too large");
+        }
+        if (nshards < 1 || nshards > P) fail(DSX_E_INVALID, "shards must be in 1..P");
+        const std::vector<int> planned = block_owners(dims, nshards);
+        std::copy(planned.begin(), planned.end(), owners);
+    });
+}
+
 int dsx_shard_owners(dsx_shard* shard, int* owners) {
     return guarded([&] {
         if (!shard || !owners) fail(DSX_E_INVALID, "null argument");

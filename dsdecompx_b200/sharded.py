@@ -185,6 +185,19 @@ def block_owners(dims, nshards: int) -> np.ndarray:
     return owners
 
 
+def plan_owners(dims, nshards: int) -> np.ndarray:
+    """block_owners as the native library plans it (dsx_shard_plan_owners,
+    host only): the owners a NativeShardedGrid created without them gets."""
+    import ctypes as C
+
+    from . import _check, lib
+    d = np.ascontiguousarray([int(v) for v in dims], dtype=np.int32)
+    out = np.zeros(int(np.prod(d, dtype=np.int64)), dtype=np.int32)
+    _check(lib().dsx_shard_plan_owners(d.ctypes.data_as(C.POINTER(C.c_int)), int(nshards),
+                                       out.ctypes.data_as(C.POINTER(C.c_int))))
+    return out.astype(np.int64)
+
+
 def halo_tables(topology):
     """(nn[P], sender_of[P, 26]) from every subdomain's neighbor list:
     receiver t's block m holds the list of its neighbor q toward -d_m, entry

@@ -61,6 +61,12 @@ int dsx_shard_destroy(dsx_shard* shard);
 /* The shard of every subdomain (P values). */
 int dsx_shard_owners(dsx_shard* shard, int* owners);
 
+/* Host only (no GPU needed): the shard of every subdomain of the process
+ * grid dims[3] (dims[0] * dims[1] * dims[2] values, subdomain rank order)
+ * that dsx_shard_create chooses when given no owners, so that a process can
+ * load just its own subdomains' particles before it creates its shard. */
+int dsx_shard_plan_owners(const int* dims, int nshards, int* owners);
+
 /* This shard's particles: counts[P] (zero outside its subdomains) and host
  * or device arrays as dsx_grid_upload. */
 int dsx_shard_upload(dsx_shard* shard, const long long* counts, const void* const* arrays,

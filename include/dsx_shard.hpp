@@ -13,6 +13,7 @@
 #include "dsx_grid.hpp"
 #include "dsx_shard.h"
 
+#include <array>
 #include <functional>
 #include <memory>
 #include <vector>
@@ -61,6 +62,13 @@ public:
     std::vector<int> owners() const {
         std::vector<int> o(static_cast<std::size_t>(nranks_));
         check(dsx_shard_owners(handle_, o.data()));
+        return o;
+    }
+    // The owners a shard created without them would get (host only).
+    static std::vector<int> plan_owners(const std::array<int, 3>& dims, int nshards) {
+        std::vector<int> o(static_cast<std::size_t>(dims[0]) * static_cast<std::size_t>(dims[1]) *
+                           static_cast<std::size_t>(dims[2]));
+        check(dsx_shard_plan_owners(dims.data(), nshards, o.data()));
         return o;
     }
     void upload(const std::vector<long long>& counts, const std::vector<const void*>& arrays,

@@ -281,6 +281,12 @@ void run(const Case& cs) {
     }
     std::vector<int> owners(P);
     must(dsx_shard_owners(shards[0], owners.data()), "owners");
+    {
+        // a shard created without owners takes the host-side plan
+        std::vector<int> planned(P);
+        must(dsx_shard_plan_owners(place.dims, R, planned.data()), "plan owners");
+        for (int t = 0; t < P; ++t) expect(planned[t] == owners[t], "planned owners", t);
+    }
     // each shard uploads its subdomains' particles as the one grid holds them
     {
         std::vector<long long> o(P), g(P);
@@ -476,6 +482,7 @@ void shortfall() {
                                                             r == 0 ? N : 10, r, 2, tr));
     }
     const std::vector<int> owners = shards[0]->owners();
+    if (dsx::ShardedGrid::plan_owners({2, 2, 2}, 2) != owners) expect(false, "planned owners (C++)", 0);
     int first = 0;
     while (owners[first] != 0) ++first;
     std::vector<double> x(N), y(N), z(N);

@@ -7,6 +7,7 @@ shards as gloo ranks, and every array of every subdomain is compared bit for
 bit with one oracle grid holding all subdomains.
 """
 import datetime
+import itertools
 import os
 import socket
 import sys
@@ -55,6 +56,19 @@ def test_block_owners(dims, R, blocks):
             c = np.array([shd.subdomain_coords(t, dims) for t in np.flatnonzero(owners == s)])
             span = c.max(axis=0) - c.min(axis=0) + 1
             assert np.prod(span) == len(c)
+
+
+def test_native_plan_matches_block_owners():
+    """The library's default owners (dsx_shard_plan_owners, host only) are
+    block_owners' on every grid of up to 6 per axis and every shard count,
+    and it refuses what block_owners refuses."""
+    for dims in itertools.product(range(1, 7), repeat=3):
+        P = int(np.prod(dims))
+        for R in range(1, min(P, 12) + 1):
+            assert (shd.plan_owners(dims, R) == shd.block_owners(dims, R)).all(), (dims, R)
+    for dims, R in (((2, 2, 2), 9), ((2, 2, 2), 0), ((0, 2, 2), 1)):
+        with pytest.raises(Exception):
+            shd.plan_owners(dims, R)
 
 
 def test_block_owners_prefers_the_smallest_cut():
