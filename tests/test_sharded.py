@@ -406,3 +406,39 @@ def test_lockstep_edge_cases(case, R, start):
     for sh in shards:
         sh.upload({t: per[t] for t in sh.mine})
     Scenario(shards, lockstep_drive(shards), ref, kw["nranks"], fields).run(steps=2, sigma=0.5)
+
+
+def gloo_transport_rank(rank, world, port, out_dir):
+    import ctypes as C
+
+    import torch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world,
+                                         timeout=datetime.timedelta(seconds=20))
+    tr = shd.TorchTransport(device="cpu")
+    lines = []
+    # the callbacks as the library calls them: through the struct's pointers
+    v = (C.c_longlong * 4)(1, -2, 3 + rank, 1 << 40)
+    lines.append(str(tr.struct.allreduce_i64(None, v, 4)) + " " + " ".join(str(x) for x in v))
+    d = (C.c_double * 3)(0.5, -1.25 * (rank + 1), 1e300)
+    lines.append(str(tr.struct.allreduce_f64(None, d, 3)) + " " + " ".join(repr(x) for x in d))
+    torch.distributed.destroy_process_group()
+    # without a process group the call fails: a status, not an exception
+    # through the C frames, and the cause kept for the caller
+    status = tr.struct.allreduce_i64(None, v, 4)
+    lines.append(f"{status} {type(tr.error).__name__ if tr.error is not None else None}")
+    with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as f:
+        f.write("\n".join(lines))
+
+
+def test_torch_transport_sums_over_gloo_ranks(tmp_path):
+    """The native shard's torch.distributed transport: its C callbacks sum
+    int64 and float64 vectors over every rank in place, and report a failed
+    collective as DSX_E_RUNTIME with the exception kept for the caller."""
+    mp.start_processes(gloo_transport_rank, args=(2, free_port(), str(tmp_path)), nprocs=2,
+                       start_method="spawn")
+    for rank in range(2):
+        i64, f64, fail = open(os.path.join(tmp_path, f"rank{rank}.txt")).read().split("\n")
+        assert i64.split() == ["0", "2", "-4", "7", str(2 << 40)]
+        assert f64.split() == ["0", "1.0", "-3.75", "2e+300"]
+        assert fail.split()[0] == "-3" and fail.split()[1] != "None"
