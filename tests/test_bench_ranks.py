@@ -61,6 +61,36 @@ def test_reference_arm_runs_on_rank_zero_only():
     assert p.stdout.strip() == ""
 
 
+def test_reference_arm_line():
+    """Rank 0 of the reference arm prints one JSON line with the contract's
+    keys: the reference Host path's rate as value, cpu_baseline and e2e
+    describing the same run, no host-device bytes (one-rank workload, a
+    second of CPU work)."""
+    import oracle
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--workload", "drop_in_1rank", "--steps", "1", "--warmup", "1"],
+                       env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    lines = p.stdout.strip().splitlines()
+    assert len(lines) == 1, p.stdout
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference"
+    if not oracle.available("ref"):
+        assert "unavailable" in line
+        return
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["config"]["workload"] == "drop_in_1rank"
+    base = line["cpu_baseline"]
+    assert base["kind"] == "reference" and base["value"] == line["value"] and base["cores"] == 1
+    assert base["unit"] == line["unit"] and base["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+
+
 def test_shard_factors_cover_the_rank_count():
     """bench.py's weak-scaling layout: N ranks as (a, b, c) blocks of the
     workload, a * b * c = N, the prime factors spread over the axes."""
