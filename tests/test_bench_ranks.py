@@ -1,9 +1,11 @@
-"""Host logic of bench.py's multi-process path, on CPU with gloo.
+"""Host logic of bench.py, on CPU (no GPU).
 
 bench.py --gpus N runs one process per GPU (the sharded grid, one block of
 subdomains per rank, weak scaling): every rank times its own steps and the
-job reports the slowest rank's time; the reference arm runs on rank 0 only.
-Both are checked here with two gloo ranks and no GPU.
+job reports the slowest rank's time; the reference arm runs on rank 0 only
+and prints the contract's line.  Both are checked here, the first with two
+gloo ranks.  The clock sampler that fills the line's `clocks` runs against an
+nvidia-smi stand-in.
 """
 import json
 import os
@@ -120,3 +122,43 @@ def test_sharded_process_grids_are_blocks_of_the_workload():
         upper = tuple(u * k for u, k in zip(w.upper, fa))
         dims, _ = dsx.plan_topology(w.nranks * n, 0, (0, 0, 0), w.policy, w.lower, upper)
         assert tuple(dims) == tuple(d * k for d, k in zip(block, fa)), (n, dims)
+
+
+def _fake_nvidia_smi(tmp_path, row):
+    """An nvidia-smi stand-in on PATH that prints `row` every 10 ms."""
+    tool = tmp_path / "nvidia-smi"
+    tool.write_text("#!/bin/sh\nwhile true; do echo '%s'; sleep 0.01; done\n" % row)
+    tool.chmod(0o755)
+    return dict(os.environ, PATH=str(tmp_path) + os.pathsep + os.environ.get("PATH", ""))
+
+
+def _sample(env):
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+    old = os.environ["PATH"]
+    os.environ["PATH"] = env["PATH"]
+    try:
+        with bench.ClockSampler(0) as clocks:
+            time.sleep(0.2)
+        return clocks.summary()
+    finally:
+        os.environ["PATH"] = old
+
+
+def test_clock_sampler_reads_clocks_and_reasons(tmp_path):
+    """The sampler behind the bench line's `clocks`: the median SM clock, the
+    maximum, and every throttle reason seen active during the region."""
+    capped = _sample(_fake_nvidia_smi(
+        tmp_path, "0, 1965, 1965, 990.10, 0x4, Not Active, Not Active, Not Active, Active"))
+    assert capped["sm_mhz"] == 1965.0 and capped["sm_max_mhz"] == 1965.0
+    assert capped["reasons"] == ["sw_power_cap"] and capped["samples"] >= 1
+    slowed = _sample(_fake_nvidia_smi(
+        tmp_path, "0, 1200, 1965, 500.00, 0x8, Active, Active, Not Active, Not Active"))
+    assert slowed["sm_mhz"] == 1200.0
+    assert slowed["reasons"] == ["hw_slowdown", "hw_thermal_slowdown"]
+
+
+def test_clock_sampler_without_nvidia_smi(tmp_path):
+    env = dict(os.environ, PATH=str(tmp_path))   # no nvidia-smi anywhere on PATH
+    assert _sample(env)["reasons"] == ["unavailable"]
