@@ -386,12 +386,9 @@ def run_ours(args, rank, world, device):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded numpy PCG64 + counter-based device deviates)",
-        "config": {"workload": w.name, "description": w.description, "subdomains": w.nranks,
-                   "grid": list(dims), "particles": N, "record_bytes": S,
-                   "step": "graph-captured batched step (dsx_grid_step)",
-                   "l2": "inputs larger than L2 (%.2f GB of owned records)" % (N * S / 1e9),
-                   "parallelism": "1 GPU",
-                   "autotune": tune},
+        "config": workload_config(w, world, dims),
+        "step": "graph-captured batched step (dsx_grid_step)",
+        "autotune": tune,
         "roofline": roof,
         "step_roofline": {"algorithmic_bytes": int(step_bytes),
                           "kernels_ms": round(ours_ms, 4),
@@ -743,14 +740,10 @@ def run_sharded(args, rank, world, device):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded numpy PCG64 + counter-based device deviates)",
-        "config": {"workload": w.name, "description": w.description + f"; one block per GPU, "
-                   f"{fa[0]}x{fa[1]}x{fa[2]} blocks", "subdomains": P, "grid": list(dims),
-                   "particles": Ntot, "record_bytes": S,
-                   "step": ("native sharded grid (dsx_shard_*" if native else
-                            "sharded grid (ShardedGrid") + ": per-call operations, one NCCL "
-                           "exchange step per call)",
-                   "l2": "inputs larger than L2 (%.2f GB of owned records per GPU)" % (N * S / 1e9),
-                   "parallelism": f"subdomain blocks x{world}"},
+        "config": workload_config(w, world, dims),
+        "step": ("native sharded grid (dsx_shard_*" if native else
+                 "sharded grid (ShardedGrid") + ": per-call operations, one NCCL "
+                "exchange step per call)",
         "roofline": roof,
         "clocks": clock,
         "e2e": e2e,
@@ -868,52 +861,120 @@ def run_drop_in(args, w, wl, stream, rank, world):
             "unit": "M particles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w.name, "description": w.description,
-                       "step": "drift + dsx_rank_migrate (one rank: no ghosts, as in the reference)",
-                       "l2": "L2 flushed (256 MB write) before every timed step"},
+            "config": workload_config(w, world, (1, 1, 1)),
+            "step": "drift + dsx_rank_migrate (one rank: no ghosts, as in the reference)",
             "clocks": clocks.summary(), "gpu_launches": 3 * args.steps, "roofline": roof,
             "e2e": e2e}
 
 
 # --------------------------------------------------------- reference (CPU)
 
-def reference_rate(w, seed, steps, warmup, budget_s=120.0):
+def load_workloads():
+    """The workload definitions (numpy only), loaded from their file: the
+    reference arm imports nothing of the product package or its library."""
+    import importlib.util
+    name = "dsx_bench_workloads"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(ROOT, "dsdecompx_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(w, world, dims):
+    """The `config` object of the bench line: the workload alone (box, grid,
+    particles, record), identical for both arms at the same N."""
+    S = w.record_bytes()
+    fa = shard_factors(world)
+    cfg = {"workload": w.name, "description": w.description, "subdomains": w.nranks * world,
+           "grid": [int(d) for d in dims], "particles": w.particles * world, "record_bytes": S}
+    if world > 1:
+        cfg["description"] += f"; one block per GPU, {fa[0]}x{fa[1]}x{fa[2]} blocks"
+    if w.nranks == 1:
+        cfg["l2"] = "L2 flushed (256 MB write) before every timed step"
+    else:
+        cfg["l2"] = "inputs larger than L2 (%.2f GB of owned records per GPU)" % (
+            w.particles * S / 1e9)
+    cfg["parallelism"] = "1 GPU" if world == 1 else f"subdomain blocks x{world}"
+    return cfg
+
+
+def reference_sample(W, w, world, seed, per_block):
+    """Host arrays and initial owners of `per_block` particles per GPU block
+    of the workload grown to `world` blocks (world 1: the workload itself),
+    drawn as the GPU arm draws them."""
+    import numpy as np
+    fa = shard_factors(world)
+    upper = tuple(u * k for u, k in zip(w.upper, fa))
+    parts = []
+    for rank in range(world):
+        d = W.generate(w, seed=seed + 7919 * rank if world > 1 else seed, particles=per_block)
+        k3 = (rank // (fa[1] * fa[2]), (rank // fa[2]) % fa[1], rank % fa[2])
+        for a, name in enumerate("xyz"):
+            d[name] = d[name] + k3[a] * w.upper[a]
+        d["global_id"] = (d["global_id"] + rank * per_block).astype(np.int32)
+        if "id64" in d:
+            d["id64"] = d["id64"] + rank * per_block
+        d["_block"] = np.full(per_block, rank, dtype=np.int64)
+        parts.append(d)
+    data = {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+    return data, upper
+
+
+def reference_rate(w, world, seed, steps, warmup, budget_s=150.0):
     """The reference's own Host path (oracle/_ref, built from its sources)
     with one thread per subdomain: M particles/s of migrate + exchange_halo
     (rebuild) + reverse_halo, timed like its communication_test (slowest rank
-    per call), on a sample of the workload sized to fit `budget_s`."""
+    per call), `steps` timed steps after `warmup`, on a sample of the workload
+    sized so that all of them fit `budget_s`.  Returns (cpu_baseline, dims,
+    seconds per step) or (None, reason, None)."""
     import numpy as np
 
     import oracle
-    from dsdecompx_b200 import workloads as W
 
     if not oracle.available("ref"):
-        return None, "reference build oracle/_ref/libdsx_ref.so is missing"
-    import dsdecompx_b200 as dsx
-    dims, _ = dsx.plan_topology(w.nranks, 0, w.dims, w.policy, w.lower, w.upper)
+        return None, "reference build oracle/_ref/libdsx_ref.so is missing", None
+    W = load_workloads()
+    P = w.nranks * world
+    fa = shard_factors(world)
     fields = [(n, ["int32", "int64", "uint32", "uint64", "float32", "float64"].index(t), c)
               for n, t, c in w.fields]
+    manual_dims = tuple(d * k for d, k in zip(w.dims, fa)) if w.policy == "manual" else (0, 0, 0)
 
-    def run(n_sample, nsteps, nwarm):
-        data = W.generate(w, seed=seed, particles=n_sample)
-        owner = W.initial_owner(w, dims, data["x"], data["y"], data["z"])
-        counts = np.bincount(owner, minlength=w.nranks)
-        cap = int(max(4 * counts.max(), 3 * n_sample // w.nranks) + 4096)
-        g = oracle.Grid("ref", w.nranks, w.dims, w.policy, w.lower, w.upper, (True,) * 3, w.halo,
-                        fields=fields, field_capacity=cap)
-        for r in range(w.nranks):
-            m = owner == r
-            g.set_owned(r, {k: v[m] for k, v in data.items()})
+    def run(per_block, nsteps, nwarm):
+        data, upper = reference_sample(W, w, world, seed, per_block)
+        n_sample = len(data["x"])
+        block = data.pop("_block")
+        g = oracle.Grid("ref", P, manual_dims, w.policy, w.lower, upper, (True,) * 3, w.halo,
+                        fields=fields, field_capacity=int(6 * n_sample // P + 4096))
+        dims = g.topology(0)[0]
+        bdims = [d // k for d, k in zip(dims, fa)]
+        k3 = np.stack([block // (fa[1] * fa[2]), (block // fa[2]) % fa[1], block % fa[2]])
+        cell = []
+        for a, name in enumerate("xyz"):
+            rel = np.floor((data[name] - w.lower[a]) / (upper[a] - w.lower[a]) * dims[a])
+            cell.append(np.clip(rel.astype(np.int64), k3[a] * bdims[a],
+                                (k3[a] + 1) * bdims[a] - 1))
+        owner = (cell[0] * dims[1] + cell[1]) * dims[2] + cell[2]
+        order = np.argsort(owner, kind="stable")
+        bounds = np.searchsorted(owner[order], np.arange(P + 1))
+        for r in range(P):
+            idx = order[bounds[r]:bounds[r + 1]]
+            g.set_owned(r, {k: v[idx] for k, v in data.items()})
+        del data, owner, order
         rng = np.random.default_rng(seed + 1)
         times = []
         for step in range(nwarm + nsteps):
-            for r in range(w.nranks):       # drift (harness, not timed)
+            for r in range(P):              # drift (harness, not timed)
                 o, _ = g.counts(r)
                 if o:
                     for name in "xyz":
                         g.write(r, name, 0, g.read(r, name, 0, o) + rng.normal(0, w.drift, o))
             t = g.timed("migrate") + g.timed("halo_rebuild")
-            for r in range(w.nranks):       # ghost forces (harness, not timed)
+            for r in range(P):              # ghost forces (harness, not timed)
                 o, gh = g.counts(r)
                 for name in ("fx", "fy", "fz"):
                     g.write(r, name, o, rng.normal(size=gh))
@@ -921,20 +982,20 @@ def reference_rate(w, seed, steps, warmup, budget_s=120.0):
             if step >= nwarm:
                 times.append(t)
         g.close()
-        return n_sample / statistics.mean(times) / 1e6, statistics.mean(times)
+        return n_sample, n_sample / statistics.mean(times) / 1e6, statistics.mean(times), dims
 
-    probe_n = min(w.particles, 1_000_000)
-    rate, _ = run(probe_n, 1, 1)
+    probe = min(w.particles, max(1, 1_000_000 // world))
+    _, rate, _, _ = run(probe, 1, 1)
     # size the sample so that (steps + warmup) steps fit the budget
     per_particle = 1.0 / (rate * 1e6)
-    n_sample = int(min(w.particles, max(probe_n, budget_s / (steps + warmup) / per_particle)))
-    rate, step_s = run(n_sample, steps, warmup)
-    sample = (f"{n_sample} of the {w.particles}-particle {w.name} workload (same box, grid, halo "
-              f"and distributions), {steps} timed steps after {warmup} warm-up; "
-              f"{w.nranks} thread-ranks on {os.cpu_count()} host CPUs; "
-              f"{step_s:.3f} s per step")
-    return {"value": round(rate, 4), "unit": "M particles/s", "cores": w.nranks,
-            "kind": "reference", "sample": sample}, None
+    per_block = int(min(w.particles,
+                        max(probe, budget_s / max(1, steps + warmup) / per_particle / world)))
+    n_sample, rate, step_s, dims = run(per_block, steps, warmup)
+    sample = (f"{n_sample} of the {w.particles * world}-particle {w.name} workload (same box, "
+              f"grid, halo and distributions), {steps} timed steps after {warmup} warm-up; "
+              f"{P} thread-ranks on {os.cpu_count()} host CPUs; {step_s:.3f} s per step")
+    return ({"value": round(rate, 4), "unit": "M particles/s", "cores": P,
+             "kind": "reference", "sample": sample}, dims, step_s)
 
 
 def main():
@@ -943,19 +1004,27 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
+        # the reference's Host path on the host cores, on this arm's config
+        # (the workload grown to --gpus blocks); rank 0 alone runs it
         if rank != 0:
             return
-        from dsdecompx_b200 import workloads as W
+        W = load_workloads()
         w = W.WORKLOADS[args.workload]
-        base, why = reference_rate(w, args.seed, max(1, min(args.steps, 5)), 1)
+        if args.particles:
+            import dataclasses
+            w = dataclasses.replace(w, particles=args.particles)
+        base, dims, step_s = reference_rate(w, args.gpus, args.seed, args.steps, args.warmup)
         if base is None:
-            print(json.dumps({"impl": "reference", "unavailable": why}))
+            print(json.dumps({"impl": "reference", "unavailable": dims}))
             return
         line = {"metric": METRIC, "value": base["value"], "unit": base["unit"],
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(step_s * 1e3, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "impl": "reference",
-                "config": {"workload": w.name, "description": w.description},
+                "data": "synthetic (seeded numpy PCG64)", "impl": "reference",
+                "config": workload_config(w, args.gpus, dims),
+                "step": "reference Host path (oracle/_ref): migrate + exchange_halo(rebuild) + "
+                        "reverse_halo, one thread per subdomain",
                 "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": base["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
@@ -985,8 +1054,12 @@ def main():
         line = run_ours(args, rank, world, local)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            from dsdecompx_b200 import workloads as W
-            base, why = reference_rate(W.WORKLOADS[args.workload], args.seed, 2, 1, budget_s=25.0)
+            W = load_workloads()
+            w = W.WORKLOADS[args.workload]
+            if args.particles:
+                import dataclasses
+                w = dataclasses.replace(w, particles=args.particles)
+            base, why, _ = reference_rate(w, 1, args.seed, 2, 1, budget_s=25.0)
             line["cpu_baseline"] = base if base else {"unavailable": why}
         print(json.dumps(line))
 

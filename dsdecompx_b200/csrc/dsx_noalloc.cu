@@ -10,8 +10,10 @@
 // dsx_grid (which allocates its storage once), so this entry point takes
 // inputs and outputs from the caller and keeps its scratch (layout tables,
 // per-tile counters, the emigrant list) in one file-scope device array of a
-// fixed size, reserved on every GPU that loads the library until the process
-// exits.
+// fixed size.  The driver places that array on a device when it loads the
+// library's device code there: at the first call on that device with lazy
+// module loading (CUDA's default), or at library load with eager loading.
+// From then on it is held until the process exits.
 //
 // Limits: at most kMaxRanks subdomains and kMaxParticles particles; core
 // arrays only (no registered fields); the cuts are an input, so there is no
@@ -23,6 +25,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -49,7 +52,9 @@ constexpr std::size_t info = align256(results + kMaxRanks * 6 * 8);        // 4 
 constexpr std::size_t total = align256(info + 4 * 4);
 }  // namespace Layout
 
-// The scratch: about 2.2 MB per GPU, held from library load to process exit.
+// The scratch: about 2.2 MB per GPU, placed on a device when the library's
+// device code is loaded there (the first call, with lazy loading) and held
+// until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[Layout::total];
 
 // tables: 0 n_in, 1 obase_in, 2 tile_start_in, 3 imm_total, 4 n_out,
@@ -334,7 +339,13 @@ int dsx_migrate_noalloc(const dsx_grid_desc* desc, const double* cuts, const lon
         return noalloc_fail(error, error_capacity, DSX_E_LENGTH,
                             "dsx_migrate_noalloc handles 1 to 64 subdomains", P);
     const int dims[3] = {desc->dims[0], desc->dims[1], desc->dims[2]};
-    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || dims[0] * dims[1] * dims[2] != P)
+    // each factor is checked against P before the product is formed, so the
+    // product cannot overflow (and the cut tables below cannot be overrun)
+    for (int a = 0; a < 3; ++a)
+        if (dims[a] < 1 || dims[a] > P)
+            return noalloc_fail(error, error_capacity, DSX_E_INVALID,
+                                "dsx_migrate_noalloc needs explicit dims whose product is nranks");
+    if (static_cast<long long>(dims[0]) * dims[1] * dims[2] != P)
         return noalloc_fail(error, error_capacity, DSX_E_INVALID,
                             "dsx_migrate_noalloc needs explicit dims whose product is nranks");
     long long total = 0;
@@ -349,6 +360,19 @@ int dsx_migrate_noalloc(const dsx_grid_desc* desc, const double* cuts, const lon
         if (total && (!arrays_in[a] || !arrays_out[a]))
             return noalloc_fail(error, error_capacity, DSX_E_INVALID,
                                 "dsx_migrate_noalloc needs all 13 core arrays in and out");
+    // Inputs and outputs must not overlap: the kernels read the inputs while
+    // other CTAs write the outputs.
+    const std::size_t elem[13] = {8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 4, 4};
+    for (int a = 0; a < 13 && total; ++a)
+        for (int b = 0; b < 13; ++b) {
+            const auto in_lo = reinterpret_cast<std::uintptr_t>(arrays_in[a]);
+            const auto out_lo = reinterpret_cast<std::uintptr_t>(arrays_out[b]);
+            const std::uintptr_t in_hi = in_lo + elem[a] * static_cast<std::size_t>(total);
+            const std::uintptr_t out_hi = out_lo + elem[b] * static_cast<std::size_t>(total);
+            if (in_lo < out_hi && out_lo < in_hi)
+                return noalloc_fail(error, error_capacity, DSX_E_INVALID,
+                                    "dsx_migrate_noalloc: input and output arrays overlap");
+        }
     Box B{};
     B.P = P;
     double host_cuts[3 * (kMaxRanks + 1)];
@@ -365,6 +389,14 @@ int dsx_migrate_noalloc(const dsx_grid_desc* desc, const double* cuts, const lon
             host_cuts[ncuts] = cuts ? cuts[ncuts]
                                     : desc->lower[a] + B.extent[a] * static_cast<double>(i) /
                                                            static_cast<double>(dims[a]);
+        // the rule of dsx_grid_set_cuts (Decomposition::set_axis_cuts,
+        // dsDecompX src/decomp.cpp:146-163): span the domain, increase strictly
+        const double* c = host_cuts + B.cut_offset[a];
+        bool ok = c[0] == desc->lower[a] && c[dims[a]] == desc->upper[a];
+        for (int i = 0; i < dims[a]; ++i) ok = ok && c[i] < c[i + 1];
+        if (!ok)
+            return noalloc_fail(error, error_capacity, DSX_E_INVALID,
+                                "cuts must be strictly increasing and span the domain");
     }
     // Once per device, with that device current: the device address of the
     // scratch array (in host code its name is only a host-side stand-in).

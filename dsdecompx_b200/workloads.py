@@ -5,6 +5,10 @@ box, process grid, halo width, particle count and value distributions, and
 the particles are drawn here with numpy's PCG64 generator from a fixed seed.
 The per-step drift and ghost forces are drawn on the device by the harness
 kernels of ``workload/workload.cu`` (counter-based, keyed by particle id).
+
+The module needs only numpy until :func:`harness` is called, so a CPU-only
+caller (the reference timing in ``bench.py``) can load it from its file
+without importing the package or its native library.
 """
 from __future__ import annotations
 
@@ -14,8 +18,6 @@ from dataclasses import dataclass, field
 from typing import Dict, List, Tuple
 
 import numpy as np
-
-from . import _build
 
 
 @dataclass
@@ -123,6 +125,7 @@ def harness() -> C.CDLL:
     """The synthetic drift / ghost-force kernels."""
     global _WL
     if _WL is None:
+        from . import _build
         path = _build.WORKLOAD_LIB
         if not os.path.exists(path):
             raise RuntimeError(f"{path} is missing: run __graft_entry__.build()")

@@ -406,11 +406,14 @@ int dsx_grid_step_kernel_count(dsx_grid* grid);
  * synchronizes `stream`.
  *
  * Limits: at most 64 subdomains and 262144 particles (DSX_E_LENGTH beyond).
- * Scratch: one fixed 2.2 MB device array inside the library, reserved on every
- * GPU that loads it until the process exits; nothing else is allocated.  The
- * first call on a device looks up that array's device address (and may make
- * the driver load the library's device code): make the first call before any
- * CUDA-graph capture.  All calls share the array and it keeps the previous
+ * Input and output arrays must not overlap (DSX_E_INVALID otherwise); cuts
+ * must span the domain and increase strictly, as for dsx_grid_set_cuts.
+ * Scratch: one fixed 2.2 MB device array inside the library, placed on a GPU
+ * at the first call there (or when the library's device code is loaded, if
+ * module loading is eager) and held until the process exits; nothing else is
+ * allocated.  The first call on a device looks up that array's device address
+ * (and may make the driver load the library's device code): make the first
+ * call before any CUDA-graph capture.  All calls share the array and it keeps the previous
  * call's contents, so calls that overlap on the GPU (other streams or host
  * threads) race: serialize them.  Errors: a DSX_E_* code and, if `error` is
  * not null, a message in the caller's buffer of `error_capacity` bytes. */

@@ -121,3 +121,64 @@ def test_struct_layouts_match_headers(tmp_path):
         assert size == want[(name, "size")], (name, size, want[(name, "size")])
         for f, off in offsets.items():
             assert off == want[(name, f)], (name, f, off, want[(name, f)])
+
+
+def _noalloc():
+    import ctypes as C
+    fn = dsx.lib().dsx_migrate_noalloc
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(dsx._GridDesc), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                   C.POINTER(C.c_void_p), C.POINTER(C.c_longlong), C.POINTER(C.c_void_p),
+                   C.POINTER(C.c_longlong), C.c_void_p, C.c_char_p, C.c_int]
+    return fn
+
+
+def _noalloc_call(nranks, dims, counts, ins, outs, cuts=None, upper=(10.0, 10.0, 10.0)):
+    """Calls that the entry point refuses on the host, before any CUDA call."""
+    import ctypes as C
+
+    import numpy as np
+    desc = dsx._grid_desc(nranks, dims, "manual", (0, 0, 0), upper, (True, True, True),
+                          1.0, True, None)
+    counts = np.asarray(counts, dtype=np.int64)
+    out = np.zeros(max(nranks, 1), dtype=np.int64)
+    err = C.create_string_buffer(256)
+    cut_arg = None
+    if cuts is not None:
+        cuts = np.ascontiguousarray(cuts, dtype=np.float64)
+        cut_arg = cuts.ctypes.data_as(C.POINTER(C.c_double))
+    status = _noalloc()(C.byref(desc), cut_arg, counts.ctypes.data_as(C.POINTER(C.c_longlong)),
+                        (C.c_void_p * 13)(*ins), out.ctypes.data_as(C.POINTER(C.c_longlong)),
+                        (C.c_void_p * 13)(*outs), None, None, err, 256)
+    return status, err.value
+
+
+def test_noalloc_refuses_overflowing_dims():
+    # 3 * 1431655768 * 1 wraps to 8 in 32-bit arithmetic
+    status, msg = _noalloc_call(8, (3, 1431655768, 1), [0] * 8, [0] * 13, [0] * 13)
+    assert status == -1 and b"dims whose product is nranks" in msg
+    status, msg = _noalloc_call(8, (2, 2, 3), [0] * 8, [0] * 13, [0] * 13)
+    assert status == -1
+
+
+def test_noalloc_refuses_overlapping_arrays():
+    base = 1 << 40            # never dereferenced: the call refuses first
+    ins = [base + 0x100000 * a for a in range(13)]
+    outs = [base + 0x4000000 + 0x100000 * a for a in range(13)]
+    outs[5] = ins[5] + 64     # output 5 starts inside input 5
+    status, msg = _noalloc_call(1, (1, 1, 1), [1000], ins, outs)
+    assert status == -1 and b"overlap" in msg
+    outs[5] = ins[12]         # aliasing across arrays of different widths
+    status, msg = _noalloc_call(1, (1, 1, 1), [1000], ins, outs)
+    assert status == -1 and b"overlap" in msg
+
+
+@pytest.mark.parametrize("cuts", [
+    [0.0, 0.0, 10.0, 0.0, 10.0, 0.0, 10.0],     # x cuts not strictly increasing
+    [0.0, 11.0, 10.0, 0.0, 10.0, 0.0, 10.0],    # x cuts decrease
+    [1.0, 5.0, 10.0, 0.0, 10.0, 0.0, 10.0],     # x cuts do not start at lower
+    [0.0, 5.0, 10.0, 0.0, 9.0, 0.0, 10.0],      # y cuts do not end at upper
+])
+def test_noalloc_refuses_bad_cuts(cuts):
+    status, msg = _noalloc_call(2, (2, 1, 1), [0, 0], [0] * 13, [0] * 13, cuts=cuts)
+    assert status == -1 and b"strictly increasing and span" in msg

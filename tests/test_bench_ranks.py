@@ -13,6 +13,7 @@ import socket
 import subprocess
 import sys
 
+import pytest
 import torch.multiprocessing as mp
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -91,6 +92,36 @@ def test_reference_arm_line():
     assert base["unit"] == line["unit"] and base["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+    # the same config object as the GPU arm prints, and the declared step counts
+    sys.path.insert(0, ROOT)
+    import bench
+    w = bench.load_workloads().WORKLOADS["drop_in_1rank"]
+    assert line["config"] == bench.workload_config(w, 1, (1, 1, 1))
+    assert line["steps"] == 1 and line["warmup"] == 1 and line["ms_per_step"] > 0
+    assert "1 timed steps after 1 warm-up" in base["sample"]
+
+
+def test_reference_arm_loads_nothing_of_the_product():
+    """The reference arm runs the reference build alone: no module of the
+    product package is imported and no library of it is mapped."""
+    import oracle
+    if not oracle.available("ref"):
+        pytest.skip("reference build not present")
+    probe = (
+        "import runpy, sys\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'clustered_64',\n"
+        "            '--steps', '1', '--warmup', '1', '--particles', '20000']\n"
+        "runpy.run_path('bench.py', run_name='__main__')\n"
+        "mods = sorted(m for m in sys.modules if m.startswith('dsdecompx_b200'))\n"
+        "maps = sorted({l.split()[-1] for l in open('/proc/self/maps') if l.rstrip().endswith('.so')})\n"
+        "print('PROBE', mods, [m for m in maps if 'dsdecompx_b200' in m], file=sys.stderr)\n")
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    p = subprocess.run([sys.executable, "-c", probe], cwd=ROOT, env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    assert "PROBE [] []" in p.stderr, p.stderr[-2000:]
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["config"]["subdomains"] == 64 and line["config"]["grid"] == [4, 4, 4]
 
 
 def test_shard_factors_cover_the_rank_count():

@@ -8,7 +8,8 @@ synchronization.  Its scratch lives in one fixed device array inside the
 library, so the checks here are: the same result as the existing entry point
 (bit for bit, as every parity test in this suite), on two calls in a row (the
 second call sees the scratch the first one left behind), and no change in the
-device's free memory across the second call.
+device's free memory across the second call, with uniform cuts and with
+explicit non-uniform cuts (the latter against a grid given the same cuts).
 """
 import ctypes as C
 
@@ -36,7 +37,12 @@ def make_desc(nranks=P, dims=DIMS):
                           1.0, True, None)
 
 
-def test_noalloc_migrate_matches_grid_migrate(cuda):
+# non-uniform cuts (3 per axis: lower, one interior plane, upper)
+CUTS = np.array([0.0, 3.5, 10.0, 0.0, 6.25, 10.0, 0.0, 4.0, 10.0])
+
+
+@pytest.mark.parametrize("cuts", [None, CUTS], ids=["uniform", "explicit_cuts"])
+def test_noalloc_migrate_matches_grid_migrate(cuda, cuts):
     import torch
 
     import dsdecompx_b200 as dsx
@@ -44,7 +50,10 @@ def test_noalloc_migrate_matches_grid_migrate(cuda):
 
     rng = np.random.default_rng(77)
     pos = rng.uniform(0, L, size=(N, 3))
-    owner = Grid("port", P, DIMS, "manual", (0, 0, 0), (L, L, L)).owner_rank(pos)
+    shape = Grid("port", P, DIMS, "manual", (0, 0, 0), (L, L, L))
+    if cuts is not None:
+        shape.set_cuts(np.split(cuts, 3))
+    owner = shape.owner_rank(pos)
     order = np.argsort(owner, kind="stable")
     counts = np.bincount(owner, minlength=P).astype(np.int64)
     host = {"x": pos[order, 0], "y": pos[order, 1], "z": pos[order, 2]}
@@ -55,6 +64,10 @@ def test_noalloc_migrate_matches_grid_migrate(cuda):
     host["global_id"] = order.astype(np.int32)
 
     grid = dsx.VirtualGrid(P, DIMS, "manual", (0, 0, 0), (L, L, L), halo_width=1.0, particles=N)
+    if cuts is not None:
+        grid.set_cuts(np.split(cuts, 3))
+    cut_arg = None if cuts is None else np.ascontiguousarray(cuts).ctypes.data_as(
+        C.POINTER(C.c_double))
     starts = np.concatenate([[0], np.cumsum(counts)])
     grid.upload([{k: v[starts[r]:starts[r + 1]] for k, v in host.items()} for r in range(P)])
 
@@ -65,7 +78,6 @@ def test_noalloc_migrate_matches_grid_migrate(cuda):
     stream = torch.cuda.current_stream().cuda_stream
     counts_in = counts.copy()
     err = C.create_string_buffer(256)
-    free_after_first = None
     for call in range(2):
         # the same displacement for both paths, in rank order
         delta = rng.normal(0.0, 0.8, size=(N, 3))
@@ -82,15 +94,19 @@ def test_noalloc_migrate_matches_grid_migrate(cuda):
         results = np.zeros((P, 6), dtype=np.int64)
         ins = (C.c_void_p * 13)(*[t.data_ptr() for t in dev_in])
         outs = (C.c_void_p * 13)(*[t.data_ptr() for t in dev_out])
-        status = fn(C.byref(desc), None, counts_in.ctypes.data_as(C.POINTER(C.c_longlong)), ins,
-                    counts_out.ctypes.data_as(C.POINTER(C.c_longlong)), outs,
-                    results.ctypes.data_as(C.POINTER(C.c_longlong)), stream, err, 256)
-        assert status == 0, err.value
+        # the free-memory window covers the entry point alone
         torch.cuda.synchronize()
-        if call == 0:
-            free_after_first = torch.cuda.mem_get_info()[0]
-        else:
-            assert torch.cuda.mem_get_info()[0] == free_after_first, "the call allocated device memory"
+        free_before = torch.cuda.mem_get_info()[0]
+        status = fn(C.byref(desc), cut_arg, counts_in.ctypes.data_as(C.POINTER(C.c_longlong)),
+                    ins, counts_out.ctypes.data_as(C.POINTER(C.c_longlong)), outs,
+                    results.ctypes.data_as(C.POINTER(C.c_longlong)), stream, err, 256)
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        assert status == 0, err.value
+        if call == 1:
+            # the first call may load the library's device code (and with it
+            # the scratch array); the second must leave free memory unchanged
+            assert free_after == free_before, "the call allocated device memory"
 
         assert (results == expect).all(), (results, expect)
         assert (counts_out == expect[:, 5]).all()
