@@ -948,9 +948,10 @@ def reference_rate(w, world, seed, steps, warmup, budget_s=150.0):
         data, upper = reference_sample(W, w, world, seed, per_block)
         n_sample = len(data["x"])
         block = data.pop("_block")
-        g = oracle.Grid("ref", P, manual_dims, w.policy, w.lower, upper, (True,) * 3, w.halo,
-                        fields=fields, field_capacity=int(6 * n_sample // P + 4096))
-        dims = g.topology(0)[0]
+        # the process grid first (the reference's own planner), then the
+        # owners, then the grid with field storage sized by the largest rank
+        with oracle.Grid("ref", P, manual_dims, w.policy, w.lower, upper) as probe_grid:
+            dims = probe_grid.topology(0)[0]
         bdims = [d // k for d, k in zip(dims, fa)]
         k3 = np.stack([block // (fa[1] * fa[2]), (block // fa[2]) % fa[1], block % fa[2]])
         cell = []
@@ -961,6 +962,9 @@ def reference_rate(w, world, seed, steps, warmup, budget_s=150.0):
         owner = (cell[0] * dims[1] + cell[1]) * dims[2] + cell[2]
         order = np.argsort(owner, kind="stable")
         bounds = np.searchsorted(owner[order], np.arange(P + 1))
+        cap = int(max(4 * np.diff(bounds).max(), 3 * n_sample // P) + 4096)
+        g = oracle.Grid("ref", P, manual_dims, w.policy, w.lower, upper, (True,) * 3, w.halo,
+                        fields=fields, field_capacity=cap)
         for r in range(P):
             idx = order[bounds[r]:bounds[r + 1]]
             g.set_owned(r, {k: v[idx] for k, v in data.items()})

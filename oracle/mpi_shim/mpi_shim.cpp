@@ -7,6 +7,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <memory>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -44,17 +45,25 @@ struct RequestState {
 
 using MailKey = std::tuple<int, int, int, int>;  // comm, source, dest, tag
 
+// One mailbox per destination rank: a send wakes only the rank it is
+// addressed to (a single shared condition variable would wake every waiting
+// rank on every message).
+struct Mailbox {
+    std::mutex mutex;
+    std::condition_variable cv;
+    std::map<MailKey, std::deque<std::vector<char>>> mail;
+};
+
 }  // namespace
 
 struct shim_world_t {
     int size = 1;
     std::mutex mutex;
-    std::condition_variable mail_cv;
     std::map<int, CommState*> comms;
     std::map<int, int> creation_handle;   // creation sequence -> handle
     std::vector<int> creation_sequence;   // per rank
     int next_handle = 16;
-    std::map<MailKey, std::deque<std::vector<char>>> mail;
+    std::vector<std::unique_ptr<Mailbox>> boxes;   // per destination rank
 };
 
 namespace {
@@ -196,6 +205,7 @@ shim_world* shim_world_create(int size) {
     auto* w = new shim_world();
     w->size = size;
     w->creation_sequence.assign(static_cast<std::size_t>(size), 0);
+    for (int r = 0; r < size; ++r) w->boxes.emplace_back(new Mailbox());
     auto* world_comm = new CommState();
     world_comm->handle = MPI_COMM_WORLD;
     world_comm->slot_a.assign(static_cast<std::size_t>(size), nullptr);
@@ -384,11 +394,16 @@ int MPI_Isend(const void* buffer, int count, MPI_Datatype type, int dest,
     std::vector<char> payload(bytes);
     if (bytes) std::memcpy(payload.data(), buffer, bytes);
     shim_world* w = world();
-    {
-        std::lock_guard<std::mutex> lock(w->mutex);
-        w->mail[MailKey{comm, tl_rank, dest, tag}].push_back(std::move(payload));
+    if (dest < 0 || dest >= w->size) {
+        std::fprintf(stderr, "mpi shim: send to rank %d of %d\n", dest, w->size);
+        std::abort();
     }
-    w->mail_cv.notify_all();
+    Mailbox& box = *w->boxes[static_cast<std::size_t>(dest)];
+    {
+        std::lock_guard<std::mutex> lock(box.mutex);
+        box.mail[MailKey{comm, tl_rank, dest, tag}].push_back(std::move(payload));
+    }
+    box.cv.notify_all();
     return MPI_SUCCESS;
 }
 
@@ -412,13 +427,14 @@ int MPI_Wait(MPI_Request* request, MPI_Status* status) {
     shim_world* w = world();
     std::vector<char> payload;
     {
-        std::unique_lock<std::mutex> lock(w->mutex);
+        Mailbox& box = *w->boxes[static_cast<std::size_t>(tl_rank)];
+        std::unique_lock<std::mutex> lock(box.mutex);
         const MailKey key{state->comm, state->source, tl_rank, state->tag};
-        w->mail_cv.wait(lock, [&] {
-            auto found = w->mail.find(key);
-            return found != w->mail.end() && !found->second.empty();
+        box.cv.wait(lock, [&] {
+            auto found = box.mail.find(key);
+            return found != box.mail.end() && !found->second.empty();
         });
-        auto& queue = w->mail[key];
+        auto& queue = box.mail[key];
         payload = std::move(queue.front());
         queue.pop_front();
     }
