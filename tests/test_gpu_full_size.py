@@ -1,5 +1,7 @@
 """The batched step at the benchmark workloads' full sizes, through
-properties that hold at any size (the oracle finishes only small cases):
+properties that hold at any size (these complement the element-by-element
+comparison with the reference's Host path at the same sizes in
+test_gpu_config_parity.py, over more drifted steps and after a rebuild):
 
 * ids are conserved: after every step the owned global ids are a
   permutation of 0..N-1;

@@ -365,6 +365,56 @@ def test_halo_backward_is_reverse_halo(cuda):
     pair.close()
 
 
+def test_halo_backward_is_the_references_reverse_halo(cuda):
+    """The adjoint of the ghost copy (dsx_grid_halo_backward) equals the
+    reference's own reverse_halo (oracle/_ref, src/halo.cpp:1288-1347) on
+    identical cotangents written as ghost forces, bit for bit."""
+    import torch
+
+    import oracle
+    assert oracle.available("ref"), "the reference build oracle/_ref is required"
+    lower, upper, halo = (0.0, 0.0, 0.0), (10.0, 10.0, 10.0), 1.2
+    pair = run_scenario(cuda, P=8, dims=(2, 2, 2), L=(10.0, 10.0, 10.0), halo=halo, N=5000,
+                        steps=1, seed=17, fields=())
+    gpu = pair.gpu
+    try:
+        gpu.exchange_halo(rebuild=True)
+        o, g = gpu.all_counts()
+        ob = np.concatenate([[0], np.cumsum(o)])
+        gb = np.concatenate([[0], np.cumsum(g)])
+        N, G = int(o.sum()), int(g.sum())
+        with oracle.Grid("ref", 8, (2, 2, 2), "manual", lower, upper, (True,) * 3, halo) as ref:
+            for r in range(8):
+                snap = gpu.snapshot(r)
+                ref.set_owned(r, {k: np.asarray(snap[k])[:o[r]]
+                                  for k in ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz",
+                                            "mass", "charge", "type", "global_id")})
+            ref.exchange_halo(rebuild=True)
+            for r in range(8):
+                assert ref.counts(r) == (o[r], g[r])
+                snap = gpu.snapshot(r)
+                for k in ("x", "y", "z", "global_id"):
+                    assert same(ref.read(r, k), snap[k]), (r, k)
+            gen = torch.Generator(device="cuda").manual_seed(5)
+            cot = torch.randn(3, G, dtype=torch.float64, device="cuda", generator=gen)
+            grad0 = torch.randn(3, N, dtype=torch.float64, device="cuda", generator=gen)
+            grad = grad0.clone()
+            gpu.halo_backward(cot, grad)
+            torch.cuda.synchronize()
+            cot_h, grad0_h, grad_h = cot.cpu().numpy(), grad0.cpu().numpy(), grad.cpu().numpy()
+            for r in range(8):
+                for j, name in enumerate(("fx", "fy", "fz")):
+                    ref.write(r, name, 0, grad0_h[j, ob[r]:ob[r + 1]])
+                    ref.write(r, name, int(o[r]), cot_h[j, gb[r]:gb[r + 1]])
+            ref.reverse_halo()
+            for r in range(8):
+                for j, name in enumerate(("fx", "fy", "fz")):
+                    assert same(ref.read(r, name, 0, int(o[r])), grad_h[j, ob[r]:ob[r + 1]]), \
+                        (r, name)
+    finally:
+        pair.close()
+
+
 @pytest.mark.parametrize("fields,particles,box,halo", [
     (ALL_FIELDS[:1], 300_000, 12.0, 0.6),
     (ALL_FIELDS[:2], 300_000, 12.0, 0.6),
