@@ -138,6 +138,7 @@ def lib() -> C.CDLL:
             "dsx_grid_set_cuts": [vp, C.POINTER(C.c_double), vp],
             "dsx_grid_owner_rank": [vp, vp, vp, vp, C.c_longlong, vp, vp],
             "dsx_grid_begin_halo_exchange": [vp, C.c_int, C.c_int, vp],
+            "dsx_grid_set_split_share": [vp, C.c_int],
             "dsx_grid_end_halo_exchange": [vp, vp, C.POINTER(C.c_longlong)],
             "dsx_grid_out_of_domain": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
             "dsx_grid_rescale_domain": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, vp],
@@ -510,6 +511,10 @@ class VirtualGrid:
         _check(self.L.dsx_grid_end_halo_exchange(self.h, _stream(stream),
                                                  res.ctypes.data_as(C.POINTER(C.c_longlong))))
         return res
+
+    def set_split_share(self, ctas_per_sm: int = 0):
+        """CTAs per SM the split-phase refresh may occupy (0: all resident)."""
+        _check(self.L.dsx_grid_set_split_share(self.h, int(ctas_per_sm)))
 
     def owner_rank(self, x, y, z, out, n: Optional[int] = None, stream=None):
         """Owning subdomain of n device positions into the int32 device array

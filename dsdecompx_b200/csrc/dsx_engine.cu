@@ -274,11 +274,48 @@ struct dsx_grid {
         if (pinned_status) cudaFreeHost(pinned_status);
     }
 
+    // Split-phase halo as two captured graph segments: segment 1 is the
+    // exchange itself, per {full refresh, positions-only refresh, build} and
+    // owned half; segment 2 the completion (status and totals to the host),
+    // per owned half.  Rebuilt like the step's graphs when the storage, the
+    // box or the launch shapes change.
+    cudaGraphExec_t split_begin[3][2] = {};
+    cudaGraphExec_t split_end[2] = {nullptr, nullptr};
+    int split_ctas_per_sm = 0;
+
     void destroy_graphs() {
         for (auto& g : graph) {
             if (g) cudaGraphExecDestroy(g);
             g = nullptr;
         }
+        for (auto& row : split_begin)
+            for (auto& g : row) {
+                if (g) cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        for (auto& g : split_end) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    }
+
+    // Captures `enqueue` into `exec` once, then launches it on `stream`.
+    template <class F>
+    void run_captured(cudaGraphExec_t& exec, cudaStream_t stream, F&& enqueue) {
+        if (!exec) {
+            cudaGraph_t g = nullptr;
+            cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            enqueue();
+            cuda_check(cudaStreamEndCapture(stream, &g), "end capture");
+            const cudaError_t st = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            cuda_check(st, "instantiate graph");
+        }
+        cuda_check(cudaGraphLaunch(exec, stream), "launch graph");
+    }
+
+    static bool capturable(cudaStream_t stream) {
+        return stream != nullptr && stream != cudaStreamLegacy && stream != cudaStreamPerThread;
     }
 
     long long owned_off() const { return parity ? ncap : 0; }
@@ -752,31 +789,65 @@ struct dsx_grid {
             fail(DSX_E_LOGIC, std::string(what) + " while a split halo exchange is in progress");
     }
 
+    // Segment 1 is a captured graph on an explicit stream (the default
+    // streams cannot capture; plain mode reads layouts on the host): one
+    // launch, and begin returns.  Refreshes use split_ctas_per_sm (0: every
+    // resident CTA) so that interior work on other streams finds SM room.
     void begin_halo(bool rebuild, bool positions_only, cudaStream_t stream) {
         not_pending("begin_halo_exchange");
         if (rebuild) plan_valid = false;
         pending_rebuild = rebuild;
         pending_reused = false;
         pending_build = false;
+        const bool graphs = capturable(stream) && !plain;
         if (P == 1) {
             plan_valid = false;
             ghosts_valid = false;
         } else if (plan_valid) {
-            dsx::launch_halo_refresh(params(), A, owned_off(), ghost_off(), positions_only, S, stream);
+            auto enqueue = [&] {
+                dsx::launch_halo_refresh(params(), A, owned_off(), ghost_off(), positions_only, S,
+                                         stream, split_ctas_per_sm);
+            };
+            if (graphs) run_captured(split_begin[positions_only ? 1 : 0][parity], stream, enqueue);
+            else enqueue();
             pending_reused = true;
         } else {
-            clear_status(stream);
-            enqueue_halo_build(stream, plain_layout(stream));
+            if (graphs) {
+                run_captured(split_begin[2][parity], stream, [&] {
+                    clear_status(stream);
+                    enqueue_halo_build(stream);
+                });
+                plain_bounds.clear();
+            } else {
+                clear_status(stream);
+                enqueue_halo_build(stream, plain_layout(stream));
+            }
             pending_build = true;
         }
+        pending_graphs = graphs;
         halo_pending = true;
     }
+
+    bool pending_graphs = false;
 
     void end_halo(cudaStream_t stream, long long* results) {
         if (!halo_pending) fail(DSX_E_LOGIC, "end_halo_exchange without begin_halo_exchange");
         halo_pending = false;
         if (pending_build) {
-            const unsigned st = read_status(stream);
+            unsigned st;
+            if (pending_graphs) {
+                // segment 2: the build's status and totals to the host
+                run_captured(split_end[parity], stream, [&] {
+                    cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned),
+                                               cudaMemcpyDeviceToHost, stream), "read status");
+                    cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int),
+                                               cudaMemcpyDeviceToHost, stream), "read status");
+                });
+                cuda_check(cudaStreamSynchronize(stream), "synchronize");
+                st = pinned_status[0];
+            } else {
+                st = read_status(stream);
+            }
             if (st & dsx::kStatusGhostOverflow) {
                 grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
                 build_checked(stream);
@@ -1591,9 +1662,23 @@ int dsx_grid_rebalance(dsx_grid* grid, const double* work, int force, void* stre
 int dsx_grid_set_halo_width(dsx_grid* grid, double width) {
     return guarded([&] {
         if (width < 0.0) fail(DSX_E_INVALID, "halo width cannot be negative");
+        grid->not_pending("set_halo_width");
         if (grid->halo_width != width) {
             grid->halo_width = width;
             grid->plan_valid = false;
+            grid->destroy_graphs();   // captured kernels hold the old width
+        }
+    });
+}
+
+int dsx_grid_set_split_share(dsx_grid* grid, int ctas_per_sm) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        if (ctas_per_sm < 0) fail(DSX_E_INVALID, "CTAs per SM cannot be negative");
+        grid->not_pending("set_split_share");
+        if (grid->split_ctas_per_sm != ctas_per_sm) {
+            grid->split_ctas_per_sm = ctas_per_sm;
+            grid->destroy_graphs();
         }
     });
 }

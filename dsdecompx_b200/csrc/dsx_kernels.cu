@@ -2728,8 +2728,10 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
 }
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
-                         bool positions_only, const Scratch& S, cudaStream_t s) {
-    k_halo_refresh<<<resident_grid(reinterpret_cast<const void*>(k_halo_refresh), G.gcap), NT, 0, s>>>(G, A, owned_off, ghost_off,
+                         bool positions_only, const Scratch& S, cudaStream_t s, int ctas_per_sm) {
+    int grid = resident_grid(reinterpret_cast<const void*>(k_halo_refresh), G.gcap);
+    if (ctas_per_sm > 0 && grid > sm_count() * ctas_per_sm) grid = sm_count() * ctas_per_sm;
+    k_halo_refresh<<<grid, NT, 0, s>>>(G, A, owned_off, ghost_off,
                                                       positions_only ? 1 : 0, S.halo_info,
                                                       S.ghost_owner, S.ghost_entry);
 }

@@ -116,9 +116,12 @@ void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long lon
 // the stays read from HBM (kind 3: ghosts never need their owner's force).
 int staged_move_modes(const Arrays& A);
 
+// ctas_per_sm > 0 caps the grid at that many CTAs per SM (the split phase
+// leaves room on every SM for independent work on other streams); 0 fills
+// the GPU with resident CTAs.
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off,
                          long long ghost_off, bool positions_only, const Scratch& S,
-                         cudaStream_t s);
+                         cudaStream_t s, int ctas_per_sm = 0);
 
 struct FieldOps {
     int count = 0;

@@ -1,9 +1,11 @@
 // Synthetic-workload kernels for the benchmark harness (not part of the
 // bookkeeping path): the per-step drift of the owned particles and the ghost
-// forces that stand in for a user's force computation.  Both draw N(0,1)
-// deviates from a counter-based generator (splitmix64 of seed, step, particle
-// id and axis, then Box-Muller), so a step's inputs do not depend on the order
-// the particles sit in and the kernels can be captured in a CUDA graph.
+// forces that stand in for a user's force computation, and a compute-bound
+// stand-in for interior force work (split-phase timings).  The first two draw
+// N(0,1) deviates from a counter-based generator (splitmix64 of seed, step,
+// particle id and axis, then Box-Muller), so a step's inputs do not depend on
+// the order the particles sit in and the kernels can be captured in a CUDA
+// graph.
 #include "dsx.h"
 
 #include <cuda_runtime.h>
@@ -69,6 +71,25 @@ __global__ void k_ghost_forces(double* fx, double* fy, double* fz, const int* to
 
 __global__ void k_advance() { ++g_step; }
 
+// Stand-in for interior (owned-owned) force work between begin and end of a
+// split halo exchange: per owned particle 24 B of positions in, `rounds` x 4
+// independent FP64 multiply-add chains, 8 B out.  Bandwidth-light: it needs
+// the SMs, not HBM.
+__global__ void k_interior(const double* x, const double* y, const double* z, long long n,
+                           int rounds, double* out) {
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += gridDim.x * 256ll) {
+        double a = x[i], b = y[i], c = z[i], d = a + b;
+        const double k1 = 0.999999, k2 = 1.0e-7;
+        for (int r = 0; r < rounds; ++r) {
+            a = fma(a, k1, k2);
+            b = fma(b, k1, k2);
+            c = fma(c, k1, k2);
+            d = fma(d, k1, k2);
+        }
+        out[i] = a + b + c + d;
+    }
+}
+
 int grid_for(long long n) {
     int sms = 148, device = 0;
     cudaGetDevice(&device);
@@ -108,6 +129,15 @@ int dsxw_ghost_forces(const dsx_grid_view* v, unsigned long long seed, long long
     k_ghost_forces<<<grid_for(v->ghost_capacity), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double*>(v->base[6]) + g, static_cast<double*>(v->base[7]) + g,
         static_cast<double*>(v->base[8]) + g, v->halo_totals, seed, static_cast<std::uint64_t>(step));
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+// interior stand-in over the owned particles of a view; out holds v->particles
+int dsxw_interior(const dsx_grid_view* v, int rounds, double* out, void* stream) {
+    const long long o = v->owned_offset;
+    k_interior<<<grid_for(v->particles), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const double*>(v->base[0]) + o, static_cast<const double*>(v->base[1]) + o,
+        static_cast<const double*>(v->base[2]) + o, v->particles, rounds, out);
     return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

@@ -241,9 +241,17 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
  * interior work can run on other streams; end waits for it (growing the ghost
  * region and rebuilding if it overflowed) and fills results like
  * dsx_grid_exchange_halo.  Between the two, every other operation on the
- * grid fails with DSX_E_LOGIC, as does end without begin or a second begin. */
+ * grid fails with DSX_E_LOGIC, as does end without begin or a second begin.
+ * On an explicit (non-default) stream the two halves are captured CUDA graphs,
+ * one launch each: begin's segment is the refresh or the build, end's the
+ * completion (the build's status and totals to the host). */
 int dsx_grid_begin_halo_exchange(dsx_grid* grid, int rebuild, int positions_only, void* stream);
 int dsx_grid_end_halo_exchange(dsx_grid* grid, void* stream, long long* results);
+
+/* CTAs per SM that begin_halo_exchange's refresh may occupy (0, the default:
+ * every resident CTA).  A small number leaves room on every SM for interior
+ * work launched on other streams between begin and end. */
+int dsx_grid_set_split_share(dsx_grid* grid, int ctas_per_sm);
 
 /* Owning subdomain of n positions (Decomposition::owner_rank, dsDecompX
  * src/migration.cpp:74-98: one periodic wrap, then the cut planes): x, y, z

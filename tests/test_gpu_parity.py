@@ -791,51 +791,69 @@ def test_owner_rank_and_out_of_domain(cuda):
         pair.close()
 
 
-def test_split_phase_halo_exchange(cuda):
+@pytest.mark.parametrize("mode", ["default_stream", "graphs", "graphs_lean"])
+def test_split_phase_halo_exchange(cuda, mode):
     """begin/end halo exchange with other GPU work in between: the same
     ghosts as the oracle's exchange_halo (builds, refreshes and a build that
-    overflows and is redone in end); misuse is refused."""
+    overflows and is redone in end); misuse is refused.  On the default
+    stream the two halves are plain launches; on an explicit stream they are
+    the captured graph segments, replayed over both owned halves, with the
+    refresh on every resident CTA or on 2 CTAs per SM ("lean")."""
+    import contextlib
+
     import torch
     rng = np.random.default_rng(23)
     L = (12.0, 10.0, 9.0)
     pair = Pair(12, (3, 2, 2), "manual", (0, 0, 0), L, (True, True, True), 0.8, True, None,
                 ALL_FIELDS[:2], particles=8000, ghost_capacity=128)
+    if mode == "graphs_lean":
+        pair.gpu.set_split_share(2)
     other = torch.cuda.Stream()
     busy = torch.empty(1 << 24, device="cuda")
+    scope = contextlib.nullcontext() if mode == "default_stream" else \
+        torch.cuda.stream(torch.cuda.Stream())
     try:
-        data = uniform_particles(rng, 8000, (0, 0, 0), L, ALL_FIELDS[:2])
-        owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
-        pair.upload(split_by_owner(owner, data, 12))
-        for step in range(4):
-            pair.displace(rng, 0.3 if step % 2 == 0 else 0.02)
-            if step % 2 == 0:
-                pair.gpu.migrate()
-                pair.ref.migrate()
-            rebuild = step % 2 == 0
-            pair.gpu.begin_halo_exchange(rebuild=rebuild)
-            with torch.cuda.stream(other):     # "interior" work meanwhile
-                busy.normal_()
-            hg = pair.gpu.end_halo_exchange()
-            hr = pair.ref.exchange_halo(rebuild=rebuild)
-            assert (hg[:, 0] == hr[:, 0]).all(), step
-            assert (hg[:, 3] == (0 if rebuild else 1)).all(), step
-            pair.compare(f"split {step}")
-            pair.set_ghost(rng, ["fx", "fy", "fz"])
-            pair.gpu.reverse_halo()
-            pair.ref.reverse_halo()
-            pair.compare(f"reverse {step}")
-        pair.gpu.begin_halo_exchange()
-        with pytest.raises(RuntimeError, match="in progress"):
-            pair.gpu.begin_halo_exchange()
-        with pytest.raises(RuntimeError, match="in progress"):
-            pair.gpu.migrate()
-        with pytest.raises(RuntimeError, match="in progress"):
-            pair.gpu.rescale_domain((0, 0, 0), L)
-        with pytest.raises(RuntimeError, match="in progress"):
-            pair.gpu.autotune()
-        pair.gpu.end_halo_exchange()
-        with pytest.raises(RuntimeError, match="without begin"):
-            pair.gpu.end_halo_exchange()
+        with scope:
+            split_phase_steps(pair, rng, other, busy, L)
     finally:
         torch.cuda.synchronize()
         pair.close()
+
+
+def split_phase_steps(pair, rng, other, busy, L):
+    import torch
+    data = uniform_particles(rng, 8000, (0, 0, 0), L, ALL_FIELDS[:2])
+    owner = pair.ref.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    pair.upload(split_by_owner(owner, data, 12))
+    for step in range(8):
+        pair.displace(rng, 0.3 if step % 2 == 0 else 0.02)
+        if step % 2 == 0:
+            pair.gpu.migrate()
+            pair.ref.migrate()
+        rebuild = step % 2 == 0
+        pair.gpu.begin_halo_exchange(rebuild=rebuild)
+        with torch.cuda.stream(other):     # "interior" work meanwhile
+            busy.normal_()
+        hg = pair.gpu.end_halo_exchange()
+        hr = pair.ref.exchange_halo(rebuild=rebuild)
+        assert (hg[:, 0] == hr[:, 0]).all(), step
+        assert (hg[:, 3] == (0 if rebuild else 1)).all(), step
+        pair.compare(f"split {step}")
+        pair.set_ghost(rng, ["fx", "fy", "fz"])
+        pair.gpu.reverse_halo()
+        pair.ref.reverse_halo()
+        pair.compare(f"reverse {step}")
+    pair.gpu.begin_halo_exchange()
+    with pytest.raises(RuntimeError, match="in progress"):
+        pair.gpu.begin_halo_exchange()
+    with pytest.raises(RuntimeError, match="in progress"):
+        pair.gpu.migrate()
+    with pytest.raises(RuntimeError, match="in progress"):
+        pair.gpu.rescale_domain((0, 0, 0), L)
+    with pytest.raises(RuntimeError, match="in progress"):
+        pair.gpu.autotune()
+    with pytest.raises(RuntimeError, match="in progress"):
+        pair.gpu.set_split_share(1)
+    pair.gpu.end_halo_exchange()
+    with pytest.raises(RuntimeError, match="without begin"):
+        pair.gpu.end_halo_exchange()
