@@ -167,6 +167,38 @@ def algorithmic_bytes(S, N, E, G, B):
     }
 
 
+def harness_bytes(w, N, G, B):
+    """Least bytes of the benchmark's step callback (the stand-in for the
+    user's integrator and force loop): the drift reads each owned particle's
+    id and position and writes the position back (52 B), the ghost forces
+    write 24 B per ghost; workloads with field exchanges add the library's
+    forward_exchange (2b G + 4 G) and reverse_exchange sum (b G + 4 G + 2b B)
+    of every field of b bytes per particle."""
+    sizes = {"int32": 4, "int64": 8, "uint32": 4, "uint64": 8, "float32": 4, "float64": 8}
+    total = 52 * N + 24 * G
+    if w.field_exchange:
+        for _, t, c in w.fields:
+            b = sizes[t] * c
+            total += (2 * b * G + 4 * G) + (b * G + 4 * G + 2 * b * B)
+    return int(total)
+
+
+def step_accounting(step_bytes, harness, ms_per_step, kernels_ms, peak):
+    """The step's roofline under one stated accounting: every byte the timed
+    step must move (the library's kernels and the callback inside the step)
+    over the device-timed wall time of the step."""
+    whole = step_bytes + harness
+    gbs = whole / (ms_per_step / 1e3) / 1e9
+    return {"accounting": "library kernels' algorithmic bytes + the step callback's "
+                          "(drift 52 B/particle, ghost forces 24 B/ghost, field exchanges) "
+                          "over the timed ms_per_step",
+            "bytes": int(whole), "library_bytes": int(step_bytes), "callback_bytes": int(harness),
+            "ms_per_step": round(ms_per_step, 4), "achieved_gbs": round(gbs, 1),
+            "frac_of_peak": round(gbs / peak, 4),
+            "library_bytes_over_wall_frac": round(step_bytes / (ms_per_step / 1e3) / 1e9 / peak, 4),
+            "library_kernels_ms": round(kernels_ms, 4)}
+
+
 # ------------------------------------------------------------------- our arm
 
 class DeviceBytes:
@@ -232,15 +264,15 @@ def run_ours(args, rank, world, device):
     seed = args.seed + 1000 * rank
 
     def user_work(view, s):
-        vp = C.byref(view)
-        wl.dsxw_ghost_forces(vp, seed, 0, s)
+        # the user's integrator and force loop: ghost forces and the drift of
+        # the owned particles (one launch), field exchanges where the
+        # workload has them
+        wl.dsxw_step_work(C.byref(view), seed, w.drift, s)
         if field_ids:
             grid.forward_exchange([w.fields[i][0] for i in field_ids], stream=s)
             grid.reverse_exchange([(w.fields[i][0], "sum") for i in field_ids], stream=s)
-        wl.dsxw_drift(vp, seed, 0, w.drift, s)
-        wl.dsxw_advance(s)
 
-    harness_kernels = 3 + (0 if not field_ids else 2)
+    harness_kernels = 1 + (0 if not field_ids else 2)
 
     def barrier():
         if world > 1:
@@ -311,6 +343,8 @@ def run_ours(args, rank, world, device):
     peak, peak_kind = peaks()
     step_bytes = sum(v for k, v in alg.items() if k in ours)
     ours_ms = sum(ours.values())
+    harness = harness_bytes(w, mean_tot["particles"] or N, mean_tot["ghosts"],
+                            mean_tot["boundary"])
     roof = None
     if dominant in alg:
         achieved = alg[dominant] / (avg[dominant] / 1e3) / 1e9
@@ -426,11 +460,7 @@ def run_ours(args, rank, world, device):
         "step": "graph-captured batched step (dsx_grid_step)",
         "autotune": tune,
         "roofline": roof,
-        "step_roofline": {"algorithmic_bytes": int(step_bytes),
-                          "kernels_ms": round(ours_ms, 4),
-                          "achieved_gbs": round(step_bytes / (ours_ms / 1e3) / 1e9, 1),
-                          "frac_of_peak": round(step_bytes / (ours_ms / 1e3) / 1e9 / peak, 4),
-                          "achieved_gbs_wall": round(step_bytes / (ms_per_step / 1e3) / 1e9, 1)},
+        "step_roofline": step_accounting(step_bytes, harness, ms_per_step, ours_ms, peak),
         "kernel_ms": {k: round(v, 4) for k, v in avg.items()},
         "totals_per_step": {k: int(v) for k, v in mean_tot.items()},
         "per_call_ms_per_step": plain,

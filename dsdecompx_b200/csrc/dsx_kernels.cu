@@ -283,14 +283,23 @@ __global__ void __launch_bounds__(NT, 4) k_mig_classify(Grid G, const double* __
             stay += valid ? 1 : 0;
             continue;
         }
-        if (!valid) continue;
-        double wx, wy, wz;
-        const int d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
-        if (d == s) {
-            ++stay;
-        } else {
-            ++emig;
-            atomicAdd(&imm_total[d], 1);
+        int key = -1;   // destination of an emigrant
+        if (valid) {
+            double wx, wy, wz;
+            const int d = destination_near(G, cell, px[j], py[j], pz[j], wx, wy, wz);
+            if (d == s) {
+                ++stay;
+            } else {
+                ++emig;
+                key = d;
+            }
+        }
+        // one atomic per destination and warp: after the cut planes moved,
+        // most of a group can leave for the same few subdomains
+        if (__any_sync(0xffffffffu, key >= 0)) {
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            if (key >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1)
+                atomicAdd(&imm_total[key], __popc(peers));
         }
     }
     int stays, emigs;

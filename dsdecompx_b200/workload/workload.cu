@@ -71,6 +71,42 @@ __global__ void k_ghost_forces(double* fx, double* fy, double* fz, const int* to
 
 __global__ void k_advance() { ++g_step; }
 
+// Drift of the owned particles and ghost forces in one launch (the step
+// callback's work): one grid-stride pass over max(owned, ghost capacity)
+// slots; the CTA that finishes last moves the step counter on, after every
+// CTA has read it.
+__device__ unsigned int g_done = 0;
+
+__global__ void k_step_work(double* x, double* y, double* z, const int* gid, long long n,
+                            double* fx, double* fy, double* fz, const int* totals,
+                            long long span, std::uint64_t seed, double sigma) {
+    const std::uint64_t step = g_step;
+    const long long g = totals[0];
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < span; i += gridDim.x * 256ll) {
+        double a, b, c;
+        if (i < n) {
+            normals3(seed, step, static_cast<std::uint32_t>(gid[i]), a, b, c);
+            x[i] += sigma * a;
+            y[i] += sigma * b;
+            z[i] += sigma * c;
+        }
+        if (i < g) {
+            normals3(seed, step, static_cast<std::uint64_t>(i), a, b, c);
+            fx[i] = a;
+            fy[i] = b;
+            fz[i] = c;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&g_done, 1u) == gridDim.x - 1) {
+            g_done = 0;
+            ++g_step;
+        }
+    }
+}
+
 // Stand-in for interior (owned-owned) force work between begin and end of a
 // split halo exchange: per owned particle 24 B of positions in, `rounds` x 4
 // independent FP64 multiply-add chains, 8 B out.  Bandwidth-light: it needs
@@ -129,6 +165,19 @@ int dsxw_ghost_forces(const dsx_grid_view* v, unsigned long long seed, long long
     k_ghost_forces<<<grid_for(v->ghost_capacity), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double*>(v->base[6]) + g, static_cast<double*>(v->base[7]) + g,
         static_cast<double*>(v->base[8]) + g, v->halo_totals, seed, static_cast<std::uint64_t>(step));
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+// dsxw_drift + dsxw_ghost_forces + dsxw_advance in one launch: the same
+// values as the three calls with the same seed (step 0 offsets)
+int dsxw_step_work(const dsx_grid_view* v, unsigned long long seed, double sigma, void* stream) {
+    const long long o = v->owned_offset, g = v->ghost_offset;
+    const long long span = v->particles > v->ghost_capacity ? v->particles : v->ghost_capacity;
+    k_step_work<<<grid_for(span), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<double*>(v->base[0]) + o, static_cast<double*>(v->base[1]) + o,
+        static_cast<double*>(v->base[2]) + o, static_cast<const int*>(v->base[12]) + o,
+        v->particles, static_cast<double*>(v->base[6]) + g, static_cast<double*>(v->base[7]) + g,
+        static_cast<double*>(v->base[8]) + g, v->halo_totals, span, seed, sigma);
     return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 
