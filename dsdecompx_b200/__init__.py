@@ -139,6 +139,7 @@ def lib() -> C.CDLL:
             "dsx_grid_owner_rank": [vp, vp, vp, vp, C.c_longlong, vp, vp],
             "dsx_grid_begin_halo_exchange": [vp, C.c_int, C.c_int, vp],
             "dsx_grid_set_split_share": [vp, C.c_int],
+            "dsx_grid_set_refresh_kind": [vp, C.c_int],
             "dsx_grid_end_halo_exchange": [vp, vp, C.POINTER(C.c_longlong)],
             "dsx_grid_out_of_domain": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp],
             "dsx_grid_rescale_domain": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, vp],
@@ -511,6 +512,10 @@ class VirtualGrid:
         _check(self.L.dsx_grid_end_halo_exchange(self.h, _stream(stream),
                                                  res.ctypes.data_as(C.POINTER(C.c_longlong))))
         return res
+
+    def set_refresh_kind(self, owner_by_owner: bool = True):
+        """Refresh walk: owner by owner (default) or ghost by ghost."""
+        _check(self.L.dsx_grid_set_refresh_kind(self.h, 1 if owner_by_owner else 0))
 
     def set_split_share(self, ctas_per_sm: int = 0):
         """CTAs per SM the split-phase refresh may occupy (0: all resident)."""

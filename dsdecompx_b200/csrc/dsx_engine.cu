@@ -1671,6 +1671,18 @@ int dsx_grid_set_halo_width(dsx_grid* grid, double width) {
     });
 }
 
+int dsx_grid_set_refresh_kind(dsx_grid* grid, int owner_by_owner) {
+    return guarded([&] {
+        if (!grid) fail(DSX_E_INVALID, "null grid");
+        grid->not_pending("set_refresh_kind");
+        const int kind = owner_by_owner ? 1 : 0;
+        if (grid->S.refresh_owners != kind) {
+            grid->S.refresh_owners = kind;
+            grid->destroy_graphs();
+        }
+    });
+}
+
 int dsx_grid_set_split_share(dsx_grid* grid, int ctas_per_sm) {
     return guarded([&] {
         if (!grid) fail(DSX_E_INVALID, "null grid");

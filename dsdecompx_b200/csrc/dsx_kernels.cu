@@ -1973,6 +1973,68 @@ __global__ void __launch_bounds__(NT) k_halo_refresh(Grid G, Arrays A, long long
     }
 }
 
+// Refresh along the plan, owner by owner: every boundary owner's record is
+// read once (the reverse sum's CSR lists its images in neighbor order) and
+// written to each of its images with that image's periodic shift.  The
+// owners' reads then touch each sector of the owned arrays once, where a
+// ghost-by-ghost gather reads a sector per image (the owners of one send
+// list are sparse in the owned order).  Two owners per thread and pass keep
+// their loads in flight together.
+__global__ void __launch_bounds__(NT) k_halo_refresh_owners(Grid G, Arrays A, long long owned_off,
+                                                            long long ghost_off, int positions_only,
+                                                            const int* info,
+                                                            const int* __restrict__ bowner,
+                                                            const int* __restrict__ boff,
+                                                            const int* __restrict__ bslot,
+                                                            const int* __restrict__ ghost_entry) {
+    if (*G.status & kStatusGhostOverflow) return;
+    const int B = info[1];
+    constexpr int U = 2;
+    const int step = gridDim.x * NT;
+    for (int b0 = blockIdx.x * NT + threadIdx.x; b0 < B; b0 += U * step) {
+        long long src[U];
+        int k0[U], k1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int b = b0 + u * step;
+            const bool in = b < B;
+            src[u] = owned_off + (in ? ro(bowner + b) : 0);
+            k0[u] = in ? ro(boff + b) : 0;
+            k1[u] = in ? ro(boff + b + 1) : 0;
+        }
+        double p[U][6];
+        int first[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (k0[u] >= k1[u]) continue;
+            first[u] = ro(bslot + k0[u]);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) p[u][a] = ro(A.d[a] + src[u]);
+            if (!positions_only)
+#pragma unroll
+                for (int a = 3; a < 6; ++a) p[u][a] = ro(A.d[a] + src[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            for (int k = k0[u]; k < k1[u]; ++k) {
+                const int slot = k == k0[u] ? first[u] : ro(bslot + k);
+                const double* sh = G.shift + 3ll * ro(ghost_entry + slot);
+                const long long gi = ghost_off + slot;
+                A.d[0][gi] = __dadd_rn(p[u][0], sh[0]);
+                A.d[1][gi] = __dadd_rn(p[u][1], sh[1]);
+                A.d[2][gi] = __dadd_rn(p[u][2], sh[2]);
+                A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+                if (!positions_only) {
+                    A.d[3][gi] = p[u][3];
+                    A.d[4][gi] = p[u][4];
+                    A.d[5][gi] = p[u][5];
+                    copy_fields(A.f, src[u], gi);
+                }
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(NT) k_forward_fields(Arrays A, long long owned_off,
                                                        long long ghost_off, FieldOps F,
                                                        const int* info,
@@ -2738,6 +2800,14 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
 
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                          bool positions_only, const Scratch& S, cudaStream_t s, int ctas_per_sm) {
+    if (S.refresh_owners) {
+        int grid = resident_grid(reinterpret_cast<const void*>(k_halo_refresh_owners), G.ncap);
+        if (ctas_per_sm > 0 && grid > sm_count() * ctas_per_sm) grid = sm_count() * ctas_per_sm;
+        k_halo_refresh_owners<<<grid, NT, 0, s>>>(G, A, owned_off, ghost_off, positions_only ? 1 : 0,
+                                                  S.halo_info, S.bowner, S.boff, S.bslot,
+                                                  S.ghost_entry);
+        return;
+    }
     int grid = resident_grid(reinterpret_cast<const void*>(k_halo_refresh), G.gcap);
     if (ctas_per_sm > 0 && grid > sm_count() * ctas_per_sm) grid = sm_count() * ctas_per_sm;
     k_halo_refresh<<<grid, NT, 0, s>>>(G, A, owned_off, ghost_off,

@@ -154,9 +154,30 @@ def test_rebalance_api(cuda):
     pair.close()
 
 
-def test_positions_only_refresh(cuda):
+@pytest.mark.parametrize("owner_by_owner", [True, False], ids=["owners", "ghosts"])
+def test_refresh_kinds_follow_the_reference(cuda, owner_by_owner):
+    """Full refreshes along the plan (every field type, a halo wider than
+    half a cell so that owners have many images) walked owner by owner and
+    ghost by ghost give the oracle's ghosts."""
+    rng = np.random.default_rng(41)
+    pair = run_scenario(cuda, P=12, dims=(3, 2, 2), L=(9.0, 7.0, 6.0), halo=1.9, N=6000,
+                        steps=1, seed=40)
+    try:
+        pair.gpu.set_refresh_kind(owner_by_owner)
+        for k in range(3):
+            pair.displace(rng, 0.05)
+            hg, hr = pair.gpu.exchange_halo(), pair.ref.exchange_halo()
+            assert hg[:, 3].all() and (hg[:, 0] == hr[:, 0]).all()
+            pair.compare(f"refresh {k}")
+    finally:
+        pair.close()
+
+
+@pytest.mark.parametrize("owner_by_owner", [True, False], ids=["owners", "ghosts"])
+def test_positions_only_refresh(cuda, owner_by_owner):
     pair = run_scenario(cuda, P=8, dims=(2, 2, 2), L=(10.0, 10.0, 10.0), halo=1.0, N=5000,
                         steps=1, seed=10, fields=ALL_FIELDS[:2])
+    pair.gpu.set_refresh_kind(owner_by_owner)
     rng = np.random.default_rng(11)
     before = [pair.gpu.snapshot(r) for r in range(8)]
     pair.displace(rng, 0.05)
