@@ -2398,22 +2398,37 @@ __global__ void __launch_bounds__(NT) k_out_of_domain(Grid G, const double* __re
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z, int* flags) {
     __shared__ double s_cuts[kMaxRanks + 16];   // cut_offset[a] + kCountedCells <= 1036
-    const int g = blockIdx.x;
-    const int4 td = G.tiles[g];
-    if (g >= G.tile_start[G.P]) return;
     stage_cuts(G, s_cuts);
-    // a position inside the subdomain's own cut planes is owned there (the
-    // wrap leaves a position inside the box as it is, -0 aside, which lies
-    // in the same cell); only the others are searched
-    const Cell cell = cell_of(G, td.x);
-    bool out = false;
-    for (int i = td.y + threadIdx.x; i < td.z; i += NT) {
-        const double px = ro(x + i), py = ro(y + i), pz = ro(z + i);
-        const bool inside = cell.lo[0] <= px && px < cell.hi[0] && cell.lo[1] <= py &&
-                            py < cell.hi[1] && cell.lo[2] <= pz && pz < cell.hi[2];
-        if (!inside) out = out || owner_of_staged(G, s_cuts, px, py, pz) != td.x;
+    // one wave of CTAs strides over the tiles (the cuts are staged once per
+    // CTA); a position inside the subdomain's own cut planes is owned there
+    // (the wrap leaves a position inside the box as it is, -0 aside, which
+    // lies in the same cell); only the others are searched
+    const int ntiles = G.tile_start[G.P];
+    constexpr int U = TILE / NT;
+    for (int g = blockIdx.x; g < ntiles; g += gridDim.x) {
+        const int4 td = G.tiles[g];
+        const Cell cell = cell_of(G, td.x);
+        double px[U], py[U], pz[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = td.y + threadIdx.x + u * NT;
+            if (i < td.z) {
+                px[u] = ro(x + i);
+                py[u] = ro(y + i);
+                pz[u] = ro(z + i);
+            }
+        }
+        bool out = false;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = td.y + threadIdx.x + u * NT;
+            if (i >= td.z) continue;
+            const bool inside = cell.lo[0] <= px[u] && px[u] < cell.hi[0] && cell.lo[1] <= py[u] &&
+                                py[u] < cell.hi[1] && cell.lo[2] <= pz[u] && pz[u] < cell.hi[2];
+            if (!inside) out = out || owner_of_staged(G, s_cuts, px[u], py[u], pz[u]) != td.x;
+        }
+        if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(&flags[td.x], 1);
     }
-    if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(&flags[td.x], 1);
 }
 
 // Emigrants of the last migration counted per (destination, source):
@@ -2861,7 +2876,8 @@ void launch_owner_rank(const Grid& G, const double* x, const double* y, const do
 void launch_out_of_domain(const Grid& G, const double* x, const double* y, const double* z,
                           int* flags, cudaStream_t s) {
     cudaMemsetAsync(flags, 0, sizeof(int) * G.P, s);
-    k_out_of_domain<<<G.max_tiles, NT, 0, s>>>(G, x, y, z, flags);
+    k_out_of_domain<<<resident_grid(reinterpret_cast<const void*>(k_out_of_domain),
+                                    static_cast<long long>(G.max_tiles) * NT), NT, 0, s>>>(G, x, y, z, flags);
 }
 
 void mark(const Scratch& S, cudaStream_t s, const char* what) {
