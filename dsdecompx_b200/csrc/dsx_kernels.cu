@@ -1120,8 +1120,6 @@ struct StepTables {
 __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, int stride,
                                                        StepTables T) {
     __shared__ int ws[33];
-    __shared__ int s_n[kMaxRanks + 1], s_ob[kMaxRanks + 1], s_ts[kMaxRanks + 1];
-    __shared__ int s_in[kMaxRanks + 1], s_ib[kMaxRanks + 1], s_its[kMaxRanks + 1];
     __shared__ int s_rcv[kMaxRanks + 1];
     const int P = G.P;
     const int t = threadIdx.x;
@@ -1145,12 +1143,6 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
     const int itl = t < P ? (received + G.tile - 1) / G.tile : 0;
     const int its = block_scan_excl<1024>(itl, total_imm_tiles, ws);
     if (t < P) {
-        s_n[t] = next;
-        s_ob[t] = ob;
-        s_ts[t] = ts;
-        s_in[t] = received;
-        s_ib[t] = ob + retained;
-        s_its[t] = its;
         G.n_next[t] = next;
         G.obase_next[t] = ob;
         G.tile_start_next[t] = ts;
@@ -1165,9 +1157,6 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
         o[0] = (o[3] != 0 || o[4] != 0) ? 1 : 0;
     }
     if (t == 0) {
-        s_ob[P] = total_next;
-        s_ts[P] = total_tiles;
-        s_its[P] = total_imm_tiles;
         G.obase_next[P] = total_next;
         G.tile_start_next[P] = total_tiles;
         T.imm_tile_start[P] = total_imm_tiles;
@@ -1186,8 +1175,8 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
         T.list_len[idx] = active ? ret + T.imm_list[idx] : 0;
     }
     __syncthreads();
-    fill_tiles(P, G.tile, s_n, s_ob, s_ts, G.tiles_next);
-    fill_tiles(P, G.tile, s_in, s_ib, s_its, T.imm_tiles);
+    // (the tile descriptors of the next layout and of the immigrant segments
+    // are written by k_tile_bases, over the whole grid)
     // receivers: blocks in the receiver's neighbor order, one warp per
     // receiver (lane m reads the block of neighbor m)
     const int warp = t >> 5, lane = t & 31, nwarps = blockDim.x >> 5;
@@ -1655,16 +1644,41 @@ __device__ __forceinline__ void ghost_array_from_stage(const Grid& G, const Arra
     }
 }
 
+// Tile descriptors {s, begin, end, first tile of s} of a layout given by its
+// global counts, bases and tile starts (P + 1 entries each), the tiles
+// strided over the threads of the grid.
+__device__ __forceinline__ void fill_tiles_grid(int P, int tile, const int* n, const int* ob,
+                                                const int* ts, int4* tiles) {
+    const int total = ts[P];
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        int lo = 0, hi = P;   // largest s with ts[s] <= g
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (ts[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        const int begin = ob[lo] + (g - ts[lo]) * tile;
+        const int end = min(begin + tile, ob[lo] + n[lo]);
+        tiles[g] = make_int4(lo, begin, end, ts[lo]);
+    }
+}
+
 // Counter bases of every tile of the layout (30 per tile, row stride 32), so
-// that the move reads them with one load per tile.
+// that the move reads them with one load per tile; and the tile descriptors
+// of the next layout and of its immigrant segments (imm_in: immigrants per
+// subdomain, imm_base: where they start, imm_ts: their tile starts).
 __global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int stride,
-                                                   const int* cbase_ret, int* tile_bases) {
+                                                   const int* cbase_ret, int* tile_bases,
+                                                   const int* imm_in, const int* imm_base,
+                                                   const int* imm_ts, int4* imm_tiles) {
     const int ntiles = G.tile_start[G.P];
     for (long long idx = blockIdx.x * static_cast<long long>(NT) + threadIdx.x;
          idx < static_cast<long long>(ntiles) * 32; idx += static_cast<long long>(gridDim.x) * NT) {
         const int g = static_cast<int>(idx >> 5), k = static_cast<int>(idx & 31);
         if (k < kStepCounters) tile_bases[idx] = tile_base(G, pre, stride, cbase_ret, g, G.tiles[g], k);
     }
+    fill_tiles_grid(G.P, G.tile, G.n_next, G.obase_next, G.tile_start_next, G.tiles_next);
+    fill_tiles_grid(G.P, G.tile, imm_in, imm_base, imm_ts, imm_tiles);
 }
 
 // F4 with the tile's records staged in shared memory (same output as
@@ -2713,7 +2727,8 @@ void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s) {
                  S.halo_info, S.cbase, S.cbase_imm, S.imm_tile_start, S.imm_tiles};
     k_step_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, T);
     k_tile_bases<<<stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s>>>(
-        G, S.pre, S.stride, S.cbase, S.tile_bases);
+        G, S.pre, S.stride, S.cbase, S.tile_bases, S.imm_total, S.imm_base, S.imm_tile_start,
+        S.imm_tiles);
 }
 
 int staged_move_modes(const Arrays& A) {
