@@ -526,6 +526,8 @@ struct dsx_grid {
         S.list_ret = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * E);
         S.cbase_imm = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * dsx::kHaloCounters);
         S.imm_tile_start = device_alloc<int>(fixed_owned, P + 1);
+        S.ticket = device_alloc<unsigned>(fixed_owned, 1);
+        cuda_check(cudaMemset(S.ticket, 0, sizeof(unsigned)), "memset");
         S.imm_tiles = device_alloc<int4>(fixed_owned, static_cast<std::size_t>(max_tiles));
         S.imm_base = device_alloc<int>(fixed_owned, P);
         S.emig_src = device_alloc<int>(fixed_owned, ncap);

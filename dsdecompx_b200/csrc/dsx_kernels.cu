@@ -200,8 +200,16 @@ __global__ void __launch_bounds__(1024) k_layout(int P, int tile, const int* n, 
 
 // Exclusive prefix of counter k (= blockIdx.x) over the tiles of the layout.
 // cnt/pre are counter-major: [k * stride + tile]; pre[k*stride + ntiles] = total.
+__device__ __forceinline__ void scan_counter(const int* cnt, int* pre, int stride,
+                                             const int* tile_start_end);
+
 __global__ void __launch_bounds__(1024) k_scan_counters(const int* cnt, int* pre, int stride,
                                                          const int* tile_start_end) {
+    scan_counter(cnt, pre, stride, tile_start_end);
+}
+
+__device__ __forceinline__ void scan_counter(const int* cnt, int* pre, int stride,
+                                             const int* tile_start_end) {
     constexpr int PER = 8;
     constexpr int CHUNK = 1024 * PER;
     __shared__ int ws[33];
@@ -1117,8 +1125,32 @@ struct StepTables {
     int4* imm_tiles;
 };
 
-__global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, int stride,
-                                                       StepTables T) {
+__device__ __forceinline__ void step_layout_body(const Grid& G, const int* pre, int stride,
+                                                 const StepTables& T);
+
+// The counter scan (one CTA per counter) and, in the CTA that finishes
+// last, the layout: one launch instead of two.  The last CTA reads the
+// prefixes the others wrote through L2 (after the fence that orders them
+// before its ticket) and puts the ticket back to 0 for the next launch.
+__global__ void __launch_bounds__(1024) k_step_scan_layout(Grid G, const int* cnt, int* pre,
+                                                            int stride, StepTables T,
+                                                            unsigned* ticket) {
+    __shared__ bool s_last;
+    scan_counter(cnt, pre, stride, G.tile_start + G.P);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    step_layout_body(G, pre, stride, T);
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+__device__ __forceinline__ void step_layout_body(const Grid& G, const int* pre, int stride,
+                                                 const StepTables& T) {
     __shared__ int ws[33];
     __shared__ int s_rcv[kMaxRanks + 1];
     const int P = G.P;
@@ -1126,7 +1158,7 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
     const int ntiles = G.tile_start[P];
     const int* ts_old = G.tile_start;
     auto tile_sum = [&](int k, int r) {
-        return pre[k * stride + ts_old[r + 1]] - pre[k * stride + ts_old[r]];
+        return __ldcg(pre + k * stride + ts_old[r + 1]) - __ldcg(pre + k * stride + ts_old[r]);
     };
     // new owned layout and migration results
     int retained = 0, received = 0, old = 0, next = 0;
@@ -1160,7 +1192,7 @@ __global__ void __launch_bounds__(1024) k_step_layout(Grid G, const int* pre, in
         G.obase_next[P] = total_next;
         G.tile_start_next[P] = total_tiles;
         T.imm_tile_start[P] = total_imm_tiles;
-        const int E = pre[kStepEmig * stride + ntiles];
+        const int E = __ldcg(pre + kStepEmig * stride + ntiles);
         T.emig_info[0] = E;
         T.emig_info[1] = (E + TILE - 1) / TILE;
         if (total_next != G.obase[P]) atomicOr(G.status, kStatusMigrationMismatch);
@@ -2720,12 +2752,10 @@ void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, con
 }
 
 void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s) {
-    k_scan_counters<<<kStepCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
-    if (S.marks) S.marks->mark(s, "step_scan");
     StepTables T{S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.imm_base, S.emig_info,
                  S.mig_results, S.list_ret, S.list_len, S.send_base, S.g, S.gbase, S.boff,
                  S.halo_info, S.cbase, S.cbase_imm, S.imm_tile_start, S.imm_tiles};
-    k_step_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, T);
+    k_step_scan_layout<<<kStepCounters, 1024, 0, s>>>(G, S.cnt, S.pre, S.stride, T, S.ticket);
     k_tile_bases<<<stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s>>>(
         G, S.pre, S.stride, S.cbase, S.tile_bases, S.imm_total, S.imm_base, S.imm_tile_start,
         S.imm_tiles);

@@ -61,6 +61,7 @@ struct Scratch {
     int* list_ret = nullptr;   // [P*26] retained part of each send list
     int* cbase_imm = nullptr;  // [P*28] bases of the immigrant parts
     int* imm_tile_start = nullptr;  // [P+1] tiles over the immigrant segments
+    unsigned* ticket = nullptr;     // [1] CTAs done in the step's counter scan (0 between launches)
     int4* imm_tiles = nullptr;      // their descriptors
     int* cnt2 = nullptr;       // [28][stride] immigrant-tile counters
     int* pre2 = nullptr;
