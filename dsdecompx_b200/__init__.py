@@ -513,8 +513,8 @@ class VirtualGrid:
                                                  res.ctypes.data_as(C.POINTER(C.c_longlong))))
         return res
 
-    def set_refresh_kind(self, owner_by_owner: bool = True):
-        """Refresh walk: owner by owner (default) or ghost by ghost."""
+    def set_refresh_kind(self, owner_by_owner: bool = False):
+        """Refresh walk: ghost by ghost (default) or owner by owner."""
         _check(self.L.dsx_grid_set_refresh_kind(self.h, 1 if owner_by_owner else 0))
 
     def set_split_share(self, ctas_per_sm: int = 0):

@@ -72,7 +72,7 @@ struct Scratch {
     int classify_combine = 0;     // immigrant counters combined per warp before the atomics
     int move_staged = 1;          // 1: staged (one pass if it fits), 2: staged in passes,
                                   // 3: staged without forces, 0: direct reads
-    int refresh_owners = 1;       // refresh owner by owner (the CSR) instead of ghost by ghost
+    int refresh_owners = 0;       // refresh owner by owner (the CSR) instead of ghost by ghost
     int reverse_per_sm = 0;       // CTAs per SM of the reverse sum; 0: one wave of the default shape
 };
 

@@ -72,30 +72,46 @@ __global__ void k_ghost_forces(double* fx, double* fy, double* fz, const int* to
 __global__ void k_advance() { ++g_step; }
 
 // Drift of the owned particles and ghost forces in one launch (the step
-// callback's work): one grid-stride pass over max(owned, ghost capacity)
-// slots; the CTA that finishes last moves the step counter on, after every
-// CTA has read it.
+// callback's work): a grid-stride pass over the owned particles (two per
+// thread and pass, their loads issued together), then one over the ghosts;
+// the CTA that finishes last moves the step counter on, after every CTA has
+// read it.
 __device__ unsigned int g_done = 0;
 
 __global__ void k_step_work(double* x, double* y, double* z, const int* gid, long long n,
                             double* fx, double* fy, double* fz, const int* totals,
-                            long long span, std::uint64_t seed, double sigma) {
+                            std::uint64_t seed, double sigma) {
     const std::uint64_t step = g_step;
-    const long long g = totals[0];
-    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < span; i += gridDim.x * 256ll) {
+    const long long stride = gridDim.x * 256ll;
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += 2 * stride) {
+        const long long k = i + stride;
+        const bool two = k < n;
+        const int id0 = gid[i], id1 = two ? gid[k] : 0;
+        double x0 = x[i], y0 = y[i], z0 = z[i], x1 = 0.0, y1 = 0.0, z1 = 0.0;
+        if (two) {
+            x1 = x[k];
+            y1 = y[k];
+            z1 = z[k];
+        }
         double a, b, c;
-        if (i < n) {
-            normals3(seed, step, static_cast<std::uint32_t>(gid[i]), a, b, c);
-            x[i] += sigma * a;
-            y[i] += sigma * b;
-            z[i] += sigma * c;
+        normals3(seed, step, static_cast<std::uint32_t>(id0), a, b, c);
+        x[i] = x0 + sigma * a;
+        y[i] = y0 + sigma * b;
+        z[i] = z0 + sigma * c;
+        if (two) {
+            normals3(seed, step, static_cast<std::uint32_t>(id1), a, b, c);
+            x[k] = x1 + sigma * a;
+            y[k] = y1 + sigma * b;
+            z[k] = z1 + sigma * c;
         }
-        if (i < g) {
-            normals3(seed, step, static_cast<std::uint64_t>(i), a, b, c);
-            fx[i] = a;
-            fy[i] = b;
-            fz[i] = c;
-        }
+    }
+    const long long g = totals[0];
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < g; i += stride) {
+        double a, b, c;
+        normals3(seed, step, static_cast<std::uint64_t>(i), a, b, c);
+        fx[i] = a;
+        fy[i] = b;
+        fz[i] = c;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -177,7 +193,7 @@ int dsxw_step_work(const dsx_grid_view* v, unsigned long long seed, double sigma
         static_cast<double*>(v->base[0]) + o, static_cast<double*>(v->base[1]) + o,
         static_cast<double*>(v->base[2]) + o, static_cast<const int*>(v->base[12]) + o,
         v->particles, static_cast<double*>(v->base[6]) + g, static_cast<double*>(v->base[7]) + g,
-        static_cast<double*>(v->base[8]) + g, v->halo_totals, span, seed, sigma);
+        static_cast<double*>(v->base[8]) + g, v->halo_totals, seed, sigma);
     return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

@@ -249,9 +249,9 @@ int dsx_grid_begin_halo_exchange(dsx_grid* grid, int rebuild, int positions_only
 int dsx_grid_end_halo_exchange(dsx_grid* grid, void* stream, long long* results);
 
 /* How a halo refresh (exchange_halo along a valid plan, full or positions
- * only) walks the plan: 1 (the default) owner by owner, reading each boundary
- * owner once and writing all its images; 0 ghost by ghost, gathering the
- * owner of every ghost.  Both write the same values. */
+ * only) walks the plan: 0 (the default) ghost by ghost, gathering the owner
+ * of every ghost; 1 owner by owner, reading each boundary owner once and
+ * writing all its images.  Both write the same values. */
 int dsx_grid_set_refresh_kind(dsx_grid* grid, int owner_by_owner);
 
 /* CTAs per SM that begin_halo_exchange's refresh may occupy (0, the default:

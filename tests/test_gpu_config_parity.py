@@ -39,8 +39,10 @@ class DeviceBytes:
 
 
 def reference_grid(w, field_capacity=0):
+    """The reference's grid of the workload; without a field capacity it
+    carries no fields (a probe for the process grid)."""
     dims = w.dims if w.policy == "manual" else (0, 0, 0)
-    fields = [(n, FIELD_TYPES.index(t), c) for n, t, c in w.fields]
+    fields = [(n, FIELD_TYPES.index(t), c) for n, t, c in w.fields] if field_capacity else []
     return oracle.Grid("ref", w.nranks, dims, w.policy, w.lower, w.upper, (True,) * 3, w.halo,
                        fields=fields, field_capacity=field_capacity)
 
