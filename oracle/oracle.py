@@ -272,6 +272,16 @@ class Grid:
         self._call("read", rank, self.array_id(name), start, count, _ptr(out))
         return out.reshape(count, comps) if comps > 1 else out
 
+    def read_field(self, rank: int, field: str) -> np.ndarray:
+        """Owned + ghost values of a registered field (by field name, even
+        where it shares a name with a core array)."""
+        f = self.field_index[field]
+        _, t, comps = self.fields[f]
+        owned, ghosts = self.counts(rank)
+        out = np.zeros((owned + ghosts) * comps, dtype=FIELD_DTYPES[t])
+        self._call("read", rank, 13 + f, 0, owned + ghosts, _ptr(out))
+        return out.reshape(-1, comps) if comps > 1 else out
+
     def write(self, rank: int, name: str, start: int, values: np.ndarray):
         comps = self.components(name)
         arr = np.ascontiguousarray(values, dtype=self.dtype_of(name)).reshape(-1)

@@ -47,17 +47,27 @@ def reference_grid(w, field_capacity=0):
                        fields=fields, field_capacity=field_capacity)
 
 
+def array_info(grid, a):
+    """(dtype, components) of array id a: 13 core arrays, then the fields (a
+    field may share its name with a core array, e.g. "charge")."""
+    import dsdecompx_b200 as dsx
+    if a < 13:
+        return np.dtype(dsx.CORE_DTYPES[a]), 1
+    _, t, c = grid.fields[a - 13]
+    return np.dtype(dsx.FIELD_DTYPES[t]), c
+
+
 def gpu_state(grid, names):
-    """Host copies of every array's owned and ghost regions (rank order),
-    the per-rank counts and their prefixes."""
+    """Host copies of every array's owned and ghost regions (rank order, by
+    array id), the per-rank counts and their prefixes."""
     import torch
     v = grid.view()
     o, g = grid.all_counts()
     N, G = int(o.sum()), int(g.sum())
     state = {}
     for a, name in enumerate(names):
-        dtype = np.dtype(grid.dtype_of(name))
-        size = dtype.itemsize * grid.components(name)
+        dtype, comps = array_info(grid, a)
+        size = dtype.itemsize * comps
 
         def region(offset, count):
             if count == 0:
@@ -65,15 +75,15 @@ def gpu_state(grid, names):
             t = torch.as_tensor(DeviceBytes(v.base[a] + size * int(offset), size * count),
                                 device="cuda")
             return t.cpu().numpy().view(dtype)
-        state[name] = (region(v.owned_offset, N), region(v.ghost_offset, G))
+        state[a] = (region(v.owned_offset, N), region(v.ghost_offset, G))
     ob = np.concatenate([[0], np.cumsum(o)])
     gb = np.concatenate([[0], np.cumsum(g)])
     return state, o, g, ob, gb
 
 
-def rank_arrays(grid, state, ob, gb, r, name):
-    comps = grid.components(name)
-    owned, ghosts = state[name]
+def rank_arrays(grid, state, ob, gb, r, a):
+    comps = array_info(grid, a)[1]
+    owned, ghosts = state[a]
     got = np.concatenate([owned[ob[r] * comps:ob[r + 1] * comps],
                           ghosts[gb[r] * comps:gb[r + 1] * comps]])
     return got.reshape(-1, comps) if comps > 1 else got
@@ -154,16 +164,15 @@ def run_config(cuda, workload, steps, seed=2024):
             # the reference receives the GPU's ghost forces in its own slots
             for r in range(P):
                 if g[r]:
-                    for name in ("fx", "fy", "fz"):
-                        ref.write(r, name, int(o[r]),
-                                  state[name][1][gb[r]:gb[r + 1]])
+                    for a, name in ((6, "fx"), (7, "fy"), (8, "fz")):
+                        ref.write(r, name, int(o[r]), state[a][1][gb[r]:gb[r + 1]])
             if field_names:
                 ref.reverse_exchange([(n, "sum") for n in field_names])
             ref.reverse_halo()
             for r in range(P):
-                for name in names:
-                    want = ref.read(r, name)
-                    got = rank_arrays(grid, state, ob, gb, r, name)
+                for a, name in enumerate(names):
+                    want = ref.read(r, name) if a < 13 else ref.read_field(r, name)
+                    got = rank_arrays(grid, state, ob, gb, r, a)
                     assert got.shape == want.shape, (workload, step, r, name)
                     if not np.array_equal(bits(got), bits(want)):
                         bad = np.flatnonzero((got != want).reshape(len(got), -1).any(axis=1))
