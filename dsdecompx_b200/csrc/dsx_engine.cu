@@ -551,6 +551,7 @@ struct dsx_grid {
         cuda_check(cudaMemset(S.gbase, 0, sizeof(int) * (P + 1)), "memset");
         S.bowner = device_alloc<int>(fixed_owned, ncap);
         S.boff = device_alloc<int>(fixed_owned, ncap + 1);
+        S.bfirst = device_alloc<int>(fixed_owned, ncap);
         S.cbase = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * dsx::kHaloCounters);
         S.halo_info = device_alloc<int>(fixed_owned, 4);
         cuda_check(cudaMemset(S.halo_info, 0, 4 * sizeof(int)), "memset");

@@ -828,7 +828,8 @@ __device__ __forceinline__ void halo_scatter_tile(int g, const Grid& G, const Ar
                                                   const unsigned* __restrict__ mask,
                                                   const int* pre, int stride, const int* cbase,
                                                   int* ghost_owner, int* ghost_entry,
-                                                  int* bowner, int* boff, int* bslot) {
+                                                  int* bowner, int* boff, int* bslot,
+                                                  int* bfirst) {
     __shared__ int s_cnt[NW][32];
     __shared__ int s_base[32];
     __shared__ int s_off[kMaxNeighbors + 1];
@@ -905,6 +906,7 @@ __device__ __forceinline__ void halo_scatter_tile(int g, const Grid& G, const Ar
                 const int rank = __popc(hit & lt);
                 const int slot = list_base + rank;
                 bslot[img + k] = slot;
+                if (k == 0) bfirst[b] = slot;
                 ++k;
                 if (staged) {
                     s_own[stage_base + rank] = static_cast<unsigned short>(i - begin);
@@ -949,12 +951,12 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
                                                      const int* pre, int stride,
                                                      const int* cbase, int* ghost_owner,
                                                      int* ghost_entry, int* bowner, int* boff,
-                                                     int* bslot) {
+                                                     int* bslot, int* bfirst) {
     if (*G.status & kStatusGhostOverflow) return;
     const int nt = tile_limit(G, ntiles);
     for (int g = G.tile_first + blockIdx.x; g < nt; g += gridDim.x) {
         halo_scatter_tile(g, G, A, owned_off, ghost_off, tiles, mask, pre, stride, cbase,
-                          ghost_owner, ghost_entry, bowner, boff, bslot);
+                          ghost_owner, ghost_entry, bowner, boff, bslot, bfirst);
         __syncthreads();
     }
 }
@@ -1303,7 +1305,7 @@ __global__ void __launch_bounds__(NT, 4) k_step_move(Grid G, Arrays A, long long
                                                   const unsigned* __restrict__ mask_in,
                                                   int* emig_src, int* emig_dst, int* ghost_owner,
                                                   int* ghost_entry, int* bowner, int* boff,
-                                                  int* bslot) {
+                                                  int* bslot, int* bfirst) {
     __shared__ int s_cnt[NW][32];
     __shared__ int s_base[32];
     __shared__ int s_off[kMaxNeighbors + 1];
@@ -1410,6 +1412,7 @@ __global__ void __launch_bounds__(NT, 4) k_step_move(Grid G, Arrays A, long long
                     const int rank = __popc(hit & lt);
                     const int slot = list_base + rank;
                     bslot[img + k] = slot;
+                    if (k == 0) bfirst[b] = slot;
                     ++k;
                     if (staged) {
                         s_own[stage_base + rank] = static_cast<unsigned short>(i - begin);
@@ -1726,7 +1729,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     Grid G, Arrays A, long long src_off, long long dst_off, long long ghost_off, const int* pre,
     int stride, const int* cbase_ret, const unsigned short* __restrict__ dest_in,
     const unsigned* __restrict__ mask_in, const int* __restrict__ tile_bases, int* emig_src,
-    int* emig_dst, int* ghost_owner, int* ghost_entry, int* bowner, int* boff, int* bslot, int a0,
+    int* emig_dst, int* ghost_owner, int* ghost_entry, int* bowner, int* boff, int* bslot, int* bfirst, int a0,
     int a1, int index_outputs) {
     extern __shared__ __align__(16) unsigned char s_rec[];
     __shared__ __align__(8) unsigned long long s_bar;
@@ -1853,7 +1856,10 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
                 const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
                 if ((mj >> n) & 1u) {
                     const int rank = __popc(hit & lt);
-                    if (index_outputs) bslot[img + k] = list_base + rank;
+                    if (index_outputs) {
+                        bslot[img + k] = list_base + rank;
+                        if (k == 0) bfirst[b] = list_base + rank;
+                    }
                     ++k;
                     if (staged) s_own[stage_base + rank] = static_cast<unsigned short>(l);
                 }
@@ -2110,11 +2116,17 @@ __global__ void __launch_bounds__(NT) k_forward_fields(Arrays A, long long owned
 
 // Owner-centric deterministic sum: owner += ghost images in the order the
 // reference's Host reverse_exchange visits them (neighbor n ascending,
-// dsDecompX src/halo.cpp:1507-1530).  No atomics.
+// dsDecompX src/halo.cpp:1507-1530).  No atomics.  The first image's slot is
+// read beside the owner index (bfirst), so the owner's force and its first
+// image arrive in one round trip; further images (edges, corners) follow
+// from the CSR.
 __global__ void __launch_bounds__(NT) k_reverse_sum3(const int* info, const int* __restrict__ bowner,
                                                      const int* __restrict__ boff,
-                                                     const int* __restrict__ bslot, double* ox,
-                                                     double* oy, double* oz,
+                                                     const int* __restrict__ bslot,
+                                                     const int* __restrict__ bfirst,
+                                                     double* __restrict__ ox,
+                                                     double* __restrict__ oy,
+                                                     double* __restrict__ oz,
                                                      const double* __restrict__ gx,
                                                      const double* __restrict__ gy,
                                                      const double* __restrict__ gz,
@@ -2124,9 +2136,13 @@ __global__ void __launch_bounds__(NT) k_reverse_sum3(const int* info, const int*
     const int B = b_end >= 0 ? b_end : info[1];
     for (int b = b_first + blockIdx.x * NT + threadIdx.x; b < B; b += gridDim.x * NT) {
         const int i = bowner[b];
+        const int s0 = bfirst[b];
         const int k0 = boff[b], k1 = boff[b + 1];
         double fx = ox[i], fy = oy[i], fz = oz[i];
-        for (int k = k0; k < k1; ++k) {
+        fx = __dadd_rn(fx, gx[s0]);
+        fy = __dadd_rn(fy, gy[s0]);
+        fz = __dadd_rn(fz, gz[s0]);
+        for (int k = k0 + 1; k < k1; ++k) {
             const int slot = bslot[k];
             fx = __dadd_rn(fx, gx[slot]);
             fy = __dadd_rn(fy, gy[slot]);
@@ -2688,7 +2704,7 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long
         k_halo_scatter<<<grid, NT, 0, s>>>(Gs, A, owned_off, ghost_off, G.tiles,
                                            G.tile_start + G.P, S.mask, S.pre, S.stride, S.cbase,
                                            S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
-                                           S.bslot);
+                                           S.bslot, S.bfirst);
     });
     if (S.marks) S.marks->mark(s, "halo_scatter");
 }
@@ -2735,17 +2751,17 @@ void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, con
     auto pick = [&](auto plain, auto combined) { return S.classify_combine ? combined : plain; };
     switch (S.classify_threads) {
     case 64:
-        pick(k_step_classify<64, 12, false>, k_step_classify<64, 12, true>)<<<G.max_tiles, 64, 0, s>>>(
+        pick(k_step_classify<64, 16, false>, k_step_classify<64, 16, true>)<<<G.max_tiles, 64, 0, s>>>(
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
             S.mask);
         break;
     case 256:
-        pick(k_step_classify<256, 4, false>, k_step_classify<256, 4, true>)<<<G.max_tiles, 256, 0, s>>>(
+        pick(k_step_classify<256, 5, false>, k_step_classify<256, 5, true>)<<<G.max_tiles, 256, 0, s>>>(
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
             S.mask);
         break;
     default:
-        pick(k_step_classify<128, 8, false>, k_step_classify<128, 8, true>)<<<G.max_tiles, 128, 0, s>>>(
+        pick(k_step_classify<128, 12, false>, k_step_classify<128, 12, true>)<<<G.max_tiles, 128, 0, s>>>(
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
             S.mask);
     }
@@ -2794,18 +2810,18 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
             k_step_move_staged<true, false><<<G.max_tiles, NT, bytes, s>>>(
                 G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
                 S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
-                S.boff, S.bslot, a0, a1, index_outputs);
+                S.boff, S.bslot, S.bfirst, a0, a1, index_outputs);
         else
             k_step_move_staged<false, false><<<G.max_tiles, NT, bytes, s>>>(
                 G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
                 S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
-                S.boff, S.bslot, a0, a1, index_outputs);
+                S.boff, S.bslot, S.bfirst, a0, a1, index_outputs);
     };
     if (S.move_staged == 3 && whole - kForceStageBytes <= kStagedMaxBytes) {
         k_step_move_staged<true, true><<<G.max_tiles, NT, whole - kForceStageBytes, s>>>(
             G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
             S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
-            S.bslot, 0, narrays, 1);
+            S.bslot, S.bfirst, 0, narrays, 1);
     } else if (S.move_staged == 1 && whole <= kStagedMaxBytes) {
         staged(true, 0, narrays, 1);
     } else if (S.move_staged != 0 && split) {
@@ -2819,7 +2835,7 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
         k_step_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
                                                S.cbase, S.dest16, S.mask, S.emig_src, S.emig_dst,
                                                S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
-                                               S.bslot);
+                                               S.bslot, S.bfirst);
     }
 }
 
@@ -2843,7 +2859,7 @@ void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long lon
     k_halo_scatter<<<imm_grid, NT, 0, s>>>(Gn, A, dst_off, ghost_off, S.imm_tiles,
                                            S.imm_tile_start + G.P, S.mask, S.pre2, S.stride,
                                            S.cbase_imm, S.ghost_owner, S.ghost_entry, S.bowner,
-                                           S.boff, S.bslot);
+                                           S.boff, S.bslot, S.bfirst);
 }
 
 void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
@@ -2890,12 +2906,12 @@ void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, cons
             const int b0 = plain->boundary_start[r], b1 = plain->boundary_start[r + 1];
             if (b1 <= b0) continue;
             k_reverse_sum3<<<stream_grid(b1 - b0), NT, 0, s>>>(S.halo_info, S.bowner, S.boff,
-                                                               S.bslot, ox, oy, oz, gx, gy, gz,
+                                                               S.bslot, S.bfirst, ox, oy, oz, gx, gy, gz,
                                                                G.status, b0, b1);
         }
     } else {
         const int grid = S.reverse_per_sm > 0 ? sm_count() * S.reverse_per_sm : stream_grid(G.ncap);
-        k_reverse_sum3<<<grid, NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot, ox, oy, oz, gx,
+        k_reverse_sum3<<<grid, NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot, S.bfirst, ox, oy, oz, gx,
                                            gy, gz, G.status, 0, -1);
     }
     if (S.marks) S.marks->mark(s, "reverse_sum");

@@ -52,6 +52,7 @@ struct Scratch {
     int* bowner = nullptr;     // [ncap] owned index of each boundary owner
     int* boff = nullptr;       // [ncap+1] CSR offsets into bslot
     int* bslot = nullptr;      // [gcap] ghost slots of each boundary owner, n ascending
+    int* bfirst = nullptr;     // [ncap] ghost slot of each boundary owner's first image
     int* halo_info = nullptr;  // {G, B}
     int* cbase = nullptr;      // [P*28] per subdomain: tile prefix -> global index
     // fused step

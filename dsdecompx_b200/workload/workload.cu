@@ -78,7 +78,7 @@ __global__ void k_advance() { ++g_step; }
 // read it.
 __device__ unsigned int g_done = 0;
 
-__global__ void k_step_work(double* x, double* y, double* z, const int* gid, long long n,
+__global__ void __launch_bounds__(256, 5) k_step_work(double* x, double* y, double* z, const int* gid, long long n,
                             double* fx, double* fy, double* fz, const int* totals,
                             std::uint64_t seed, double sigma) {
     const std::uint64_t step = g_step;
@@ -142,12 +142,12 @@ __global__ void k_interior(const double* x, const double* y, const double* z, lo
     }
 }
 
-int grid_for(long long n) {
+int grid_for(long long n, int per_sm = 8) {
     int sms = 148, device = 0;
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const long long want = (n + 255) / 256;
-    const long long cap = static_cast<long long>(sms) * 8;
+    const long long cap = static_cast<long long>(sms) * per_sm;
     return static_cast<int>(want < 1 ? 1 : (want < cap ? want : cap));
 }
 
@@ -189,7 +189,7 @@ int dsxw_ghost_forces(const dsx_grid_view* v, unsigned long long seed, long long
 int dsxw_step_work(const dsx_grid_view* v, unsigned long long seed, double sigma, void* stream) {
     const long long o = v->owned_offset, g = v->ghost_offset;
     const long long span = v->particles > v->ghost_capacity ? v->particles : v->ghost_capacity;
-    k_step_work<<<grid_for(span), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    k_step_work<<<grid_for(span, 5), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double*>(v->base[0]) + o, static_cast<double*>(v->base[1]) + o,
         static_cast<double*>(v->base[2]) + o, static_cast<const int*>(v->base[12]) + o,
         v->particles, static_cast<double*>(v->base[6]) + g, static_cast<double*>(v->base[7]) + g,
