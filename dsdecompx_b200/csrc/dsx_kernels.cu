@@ -2038,6 +2038,7 @@ __global__ void __launch_bounds__(NT) k_halo_refresh_owners(Grid G, Arrays A, lo
                                                             const int* __restrict__ bowner,
                                                             const int* __restrict__ boff,
                                                             const int* __restrict__ bslot,
+                                                            const int* __restrict__ bfirst,
                                                             const int* __restrict__ ghost_entry) {
     if (*G.status & kStatusGhostOverflow) return;
     const int B = info[1];
@@ -2045,21 +2046,23 @@ __global__ void __launch_bounds__(NT) k_halo_refresh_owners(Grid G, Arrays A, lo
     const int step = gridDim.x * NT;
     for (int b0 = blockIdx.x * NT + threadIdx.x; b0 < B; b0 += U * step) {
         long long src[U];
-        int k0[U], k1[U];
+        int k0[U], k1[U], first[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int b = b0 + u * step;
             const bool in = b < B;
             src[u] = owned_off + (in ? ro(bowner + b) : 0);
+            first[u] = in ? ro(bfirst + b) : 0;
             k0[u] = in ? ro(boff + b) : 0;
             k1[u] = in ? ro(boff + b + 1) : 0;
         }
+        // the owner's record and its first image's list entry in one round trip
         double p[U][6];
-        int first[U];
+        int entry[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             if (k0[u] >= k1[u]) continue;
-            first[u] = ro(bslot + k0[u]);
+            entry[u] = ro(ghost_entry + first[u]);
 #pragma unroll
             for (int a = 0; a < 3; ++a) p[u][a] = ro(A.d[a] + src[u]);
             if (!positions_only)
@@ -2070,7 +2073,7 @@ __global__ void __launch_bounds__(NT) k_halo_refresh_owners(Grid G, Arrays A, lo
         for (int u = 0; u < U; ++u) {
             for (int k = k0[u]; k < k1[u]; ++k) {
                 const int slot = k == k0[u] ? first[u] : ro(bslot + k);
-                const double* sh = G.shift + 3ll * ro(ghost_entry + slot);
+                const double* sh = G.shift + 3ll * (k == k0[u] ? entry[u] : ro(ghost_entry + slot));
                 const long long gi = ghost_off + slot;
                 A.d[0][gi] = __dadd_rn(p[u][0], sh[0]);
                 A.d[1][gi] = __dadd_rn(p[u][1], sh[1]);
@@ -2881,7 +2884,7 @@ void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, lo
         if (ctas_per_sm > 0 && grid > sm_count() * ctas_per_sm) grid = sm_count() * ctas_per_sm;
         k_halo_refresh_owners<<<grid, NT, 0, s>>>(G, A, owned_off, ghost_off, positions_only ? 1 : 0,
                                                   S.halo_info, S.bowner, S.boff, S.bslot,
-                                                  S.ghost_entry);
+                                                  S.bfirst, S.ghost_entry);
         return;
     }
     int grid = resident_grid(reinterpret_cast<const void*>(k_halo_refresh), G.gcap);
