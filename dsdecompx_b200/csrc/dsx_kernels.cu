@@ -497,7 +497,8 @@ __global__ void __launch_bounds__(NT) k_emig_place(Grid G, Arrays A, long long s
                                                    long long dst_off, const int* emig_info,
                                                    const int* __restrict__ emig_src,
                                                    const int* __restrict__ emig_dst,
-                                                   const int* hist, const int* imm_base) {
+                                                   const int* hist, const int* imm_base,
+                                                   const int* __restrict__ gap) {
     extern __shared__ int sm[];  // [NW][P]
     const int P = G.P;
     const int E = emig_info[0], nchunks = emig_info[1];
@@ -533,8 +534,20 @@ __global__ void __launch_bounds__(NT) k_emig_place(Grid G, Arrays A, long long s
             const int d = dj[j];
             const unsigned peers = __match_any_sync(0xffffffffu, d);
             if (d >= 0) {
-                const int pos = imm_base[d] + hist[static_cast<long long>(c) * P + d] +
-                                sm[warp * P + d] + __popc(peers & lt);
+                int pos = imm_base[d] + hist[static_cast<long long>(c) * P + d] +
+                          sm[warp * P + d] + __popc(peers & lt);
+                if (gap) {
+                    // a sharded step: other shards' groups of immigrants of
+                    // d that come before this emigrant's source q
+                    const int i = emig_src[e];
+                    int lo = 0, hi = P;   // largest q with obase[q] <= i
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (G.obase[mid] <= i) lo = mid;
+                        else hi = mid;
+                    }
+                    pos += gap[d * P + lo];
+                }
                 const long long src = src_off + emig_src[e];
                 const double ox = ro(A.d[0] + src), oy = ro(A.d[1] + src), oz = ro(A.d[2] + src);
                 const double wx = G.periodic[0] ? wrap_axis(ox, G.lower[0], G.extent[0]) : ox;
@@ -993,7 +1006,8 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                                                       int stride, int* imm_total, int* imm_list,
                                                       int* imm_bnd, int* imm_img,
                                                       unsigned short* __restrict__ dest_out,
-                                                      unsigned* __restrict__ mask_out) {
+                                                      unsigned* __restrict__ mask_out,
+                                                      int* pairs) {
     constexpr int CI = TILE / CT;   // 32-particle groups per warp
     constexpr int CW = CT / 32;
     static_assert(CI * CT == TILE && CW >= 1, "tile split");
@@ -1075,6 +1089,8 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                 mask_out[static_cast<long long>(g) * TILE + (i - begin)] = mg;
             } else {
                 me = halo_mask(halo_bounds(G, d), G.lut + d * 64, wx, wy, wz);
+                // emigrants per (destination, source), for a sharded step
+                if (pairs) atomicAdd(&pairs[d * G.P + s], 1);
                 if constexpr (!COMBINE) {
                     atomicAdd(&imm_total[d], 1);
                     if (me) {
@@ -1714,6 +1730,30 @@ __global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int s
     }
     fill_tiles_grid(G.P, G.tile, G.n_next, G.obase_next, G.tile_start_next, G.tiles_next);
     fill_tiles_grid(G.P, G.tile, imm_in, imm_base, imm_ts, imm_tiles);
+}
+
+// The tile prefixes of the step's counters summed per subdomain, for a
+// sharded step whose layout is planned on the host from the counts of every
+// shard: out[0, P) retained particles, [P, 2P) boundary owners and [2P, 3P)
+// their images (the retained parts), [3P, 3P + 26P) the retained part of
+// every send list, and out[29P] the emigrants of this shard.
+__global__ void __launch_bounds__(1024) k_step_export(Grid G, const int* pre, int stride, int* out) {
+    const int P = G.P;
+    const int* ts = G.tile_start;
+    auto tile_sum = [&](int k, int r) {
+        return pre[k * stride + ts[r + 1]] - pre[k * stride + ts[r]];
+    };
+    for (int t = threadIdx.x; t < P; t += blockDim.x) {
+        out[t] = tile_sum(kStepStay, t);
+        out[P + t] = tile_sum(kBoundaryCounter, t);
+        out[2 * P + t] = tile_sum(kImageCounter, t);
+    }
+    for (int idx = threadIdx.x; idx < P * kMaxNeighbors; idx += blockDim.x) {
+        const int r = idx / kMaxNeighbors, n = idx % kMaxNeighbors;
+        const bool active = n < G.nn[r] && G.nbr[idx] >= 0;
+        out[3 * P + idx] = active ? tile_sum(n, r) : 0;
+    }
+    if (threadIdx.x == 0) out[29 * P] = pre[kStepEmig * stride + ts[P]];
 }
 
 // F4 with the tile's records staged in shared memory (same output as
@@ -2686,7 +2726,8 @@ void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long
     k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, S.imm_total, G.status);
     if (S.marks) S.marks->mark(s, "emig_colscan");
     k_emig_place<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(
-        G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base);
+        G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base,
+        nullptr);
     if (S.marks) S.marks->mark(s, "emig_place");
 }
 
@@ -2747,6 +2788,7 @@ bool staged_passes(const Arrays& A, int* ends, int& passes) {
 void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, const Scratch& S,
                           cudaStream_t s) {
     cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P * (3 + kMaxNeighbors), s);
+    if (S.pairs) cudaMemsetAsync(S.pairs, 0, sizeof(int) * G.P * G.P, s);
     const double* x = A.d[0] + src_off;
     const double* y = A.d[1] + src_off;
     const double* z = A.d[2] + src_off;
@@ -2756,17 +2798,17 @@ void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, con
     case 64:
         pick(k_step_classify<64, 16, false>, k_step_classify<64, 16, true>)<<<G.max_tiles, 64, 0, s>>>(
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
-            S.mask);
+            S.mask, S.pairs);
         break;
     case 256:
         pick(k_step_classify<256, 5, false>, k_step_classify<256, 5, true>)<<<G.max_tiles, 256, 0, s>>>(
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
-            S.mask);
+            S.mask, S.pairs);
         break;
     default:
         pick(k_step_classify<128, 12, false>, k_step_classify<128, 12, true>)<<<G.max_tiles, 128, 0, s>>>(
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
-            S.mask);
+            S.mask, S.pairs);
     }
 }
 
@@ -2842,16 +2884,41 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
     }
 }
 
-void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
-                        long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
+void launch_step_emigrants(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
+                           const Scratch& S, const int* local_imm, const int* gap, cudaStream_t s) {
     const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
     const size_t smem = sizeof(int) * NW * G.P;
     k_emig_hist<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(G.P, S.emig_info, S.emig_dst,
                                                                   S.emig_hist);
-    k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, S.imm_total, G.status);
+    k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, local_imm, G.status);
     k_emig_place<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(
-        G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base);
+        G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base, gap);
     if (S.marks) S.marks->mark(s, "emig_place");
+}
+
+void launch_step_scan(const Grid& G, const Scratch& S, cudaStream_t s) {
+    k_scan_counters<<<kStepCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+}
+
+void launch_step_export(const Grid& G, const Scratch& S, int* out, cudaStream_t s) {
+    k_step_export<<<1, 1024, 0, s>>>(G, S.pre, S.stride, out);
+}
+
+void launch_step_bases(const Grid& G, const Scratch& S, const int* imm_in, cudaStream_t s) {
+    k_tile_bases<<<stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s>>>(
+        G, S.pre, S.stride, S.cbase, S.tile_bases, imm_in, S.imm_base, S.imm_tile_start,
+        S.imm_tiles);
+}
+
+void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
+                        long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
+    launch_step_emigrants(G, A, src_off, dst_off, S, S.imm_total, nullptr, s);
+    launch_step_immigrant_halo(Gn, A, dst_off, ghost_off, S, s);
+}
+
+void launch_step_immigrant_halo(const Grid& Gn, const Arrays& A, long long dst_off,
+                                long long ghost_off, const Scratch& S, cudaStream_t s) {
+    const Grid& G = Gn;
     // immigrants: masks, list ranks and ghost images over their segments
     const int imm_grid = G.max_tiles < sm_count() * 4 ? G.max_tiles : sm_count() * 4;
     k_halo_classify<<<imm_grid, NT, 0, s>>>(Gn, S.imm_tiles, S.imm_tile_start + G.P,

@@ -53,6 +53,11 @@ struct Scratch {
     int* boff = nullptr;       // [ncap+1] CSR offsets into bslot
     int* bslot = nullptr;      // [gcap] ghost slots of each boundary owner, n ascending
     int* bfirst = nullptr;     // [ncap] ghost slot of each boundary owner's first image
+    // sharded step only (null otherwise): emigrants per (destination, source)
+    // from the classify, and the gap before each source's group of
+    // immigrants that other shards fill
+    int* pairs = nullptr;      // [P*P] pairs[t * P + q]
+    int* gap = nullptr;        // [P*P] gap[t * P + q]
     int* halo_info = nullptr;  // {G, B}
     int* cbase = nullptr;      // [P*28] per subdomain: tile prefix -> global index
     // fused step
@@ -112,6 +117,21 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
                       long long ghost_off, const Scratch& S, cudaStream_t s);
 void launch_step_finish(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
                         long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s);
+// The finish in its two parts: the emigrants' stable multi-split into the
+// next half (local_imm: emigrants expected per destination, checked; gap:
+// null, or P x P slots left before each source's group for other shards'
+// immigrants), then the immigrants' masks and ghost images.
+void launch_step_emigrants(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
+                           const Scratch& S, const int* local_imm, const int* gap, cudaStream_t s);
+void launch_step_immigrant_halo(const Grid& Gn, const Arrays& A, long long dst_off,
+                                long long ghost_off, const Scratch& S, cudaStream_t s);
+// A sharded step's pieces around its host-planned layout: the counter scan
+// alone, the per-subdomain export of the scanned counters (29 P + 1 ints, see
+// k_step_export), and the tile bases and descriptors of the planned layout
+// (imm_in: immigrants per subdomain whose ghost images this grid makes).
+void launch_step_scan(const Grid& G, const Scratch& S, cudaStream_t s);
+void launch_step_export(const Grid& G, const Scratch& S, int* out, cudaStream_t s);
+void launch_step_bases(const Grid& G, const Scratch& S, const int* imm_in, cudaStream_t s);
 // Move kinds that apply to this record, as bits: 1 direct reads (kind 0),
 // 2 staged (kind 1: one pass when a tile of the record fits 100 KB of shared
 // memory, else passes of at most 56 KB), 4 staged in passes although one
