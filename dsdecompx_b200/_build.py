@@ -80,7 +80,8 @@ def build_cpp_tests(force: bool = False, verbose: bool = False) -> List[str]:
     """C++ programs under tests/cpp that exercise the drop-in API like the
     reference's own sanity checks."""
     out = []
-    for src in sorted(glob.glob(os.path.join(ROOT, "tests", "cpp", "*.cpp"))):
+    for src in sorted(glob.glob(os.path.join(ROOT, "tests", "cpp", "*.cpp")) +
+                      glob.glob(os.path.join(ROOT, "tests", "cpp", "*.cu"))):
         exe = os.path.join(LIBDIR, os.path.splitext(os.path.basename(src))[0])
         if force or _stale(exe, [src, LIB]):
             cmd = [nvcc()] + ARCH + ["-O2", "-std=c++17", "-I" + INCLUDE, "-I" + MPI_STUB, "-o", exe, src,

@@ -3,6 +3,7 @@
 // the extern "C" entry points declared in include/dsx.h.
 #include "dsx.h"
 #include "dsx_errors.h"
+#include "dsx_shard.h"
 #include "dsx_kernels.cuh"
 
 #include <algorithm>
@@ -267,6 +268,7 @@ struct dsx_grid {
 
     ~dsx_grid() {
         destroy_graphs();
+        free_shard_buffers();
         for (auto& e : marks.ev) if (e) cudaEventDestroy(e);
         for (void* p : arrays_owned) cudaFree(p);
         for (void* p : scratch_owned) cudaFree(p);
@@ -652,6 +654,7 @@ struct dsx_grid {
     }
 
     void commit_migrate() {
+        sharded_ghosts = false;
         pairs_valid = true;
         plain_bounds.clear();
         parity ^= 1;
@@ -725,6 +728,7 @@ struct dsx_grid {
 
     // Builds the plan; grows the ghost region and rebuilds when it overflowed.
     void build_checked(cudaStream_t stream) {
+        sharded_ghosts = false;
         for (;;) {
             clear_status(stream);
             enqueue_halo_build(stream, plain_layout(stream));
@@ -739,6 +743,7 @@ struct dsx_grid {
 
     void exchange_halo(bool rebuild, bool positions_only, cudaStream_t stream, long long* results) {
         not_pending("exchange_halo");
+        sharded_ghosts = false;
         if (rebuild) plan_valid = false;
         bool reused = false;
         if (P == 1) {
@@ -798,6 +803,7 @@ struct dsx_grid {
     // resident CTA) so that interior work on other streams finds SM room.
     void begin_halo(bool rebuild, bool positions_only, cudaStream_t stream) {
         not_pending("begin_halo_exchange");
+        sharded_ghosts = false;
         if (rebuild) plan_valid = false;
         pending_rebuild = rebuild;
         pending_reused = false;
@@ -897,6 +903,8 @@ struct dsx_grid {
 
     void reverse_exchange(int nf, const int* ids, const int* ops, cudaStream_t stream) {
         not_pending("reverse_exchange");
+        if (sharded_ghosts)
+            fail(DSX_E_LOGIC, "a sharded step's ghosts exchange fields through dsx_shard_reverse_exchange");
         const dsx::FieldOps F = field_ops(nf, ids, ops, "reverse-exchanged");
         if (P == 1 || !ghosts_valid || nf == 0) return;
         dsx::launch_reverse_fields(params(), A, owned_off(), ghost_off(), F, S, stream);
@@ -904,6 +912,8 @@ struct dsx_grid {
 
     void forward_exchange(int nf, const int* ids, cudaStream_t stream) {
         not_pending("forward_exchange");
+        if (sharded_ghosts)
+            fail(DSX_E_LOGIC, "a sharded step's ghosts exchange fields through dsx_shard_forward_exchange");
         const dsx::FieldOps F = field_ops(nf, ids, nullptr, "forward-exchanged");
         if (P == 1 || !ghosts_valid || nf == 0) return;
         dsx::launch_forward_fields(params(), A, owned_off(), ghost_off(), F, S, stream);
@@ -1336,6 +1346,543 @@ struct dsx_grid {
         if (status_out) *status_out = st;
     }
 
+    // ------------------------------------------------------ sharded step
+    // One fused step of a grid that holds only the subdomains t with
+    // owners[t] == shard, as one process of a sharded grid (include/dsx_shard.h).
+    // The counts of every shard are summed first (classify, counter scan,
+    // then one all-reduce), so the layout of the next owned half and of the
+    // ghost region is planned on the host before anything moves: the move
+    // writes retained particles and ghost images straight to their final
+    // slots, the emigrants land in the source order of the reference with
+    // gaps for the groups other shards send, and only emigrants, ghost lists
+    // toward other shards' receivers and those lists' forces cross shards.
+    //
+    // Ghost region of a shard: its own receivers first (rank order), each
+    // block in the receiver's neighbor order with the lists of every sender;
+    // then the other shards' receivers (by shard, then rank) holding only
+    // the lists of this shard's senders (sent away after the build, their
+    // forces returned before the reverse sum).
+    struct ShardPlan {
+        std::vector<int> n_next, obase_next, tile_start_next;   // P, P+1, P+1
+        std::vector<int> imm_base, imm_tiles_in, imm_tile_start, local_imm;   // P, P, P+1, P
+        std::vector<int> gap;                                    // P*P
+        std::vector<long long> results;                          // P*6
+        std::vector<int> list_ret, list_len, send_base;          // P*26
+        std::vector<int> g, gbase;                               // P, P+1
+        std::vector<int> cbase_ret, cbase_imm;                   // P*28
+        long long own_total = 0, out_total = 0, ghosts = 0, own_ghosts = 0, boundary = 0, images = 0;
+        int emigrants = 0;
+        // per peer shard: outgoing emigrants [out_start, out_end) of the next
+        // half; outgoing ghost lists [gout_start, gout_end) of the ghost region
+        std::vector<long long> out_start, out_end, gout_start, gout_end;
+        std::vector<long long> recv_particles, recv_ghosts;      // per peer
+    };
+
+    // export: this shard's 29P + 1 export ints; imm: the P * 29 immigrant
+    // counters; pairs: P * P; all three summed over shards except export[29P]
+    // (the local emigrants) and `local_pairs` (this shard's own pairs).
+    ShardPlan plan_shard(const std::vector<long long>& sum, const std::vector<int>& owners, int shard,
+                         int nshards, int local_emigrants) const {
+        const int E = dsx::kMaxNeighbors;
+        ShardPlan pl;
+        const long long* stays = sum.data();
+        const long long* bret = stays + P;
+        const long long* iret = bret + P;
+        const long long* lret = iret + P;                       // P * 26
+        const long long* imm_total = lret + static_cast<std::size_t>(P) * E;
+        const long long* imm_list = imm_total + P;             // P * 26
+        const long long* imm_bnd = imm_list + static_cast<std::size_t>(P) * E;
+        const long long* imm_img = imm_bnd + P;
+        const long long* pairs = imm_img + P;                   // P * P, [t * P + q]
+        auto own = [&](int t) { return owners[static_cast<std::size_t>(t)] == shard; };
+        auto pair = [&](int t, int q) { return pairs[static_cast<std::size_t>(t) * P + q]; };
+        pl.emigrants = local_emigrants;
+        // owned layout: own subdomains contiguous in rank order, then the
+        // outgoing emigrants by (destination's shard, destination)
+        pl.n_next.assign(P, 0);
+        pl.obase_next.assign(P + 1, 0);
+        pl.tile_start_next.assign(P + 1, 0);
+        pl.imm_base.assign(P, 0);
+        pl.imm_tiles_in.assign(P, 0);
+        pl.imm_tile_start.assign(P + 1, 0);
+        pl.local_imm.assign(P, 0);
+        pl.gap.assign(static_cast<std::size_t>(P) * P, 0);
+        pl.results.assign(static_cast<std::size_t>(P) * 6, 0);
+        for (int t = 0; t < P; ++t) {
+            long long local = 0;
+            for (int q = 0; q < P; ++q)
+                if (own(q)) local += pair(t, q);
+            pl.local_imm[t] = static_cast<int>(local);
+            if (own(t)) {
+                pl.n_next[t] = static_cast<int>(stays[t] + imm_total[t]);
+                pl.imm_tiles_in[t] = static_cast<int>(imm_total[t]);
+                long long before_remote = 0;
+                for (int q = 0; q < P; ++q) {
+                    if (own(q)) pl.gap[static_cast<std::size_t>(t) * P + q] = static_cast<int>(before_remote);
+                    else before_remote += pair(t, q);
+                }
+                long long sent = 0;
+                for (int d = 0; d < P; ++d) sent += pair(d, t);
+                long long* o = &pl.results[static_cast<std::size_t>(6) * t];
+                o[1] = stays[t] + sent;
+                o[2] = stays[t];
+                o[3] = sent;
+                o[4] = imm_total[t];
+                o[5] = stays[t] + imm_total[t];
+                o[0] = (o[3] != 0 || o[4] != 0) ? 1 : 0;
+            }
+        }
+        for (int t = 0; t < P; ++t) {
+            pl.obase_next[t + 1] = pl.obase_next[t] + pl.n_next[t];
+            pl.tile_start_next[t + 1] = pl.tile_start_next[t] + (pl.n_next[t] + dsx::kTile - 1) / dsx::kTile;
+            pl.imm_tile_start[t + 1] = pl.imm_tile_start[t] + (pl.imm_tiles_in[t] + dsx::kTile - 1) / dsx::kTile;
+            if (own(t)) pl.imm_base[t] = pl.obase_next[t] + static_cast<int>(stays[t]);
+        }
+        pl.own_total = pl.obase_next[P];
+        pl.out_start.assign(nshards, 0);
+        pl.out_end.assign(nshards, 0);
+        long long at = pl.own_total;
+        for (int p = 0; p < nshards; ++p) {
+            pl.out_start[p] = at;
+            if (p != shard)
+                for (int t = 0; t < P; ++t)
+                    if (owners[t] == p) {
+                        pl.imm_base[t] = static_cast<int>(at);
+                        at += pl.local_imm[t];
+                    }
+            pl.out_end[p] = at;
+        }
+        pl.out_total = at - pl.own_total;
+        // remote immigrants each peer sends: groups (own t, source q of p)
+        pl.recv_particles.assign(nshards, 0);
+        for (int t = 0; t < P; ++t)
+            if (own(t))
+                for (int q = 0; q < P; ++q)
+                    if (!own(q)) pl.recv_particles[owners[q]] += pair(t, q);
+        // ghost layout: list lengths, receiver order, list bases
+        pl.list_ret.assign(static_cast<std::size_t>(P) * E, 0);
+        pl.list_len.assign(static_cast<std::size_t>(P) * E, 0);
+        pl.send_base.assign(static_cast<std::size_t>(P) * E, 0);
+        pl.g.assign(P, 0);
+        pl.gbase.assign(P + 1, 0);
+        for (int r = 0; r < P; ++r)
+            for (std::size_t n = 0; n < topo[r].size(); ++n) {
+                if (topo[r][n].rank < 0) continue;
+                const std::size_t e = static_cast<std::size_t>(r) * E + n;
+                pl.list_ret[e] = static_cast<int>(lret[e]);
+                pl.list_len[e] = static_cast<int>(lret[e] + imm_list[e]);
+            }
+        std::vector<int> order;
+        for (int q = 0; q < P; ++q)
+            if (own(q)) order.push_back(q);
+        const std::size_t own_receivers = order.size();
+        for (int p = 0; p < nshards; ++p)
+            if (p != shard)
+                for (int q = 0; q < P; ++q)
+                    if (owners[q] == p) order.push_back(q);
+        pl.gout_start.assign(nshards, 0);
+        pl.gout_end.assign(nshards, 0);
+        pl.recv_ghosts.assign(nshards, 0);
+        long long run = 0;
+        for (std::size_t k = 0; k < order.size(); ++k) {
+            const int q = order[k];
+            if (k == own_receivers) pl.own_ghosts = run;
+            const int p = owners[q];
+            if (!own(q) && (k == own_receivers || owners[order[k - 1]] != p)) pl.gout_start[p] = run;
+            pl.gbase[q] = static_cast<int>(run);
+            for (std::size_t m = 0; m < topo[q].size(); ++m) {
+                const int e = sender_entry(q, static_cast<int>(m));
+                if (e < 0) continue;
+                const int r = e / E;
+                const bool present = own(q) || own(r);
+                const long long len = present ? pl.list_len[static_cast<std::size_t>(e)] : 0;
+                pl.send_base[static_cast<std::size_t>(e)] = static_cast<int>(run);
+                if (own(q) && !own(r)) pl.recv_ghosts[owners[r]] += len;
+                run += len;
+            }
+            pl.g[q] = own(q) ? static_cast<int>(run - pl.gbase[q]) : 0;
+            if (!own(q)) pl.gout_end[p] = run;
+        }
+        if (order.size() == own_receivers) pl.own_ghosts = run;
+        pl.ghosts = run;
+        pl.gbase[P] = static_cast<int>(run);
+        // counter bases of own senders: lists (retained part, immigrant
+        // part), boundary owners and images (retained first)
+        pl.cbase_ret.assign(static_cast<std::size_t>(P) * dsx::kHaloCounters, 0);
+        pl.cbase_imm.assign(static_cast<std::size_t>(P) * dsx::kHaloCounters, 0);
+        long long bb = 0, ib = 0;
+        for (int r = 0; r < P; ++r) {
+            if (!own(r)) continue;
+            for (std::size_t n = 0; n < topo[r].size(); ++n) {
+                if (topo[r][n].rank < 0) continue;
+                const std::size_t e = static_cast<std::size_t>(r) * E + n;
+                pl.cbase_ret[static_cast<std::size_t>(r) * dsx::kHaloCounters + n] = pl.send_base[e];
+                pl.cbase_imm[static_cast<std::size_t>(r) * dsx::kHaloCounters + n] = pl.send_base[e] + pl.list_ret[e];
+            }
+            int* cr = &pl.cbase_ret[static_cast<std::size_t>(r) * dsx::kHaloCounters];
+            int* ci = &pl.cbase_imm[static_cast<std::size_t>(r) * dsx::kHaloCounters];
+            cr[dsx::kBoundaryCounter] = static_cast<int>(bb);
+            ci[dsx::kBoundaryCounter] = static_cast<int>(bb + bret[r]);
+            cr[dsx::kImageCounter] = static_cast<int>(ib);
+            ci[dsx::kImageCounter] = static_cast<int>(ib + iret[r]);
+            bb += bret[r] + imm_bnd[r];
+            ib += iret[r] + imm_img[r];
+        }
+        pl.boundary = bb;
+        pl.images = ib;
+        return pl;
+    }
+
+    // message buffers of the sharded step, one per peer and direction (grow only)
+    struct PeerBuffer {
+        void* data = nullptr;
+        long long capacity = 0;
+        void* ensure(long long bytes) {
+            if (bytes > capacity) {
+                cudaFree(data);
+                data = nullptr;
+                capacity = 0;
+                cuda_check(cudaMalloc(&data, static_cast<std::size_t>(bytes)), "cudaMalloc message buffer");
+                capacity = bytes;
+            }
+            return data;
+        }
+    };
+    std::vector<PeerBuffer> shard_send, shard_recv;
+    int* d_export = nullptr;        // [29P + 1]
+    int* d_local_imm = nullptr;     // [P]
+    int* d_imm_tiles_in = nullptr;  // [P]
+    int* d_own_totals = nullptr;    // {own receivers' ghosts, boundary owners}
+    bool sharded_ghosts = false;    // the ghost region holds a sharded step's layout
+
+    void free_shard_buffers() {
+        for (auto& b : shard_send) cudaFree(b.data);
+        for (auto& b : shard_recv) cudaFree(b.data);
+        shard_send.clear();
+        shard_recv.clear();
+    }
+
+    long long array_bytes(int a) const {
+        return a < 11 ? 8 : a < 13 ? 4 : fields[static_cast<std::size_t>(a - 13)].bytes;
+    }
+
+    unsigned char* array_base(int a) const {
+        return static_cast<unsigned char*>(
+            a < 11 ? static_cast<void*>(A.d[a]) : a == 11 ? static_cast<void*>(A.type) :
+            a == 12 ? static_cast<void*>(A.gid) : static_cast<void*>(A.f.base[a - 13]));
+    }
+
+    // One message per peer each way: pack `count[p]` records of `arrays`
+    // starting at element `first[p]` of `region` (an element offset into
+    // the arrays) into peer p's send buffer, one 16-byte aligned section per
+    // array; the received messages are scattered by `place(p, buffer
+    // sections)`.
+    template <class Place>
+    void shard_exchange(const dsx_transport& tr, int shard, int nshards, const std::vector<int>& arrays,
+                        long long region, const std::vector<long long>& first,
+                        const std::vector<long long>& count, const std::vector<long long>& incoming,
+                        cudaStream_t stream, Place&& place) {
+        auto packed = [&](long long n) {
+            long long b = 0;
+            for (int a : arrays) b += (n * array_bytes(a) + 15) / 16 * 16;
+            return b;
+        };
+        auto sections = [&](void* buf, long long n) {
+            std::vector<unsigned char*> out;
+            long long at = 0;
+            for (int a : arrays) {
+                out.push_back(static_cast<unsigned char*>(buf) + at);
+                at += (n * array_bytes(a) + 15) / 16 * 16;
+            }
+            return out;
+        };
+        if (static_cast<int>(shard_send.size()) < nshards) {
+            shard_send.resize(static_cast<std::size_t>(nshards));
+            shard_recv.resize(static_cast<std::size_t>(nshards));
+        }
+        std::vector<int> to, from;
+        std::vector<const void*> sb;
+        std::vector<void*> rb;
+        std::vector<long long> sn, rn;
+        std::vector<dsx::CopyPiece> pack;
+        for (int p = 0; p < nshards; ++p) {
+            if (p == shard) continue;
+            if (count[p] > 0) {
+                void* buf = shard_send[p].ensure(packed(count[p]));
+                const std::vector<unsigned char*> sec = sections(buf, count[p]);
+                for (std::size_t j = 0; j < arrays.size(); ++j) {
+                    const long long b = array_bytes(arrays[j]);
+                    pack.push_back({array_base(arrays[j]) + (region + first[p]) * b, sec[j], count[p] * b});
+                }
+                to.push_back(p);
+                sb.push_back(buf);
+                sn.push_back(packed(count[p]));
+            }
+            if (incoming[p] > 0) {
+                from.push_back(p);
+                rb.push_back(shard_recv[p].ensure(packed(incoming[p])));
+                rn.push_back(packed(incoming[p]));
+            }
+        }
+        if (!pack.empty()) cuda_check(dsx::launch_copies(pack, stream), "pack messages");
+        if (!to.empty() || !from.empty()) {
+            if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
+                            static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
+                            stream) != DSX_OK)
+                fail(DSX_E_RUNTIME, "transport exchange failed");
+        }
+        std::vector<dsx::CopyPiece> unpack;
+        for (std::size_t k = 0; k < from.size(); ++k)
+            place(from[k], sections(rb[k], incoming[from[k]]), unpack);
+        if (!unpack.empty()) cuda_check(dsx::launch_copies(unpack, stream), "unpack messages");
+    }
+
+    void sharded_step(const int* owners_in, int shard, int nshards, const dsx_transport& tr,
+                      dsx_step_callback cb, void* user, cudaStream_t stream, unsigned* status_out) {
+        not_pending("the sharded step");
+        if (!tr.allreduce_i64 || !tr.allreduce_f64 || !tr.exchange)
+            fail(DSX_E_INVALID, "the transport needs both all-reduces and the exchange");
+        if (nshards < 1 || shard < 0 || shard >= nshards) fail(DSX_E_INVALID, "shard out of range");
+        const std::vector<int> owners(owners_in, owners_in + P);
+        for (int t = 0; t < P; ++t)
+            if (owners[t] < 0 || owners[t] >= nshards) fail(DSX_E_INVALID, "subdomain owner out of range");
+        const int E = dsx::kMaxNeighbors;
+        const std::size_t PP = static_cast<std::size_t>(P) * P;
+        if (!S.pairs) {
+            S.pairs = device_alloc<int>(fixed_owned, PP);
+            S.gap = device_alloc<int>(fixed_owned, PP);
+            d_export = device_alloc<int>(fixed_owned, static_cast<std::size_t>(29) * P + 1);
+            d_local_imm = device_alloc<int>(fixed_owned, P);
+            d_imm_tiles_in = device_alloc<int>(fixed_owned, P);
+            d_own_totals = device_alloc<int>(fixed_owned, 2);
+        }
+        clear_status(stream);
+        // Dynamic cut planes from the owned counts of every shard
+        const double* work_in = nullptr;
+        if (desc.policy == DSX_DYNAMIC) {
+            const std::vector<int> n = read_ints(layout[cur][0], P, stream);
+            std::vector<double> w(n.begin(), n.end());
+            if (tr.allreduce_f64(tr.user, w.data(), P) != DSX_OK) fail(DSX_E_RUNTIME, "transport all-reduce failed");
+            cuda_check(cudaMemcpyAsync(work, w.data(), sizeof(double) * P, cudaMemcpyHostToDevice, stream),
+                       "upload work");
+            work_in = work;
+        }
+        enqueue_rebalance(stream, true, work_in);
+        const dsx::Grid G = params();
+        dsx::launch_step_classify(G, A, owned_off(), S, stream);
+        dsx::launch_step_scan(G, S, stream);
+        dsx::launch_step_export(G, S, d_export, stream);
+        // this shard's counts, summed over every shard
+        const std::size_t nx = static_cast<std::size_t>(29) * P;
+        std::vector<int> ex(nx + 1), imm(nx), pr(PP);
+        cuda_check(cudaMemcpyAsync(ex.data(), d_export, sizeof(int) * (nx + 1), cudaMemcpyDeviceToHost, stream), "read counts");
+        cuda_check(cudaMemcpyAsync(imm.data(), S.imm_total, sizeof(int) * nx, cudaMemcpyDeviceToHost, stream), "read counts");
+        cuda_check(cudaMemcpyAsync(pr.data(), S.pairs, sizeof(int) * PP, cudaMemcpyDeviceToHost, stream), "read counts");
+        cuda_check(cudaStreamSynchronize(stream), "read counts");
+        std::vector<long long> sum(2 * nx + PP + static_cast<std::size_t>(nshards), 0);
+        for (std::size_t k = 0; k < nx; ++k) sum[k] = ex[k];
+        for (std::size_t k = 0; k < nx; ++k) sum[nx + k] = imm[k];
+        for (std::size_t k = 0; k < PP; ++k) sum[2 * nx + k] = pr[k];
+        sum[2 * nx + PP + static_cast<std::size_t>(shard)] = ncap;
+        if (tr.allreduce_i64(tr.user, sum.data(), static_cast<long long>(sum.size())) != DSX_OK)
+            fail(DSX_E_RUNTIME, "transport all-reduce failed");
+        const long long* pairs = sum.data() + 2 * nx;
+        const long long* imm_total = sum.data() + nx;
+        auto pair = [&](int t, int q) { return pairs[static_cast<std::size_t>(t) * P + q]; };
+        // every shard checks every shard's storage with the same numbers, so
+        // a shortfall anywhere fails everywhere before data moves
+        for (int p = 0; p < nshards; ++p) {
+            long long need = 0;
+            for (int t = 0; t < P; ++t) {
+                if (owners[t] == p) need += sum[static_cast<std::size_t>(t)] + imm_total[t];
+                else
+                    for (int q = 0; q < P; ++q)
+                        if (owners[q] == p) need += pair(t, q);
+            }
+            if (need > sum[2 * nx + PP + static_cast<std::size_t>(p)])
+                fail(DSX_E_LENGTH, "particle storage of shard " + std::to_string(p) +
+                                       " is smaller than its particles after the step's migration");
+        }
+        const ShardPlan pl = plan_shard(sum, owners, shard, nshards, ex[nx]);
+        if (pl.ghosts > gcap) grow_ghosts(pl.ghosts, stream);   // nothing is written yet
+        // the planned layout to the device
+        auto up = [&](void* dst, const void* src, std::size_t bytes) {
+            if (bytes) cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "upload plan");
+        };
+        const int emig_info[2] = {pl.emigrants, (pl.emigrants + dsx::kTile - 1) / dsx::kTile};
+        const int halo_info[2] = {static_cast<int>(pl.ghosts), static_cast<int>(pl.boundary)};
+        const int own_totals[2] = {static_cast<int>(pl.own_ghosts), static_cast<int>(pl.boundary)};
+        const int images = static_cast<int>(pl.images);
+        up(layout[cur ^ 1][0], pl.n_next.data(), sizeof(int) * P);
+        up(layout[cur ^ 1][1], pl.obase_next.data(), sizeof(int) * (P + 1));
+        up(layout[cur ^ 1][2], pl.tile_start_next.data(), sizeof(int) * (P + 1));
+        up(S.imm_base, pl.imm_base.data(), sizeof(int) * P);
+        up(S.imm_tile_start, pl.imm_tile_start.data(), sizeof(int) * (P + 1));
+        up(d_imm_tiles_in, pl.imm_tiles_in.data(), sizeof(int) * P);
+        up(d_local_imm, pl.local_imm.data(), sizeof(int) * P);
+        up(S.gap, pl.gap.data(), sizeof(int) * PP);
+        up(S.emig_info, emig_info, sizeof(emig_info));
+        up(S.mig_results, pl.results.data(), sizeof(long long) * 6 * P);
+        up(S.list_ret, pl.list_ret.data(), sizeof(int) * P * E);
+        up(S.list_len, pl.list_len.data(), sizeof(int) * P * E);
+        up(S.send_base, pl.send_base.data(), sizeof(int) * P * E);
+        up(S.g, pl.g.data(), sizeof(int) * P);
+        up(S.gbase, pl.gbase.data(), sizeof(int) * (P + 1));
+        up(S.cbase, pl.cbase_ret.data(), sizeof(int) * P * dsx::kHaloCounters);
+        up(S.cbase_imm, pl.cbase_imm.data(), sizeof(int) * P * dsx::kHaloCounters);
+        up(S.halo_info, halo_info, sizeof(halo_info));
+        up(d_own_totals, own_totals, sizeof(own_totals));
+        up(S.boff + pl.boundary, &images, sizeof(int));
+        // stays and ghost images of the retained particles, then the
+        // emigrants in the reference's order with gaps for other shards'
+        const dsx::Grid Gp = params();
+        dsx::launch_step_bases(Gp, S, d_imm_tiles_in, stream);
+        dsx::launch_step_move(Gp, A, owned_off(), next_off(), ghost_off(), S, stream);
+        dsx::launch_step_emigrants(Gp, A, owned_off(), next_off(), S, d_local_imm, S.gap, stream);
+        cuda_check(cudaStreamSynchronize(stream), "step move");   // the host vectors above are read
+        std::vector<int> all(static_cast<std::size_t>(13 + fields.size()));
+        for (std::size_t a = 0; a < all.size(); ++a) all[a] = static_cast<int>(a);
+        // emigrants to other shards' subdomains, and their emigrants into the gaps
+        std::vector<long long> first(nshards, 0), count(nshards, 0);
+        for (int p = 0; p < nshards; ++p) {
+            first[p] = pl.out_start[p];
+            count[p] = pl.out_end[p] - pl.out_start[p];
+        }
+        shard_exchange(tr, shard, nshards, all, next_off(), first, count, pl.recv_particles, stream,
+                       [&](int p, const std::vector<unsigned char*>& sec, std::vector<dsx::CopyPiece>& out) {
+            long long off = 0;
+            for (int t = 0; t < P; ++t) {
+                if (owners[t] != shard) continue;
+                long long before = 0;
+                for (int q = 0; q < P; ++q) {
+                    const long long c = pair(t, q);
+                    if (owners[q] == p && c > 0) {
+                        for (std::size_t j = 0; j < all.size(); ++j) {
+                            const long long b = array_bytes(all[j]);
+                            out.push_back({sec[j] + off * b,
+                                           array_base(all[j]) + (next_off() + pl.imm_base[t] + before) * b,
+                                           c * b});
+                        }
+                        off += c;
+                    }
+                    before += c;
+                }
+            }
+        });
+        // the immigrants' ghost images (this shard's and the others')
+        cur ^= 1;
+        const dsx::Grid Gn = params();
+        cur ^= 1;
+        dsx::launch_step_immigrant_halo(Gn, A, next_off(), ghost_off(), S, stream);
+        // ghost lists toward other shards' receivers, theirs into this shard's blocks
+        for (int p = 0; p < nshards; ++p) {
+            first[p] = pl.gout_start[p];
+            count[p] = pl.gout_end[p] - pl.gout_start[p];
+        }
+        auto own_rows = [&](int p, auto&& row) {
+            long long off = 0;
+            for (int q = 0; q < P; ++q) {
+                if (owners[q] != shard) continue;
+                for (std::size_t m = 0; m < topo[q].size(); ++m) {
+                    const int e = sender_entry(q, static_cast<int>(m));
+                    if (e < 0 || owners[e / E] != p) continue;
+                    const long long len = pl.list_len[static_cast<std::size_t>(e)];
+                    if (len > 0) row(off, pl.send_base[static_cast<std::size_t>(e)], len);
+                    off += len;
+                }
+            }
+        };
+        shard_exchange(tr, shard, nshards, all, ghost_off(), first, count, pl.recv_ghosts, stream,
+                       [&](int p, const std::vector<unsigned char*>& sec, std::vector<dsx::CopyPiece>& out) {
+            own_rows(p, [&](long long off, long long slot, long long len) {
+                for (std::size_t j = 0; j < all.size(); ++j) {
+                    const long long b = array_bytes(all[j]);
+                    out.push_back({sec[j] + off * b, array_base(all[j]) + (ghost_off() + slot) * b, len * b});
+                }
+            });
+        });
+        // the new layout is the current one for the callback and the reverse sum
+        parity ^= 1;
+        cur ^= 1;
+        total = pl.own_total;
+        pairs_valid = false;
+        plan_valid = false;
+        ghosts_valid = false;
+        sharded_ghosts = true;
+        plain_bounds.clear();
+        std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
+        if (cb) {
+            dsx_grid_view v = view();
+            v.halo_totals = d_own_totals;
+            cb(user, stream, &v);
+        }
+        // forces of this shard's blocks back to the senders' shards, and the
+        // forces of this shard's lists from theirs
+        const std::vector<int> forces = {6, 7, 8};
+        {
+            // gather this shard's receivers' ghosts of each peer's lists
+            std::vector<long long> back(nshards, 0);
+            for (int p = 0; p < nshards; ++p)
+                if (p != shard) back[p] = pl.recv_ghosts[p];
+            std::vector<long long> theirs(nshards, 0);
+            for (int p = 0; p < nshards; ++p) theirs[p] = pl.gout_end[p] - pl.gout_start[p];
+            if (static_cast<int>(shard_send.size()) < nshards) {
+                shard_send.resize(static_cast<std::size_t>(nshards));
+                shard_recv.resize(static_cast<std::size_t>(nshards));
+            }
+            std::vector<int> to, from;
+            std::vector<const void*> sb;
+            std::vector<void*> rb;
+            std::vector<long long> sn, rn;
+            std::vector<dsx::CopyPiece> pack, unpack;
+            auto packed = [&](long long n) { return 3 * ((n * 8 + 15) / 16 * 16); };
+            auto section = [&](void* buf, long long n, int j) {
+                return static_cast<unsigned char*>(buf) + j * ((n * 8 + 15) / 16 * 16);
+            };
+            for (int p = 0; p < nshards; ++p) {
+                if (p == shard) continue;
+                if (back[p] > 0) {
+                    void* buf = shard_send[p].ensure(packed(back[p]));
+                    own_rows(p, [&](long long off, long long slot, long long len) {
+                        for (int j = 0; j < 3; ++j)
+                            pack.push_back({array_base(forces[j]) + (ghost_off() + slot) * 8,
+                                            section(buf, back[p], j) + off * 8, len * 8});
+                    });
+                    to.push_back(p);
+                    sb.push_back(buf);
+                    sn.push_back(packed(back[p]));
+                }
+                if (theirs[p] > 0) {
+                    void* buf = shard_recv[p].ensure(packed(theirs[p]));
+                    for (int j = 0; j < 3; ++j)
+                        unpack.push_back({section(buf, theirs[p], j),
+                                          array_base(forces[j]) + (ghost_off() + pl.gout_start[p]) * 8,
+                                          theirs[p] * 8});
+                    from.push_back(p);
+                    rb.push_back(buf);
+                    rn.push_back(packed(theirs[p]));
+                }
+            }
+            if (!pack.empty()) cuda_check(dsx::launch_copies(pack, stream), "pack forces");
+            if (!to.empty() || !from.empty()) {
+                if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
+                                static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
+                                stream) != DSX_OK)
+                    fail(DSX_E_RUNTIME, "transport exchange failed");
+            }
+            if (!unpack.empty()) cuda_check(dsx::launch_copies(unpack, stream), "unpack forces");
+        }
+        enqueue_reverse(stream);
+        const unsigned st = read_status(stream);
+        if (st & dsx::kStatusCopyTimeout)
+            fail(DSX_E_RUNTIME, "a bulk copy of particle records did not complete within 1 s");
+        if (st & dsx::kStatusMigrationMismatch) fail(DSX_E_RUNTIME, "migration count mismatch");
+        if (st & dsx::kStatusCutsInvalid)
+            fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");
+        if (st & dsx::kStatusGhostOverflow) fail(DSX_E_RUNTIME, "ghost region overflow in a planned step");
+        if (status_out) *status_out = st;
+    }
+
     void upload(const long long* counts, const void* const* arrays, cudaStream_t stream) {
         long long sum = 0;
         for (int s = 0; s < P; ++s) {
@@ -1394,7 +1941,7 @@ struct dsx_grid {
         const std::vector<int> n = read_ints(layout[cur][0], P, stream);
         const std::vector<int> ob = read_ints(layout[cur][1], P, stream);
         std::vector<int> g(static_cast<std::size_t>(P), 0), gb(static_cast<std::size_t>(P), 0);
-        if (ghosts_valid) {
+        if (ghosts_valid || sharded_ghosts) {
             g = read_ints(S.g, P, stream);
             gb = read_ints(S.gbase, P, stream);
         }
@@ -1596,7 +2143,7 @@ int dsx_grid_counts(dsx_grid* grid, long long* owned, long long* ghosts, void* s
         const auto s = static_cast<cudaStream_t>(stream);
         const std::vector<int> n = grid->read_ints(grid->layout[grid->cur][0], grid->P, s);
         std::vector<int> g(static_cast<std::size_t>(grid->P), 0);
-        if (grid->ghosts_valid) g = grid->read_ints(grid->S.g, grid->P, s);
+        if (grid->ghosts_valid || grid->sharded_ghosts) g = grid->read_ints(grid->S.g, grid->P, s);
         for (int r = 0; r < grid->P; ++r) {
             if (owned) owned[r] = n[static_cast<std::size_t>(r)];
             if (ghosts) ghosts[r] = g[static_cast<std::size_t>(r)];
@@ -1721,6 +2268,18 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
             fail(DSX_E_INVALID, "capturing the step in a CUDA graph needs a created stream, not the default stream");
         grid->step(callback, user, capture != 0, static_cast<cudaStream_t>(stream), status);
         cuda_check(cudaGetLastError(), "launch step");
+    });
+}
+
+int dsx_grid_sharded_step(dsx_grid* grid, const int* owners, int shard, int nshards,
+                          const dsx_transport* transport, dsx_step_callback callback, void* user,
+                          void* stream, unsigned* status) {
+    return guarded([&] {
+        if (!grid || !owners || !transport) fail(DSX_E_INVALID, "null argument");
+        if (grid->P == 1) fail(DSX_E_INVALID, "the sharded step needs at least two subdomains");
+        grid->sharded_step(owners, shard, nshards, *transport, callback, user,
+                           static_cast<cudaStream_t>(stream), status);
+        cuda_check(cudaGetLastError(), "launch sharded step");
     });
 }
 

@@ -821,6 +821,20 @@ int dsx_shard_reverse_halo(dsx_shard* shard, void* stream) {
     });
 }
 
+int dsx_shard_step(dsx_shard* shard, dsx_step_callback callback, void* user, void* stream,
+                   unsigned* status) {
+    return guarded([&] {
+        if (!shard) fail(DSX_E_INVALID, "null shard");
+        shard->planned = false;   // the per-call plan and the assembled region are stale
+        check(dsx_grid_sharded_step(shard->grid, shard->owners.data(), shard->shard, shard->nshards,
+                                    &shard->tr, callback, user, stream, status));
+        // rebalance, classify + scan + export, bases, move, emigrant
+        // histogram / scan / placement, immigrant masks / scan / scatter,
+        // the reverse sum, and the message copies
+        shard->launches += 12 + (shard->dynamic ? 1 : 0) + 6;
+    });
+}
+
 int dsx_shard_forward_exchange(dsx_shard* shard, int nfields, const int* field_ids, void* stream) {
     return guarded([&] {
         if (!shard || (nfields > 0 && !field_ids)) fail(DSX_E_INVALID, "null argument");
@@ -890,10 +904,14 @@ int dsx_shard_counts(dsx_shard* shard, long long* owned, long long* ghosts, void
     return guarded([&] {
         if (!shard || !owned || !ghosts) fail(DSX_E_INVALID, "null argument");
         const std::vector<long long> o = shard->owned_counts(static_cast<cudaStream_t>(stream));
+        // after a fused step (dsx_shard_step) the grid's own ghost blocks
+        // are this shard's receivers' ghosts
+        std::vector<long long> gg(static_cast<std::size_t>(shard->P), 0), oo(gg.size(), 0);
+        if (!shard->planned) check(dsx_grid_counts(shard->grid, oo.data(), gg.data(), stream));
         for (int t = 0; t < shard->P; ++t) {
             const bool mine = shard->owners[t] == shard->shard;
             owned[t] = mine ? o[t] : 0;
-            ghosts[t] = (mine && shard->planned) ? shard->g[t] : 0;
+            ghosts[t] = !mine ? 0 : shard->planned ? shard->g[t] : gg[static_cast<std::size_t>(t)];
         }
     });
 }

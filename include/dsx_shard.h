@@ -98,6 +98,29 @@ int dsx_shard_exchange_halo(dsx_shard* shard, int rebuild, int positions_only, v
  * added to its owner, in the reference's order. */
 int dsx_shard_reverse_halo(dsx_shard* shard, void* stream);
 
+/* One fused step on every shard: migrate (with the Dynamic rebalance over
+ * all shards' counts), halo build, callback(user, stream, view), reverse_halo
+ * -- the batched step of dsx_grid_step for a sharded grid.  The counts of
+ * every shard are summed before anything moves (one all-reduce), so each
+ * shard plans its layout on the host and its kernels write retained
+ * particles and ghost images straight to their final slots; the transport
+ * then carries only the emigrants to other shards' subdomains, the ghost
+ * lists toward other shards' receivers and, after the callback, those
+ * ghosts' forces.  The view gives this shard's owned particles and its own
+ * receivers' ghosts (halo_totals: {ghosts, boundary owners}); the callback
+ * must not call the field exchanges (they refuse with DSX_E_LOGIC until the
+ * next halo build).  Afterwards the per-call calls start from a rebuild
+ * (exchange_halo builds the plan anew).  status as dsx_grid_step's. */
+int dsx_shard_step(dsx_shard* shard, dsx_step_callback callback, void* user, void* stream,
+                   unsigned* status);
+
+/* The grid-level form of dsx_shard_step, for hosts that keep their own
+ * dsx_grid per process: owners[P] the shard of every subdomain, shard and
+ * nshards this process's place, transport as in dsx_shard_create. */
+int dsx_grid_sharded_step(dsx_grid* grid, const int* owners, int shard, int nshards,
+                          const dsx_transport* transport, dsx_step_callback callback, void* user,
+                          void* stream, unsigned* status);
+
 /* Field exchanges as dsx_grid_forward_exchange / dsx_grid_reverse_exchange,
  * on the assembled ghosts. */
 int dsx_shard_forward_exchange(dsx_shard* shard, int nfields, const int* field_ids, void* stream);

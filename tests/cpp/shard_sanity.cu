@@ -3,8 +3,10 @@
 // copies (no kernel ever waits on another shard), checked against one grid
 // of all P subdomains: results and owned arrays after every migrate, ghost
 // arrays after every halo build and refresh, owned forces after every
-// reverse_halo, field values after a reverse and a forward field exchange;
-// Manual cuts over 4 shards and Dynamic cuts over 2.
+// reverse_halo, field values after a reverse and a forward field exchange,
+// and every owned and ghost array after fused steps (dsx_shard_step) against
+// the one grid's batched step; Manual cuts over 4 shards and Dynamic cuts
+// over 2.
 //
 // usage: shard_sanity   (exits 0 and prints "shard_sanity: ok" when every
 //                        check passed)
@@ -136,6 +138,29 @@ int exchange(void* u, int nsend, const int* to, const void* const* send, const l
     return status;
 }
 
+// The step callback of the fused-step checks: every ghost of the view
+// (halo_totals[0] of them from the ghost offset) gets a force computed from
+// its own id and position, so that equal ghosts get equal forces whatever
+// slot they sit in.
+__global__ void k_forces_from_ghosts(const double* x, const double* y, const int* id, const int* n,
+                                     double* fx, double* fy, double* fz) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n[0]; i += gridDim.x * blockDim.x) {
+        const double a = static_cast<double>(id[i] % 1009) * 0.001;
+        fx[i] = x[i] * 0.5 + a;
+        fy[i] = y[i] * 0.25 - a;
+        fz[i] = a * a + 1.0;
+    }
+}
+
+void forces_callback(void*, void* stream, const dsx_grid_view* v) {
+    const long long g = v->ghost_offset;
+    k_forces_from_ghosts<<<148, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const double*>(v->base[0]) + g, static_cast<const double*>(v->base[1]) + g,
+        static_cast<const int*>(v->base[12]) + g, v->halo_totals,
+        static_cast<double*>(v->base[6]) + g, static_cast<double*>(v->base[7]) + g,
+        static_cast<double*>(v->base[8]) + g);
+}
+
 // every shard runs `call` on its own thread
 void on_shards(int R, const std::function<void(int)>& call) {
     std::vector<std::thread> th;
@@ -206,6 +231,25 @@ void write_shard(dsx_shard* sh, int P, int t, bool ghosts, int a, const void* da
     if (c[t])
         cuda(cudaMemcpy(static_cast<unsigned char*>(v.base[a]) + (off + base) * kBytes[a], data,
                         static_cast<std::size_t>(c[t] * kBytes[a]), cudaMemcpyHostToDevice), "write shard");
+}
+
+// ghosts of subdomain t after a fused step: the shard grid's own ghost block
+std::vector<std::vector<unsigned char>> read_step_ghosts(dsx_shard* sh, int P, int t) {
+    std::vector<long long> o(P), g(P);
+    must(dsx_shard_counts(sh, o.data(), g.data(), nullptr), "counts");
+    dsx_grid_view v{};
+    must(dsx_shard_owned_view(sh, &v), "view");
+    std::vector<int> gb(P + 1);
+    cuda(cudaMemcpy(gb.data(), v.gbase, sizeof(int) * (P + 1), cudaMemcpyDeviceToHost), "gbase");
+    std::vector<std::vector<unsigned char>> out(kArrays);
+    for (int a = 0; a < kArrays; ++a) {
+        out[a].resize(static_cast<std::size_t>(g[t] * kBytes[a]));
+        if (g[t])
+            cuda(cudaMemcpy(out[a].data(),
+                            static_cast<unsigned char*>(v.base[a]) + (v.ghost_offset + gb[t]) * kBytes[a],
+                            out[a].size(), cudaMemcpyDeviceToHost), "read ghosts");
+    }
+    return out;
 }
 
 void run(const Case& cs) {
@@ -431,6 +475,42 @@ void run(const Case& cs) {
         must(dsx_grid_exchange_halo(ref, 1, 0, nullptr, nullptr), "halo");
         on_shards(R, [&](int r) { must(dsx_shard_exchange_halo(shards[r], 1, 0, streams[r], nullptr), "shard halo"); });
         compare("ghosts after the rebalance", true);
+    }
+    // the fused step (dsx_shard_step) against the one grid's batched step:
+    // owned arrays (forces summed back included) and every ghost array
+    for (int step = 0; step < 3; ++step) {
+        displace(step + 200, 1.2);
+        unsigned st = 0;
+        must(dsx_grid_step(ref, forces_callback, nullptr, 0, nullptr, &st), "grid step");
+        expect(st == 0, "grid step status", 0);
+        std::vector<unsigned> ss(R, 0);
+        on_shards(R, [&](int r) {
+            must(dsx_shard_step(shards[r], forces_callback, nullptr, streams[r], &ss[r]), "shard step");
+        });
+        for (int r = 0; r < R; ++r) expect(ss[r] == 0, "shard step status", r);
+        compare("owned after the fused step", false);
+        std::vector<long long> o(P), g(P);
+        must(dsx_grid_counts(ref, o.data(), g.data(), nullptr), "counts");
+        for (int t = 0; t < P; ++t) {
+            dsx_shard* sh = shards[owners[t]];
+            std::vector<long long> so(P), sg(P);
+            must(dsx_shard_counts(sh, so.data(), sg.data(), nullptr), "counts");
+            expect(sg[t] == g[t], "ghost count after the fused step", t);
+            const auto want = read_ref(ref, t, o[t], g[t]);
+            const auto got = read_step_ghosts(sh, P, t);
+            for (int a = 0; a < kArrays; ++a) expect(want[a] == got[a], "ghosts after the fused step", t);
+        }
+    }
+    // the per-call calls go on from the fused step (a rebuild first)
+    displace(300, 0.4);
+    {
+        std::vector<long long> mr(6 * P);
+        must(dsx_grid_migrate(ref, nullptr, mr.data()), "migrate");
+        on_shards(R, [&](int r) { must(dsx_shard_migrate(shards[r], streams[r], nullptr), "shard migrate"); });
+        compare("owned after a migrate that follows the fused step", false);
+        must(dsx_grid_exchange_halo(ref, 1, 0, nullptr, nullptr), "halo");
+        on_shards(R, [&](int r) { must(dsx_shard_exchange_halo(shards[r], 1, 0, streams[r], nullptr), "shard halo"); });
+        compare("ghosts after a rebuild that follows the fused step", true);
     }
     for (int r = 0; r < R; ++r) {
         dsx_shard_destroy(shards[r]);
