@@ -63,6 +63,9 @@ def parse():
                          "of the workload), the shards run in lockstep on one GPU")
     ap.add_argument("--sharded-impl", default="native", choices=["native", "python"],
                     help="the library's sharded protocol (dsx_shard_*) or the Python one")
+    ap.add_argument("--sharded-step", default="fused", choices=["fused", "calls"],
+                    help="native sharded grid: the fused step (dsx_shard_step) or the per-call "
+                         "operations")
     return ap.parse_args()
 
 
@@ -780,10 +783,22 @@ def run_sharded(args, rank, world, device):
     def launched():
         return sh.launches if native else engine.launches
 
+    fused = native and args.sharded_step == "fused"
+
+    def fused_work(view, s):
+        wl.dsxw_step_work(C.byref(view), seed, w.drift, s)
+
+    def one_step():
+        if fused:
+            status = sh.step_fused(fused_work, stream=stream)
+            assert status == 0, status
+        else:
+            sh.step(user_work)
+
     with torch.cuda.stream(stream):
         sh.upload_flat(counts, ptrs)
         for _ in range(args.warmup):
-            sh.step(user_work)
+            one_step()
     stream.synchronize()
     torch.distributed.barrier()
     torch.cuda.synchronize(device)
@@ -793,7 +808,7 @@ def run_sharded(args, rank, world, device):
         with torch.cuda.stream(stream):
             start.record(stream)
             for _ in range(args.steps):
-                sh.step(user_work)
+                one_step()
             end.record(stream)
         torch.cuda.synchronize(device)
     launches = launched() - launches0 + 3 * args.steps
@@ -828,7 +843,7 @@ def run_sharded(args, rank, world, device):
             e0.record(stream)
             for _ in range(args.e2e_steps):
                 sh.upload_flat(cnt, ptrs)
-                sh.step(user_work)
+                one_step()
                 cnt = sh.download_flat(ptrs)
             e1.record(stream)
         torch.cuda.synchronize(device)
@@ -844,9 +859,10 @@ def run_sharded(args, rank, world, device):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded numpy PCG64 + counter-based device deviates)",
         "config": workload_config(w, world, dims),
-        "step": ("native sharded grid (dsx_shard_*" if native else
-                 "sharded grid (ShardedGrid") + ": per-call operations, one NCCL "
-                "exchange step per call)",
+        "step": ("native sharded grid, fused step (dsx_shard_step: layout planned from every "
+                 "shard's counts, one all-reduce, three NCCL exchanges)" if fused else
+                 ("native sharded grid (dsx_shard_*" if native else "sharded grid (ShardedGrid") +
+                 ": per-call operations, one NCCL exchange step per call)"),
         "roofline": roof,
         "clocks": clock,
         "e2e": e2e,

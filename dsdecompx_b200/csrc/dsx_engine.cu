@@ -1625,12 +1625,11 @@ struct dsx_grid {
             }
         }
         if (!pack.empty()) cuda_check(dsx::launch_copies(pack, stream), "pack messages");
-        if (!to.empty() || !from.empty()) {
-            if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
-                            static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
-                            stream) != DSX_OK)
-                fail(DSX_E_RUNTIME, "transport exchange failed");
-        }
+        // every shard makes the same transport calls, with messages or not
+        if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
+                        static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
+                        stream) != DSX_OK)
+            fail(DSX_E_RUNTIME, "transport exchange failed");
         std::vector<dsx::CopyPiece> unpack;
         for (std::size_t k = 0; k < from.size(); ++k)
             place(from[k], sections(rb[k], incoming[from[k]]), unpack);
@@ -1864,12 +1863,10 @@ struct dsx_grid {
                 }
             }
             if (!pack.empty()) cuda_check(dsx::launch_copies(pack, stream), "pack forces");
-            if (!to.empty() || !from.empty()) {
-                if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
-                                static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
-                                stream) != DSX_OK)
-                    fail(DSX_E_RUNTIME, "transport exchange failed");
-            }
+            if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
+                            static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
+                            stream) != DSX_OK)
+                fail(DSX_E_RUNTIME, "transport exchange failed");
             if (!unpack.empty()) cuda_check(dsx::launch_copies(unpack, stream), "unpack forces");
         }
         enqueue_reverse(stream);
