@@ -1555,7 +1555,26 @@ struct dsx_grid {
     int* d_own_totals = nullptr;    // {own receivers' ghosts, boundary owners}
     bool sharded_ghosts = false;    // the ghost region holds a sharded step's layout
 
+    // pinned host staging of the sharded step's counts and planned tables
+    unsigned char* shard_pinned = nullptr;
+    std::size_t shard_pinned_cap = 0;
+
+    unsigned char* shard_staging(std::size_t bytes) {
+        if (bytes > shard_pinned_cap) {
+            if (shard_pinned) cudaFreeHost(shard_pinned);
+            shard_pinned = nullptr;
+            shard_pinned_cap = 0;
+            void* p = nullptr;
+            cuda_check(cudaMallocHost(&p, bytes), "cudaMallocHost staging");
+            shard_pinned = static_cast<unsigned char*>(p);
+            shard_pinned_cap = bytes;
+        }
+        return shard_pinned;
+    }
+
     void free_shard_buffers() {
+        if (shard_pinned) cudaFreeHost(shard_pinned);
+        shard_pinned = nullptr;
         for (auto& b : shard_send) cudaFree(b.data);
         for (auto& b : shard_recv) cudaFree(b.data);
         shard_send.clear();
@@ -1673,10 +1692,13 @@ struct dsx_grid {
         dsx::launch_step_export(G, S, d_export, stream);
         // this shard's counts, summed over every shard
         const std::size_t nx = static_cast<std::size_t>(29) * P;
-        std::vector<int> ex(nx + 1), imm(nx), pr(PP);
-        cuda_check(cudaMemcpyAsync(ex.data(), d_export, sizeof(int) * (nx + 1), cudaMemcpyDeviceToHost, stream), "read counts");
-        cuda_check(cudaMemcpyAsync(imm.data(), S.imm_total, sizeof(int) * nx, cudaMemcpyDeviceToHost, stream), "read counts");
-        cuda_check(cudaMemcpyAsync(pr.data(), S.pairs, sizeof(int) * PP, cudaMemcpyDeviceToHost, stream), "read counts");
+        int* staged = reinterpret_cast<int*>(shard_staging(sizeof(int) * (2 * nx + 1 + PP)));
+        const int* ex = staged;
+        const int* imm = staged + nx + 1;
+        const int* pr = imm + nx;
+        cuda_check(cudaMemcpyAsync(staged, d_export, sizeof(int) * (nx + 1), cudaMemcpyDeviceToHost, stream), "read counts");
+        cuda_check(cudaMemcpyAsync(staged + nx + 1, S.imm_total, sizeof(int) * nx, cudaMemcpyDeviceToHost, stream), "read counts");
+        cuda_check(cudaMemcpyAsync(staged + 2 * nx + 1, S.pairs, sizeof(int) * PP, cudaMemcpyDeviceToHost, stream), "read counts");
         cuda_check(cudaStreamSynchronize(stream), "read counts");
         std::vector<long long> sum(2 * nx + PP + static_cast<std::size_t>(nshards), 0);
         for (std::size_t k = 0; k < nx; ++k) sum[k] = ex[k];
@@ -1704,9 +1726,23 @@ struct dsx_grid {
         }
         const ShardPlan pl = plan_shard(sum, owners, shard, nshards, ex[nx]);
         if (pl.ghosts > gcap) grow_ghosts(pl.ghosts, stream);   // nothing is written yet
-        // the planned layout to the device
+        // the planned layout to the device, through pinned staging (the
+        // copies stay asynchronous; the staging is reused only after the
+        // step's final synchronize)
+        auto round8 = [](std::size_t b) { return (b + 7) / 8 * 8; };
+        // twenty tables, each rounded up to 8 bytes
+        const std::size_t staging_bytes =
+            sizeof(int) * (7 * static_cast<std::size_t>(P) + 4 * (P + 1) + PP + 2 +
+                           3 * static_cast<std::size_t>(P) * E + 2 * static_cast<std::size_t>(P) * dsx::kHaloCounters + 5) +
+            sizeof(long long) * 6 * static_cast<std::size_t>(P) + 20 * 8;
+        unsigned char* stage = shard_staging(staging_bytes);
+        std::size_t at = 0;
         auto up = [&](void* dst, const void* src, std::size_t bytes) {
-            if (bytes) cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "upload plan");
+            if (!bytes) return;
+            if (at + bytes > staging_bytes) fail(DSX_E_RUNTIME, "plan staging too small");
+            std::memcpy(stage + at, src, bytes);
+            cuda_check(cudaMemcpyAsync(dst, stage + at, bytes, cudaMemcpyHostToDevice, stream), "upload plan");
+            at += round8(bytes);
         };
         const int emig_info[2] = {pl.emigrants, (pl.emigrants + dsx::kTile - 1) / dsx::kTile};
         const int halo_info[2] = {static_cast<int>(pl.ghosts), static_cast<int>(pl.boundary)};
@@ -1738,7 +1774,6 @@ struct dsx_grid {
         dsx::launch_step_bases(Gp, S, d_imm_tiles_in, stream);
         dsx::launch_step_move(Gp, A, owned_off(), next_off(), ghost_off(), S, stream);
         dsx::launch_step_emigrants(Gp, A, owned_off(), next_off(), S, d_local_imm, S.gap, stream);
-        cuda_check(cudaStreamSynchronize(stream), "step move");   // the host vectors above are read
         std::vector<int> all(static_cast<std::size_t>(13 + fields.size()));
         for (std::size_t a = 0; a < all.size(); ++a) all[a] = static_cast<int>(a);
         // emigrants to other shards' subdomains, and their emigrants into the gaps
