@@ -208,3 +208,100 @@ def test_native_shard_over_nccl(cuda):
         ref.close()
         sh.close()
         dist.destroy_process_group()
+
+
+def test_native_fused_step_over_nccl(cuda):
+    """The native shard's fused step (dsx_shard_step) through its
+    torch.distributed transport on a one-rank NCCL group equals the grid's
+    own batched step: every owned array (forces summed back included) and
+    every ghost array, step after step, Dynamic cuts."""
+    import datetime
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import sharded as shd
+    kw = CASES["dynamic-4x4x2-R4"]
+    P, N = kw["nranks"], 30_000
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    owner = Grid("port", P, kw["dims"], kw["policy"], (0, 0, 0), kw["upper"], (True, True, True),
+                 kw["halo_width"], True, kw["dynamic"], [(n, TYPE_INDEX[t], c) for n, t, c in kw["fields"]])
+    per = initial(owner, P, kw["upper"], N, 53, kw["fields"])
+    owner.close()
+    ref = dsx.VirtualGrid(**grid_kw(kw), particles=N, ghost_capacity=2 * N)
+    ref.upload(per)
+    sh = shd.NativeShardedGrid(**grid_kw(kw), particles=N + 4096, ghost_capacity=N)
+
+    def region(view, a, offset, count, dtype):
+        size = np.dtype(dtype).itemsize
+        return torch.as_tensor(_Bytes(view.base[a] + size * int(offset), size * count),
+                               device="cuda").view(torch.float64 if dtype == np.float64 else torch.int32)
+
+    def forces(view, stream):
+        # every ghost slot of the view: a force from the ghost's own
+        # position and id (equal ghosts get equal forces in any slot)
+        cap = int(view.ghost_capacity)
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            x = region(view, 0, view.ghost_offset, cap, np.float64)
+            y = region(view, 1, view.ghost_offset, cap, np.float64)
+            gid = region(view, 12, view.ghost_offset, cap, np.int32)
+            a = torch.remainder(gid, 1009).double().mul(1e-3)
+            region(view, 6, view.ghost_offset, cap, np.float64).copy_(x.mul(0.5).add(a))
+            region(view, 7, view.ghost_offset, cap, np.float64).copy_(y.mul(0.25).sub(a))
+            region(view, 8, view.ghost_offset, cap, np.float64).copy_(a.mul(a).add(1.0))
+
+    try:
+        names = dsx.ARRAYS + [f[0] for f in kw["fields"]]
+        counts = np.array([len(d["x"]) for d in per], dtype=np.int64)
+        host = []
+        for name in names:
+            dt = np.dtype(ref.dtype_of(name))
+            host.append(np.ascontiguousarray(np.concatenate([np.asarray(d[name], dtype=dt).reshape(-1)
+                                                             for d in per])))
+        sh.upload_flat(counts, [h.ctypes.data for h in host])
+        rng = np.random.default_rng(9)
+        for step in range(3):
+            # the same displacement on both, keyed by the owned order (equal)
+            v = ref.view()
+            n = int(v.particles)
+            d = torch.from_numpy(rng.normal(0.0, 0.6, size=(3, n))).cuda()
+            for k, view in enumerate((v, sh.owned_view())):
+                for a in range(3):
+                    region(view, a, view.owned_offset, n, np.float64).add_(d[a])
+            torch.cuda.synchronize()
+            assert ref.step(forces, capture=False) == 0
+            assert sh.step_fused(forces) == 0
+            torch.cuda.synchronize()
+            vr, vs = ref.view(), sh.owned_view()
+            assert int(vr.particles) == int(vs.particles) == n
+            o_ref, g_ref = ref.all_counts()
+            o_sh, g_sh = sh.all_counts()
+            assert (o_ref == o_sh).all() and (g_ref == g_sh).all(), step
+            G = int(g_ref.sum())
+            for a, name in enumerate(names):
+                dt = np.dtype(ref.dtype_of(name))
+                width = dt.itemsize * ref.components(name)
+                for off_r, off_s, count in ((vr.owned_offset, vs.owned_offset, n),
+                                            (vr.ghost_offset, vs.ghost_offset, G)):
+                    got = torch.as_tensor(_Bytes(vs.base[a] + width * int(off_s), width * count),
+                                          device="cuda")
+                    want = torch.as_tensor(_Bytes(vr.base[a] + width * int(off_r), width * count),
+                                           device="cuda")
+                    assert torch.equal(got, want), (step, name)
+    finally:
+        ref.close()
+        sh.close()
+        dist.destroy_process_group()
+
+
+class _Bytes:
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = dict(shape=(int(nbytes),), typestr="|u1",
+                                             data=(int(ptr), False), version=3, strides=None)
