@@ -827,7 +827,8 @@ def run_sharded(args, rank, world, device):
                                       "reverse_sum"))
     peak, peak_kind = peaks()
     achieved = step_bytes / (ms_per_step / 1e3) / 1e9
-    roof = {"bound": "hbm", "kernel": "whole sharded step (per-call path + exchanges)",
+    roof = {"bound": "hbm", "kernel": "whole sharded step (fused: planned kernels + exchanges)"
+            if fused else "whole sharded step (per-call path + exchanges)",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4),
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
