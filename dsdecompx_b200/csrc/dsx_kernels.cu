@@ -2023,9 +2023,10 @@ __global__ void __launch_bounds__(NT) k_halo_refresh(Grid G, Arrays A, long long
                                                      const int* __restrict__ ghost_entry) {
     if (*G.status & kStatusGhostOverflow) return;
     const int total = info[0];
-    // four ghosts per thread and pass: their owner indices, then their
-    // owners' positions, are all in flight before the first store
-    constexpr int U = 4;
+    // two ghosts per thread and pass: their owner indices, then their
+    // owners' positions, are all in flight before the first store (40
+    // registers: three quarters of the SM's threads resident)
+    constexpr int U = 2;
     const int step = gridDim.x * NT;
     for (int s0 = blockIdx.x * NT + threadIdx.x; s0 < total; s0 += U * step) {
         int own[U], ent[U];
@@ -2462,20 +2463,60 @@ __device__ __forceinline__ int owner_of_staged(const Grid& G, const double* s_cu
     return (c[0] * G.dims[1] + c[1]) * G.dims[2] + c[2];
 }
 
+// The cell a position's uniform-cut image would fall in, per axis: a guess
+// that two exact comparisons with the real cuts confirm (cuts[c] <= v <
+// cuts[c+1], the first and last cells open-ended as the clamped search
+// makes them); any other case -- non-uniform cuts that moved the plane past
+// v, a NaN -- takes the full search.  The answer is the search's in every
+// case.
+struct CellGuess {
+    double lower[3], inv[3];   // dims / extent per axis
+};
+
+__device__ __forceinline__ CellGuess cell_guess(const Grid& G) {
+    CellGuess g;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        g.lower[a] = G.lower[a];
+        g.inv[a] = static_cast<double>(G.dims[a]) / G.extent[a];
+    }
+    return g;
+}
+
+__device__ __forceinline__ int owner_of_guessed(const Grid& G, const CellGuess& g,
+                                                const double* s_cuts, double px, double py,
+                                                double pz) {
+    const double p[3] = {px, py, pz};
+    int c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double v = wrap_if(G, a, p[a]);
+        const double* cuts = s_cuts + G.cut_offset[a];
+        const int dims = G.dims[a];
+        int k = static_cast<int>((v - g.lower[a]) * g.inv[a]);   // NaN and overflow land in range below
+        k = k < 0 ? 0 : (k > dims - 1 ? dims - 1 : k);
+        const bool ok = (k == 0 || cuts[k] <= v) && (k == dims - 1 || v < cuts[k + 1]);
+        c[a] = ok ? k : (dims <= kCountedCells ? axis_coordinate_count(cuts, dims, v)
+                                               : axis_coordinate(cuts, dims, v));
+    }
+    return (c[0] * G.dims[1] + c[1]) * G.dims[2] + c[2];
+}
+
 __device__ __forceinline__ void stage_cuts(const Grid& G, double* s_cuts) {
     const int total = G.dims[0] + G.dims[1] + G.dims[2] + 3;
     for (int k = threadIdx.x; k < total; k += blockDim.x) s_cuts[k] = G.cuts[k];
     __syncthreads();
 }
 
-// Four positions per thread and pass, all loaded before any search.
+// Two positions per thread and pass, both loaded before any search.
 __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restrict__ x,
                                                    const double* __restrict__ y,
                                                    const double* __restrict__ z, long long n,
                                                    int* out) {
     __shared__ double s_cuts[kMaxRanks + 16];   // cut_offset[a] + kCountedCells <= 1036
     stage_cuts(G, s_cuts);
-    constexpr int U = 4;
+    const CellGuess guess = cell_guess(G);
+    constexpr int U = 2;
     const long long step = static_cast<long long>(gridDim.x) * NT;
     for (long long i0 = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i0 < n; i0 += U * step) {
         double px[U], py[U], pz[U];
@@ -2491,7 +2532,7 @@ __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restr
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const long long i = i0 + u * step;
-            if (i < n) out[i] = owner_of_staged(G, s_cuts, px[u], py[u], pz[u]);
+            if (i < n) out[i] = owner_of_guessed(G, guess, s_cuts, px[u], py[u], pz[u]);
         }
     }
 }
