@@ -878,3 +878,38 @@ def split_phase_steps(pair, rng, other, busy, L):
     pair.gpu.end_halo_exchange()
     with pytest.raises(RuntimeError, match="without begin"):
         pair.gpu.end_halo_exchange()
+
+
+@pytest.mark.parametrize("dims", [(3, 2, 2), (10, 1, 2)], ids=["counted", "bisected"])
+def test_owner_rank_with_uneven_cuts(cuda, dims):
+    """owner_rank where the cut planes are not uniform (the cell guessed from
+    uniform cuts is then often wrong and the exact search must decide):
+    random positions, the cut values themselves and their neighbors, faces,
+    NaN and infinities, against the oracle; axes short enough to be counted
+    and long enough to be bisected."""
+    import torch
+    rng = np.random.default_rng(19)
+    L = (12.0, 10.0, 9.0)
+    P = int(np.prod(dims))
+    pair = Pair(P, dims, "manual", (0, 0, 0), L, (True, False, True), 0.5, True, None, (),
+                particles=100)
+    try:
+        cuts = []
+        for a in range(3):
+            inner = np.sort(rng.uniform(0.05, 0.95, dims[a] - 1)) * L[a]
+            cuts.append(np.concatenate([[0.0], inner, [L[a]]]))
+        pair.gpu.set_cuts(cuts)
+        pair.ref.set_cuts(cuts)
+        special = np.concatenate([np.concatenate(cuts), np.nextafter(np.concatenate(cuts), -np.inf),
+                                  np.nextafter(np.concatenate(cuts), np.inf),
+                                  [-0.0, -1e-300, 1e300, -37.5, np.inf, -np.inf, np.nan]])
+        pos = rng.uniform(-15, 25, size=(20000, 3))
+        pick = rng.random(pos.shape) < 0.4
+        pos[pick] = rng.choice(special, pick.sum())
+        dev = [torch.as_tensor(np.ascontiguousarray(pos[:, a]), device="cuda") for a in range(3)]
+        out = torch.empty(len(pos), dtype=torch.int32, device="cuda")
+        pair.gpu.owner_rank(*dev, out)
+        torch.cuda.synchronize()
+        assert (out.cpu().numpy() == pair.ref.owner_rank(pos)).all()
+    finally:
+        pair.close()
