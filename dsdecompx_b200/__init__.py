@@ -190,6 +190,26 @@ def copy_segments(copies: np.ndarray, stream=None):
         _check(lib().dsx_copy_segments(c.ctypes.data, c.size, _stream(stream)))
 
 
+def _trampoline(callback, owner):
+    """A step callback for the C ABI: callback(view, stream).  An exception
+    cannot cross the C frames, so it is kept on `owner` and raised by the
+    Python call that ran the step (_raise_callback_error)."""
+    def trampoline(user, s, view_ptr):
+        try:
+            callback(view_ptr.contents, s or 0)   # the default stream arrives as None
+        except BaseException as exc:
+            if getattr(owner, "_callback_error", None) is None:
+                owner._callback_error = exc
+    return trampoline
+
+
+def _raise_callback_error(owner):
+    exc = getattr(owner, "_callback_error", None)
+    if exc is not None:
+        owner._callback_error = None
+        raise RuntimeError(f"the step callback raised {type(exc).__name__}: {exc}") from exc
+
+
 def _check(status: int):
     if status != DSX_OK:
         msg = lib().dsx_last_error().decode()
@@ -471,13 +491,14 @@ class VirtualGrid:
             if callback is None:
                 cache[key] = (None, STEP_CALLBACK())
             else:
-                def trampoline(user, s, view_ptr, _cb=callback):
-                    _cb(view_ptr.contents, s)
-                cache[key] = (callback, STEP_CALLBACK(trampoline))
+                cache[key] = (callback, STEP_CALLBACK(_trampoline(callback, self)))
         cb = cache[key][1]
         st = C.c_uint()
-        _check(self.L.dsx_grid_step(self.h, cb, None, 1 if capture else 0, _stream(stream),
-                                    C.byref(st)))
+        self._callback_error = None
+        status = self.L.dsx_grid_step(self.h, cb, None, 1 if capture else 0, _stream(stream),
+                                      C.byref(st))
+        _raise_callback_error(self)
+        _check(status)
         return st.value
 
     def autotune(self, stream=None) -> Dict[str, object]:

@@ -1069,20 +1069,21 @@ class NativeShardedGrid:
         callback(view, stream), reverse_halo, planned from every shard's
         counts.  The view holds this shard's owned particles and its own
         receivers' ghosts.  Returns the device status bits (0 == ok)."""
-        from . import STEP_CALLBACK
+        from . import STEP_CALLBACK, _raise_callback_error, _trampoline
         cache = self.__dict__.setdefault("_fused_cb", {})
         key = id(callback)
         if key not in cache:
             if callback is None:
                 cache[key] = (None, STEP_CALLBACK())
             else:
-                def trampoline(user, s, view_ptr, _cb=callback):
-                    _cb(view_ptr.contents, s)
-                cache[key] = (callback, STEP_CALLBACK(trampoline))
+                cache[key] = (callback, STEP_CALLBACK(_trampoline(callback, self)))
         st = _C.c_uint()
         fn = self.L.dsx_shard_step
         fn.argtypes = [_C.c_void_p, STEP_CALLBACK, _C.c_void_p, _C.c_void_p, _C.POINTER(_C.c_uint)]
-        self._call(fn(self.h, cache[key][1], None, self._stream(stream), _C.byref(st)))
+        self._callback_error = None
+        status = fn(self.h, cache[key][1], None, self._stream(stream), _C.byref(st))
+        _raise_callback_error(self)
+        self._call(status)
         return st.value
 
     def owned_view(self):

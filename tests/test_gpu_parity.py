@@ -913,3 +913,18 @@ def test_owner_rank_with_uneven_cuts(cuda, dims):
         assert (out.cpu().numpy() == pair.ref.owner_rank(pos)).all()
     finally:
         pair.close()
+
+
+def test_step_callback_exception_reaches_the_caller(cuda):
+    """An exception raised by the step's callback cannot cross the C frames;
+    the Python call that ran the step raises it afterwards."""
+    pair = run_scenario(cuda, P=8, dims=(2, 2, 2), L=(10.0, 10.0, 10.0), halo=1.0, N=3000,
+                        steps=1, seed=61, fields=())
+    try:
+        def broken(view, stream):
+            raise ValueError("from the callback")
+        with pytest.raises(RuntimeError, match="from the callback"):
+            pair.gpu.step(broken, capture=False)
+        assert pair.gpu.step(None, capture=False) == 0   # the grid goes on
+    finally:
+        pair.close()

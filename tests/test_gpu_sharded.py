@@ -244,9 +244,14 @@ def test_native_fused_step_over_nccl(cuda):
         return torch.as_tensor(_Bytes(view.base[a] + size * int(offset), size * count),
                                device="cuda").view(torch.float64 if dtype == np.float64 else torch.int32)
 
+    side = torch.cuda.Stream()
+    calls = []
+    seen = []
+
     def forces(view, stream):
         # every ghost slot of the view: a force from the ghost's own
         # position and id (equal ghosts get equal forces in any slot)
+        seen.append(stream)
         cap = int(view.ghost_capacity)
         with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
             x = region(view, 0, view.ghost_offset, cap, np.float64)
@@ -276,9 +281,11 @@ def test_native_fused_step_over_nccl(cuda):
                 for a in range(3):
                     region(view, a, view.owned_offset, n, np.float64).add_(d[a])
             torch.cuda.synchronize()
-            assert ref.step(forces, capture=False) == 0
-            assert sh.step_fused(forces) == 0
+            with torch.cuda.stream(side):
+                assert ref.step(forces, capture=False) == 0
+                assert sh.step_fused(forces) == 0
             torch.cuda.synchronize()
+            calls.append(step)
             vr, vs = ref.view(), sh.owned_view()
             assert int(vr.particles) == int(vs.particles) == n
             o_ref, g_ref = ref.all_counts()
@@ -295,6 +302,9 @@ def test_native_fused_step_over_nccl(cuda):
                     want = torch.as_tensor(_Bytes(vr.base[a] + width * int(off_r), width * count),
                                            device="cuda")
                     assert torch.equal(got, want), (step, name)
+            assert G > 0
+        # both callbacks ran on every step, on the step's stream
+        assert calls == [0, 1, 2] and len(seen) == 6 and all(s == side.cuda_stream for s in seen)
     finally:
         ref.close()
         sh.close()
