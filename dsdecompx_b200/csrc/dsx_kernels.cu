@@ -2567,36 +2567,62 @@ __global__ void __launch_bounds__(NT) k_out_of_domain(Grid G, const double* __re
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z, int* flags) {
     __shared__ double s_cuts[kMaxRanks + 16];   // cut_offset[a] + kCountedCells <= 1036
+    __shared__ unsigned short s_bins[3 * kGuessBins];
+    __shared__ int s_ob[kMaxRanks + 1];
+    const int P = G.P;
+    for (int k = threadIdx.x; k <= P; k += blockDim.x) s_ob[k] = G.obase[k];
     stage_cuts(G, s_cuts);
-    // one wave of CTAs strides over the tiles (the cuts are staged once per
-    // CTA); a position inside the subdomain's own cut planes is owned there
-    // (the wrap leaves a position inside the box as it is, -0 aside, which
-    // lies in the same cell); only the others are searched
-    const int ntiles = G.tile_start[G.P];
-    constexpr int U = TILE / NT;
-    for (int g = blockIdx.x; g < ntiles; g += gridDim.x) {
-        const int4 td = G.tiles[g];
-        const Cell cell = cell_of(G, td.x);
+    stage_bins(G, s_cuts, s_bins);
+    const CellGuess guess = cell_guess(G);
+    // every owned particle in one grid-stride pass (four per thread and
+    // pass, loaded together); its subdomain from the layout's bases.  A
+    // position inside the subdomain's own cut planes is owned there (the
+    // wrap leaves a position inside the box as it is, -0 aside, which lies in
+    // the same cell); only the others are searched
+    const int n = s_ob[P];
+    const int lane = threadIdx.x & 31;
+    constexpr int U = 4;
+    const int step = gridDim.x * NT;
+    for (int i0 = blockIdx.x * NT + threadIdx.x; i0 - threadIdx.x % 32 < n; i0 += U * step) {
         double px[U], py[U], pz[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int i = td.y + threadIdx.x + u * NT;
-            if (i < td.z) {
+            const int i = i0 + u * step;
+            if (i < n) {
                 px[u] = ro(x + i);
                 py[u] = ro(y + i);
                 pz[u] = ro(z + i);
             }
         }
-        bool out = false;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int i = td.y + threadIdx.x + u * NT;
-            if (i >= td.z) continue;
-            const bool inside = cell.lo[0] <= px[u] && px[u] < cell.hi[0] && cell.lo[1] <= py[u] &&
-                                py[u] < cell.hi[1] && cell.lo[2] <= pz[u] && pz[u] < cell.hi[2];
-            if (!inside) out = out || owner_of_staged(G, s_cuts, px[u], py[u], pz[u]) != td.x;
+            const int i = i0 + u * step;
+            int key = -1;   // the subdomain this particle leaves
+            if (i < n) {
+                int lo = 0, hi = P;   // largest s with s_ob[s] <= i
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_ob[mid] <= i) lo = mid;
+                    else hi = mid;
+                }
+                const int packed = G.coord[lo];
+                const int c[3] = {packed >> 20, (packed >> 10) & 1023, packed & 1023};
+                const double p[3] = {px[u], py[u], pz[u]};
+                bool inside = true;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const double* cuts = s_cuts + G.cut_offset[a];
+                    inside = inside && cuts[c[a]] <= p[a] && p[a] < cuts[c[a] + 1];
+                }
+                if (!inside && owner_of_binned(G, guess, s_cuts, s_bins, px[u], py[u], pz[u]) != lo)
+                    key = lo;
+            }
+            // one atomic per subdomain and warp
+            if (__any_sync(0xffffffffu, key >= 0)) {
+                const unsigned peers = __match_any_sync(0xffffffffu, key);
+                if (key >= 0 && lane == __ffs(peers) - 1) atomicOr(&flags[key], 1);
+            }
         }
-        if (__syncthreads_or(out) && threadIdx.x == 0) atomicOr(&flags[td.x], 1);
     }
 }
 
@@ -3071,8 +3097,8 @@ void launch_owner_rank(const Grid& G, const double* x, const double* y, const do
 void launch_out_of_domain(const Grid& G, const double* x, const double* y, const double* z,
                           int* flags, cudaStream_t s) {
     cudaMemsetAsync(flags, 0, sizeof(int) * G.P, s);
-    k_out_of_domain<<<resident_grid(reinterpret_cast<const void*>(k_out_of_domain),
-                                    static_cast<long long>(G.max_tiles) * NT), NT, 0, s>>>(G, x, y, z, flags);
+    k_out_of_domain<<<resident_grid(reinterpret_cast<const void*>(k_out_of_domain), G.ncap), NT, 0,
+                      s>>>(G, x, y, z, flags);
 }
 
 void mark(const Scratch& S, cudaStream_t s, const char* what) {
