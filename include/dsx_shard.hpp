@@ -101,6 +101,16 @@ public:
         return r;
     }
     void reverse_halo(void* stream = nullptr) { check(dsx_shard_reverse_halo(handle_, stream)); }
+    // One fused step (dsx_shard_step): migrate -> halo build ->
+    // callback(stream, view of this shard's particles and receivers' ghosts)
+    // -> reverse_halo; returns the device status bits (0: ok).
+    unsigned step(const std::function<void(void* stream, const dsx_grid_view& view)>& callback,
+                  void* stream = nullptr) {
+        unsigned status = 0;
+        check(dsx_shard_step(handle_, callback ? &step_trampoline : nullptr,
+                             const_cast<void*>(static_cast<const void*>(&callback)), stream, &status));
+        return status;
+    }
     void forward_exchange(const std::vector<int>& ids, void* stream = nullptr) {
         check(dsx_shard_forward_exchange(handle_, static_cast<int>(ids.size()), ids.data(), stream));
     }
@@ -130,6 +140,9 @@ public:
     }
 
 private:
+    static void step_trampoline(void* user, void* stream, const dsx_grid_view* view) {
+        (*static_cast<const std::function<void(void*, const dsx_grid_view&)>*>(user))(stream, *view);
+    }
     static int sum_i64(void* u, long long* v, long long n) {
         return call([&] { static_cast<Transport*>(u)->sum_i64(v, n); });
     }
