@@ -1171,10 +1171,13 @@ __device__ __forceinline__ void step_layout_body(const Grid& G, const int* pre, 
                                                  const StepTables& T) {
     __shared__ int ws[33];
     __shared__ int s_rcv[kMaxRanks + 1];
+    __shared__ int s_ts[kMaxRanks + 1];   // the current layout's tile starts, staged once
     const int P = G.P;
     const int t = threadIdx.x;
-    const int ntiles = G.tile_start[P];
-    const int* ts_old = G.tile_start;
+    for (int k = t; k <= P; k += blockDim.x) s_ts[k] = G.tile_start[k];
+    __syncthreads();
+    const int ntiles = s_ts[P];
+    const int* ts_old = s_ts;
     auto tile_sum = [&](int k, int r) {
         return __ldcg(pre + k * stride + ts_old[r + 1]) - __ldcg(pre + k * stride + ts_old[r]);
     };
@@ -2298,6 +2301,7 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
     // clamps) run in the reference's order on one lane each; the cut
     // searches, independent per boundary, run one per lane
     __shared__ double s_work[kMaxRanks];
+    __shared__ int s_coord[kMaxRanks];         // packed grid coordinates, staged once
     __shared__ double s_next[kMaxRanks + 4];   // next cuts, axis a at G.cut_offset[a]
     __shared__ double s_slab[kMaxRanks + 3];   // slab work, axis a at slab_off[a]
     __shared__ double s_total;
@@ -2319,7 +2323,10 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
     __syncwarp();
     if (!s_go) return;
     const int P = G.P;
-    for (int s = lane; s < P; s += 32) s_work[s] = work_in ? work_in[s] : static_cast<double>(G.n[s]);
+    for (int s = lane; s < P; s += 32) {
+        s_work[s] = work_in ? work_in[s] : static_cast<double>(G.n[s]);
+        s_coord[s] = G.coord[s];
+    }
     __syncwarp();
     if (lane == 0) {
         double total = 0.0, maximum = 0.0;
@@ -2353,7 +2360,7 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
             for (int i = 0; i < slabs; ++i) sw[i] = 0.0;
             const int shift = a == 0 ? 20 : a == 1 ? 10 : 0;
             for (int s = 0; s < P; ++s) {
-                const int c = (G.coord[s] >> shift) & 1023;
+                const int c = (s_coord[s] >> shift) & 1023;
                 sw[c] = __dadd_rn(sw[c], s_work[s]);
             }
         }
