@@ -205,6 +205,201 @@ T* device_alloc(std::vector<void*>& owned, std::size_t count) {
 
 void dsx::set_last_error(const char* message) { g_error = message ? message : ""; }
 
+namespace {
+
+// sender entry of receiver (q, m): the entry of r = nbr(q,m) that points
+// toward -d_m (the MPI backend's tag matching, dsDecompX
+// src/backends/mpi_backend.cpp:398-433)
+int sender_entry_of(const std::vector<std::vector<Neighbor>>& topo, int q, int m) {
+    const Neighbor& nb = topo[static_cast<std::size_t>(q)][static_cast<std::size_t>(m)];
+    if (nb.rank < 0) return -1;
+    const int want = direction_slot(-nb.dir[0], -nb.dir[1], -nb.dir[2]);
+    const auto& list = topo[static_cast<std::size_t>(nb.rank)];
+    for (std::size_t n = 0; n < list.size(); ++n)
+        if (list[n].slot == want && list[n].rank == q) return nb.rank * dsx::kMaxNeighbors + static_cast<int>(n);
+    return -1;
+}
+
+struct ShardPlan {
+    std::vector<int> n_next, obase_next, tile_start_next;   // P, P+1, P+1
+    std::vector<int> imm_base, imm_tiles_in, imm_tile_start, local_imm;   // P, P, P+1, P
+    std::vector<int> gap;                                    // P*P
+    std::vector<long long> results;                          // P*6
+    std::vector<int> list_ret, list_len, send_base;          // P*26
+    std::vector<int> g, gbase;                               // P, P+1
+    std::vector<int> cbase_ret, cbase_imm;                   // P*28
+    long long own_total = 0, out_total = 0, ghosts = 0, own_ghosts = 0, boundary = 0, images = 0;
+    int emigrants = 0;
+    // per peer shard: outgoing emigrants [out_start, out_end) of the next
+    // half; outgoing ghost lists [gout_start, gout_end) of the ghost region
+    std::vector<long long> out_start, out_end, gout_start, gout_end;
+    std::vector<long long> recv_particles, recv_ghosts;      // per peer
+};
+
+// The layout of one shard's fused step (see dsx_grid::sharded_step), from
+// `sum`, the sum over every shard of: [0, 29P) the export of k_step_export
+// (retained particles, boundary owners and images of the retained parts,
+// the retained part of every send list), [29P, 58P) the immigrant counters
+// (per destination: total, per list, boundary owners, images), [58P, 58P +
+// P*P) the emigrant pairs [t * P + q], then one storage entry per shard.
+// local_emigrants: this shard's own emigrants (not summed).
+ShardPlan plan_shard_layout(int P, const std::vector<std::vector<Neighbor>>& topo,
+                            const std::vector<long long>& sum, const std::vector<int>& owners,
+                            int shard, int nshards, int local_emigrants) {
+    const int E = dsx::kMaxNeighbors;
+    auto sender_entry = [&](int q, int m) { return sender_entry_of(topo, q, m); };
+    ShardPlan pl;
+    const long long* stays = sum.data();
+    const long long* bret = stays + P;
+    const long long* iret = bret + P;
+    const long long* lret = iret + P;                       // P * 26
+    const long long* imm_total = lret + static_cast<std::size_t>(P) * E;
+    const long long* imm_list = imm_total + P;             // P * 26
+    const long long* imm_bnd = imm_list + static_cast<std::size_t>(P) * E;
+    const long long* imm_img = imm_bnd + P;
+    const long long* pairs = imm_img + P;                   // P * P, [t * P + q]
+    auto own = [&](int t) { return owners[static_cast<std::size_t>(t)] == shard; };
+    auto pair = [&](int t, int q) { return pairs[static_cast<std::size_t>(t) * P + q]; };
+    pl.emigrants = local_emigrants;
+    // owned layout: own subdomains contiguous in rank order, then the
+    // outgoing emigrants by (destination's shard, destination)
+    pl.n_next.assign(P, 0);
+    pl.obase_next.assign(P + 1, 0);
+    pl.tile_start_next.assign(P + 1, 0);
+    pl.imm_base.assign(P, 0);
+    pl.imm_tiles_in.assign(P, 0);
+    pl.imm_tile_start.assign(P + 1, 0);
+    pl.local_imm.assign(P, 0);
+    pl.gap.assign(static_cast<std::size_t>(P) * P, 0);
+    pl.results.assign(static_cast<std::size_t>(P) * 6, 0);
+    for (int t = 0; t < P; ++t) {
+        long long local = 0;
+        for (int q = 0; q < P; ++q)
+            if (own(q)) local += pair(t, q);
+        pl.local_imm[t] = static_cast<int>(local);
+        if (own(t)) {
+            pl.n_next[t] = static_cast<int>(stays[t] + imm_total[t]);
+            pl.imm_tiles_in[t] = static_cast<int>(imm_total[t]);
+            long long before_remote = 0;
+            for (int q = 0; q < P; ++q) {
+                if (own(q)) pl.gap[static_cast<std::size_t>(t) * P + q] = static_cast<int>(before_remote);
+                else before_remote += pair(t, q);
+            }
+            long long sent = 0;
+            for (int d = 0; d < P; ++d) sent += pair(d, t);
+            long long* o = &pl.results[static_cast<std::size_t>(6) * t];
+            o[1] = stays[t] + sent;
+            o[2] = stays[t];
+            o[3] = sent;
+            o[4] = imm_total[t];
+            o[5] = stays[t] + imm_total[t];
+            o[0] = (o[3] != 0 || o[4] != 0) ? 1 : 0;
+        }
+    }
+    for (int t = 0; t < P; ++t) {
+        pl.obase_next[t + 1] = pl.obase_next[t] + pl.n_next[t];
+        pl.tile_start_next[t + 1] = pl.tile_start_next[t] + (pl.n_next[t] + dsx::kTile - 1) / dsx::kTile;
+        pl.imm_tile_start[t + 1] = pl.imm_tile_start[t] + (pl.imm_tiles_in[t] + dsx::kTile - 1) / dsx::kTile;
+        if (own(t)) pl.imm_base[t] = pl.obase_next[t] + static_cast<int>(stays[t]);
+    }
+    pl.own_total = pl.obase_next[P];
+    pl.out_start.assign(nshards, 0);
+    pl.out_end.assign(nshards, 0);
+    long long at = pl.own_total;
+    for (int p = 0; p < nshards; ++p) {
+        pl.out_start[p] = at;
+        if (p != shard)
+            for (int t = 0; t < P; ++t)
+                if (owners[t] == p) {
+                    pl.imm_base[t] = static_cast<int>(at);
+                    at += pl.local_imm[t];
+                }
+        pl.out_end[p] = at;
+    }
+    pl.out_total = at - pl.own_total;
+    // remote immigrants each peer sends: groups (own t, source q of p)
+    pl.recv_particles.assign(nshards, 0);
+    for (int t = 0; t < P; ++t)
+        if (own(t))
+            for (int q = 0; q < P; ++q)
+                if (!own(q)) pl.recv_particles[owners[q]] += pair(t, q);
+    // ghost layout: list lengths, receiver order, list bases
+    pl.list_ret.assign(static_cast<std::size_t>(P) * E, 0);
+    pl.list_len.assign(static_cast<std::size_t>(P) * E, 0);
+    pl.send_base.assign(static_cast<std::size_t>(P) * E, 0);
+    pl.g.assign(P, 0);
+    pl.gbase.assign(P + 1, 0);
+    for (int r = 0; r < P; ++r)
+        for (std::size_t n = 0; n < topo[r].size(); ++n) {
+            if (topo[r][n].rank < 0) continue;
+            const std::size_t e = static_cast<std::size_t>(r) * E + n;
+            pl.list_ret[e] = static_cast<int>(lret[e]);
+            pl.list_len[e] = static_cast<int>(lret[e] + imm_list[e]);
+        }
+    std::vector<int> order;
+    for (int q = 0; q < P; ++q)
+        if (own(q)) order.push_back(q);
+    const std::size_t own_receivers = order.size();
+    for (int p = 0; p < nshards; ++p)
+        if (p != shard)
+            for (int q = 0; q < P; ++q)
+                if (owners[q] == p) order.push_back(q);
+    pl.gout_start.assign(nshards, 0);
+    pl.gout_end.assign(nshards, 0);
+    pl.recv_ghosts.assign(nshards, 0);
+    long long run = 0;
+    for (std::size_t k = 0; k < order.size(); ++k) {
+        const int q = order[k];
+        if (k == own_receivers) pl.own_ghosts = run;
+        const int p = owners[q];
+        if (!own(q) && (k == own_receivers || owners[order[k - 1]] != p)) pl.gout_start[p] = run;
+        pl.gbase[q] = static_cast<int>(run);
+        for (std::size_t m = 0; m < topo[q].size(); ++m) {
+            const int e = sender_entry(q, static_cast<int>(m));
+            if (e < 0) continue;
+            const int r = e / E;
+            const bool present = own(q) || own(r);
+            const long long len = present ? pl.list_len[static_cast<std::size_t>(e)] : 0;
+            pl.send_base[static_cast<std::size_t>(e)] = static_cast<int>(run);
+            if (own(q) && !own(r)) pl.recv_ghosts[owners[r]] += len;
+            run += len;
+        }
+        pl.g[q] = own(q) ? static_cast<int>(run - pl.gbase[q]) : 0;
+        if (!own(q)) pl.gout_end[p] = run;
+    }
+    if (order.size() == own_receivers) pl.own_ghosts = run;
+    pl.ghosts = run;
+    pl.gbase[P] = static_cast<int>(run);
+    // counter bases of own senders: lists (retained part, immigrant
+    // part), boundary owners and images (retained first)
+    pl.cbase_ret.assign(static_cast<std::size_t>(P) * dsx::kHaloCounters, 0);
+    pl.cbase_imm.assign(static_cast<std::size_t>(P) * dsx::kHaloCounters, 0);
+    long long bb = 0, ib = 0;
+    for (int r = 0; r < P; ++r) {
+        if (!own(r)) continue;
+        for (std::size_t n = 0; n < topo[r].size(); ++n) {
+            if (topo[r][n].rank < 0) continue;
+            const std::size_t e = static_cast<std::size_t>(r) * E + n;
+            pl.cbase_ret[static_cast<std::size_t>(r) * dsx::kHaloCounters + n] = pl.send_base[e];
+            pl.cbase_imm[static_cast<std::size_t>(r) * dsx::kHaloCounters + n] = pl.send_base[e] + pl.list_ret[e];
+        }
+        int* cr = &pl.cbase_ret[static_cast<std::size_t>(r) * dsx::kHaloCounters];
+        int* ci = &pl.cbase_imm[static_cast<std::size_t>(r) * dsx::kHaloCounters];
+        cr[dsx::kBoundaryCounter] = static_cast<int>(bb);
+        ci[dsx::kBoundaryCounter] = static_cast<int>(bb + bret[r]);
+        cr[dsx::kImageCounter] = static_cast<int>(ib);
+        ci[dsx::kImageCounter] = static_cast<int>(ib + iret[r]);
+        bb += bret[r] + imm_bnd[r];
+        ib += iret[r] + imm_img[r];
+    }
+    pl.boundary = bb;
+    pl.images = ib;
+    return pl;
+}
+
+}  // namespace
+
+
 struct dsx_grid {
     dsx_grid_desc desc{};
     int P = 1;
@@ -421,15 +616,7 @@ struct dsx_grid {
     // sender entry of receiver (q, m): the entry of r = nbr(q,m) that points
     // toward -d_m (the MPI backend's tag matching, dsDecompX
     // src/backends/mpi_backend.cpp:398-433)
-    int sender_entry(int q, int m) const {
-        const Neighbor& nb = topo[static_cast<std::size_t>(q)][static_cast<std::size_t>(m)];
-        if (nb.rank < 0) return -1;
-        const int want = direction_slot(-nb.dir[0], -nb.dir[1], -nb.dir[2]);
-        const auto& list = topo[static_cast<std::size_t>(nb.rank)];
-        for (std::size_t n = 0; n < list.size(); ++n)
-            if (list[n].slot == want && list[n].rank == q) return nb.rank * dsx::kMaxNeighbors + static_cast<int>(n);
-        return -1;
-    }
+    int sender_entry(int q, int m) const { return sender_entry_of(topo, q, m); }
 
     void allocate_fixed() {
         const int E = dsx::kMaxNeighbors;
@@ -1362,175 +1549,9 @@ struct dsx_grid {
     // then the other shards' receivers (by shard, then rank) holding only
     // the lists of this shard's senders (sent away after the build, their
     // forces returned before the reverse sum).
-    struct ShardPlan {
-        std::vector<int> n_next, obase_next, tile_start_next;   // P, P+1, P+1
-        std::vector<int> imm_base, imm_tiles_in, imm_tile_start, local_imm;   // P, P, P+1, P
-        std::vector<int> gap;                                    // P*P
-        std::vector<long long> results;                          // P*6
-        std::vector<int> list_ret, list_len, send_base;          // P*26
-        std::vector<int> g, gbase;                               // P, P+1
-        std::vector<int> cbase_ret, cbase_imm;                   // P*28
-        long long own_total = 0, out_total = 0, ghosts = 0, own_ghosts = 0, boundary = 0, images = 0;
-        int emigrants = 0;
-        // per peer shard: outgoing emigrants [out_start, out_end) of the next
-        // half; outgoing ghost lists [gout_start, gout_end) of the ghost region
-        std::vector<long long> out_start, out_end, gout_start, gout_end;
-        std::vector<long long> recv_particles, recv_ghosts;      // per peer
-    };
-
-    // export: this shard's 29P + 1 export ints; imm: the P * 29 immigrant
-    // counters; pairs: P * P; all three summed over shards except export[29P]
-    // (the local emigrants) and `local_pairs` (this shard's own pairs).
     ShardPlan plan_shard(const std::vector<long long>& sum, const std::vector<int>& owners, int shard,
                          int nshards, int local_emigrants) const {
-        const int E = dsx::kMaxNeighbors;
-        ShardPlan pl;
-        const long long* stays = sum.data();
-        const long long* bret = stays + P;
-        const long long* iret = bret + P;
-        const long long* lret = iret + P;                       // P * 26
-        const long long* imm_total = lret + static_cast<std::size_t>(P) * E;
-        const long long* imm_list = imm_total + P;             // P * 26
-        const long long* imm_bnd = imm_list + static_cast<std::size_t>(P) * E;
-        const long long* imm_img = imm_bnd + P;
-        const long long* pairs = imm_img + P;                   // P * P, [t * P + q]
-        auto own = [&](int t) { return owners[static_cast<std::size_t>(t)] == shard; };
-        auto pair = [&](int t, int q) { return pairs[static_cast<std::size_t>(t) * P + q]; };
-        pl.emigrants = local_emigrants;
-        // owned layout: own subdomains contiguous in rank order, then the
-        // outgoing emigrants by (destination's shard, destination)
-        pl.n_next.assign(P, 0);
-        pl.obase_next.assign(P + 1, 0);
-        pl.tile_start_next.assign(P + 1, 0);
-        pl.imm_base.assign(P, 0);
-        pl.imm_tiles_in.assign(P, 0);
-        pl.imm_tile_start.assign(P + 1, 0);
-        pl.local_imm.assign(P, 0);
-        pl.gap.assign(static_cast<std::size_t>(P) * P, 0);
-        pl.results.assign(static_cast<std::size_t>(P) * 6, 0);
-        for (int t = 0; t < P; ++t) {
-            long long local = 0;
-            for (int q = 0; q < P; ++q)
-                if (own(q)) local += pair(t, q);
-            pl.local_imm[t] = static_cast<int>(local);
-            if (own(t)) {
-                pl.n_next[t] = static_cast<int>(stays[t] + imm_total[t]);
-                pl.imm_tiles_in[t] = static_cast<int>(imm_total[t]);
-                long long before_remote = 0;
-                for (int q = 0; q < P; ++q) {
-                    if (own(q)) pl.gap[static_cast<std::size_t>(t) * P + q] = static_cast<int>(before_remote);
-                    else before_remote += pair(t, q);
-                }
-                long long sent = 0;
-                for (int d = 0; d < P; ++d) sent += pair(d, t);
-                long long* o = &pl.results[static_cast<std::size_t>(6) * t];
-                o[1] = stays[t] + sent;
-                o[2] = stays[t];
-                o[3] = sent;
-                o[4] = imm_total[t];
-                o[5] = stays[t] + imm_total[t];
-                o[0] = (o[3] != 0 || o[4] != 0) ? 1 : 0;
-            }
-        }
-        for (int t = 0; t < P; ++t) {
-            pl.obase_next[t + 1] = pl.obase_next[t] + pl.n_next[t];
-            pl.tile_start_next[t + 1] = pl.tile_start_next[t] + (pl.n_next[t] + dsx::kTile - 1) / dsx::kTile;
-            pl.imm_tile_start[t + 1] = pl.imm_tile_start[t] + (pl.imm_tiles_in[t] + dsx::kTile - 1) / dsx::kTile;
-            if (own(t)) pl.imm_base[t] = pl.obase_next[t] + static_cast<int>(stays[t]);
-        }
-        pl.own_total = pl.obase_next[P];
-        pl.out_start.assign(nshards, 0);
-        pl.out_end.assign(nshards, 0);
-        long long at = pl.own_total;
-        for (int p = 0; p < nshards; ++p) {
-            pl.out_start[p] = at;
-            if (p != shard)
-                for (int t = 0; t < P; ++t)
-                    if (owners[t] == p) {
-                        pl.imm_base[t] = static_cast<int>(at);
-                        at += pl.local_imm[t];
-                    }
-            pl.out_end[p] = at;
-        }
-        pl.out_total = at - pl.own_total;
-        // remote immigrants each peer sends: groups (own t, source q of p)
-        pl.recv_particles.assign(nshards, 0);
-        for (int t = 0; t < P; ++t)
-            if (own(t))
-                for (int q = 0; q < P; ++q)
-                    if (!own(q)) pl.recv_particles[owners[q]] += pair(t, q);
-        // ghost layout: list lengths, receiver order, list bases
-        pl.list_ret.assign(static_cast<std::size_t>(P) * E, 0);
-        pl.list_len.assign(static_cast<std::size_t>(P) * E, 0);
-        pl.send_base.assign(static_cast<std::size_t>(P) * E, 0);
-        pl.g.assign(P, 0);
-        pl.gbase.assign(P + 1, 0);
-        for (int r = 0; r < P; ++r)
-            for (std::size_t n = 0; n < topo[r].size(); ++n) {
-                if (topo[r][n].rank < 0) continue;
-                const std::size_t e = static_cast<std::size_t>(r) * E + n;
-                pl.list_ret[e] = static_cast<int>(lret[e]);
-                pl.list_len[e] = static_cast<int>(lret[e] + imm_list[e]);
-            }
-        std::vector<int> order;
-        for (int q = 0; q < P; ++q)
-            if (own(q)) order.push_back(q);
-        const std::size_t own_receivers = order.size();
-        for (int p = 0; p < nshards; ++p)
-            if (p != shard)
-                for (int q = 0; q < P; ++q)
-                    if (owners[q] == p) order.push_back(q);
-        pl.gout_start.assign(nshards, 0);
-        pl.gout_end.assign(nshards, 0);
-        pl.recv_ghosts.assign(nshards, 0);
-        long long run = 0;
-        for (std::size_t k = 0; k < order.size(); ++k) {
-            const int q = order[k];
-            if (k == own_receivers) pl.own_ghosts = run;
-            const int p = owners[q];
-            if (!own(q) && (k == own_receivers || owners[order[k - 1]] != p)) pl.gout_start[p] = run;
-            pl.gbase[q] = static_cast<int>(run);
-            for (std::size_t m = 0; m < topo[q].size(); ++m) {
-                const int e = sender_entry(q, static_cast<int>(m));
-                if (e < 0) continue;
-                const int r = e / E;
-                const bool present = own(q) || own(r);
-                const long long len = present ? pl.list_len[static_cast<std::size_t>(e)] : 0;
-                pl.send_base[static_cast<std::size_t>(e)] = static_cast<int>(run);
-                if (own(q) && !own(r)) pl.recv_ghosts[owners[r]] += len;
-                run += len;
-            }
-            pl.g[q] = own(q) ? static_cast<int>(run - pl.gbase[q]) : 0;
-            if (!own(q)) pl.gout_end[p] = run;
-        }
-        if (order.size() == own_receivers) pl.own_ghosts = run;
-        pl.ghosts = run;
-        pl.gbase[P] = static_cast<int>(run);
-        // counter bases of own senders: lists (retained part, immigrant
-        // part), boundary owners and images (retained first)
-        pl.cbase_ret.assign(static_cast<std::size_t>(P) * dsx::kHaloCounters, 0);
-        pl.cbase_imm.assign(static_cast<std::size_t>(P) * dsx::kHaloCounters, 0);
-        long long bb = 0, ib = 0;
-        for (int r = 0; r < P; ++r) {
-            if (!own(r)) continue;
-            for (std::size_t n = 0; n < topo[r].size(); ++n) {
-                if (topo[r][n].rank < 0) continue;
-                const std::size_t e = static_cast<std::size_t>(r) * E + n;
-                pl.cbase_ret[static_cast<std::size_t>(r) * dsx::kHaloCounters + n] = pl.send_base[e];
-                pl.cbase_imm[static_cast<std::size_t>(r) * dsx::kHaloCounters + n] = pl.send_base[e] + pl.list_ret[e];
-            }
-            int* cr = &pl.cbase_ret[static_cast<std::size_t>(r) * dsx::kHaloCounters];
-            int* ci = &pl.cbase_imm[static_cast<std::size_t>(r) * dsx::kHaloCounters];
-            cr[dsx::kBoundaryCounter] = static_cast<int>(bb);
-            ci[dsx::kBoundaryCounter] = static_cast<int>(bb + bret[r]);
-            cr[dsx::kImageCounter] = static_cast<int>(ib);
-            ci[dsx::kImageCounter] = static_cast<int>(ib + iret[r]);
-            bb += bret[r] + imm_bnd[r];
-            ib += iret[r] + imm_img[r];
-        }
-        pl.boundary = bb;
-        pl.images = ib;
-        return pl;
+        return plan_shard_layout(P, topo, sum, owners, shard, nshards, local_emigrants);
     }
 
     // message buffers of the sharded step, one per peer and direction (grow only)
@@ -2312,6 +2333,50 @@ int dsx_grid_sharded_step(dsx_grid* grid, const int* owners, int shard, int nsha
         grid->sharded_step(owners, shard, nshards, *transport, callback, user,
                            static_cast<cudaStream_t>(stream), status);
         cuda_check(cudaGetLastError(), "launch sharded step");
+    });
+}
+
+int dsx_shard_plan_step(const dsx_grid_desc* desc, const int* owners, int shard, int nshards,
+                        const long long* sums, long long nsums, long long* out) {
+    return guarded([&] {
+        if (!desc || !owners || !sums || !out) fail(DSX_E_INVALID, "null argument");
+        const int P = desc->nranks;
+        if (P < 2 || P > dsx::kMaxRanks) fail(DSX_E_INVALID, "nranks must be in 2..1024");
+        if (nshards < 1 || shard < 0 || shard >= nshards) fail(DSX_E_INVALID, "shard out of range");
+        const long long want = 58LL * P + static_cast<long long>(P) * P + nshards;
+        if (nsums != want) fail(DSX_E_INVALID, "sums must hold 58 P + P * P + nshards values");
+        std::vector<int> own(owners, owners + P);
+        for (int t = 0; t < P; ++t)
+            if (own[t] < 0 || own[t] >= nshards) fail(DSX_E_INVALID, "subdomain owner out of range");
+        int d[3];
+        if (desc->policy != DSX_MANUAL) {
+            const double len[3] = {desc->upper[0] - desc->lower[0], desc->upper[1] - desc->lower[1],
+                                   desc->upper[2] - desc->lower[2]};
+            choose_grid(P, len, desc->periodic, desc->policy, d);
+        } else {
+            for (int a = 0; a < 3; ++a) d[a] = desc->dims[a];
+        }
+        if (!fill_dims(P, d)) fail(DSX_E_INVALID, "process-grid dimensions do not match nranks");
+        std::vector<std::vector<Neighbor>> topo(static_cast<std::size_t>(P));
+        for (int r = 0; r < P; ++r) {
+            const int c[3] = {r / (d[1] * d[2]), (r / d[2]) % d[1], r % d[2]};
+            topo[static_cast<std::size_t>(r)] = neighbors_of(c, d, *desc);
+        }
+        const std::vector<long long> sum(sums, sums + nsums);
+        const ShardPlan pl = plan_shard_layout(P, topo, sum, own, shard, nshards, 0);
+        out[0] = pl.own_total;
+        out[1] = pl.out_total;
+        out[2] = pl.ghosts;
+        out[3] = pl.own_ghosts;
+        out[4] = pl.boundary;
+        out[5] = pl.images;
+        for (int p = 0; p < nshards; ++p) {
+            long long* o = out + 6 + 4 * p;
+            o[0] = pl.out_end[p] - pl.out_start[p];
+            o[1] = pl.recv_particles[p];
+            o[2] = pl.gout_end[p] - pl.gout_start[p];
+            o[3] = pl.recv_ghosts[p];
+        }
     });
 }
 

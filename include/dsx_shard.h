@@ -114,6 +114,19 @@ int dsx_shard_reverse_halo(dsx_shard* shard, void* stream);
 int dsx_shard_step(dsx_shard* shard, dsx_step_callback callback, void* user, void* stream,
                    unsigned* status);
 
+/* Host only (no GPU needed): the layout dsx_shard_step plans on `shard`
+ * from the counts summed over every shard (sums: 58 P + P * P + nshards
+ * values in the step's all-reduce order -- per subdomain retained particles,
+ * retained boundary owners and images, the retained part of its 26 send
+ * lists; per destination its immigrants, their part of each list, their
+ * boundary owners and images; the emigrant pairs [t * P + q]; each shard's
+ * storage).  out (6 + 4 nshards values): owned particles after the step,
+ * outgoing emigrants, ghost slots, this shard's receivers' ghosts, boundary
+ * owners, images; then per shard p: emigrants sent to p, emigrants received
+ * from p, ghosts sent to p, ghosts received from p. */
+int dsx_shard_plan_step(const dsx_grid_desc* desc, const int* owners, int shard, int nshards,
+                        const long long* sums, long long nsums, long long* out);
+
 /* The grid-level form of dsx_shard_step, for hosts that keep their own
  * dsx_grid per process: owners[P] the shard of every subdomain, shard and
  * nshards this process's place, transport as in dsx_shard_create. */

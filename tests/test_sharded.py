@@ -442,3 +442,125 @@ def test_torch_transport_sums_over_gloo_ranks(tmp_path):
         assert i64.split() == ["0", "2", "-4", "7", str(2 << 40)]
         assert f64.split() == ["0", "1.0", "-3.75", "2e+300"]
         assert fail.split()[0] == "-3" and fail.split()[1] != "None"
+
+
+# ---------------------------------------------------------------------------
+# The fused sharded step's host plan (dsx_shard_plan_step) over gloo ranks
+
+PLAN_P, PLAN_DIMS, PLAN_UPPER = 32, (4, 4, 2), (16.0, 16.0, 8.0)
+
+
+def plan_contribution(rank, world, seed):
+    """This rank's part of the fused step's all-reduce, in its order: the
+    export of its own subdomains, the immigrant counters and emigrant pairs
+    of its own sources, its storage."""
+    import dsdecompx_b200 as dsx
+    P, E = PLAN_P, 26
+    owners = shd.plan_owners(PLAN_DIMS, world)
+    rng = np.random.default_rng(seed + rank)
+    stays, bret, iret = np.zeros(P, np.int64), np.zeros(P, np.int64), np.zeros(P, np.int64)
+    lret = np.zeros((P, E), np.int64)
+    imm_total, imm_bnd, imm_img = np.zeros(P, np.int64), np.zeros(P, np.int64), np.zeros(P, np.int64)
+    imm_list = np.zeros((P, E), np.int64)
+    pairs = np.zeros((P, P), np.int64)
+    for q in range(P):
+        if owners[q] != rank:
+            continue
+        _, nbrs = dsx.plan_topology(P, q, PLAN_DIMS, "manual", (0, 0, 0), PLAN_UPPER)
+        stays[q] = rng.integers(500, 2000)
+        bret[q] = rng.integers(0, stays[q] // 2)
+        iret[q] = bret[q] + rng.integers(0, bret[q] + 1)
+        for n, nb in enumerate(nbrs):
+            if nb["rank"] >= 0:
+                lret[q, n] = rng.integers(0, stays[q] // 8)
+            if nb["rank"] >= 0 and nb["rank"] != q:
+                t = nb["rank"]
+                c = int(rng.integers(0, 40))
+                pairs[t, q] += c
+                imm_total[t] += c
+                b = int(rng.integers(0, c + 1))
+                imm_bnd[t] += b
+                imm_img[t] += b + int(rng.integers(0, b + 1))
+    # the receivers' lists gain the immigrants' images: spread each
+    # destination's images over its active lists
+    for t in range(P):
+        if imm_img[t]:
+            _, nbrs = dsx.plan_topology(P, t, PLAN_DIMS, "manual", (0, 0, 0), PLAN_UPPER)
+            active = [n for n, nb in enumerate(nbrs) if nb["rank"] >= 0]
+            for k in range(int(imm_img[t])):
+                imm_list[t, active[k % len(active)]] += 1
+    storage = np.zeros(world, np.int64)
+    storage[rank] = 1 << 30
+    return owners, np.concatenate([stays, bret, iret, lret.ravel(), imm_total, imm_list.ravel(),
+                                   imm_bnd, imm_img, pairs.ravel(), storage])
+
+
+def plan_step(owners, shard, world, sums):
+    import ctypes as C
+
+    import dsdecompx_b200 as dsx
+    desc = dsx._grid_desc(PLAN_P, PLAN_DIMS, "manual", (0, 0, 0), PLAN_UPPER, (True,) * 3, 1.0,
+                          True, None)
+    fn = dsx.lib().dsx_shard_plan_step
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_longlong, C.c_void_p]
+    own = np.ascontiguousarray(owners, dtype=np.int32)
+    s = np.ascontiguousarray(sums, dtype=np.int64)
+    out = np.zeros(6 + 4 * world, dtype=np.int64)
+    dsx._check(fn(C.byref(desc), own.ctypes.data, shard, world, s.ctypes.data, len(s),
+                  out.ctypes.data))
+    return out
+
+
+def gloo_plan_rank(rank, world, port, out_dir):
+    import torch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.distributed.init_process_group("gloo", rank=rank, world_size=world,
+                                         timeout=datetime.timedelta(seconds=20))
+    owners, mine = plan_contribution(rank, world, 71)
+    total = torch.from_numpy(mine.copy())
+    torch.distributed.all_reduce(total)
+    out = plan_step(owners, rank, world, total.numpy())
+    np.save(os.path.join(out_dir, f"sums{rank}.npy"), total.numpy())
+    np.save(os.path.join(out_dir, f"plan{rank}.npy"), out)
+    torch.distributed.destroy_process_group()
+
+
+def test_fused_step_plans_agree_over_gloo_ranks(tmp_path):
+    """Two gloo ranks sum their counts as the fused sharded step does and
+    each plans its layout (dsx_shard_plan_step, no GPU): every message one
+    rank plans to send is the size the other plans to receive, the owned and
+    ghost totals add up to the summed counts, and one shard alone plans the
+    same totals with nothing to send."""
+    world = 2
+    mp.start_processes(gloo_plan_rank, args=(world, free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn")
+    P, E = PLAN_P, 26
+    sums = [np.load(os.path.join(tmp_path, f"sums{r}.npy")) for r in range(world)]
+    assert np.array_equal(sums[0], sums[1])
+    s = sums[0]
+    stays, bret, iret = s[:P], s[P:2 * P], s[2 * P:3 * P]
+    lret = s[3 * P:3 * P + P * E]
+    imm_total = s[29 * P:30 * P]
+    imm_list = s[30 * P:30 * P + P * E]
+    imm_bnd, imm_img = s[56 * P:57 * P], s[57 * P:58 * P]
+    plans = [np.load(os.path.join(tmp_path, f"plan{r}.npy")) for r in range(world)]
+    owners = shd.plan_owners(PLAN_DIMS, world)
+    per_peer = [p[6:].reshape(world, 4) for p in plans]
+    for a in range(world):
+        for b in range(world):
+            if a != b:
+                assert per_peer[a][b, 0] == per_peer[b][a, 1]   # emigrants a -> b
+                assert per_peer[a][b, 2] == per_peer[b][a, 3]   # ghost lists a -> b
+        mine = owners == a
+        assert plans[a][0] == (stays + imm_total)[mine].sum()
+        assert plans[a][1] == per_peer[a][:, 0].sum()
+        assert plans[a][2] == plans[a][3] + per_peer[a][:, 2].sum()
+        assert plans[a][4] == (bret + imm_bnd)[mine].sum()
+        assert plans[a][5] == (iret + imm_img)[mine].sum()
+    every_list = int((lret + imm_list).sum())
+    assert sum(p[3] for p in plans) == every_list
+    alone = plan_step(np.zeros(P, dtype=np.int64), 0, 1,
+                      np.concatenate([s[:58 * P + P * P], [1 << 31]]))
+    assert alone[0] == (stays + imm_total).sum() and alone[1] == 0
+    assert alone[2] == alone[3] == every_list
