@@ -428,6 +428,7 @@ struct dsx_grid {
     int* layout[2][3] = {};   // [which][n, obase, tile_start]
     int4* layout_tiles[2] = {};   // per-tile descriptors of each layout
     int cur = 0;              // current layout index
+    unsigned long long layout_version = 0;   // moves with every new layout
     int parity = 0;           // current owned half
     unsigned* status = nullptr;
     long long* call_counter = nullptr;
@@ -846,6 +847,7 @@ struct dsx_grid {
         plain_bounds.clear();
         parity ^= 1;
         cur ^= 1;
+        ++layout_version;
         plan_valid = false;
         ghosts_valid = false;
         std::fill(last_ghosts.begin(), last_ghosts.end(), 0);
@@ -1193,6 +1195,7 @@ struct dsx_grid {
                    "read status");
         parity ^= 1;
         cur ^= 1;
+        ++layout_version;
     }
 
     // Decomposition::set_axis_cuts (dsDecompX src/decomp.cpp:146-163): the
@@ -1343,6 +1346,7 @@ struct dsx_grid {
         cuda_check(cudaMemcpyAsync(layout[next][0], c.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice,
                                    stream), "assemble counts");
         cur ^= 1;
+        ++layout_version;
         dsx::launch_layout(params(), layout[cur][0], layout[cur][1], layout[cur][2], layout_tiles[cur], stream);
         parity ^= 1;
         total = sum;
@@ -1575,6 +1579,10 @@ struct dsx_grid {
     int* d_imm_tiles_in = nullptr;  // [P]
     int* d_own_totals = nullptr;    // {own receivers' ghosts, boundary owners}
     bool sharded_ghosts = false;    // the ghost region holds a sharded step's layout
+    // every subdomain's owned count after the last fused step, valid while
+    // layout_version (moved by every call that changes the layout) stands
+    std::vector<double> shard_counts;
+    unsigned long long shard_counts_version = ~0ull;
 
     // pinned host staging of the sharded step's counts and planned tables
     unsigned char* shard_pinned = nullptr;
@@ -1666,7 +1674,9 @@ struct dsx_grid {
         }
         if (!pack.empty()) cuda_check(dsx::launch_copies(pack, stream), "pack messages");
         // every shard makes the same transport calls, with messages or not
-        if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
+        // (a lone shard has no peer to call)
+        if (nshards > 1 &&
+            tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
                         static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
                         stream) != DSX_OK)
             fail(DSX_E_RUNTIME, "transport exchange failed");
@@ -1696,13 +1706,27 @@ struct dsx_grid {
             d_own_totals = device_alloc<int>(fixed_owned, 2);
         }
         clear_status(stream);
-        // Dynamic cut planes from the owned counts of every shard
+        // Dynamic cut planes from the owned counts of every shard: known from
+        // the previous fused step's sums while no other call has changed the
+        // layout since, else summed now (an all-reduce over one shard is the
+        // identity, so a lone shard makes no transport call)
         const double* work_in = nullptr;
         if (desc.policy == DSX_DYNAMIC) {
-            const std::vector<int> n = read_ints(layout[cur][0], P, stream);
-            std::vector<double> w(n.begin(), n.end());
-            if (tr.allreduce_f64(tr.user, w.data(), P) != DSX_OK) fail(DSX_E_RUNTIME, "transport all-reduce failed");
-            cuda_check(cudaMemcpyAsync(work, w.data(), sizeof(double) * P, cudaMemcpyHostToDevice, stream),
+            std::vector<double> w;
+            if (shard_counts_version == layout_version && static_cast<int>(shard_counts.size()) == P) {
+                w = shard_counts;
+            } else {
+                const std::vector<int> n = read_ints(layout[cur][0], P, stream);
+                w.assign(n.begin(), n.end());
+                if (nshards > 1 && tr.allreduce_f64(tr.user, w.data(), P) != DSX_OK)
+                    fail(DSX_E_RUNTIME, "transport all-reduce failed");
+            }
+            // the staging buffer is idle here (the previous step ended with a
+            // synchronising status read) and sized for the counts read below
+            // too, so it is not reallocated under this copy
+            std::memcpy(shard_staging(std::max(sizeof(double) * P, sizeof(int) * (58 * P + 1 + PP))), w.data(),
+                        sizeof(double) * P);
+            cuda_check(cudaMemcpyAsync(work, shard_pinned, sizeof(double) * P, cudaMemcpyHostToDevice, stream),
                        "upload work");
             work_in = work;
         }
@@ -1726,7 +1750,7 @@ struct dsx_grid {
         for (std::size_t k = 0; k < nx; ++k) sum[nx + k] = imm[k];
         for (std::size_t k = 0; k < PP; ++k) sum[2 * nx + k] = pr[k];
         sum[2 * nx + PP + static_cast<std::size_t>(shard)] = ncap;
-        if (tr.allreduce_i64(tr.user, sum.data(), static_cast<long long>(sum.size())) != DSX_OK)
+        if (nshards > 1 && tr.allreduce_i64(tr.user, sum.data(), static_cast<long long>(sum.size())) != DSX_OK)
             fail(DSX_E_RUNTIME, "transport all-reduce failed");
         const long long* pairs = sum.data() + 2 * nx;
         const long long* imm_total = sum.data() + nx;
@@ -1859,6 +1883,7 @@ struct dsx_grid {
         // the new layout is the current one for the callback and the reverse sum
         parity ^= 1;
         cur ^= 1;
+        ++layout_version;
         total = pl.own_total;
         pairs_valid = false;
         plan_valid = false;
@@ -1919,7 +1944,8 @@ struct dsx_grid {
                 }
             }
             if (!pack.empty()) cuda_check(dsx::launch_copies(pack, stream), "pack forces");
-            if (tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
+            if (nshards > 1 &&
+                tr.exchange(tr.user, static_cast<int>(to.size()), to.data(), sb.data(), sn.data(),
                             static_cast<int>(from.size()), from.data(), rb.data(), rn.data(),
                             stream) != DSX_OK)
                 fail(DSX_E_RUNTIME, "transport exchange failed");
@@ -1933,6 +1959,13 @@ struct dsx_grid {
         if (st & dsx::kStatusCutsInvalid)
             fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");
         if (st & dsx::kStatusGhostOverflow) fail(DSX_E_RUNTIME, "ghost region overflow in a planned step");
+        // every subdomain's new count (retained + immigrants, from the sums)
+        // for the next fused step's rebalance
+        shard_counts.assign(static_cast<std::size_t>(P), 0.0);
+        for (int t = 0; t < P; ++t)
+            shard_counts[static_cast<std::size_t>(t)] =
+                static_cast<double>(sum[static_cast<std::size_t>(t)] + imm_total[t]);
+        shard_counts_version = layout_version;
         if (status_out) *status_out = st;
     }
 
@@ -1946,6 +1979,7 @@ struct dsx_grid {
         total = sum;
         parity = 0;
         cur = 0;
+        ++layout_version;
         pairs_valid = false;
         plan_valid = false;
         ghosts_valid = false;
