@@ -170,6 +170,40 @@ def algorithmic_bytes(S, N, E, G, B):
     }
 
 
+def host_link(stream, copy, pieces, moved, device):
+    """The host link alone, for scale beside e2e: the owned state down
+    (device -> pinned host), up (into a device scratch of the same size, so
+    the grid's state is left as it is) and both at once on two streams.  The
+    downloads rewrite the host copy with the bytes it already holds, so the
+    concurrent uploads read the same values either way."""
+    import torch
+    scratch = torch.empty(max(int(d.numel()) for d, _ in pieces), dtype=torch.uint8,
+                          device=f"cuda:{device}")
+
+    def timed(down, up):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        a.record(stream)
+        copy.wait_stream(stream)
+        for d, h in pieces:
+            if down:
+                with torch.cuda.stream(stream):
+                    h.copy_(d, non_blocking=True)
+            if up:
+                with torch.cuda.stream(copy):
+                    scratch[:h.numel()].copy_(h, non_blocking=True)
+        stream.wait_stream(copy)
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        return a.elapsed_time(b)
+
+    timed(True, True)   # warm-up
+    d2h, h2d, both = timed(True, False), timed(False, True), timed(True, True)
+    gbs = lambda ms, n: round(n / (ms / 1e3) / 1e9, 1)
+    return {"d2h_gbs": gbs(d2h, moved), "h2d_gbs": gbs(h2d, moved),
+            "both_ms": round(both, 3), "both_gbs": gbs(both, 2 * moved)}
+
+
 def harness_bytes(w, N, G, B):
     """Least bytes of the benchmark's step callback (the stand-in for the
     user's integrator and force loop): the drift reads each owned particle's
@@ -361,36 +395,42 @@ def run_ours(args, rank, world, device):
 
     # e2e: the same step with the whole owned state in pinned host memory.
     # Every step's input crosses host -> device before it and its result
-    # device -> host after it, one cudaMemcpyAsync per array through the
-    # grid's view (dsx_grid_view_get): array a's download runs on the step's
-    # stream while array a-1's upload (the next step's input, which depends
-    # only on that array's download) runs on a second stream, so the two
-    # directions of the host link overlap.
+    # device -> host after it, one cudaMemcpyAsync per piece (an array, or a
+    # 64 MB part of one) through the grid's view (dsx_grid_view_get): piece
+    # p's download runs on the step's stream while the upload of the pieces
+    # before it (the next step's input, each depending only on its own
+    # download) runs on a second stream, so the two directions of the host
+    # link overlap and only the last piece's upload trails the downloads.
     e2e = None
     if args.e2e_steps > 0:
         copy = torch.cuda.Stream(device)
         nbytes = [N * np.dtype(grid.dtype_of(n)).itemsize * grid.components(n) for n in names]
         host_bytes = [t.view(-1).view(torch.uint8)[:nb] for t, nb in zip(pinned, nbytes)]
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        piece = 64 << 20
 
-        def owned_state():
-            """The owned region of every array as a device byte tensor."""
+        def owned_pieces():
+            """(device, host) byte tensors of every piece of the owned state."""
             v = grid.view()
-            return [torch.as_tensor(DeviceBytes(int(v.base[a]) + (nb // N) * int(v.owned_offset),
+            out = []
+            for a, nb in enumerate(nbytes):
+                d = torch.as_tensor(DeviceBytes(int(v.base[a]) + (nb // N) * int(v.owned_offset),
                                                 nb), device=f"cuda:{device}")
-                    for a, nb in enumerate(nbytes)]
+                for o in range(0, nb, piece):
+                    out.append((d[o:o + piece], host_bytes[a][o:o + piece]))
+            return out
 
         with torch.cuda.stream(stream):
             grid.download_flat(ptrs)
             barrier()
             e0.record(stream)
-            for d, h in zip(owned_state(), host_bytes):    # the first step's input
+            for d, h in owned_pieces():                     # the first step's input
                 d.copy_(h, non_blocking=True)
             for k in range(args.e2e_steps):
                 status = grid.step(user_work, capture=True)
                 assert status == 0, status
                 last = k == args.e2e_steps - 1
-                for d, h in zip(owned_state(), host_bytes):
+                for d, h in owned_pieces():
                     h.copy_(d, non_blocking=True)           # this step's result (step stream)
                     if not last:
                         done = torch.cuda.Event()
@@ -408,25 +448,37 @@ def run_ours(args, rank, world, device):
         e2e = {"value": round(world * N / (e_ms / 1e3) / 1e6, 3), "unit": "M particles/s",
                "h2d_bytes_per_step": moved, "d2h_bytes_per_step": moved,
                "ms_per_step": round(e_ms, 3), "steps": args.e2e_steps,
-               "path": "pinned host -> owned state (per array) -> dsx_grid_step -> pinned host "
-                       "(per array; each download overlaps the previous array's upload)"}
+               "path": "pinned host -> owned state (64 MB pieces) -> dsx_grid_step -> pinned host "
+                       "(each piece's download overlaps the earlier pieces' uploads)",
+               "link": host_link(stream, copy, owned_pieces(), moved, device)}
 
-    # per-call path (every call returns its counts synchronously, no graph)
+    # per-call path (every call returns its counts synchronously, no graph);
+    # events between the calls give each call's share (host time between
+    # them included)
     plain = None
+    plain_parts = None
     if args.plain_steps > 0:
-        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        parts = ["migrate", "exchange_halo", "callback", "reverse_halo", "counts"]
+        marks = [[torch.cuda.Event(enable_timing=True) for _ in range(len(parts) + 1)]
+                 for _ in range(args.plain_steps)]
         grid.profile(False)
         with torch.cuda.stream(stream):
-            p0.record(stream)
-            for _ in range(args.plain_steps):
+            for ev in marks:
+                ev[0].record(stream)
                 grid.migrate(stream=stream)
+                ev[1].record(stream)
                 grid.exchange_halo(rebuild=True, stream=stream)
+                ev[2].record(stream)
                 user_work(grid.view(), stream.cuda_stream)
+                ev[3].record(stream)
                 grid.reverse_halo(stream=stream)
+                ev[4].record(stream)
                 grid.all_counts(stream=stream)
-            p1.record(stream)
+                ev[5].record(stream)
         torch.cuda.synchronize(device)
-        plain = round(p0.elapsed_time(p1) / args.plain_steps, 3)
+        plain = round(marks[0][0].elapsed_time(marks[-1][-1]) / args.plain_steps, 3)
+        plain_parts = {name: round(sum(ev[k].elapsed_time(ev[k + 1]) for ev in marks)
+                                   / args.plain_steps, 4) for k, name in enumerate(parts)}
 
     # plain launches: the same per-call operations, every tile kernel launched
     # once per subdomain (the launch pattern of one process per subdomain)
@@ -466,7 +518,7 @@ def run_ours(args, rank, world, device):
         "step_roofline": step_accounting(step_bytes, harness, ms_per_step, ours_ms, peak),
         "kernel_ms": {k: round(v, 4) for k, v in avg.items()},
         "totals_per_step": {k: int(v) for k, v in mean_tot.items()},
-        "per_call_ms_per_step": plain,
+        "per_call_ms_per_step": plain, "per_call_parts_ms": plain_parts,
         "plain_ms_per_step": per_subdomain,
         "batched_vs_plain": round(per_subdomain / ms_per_step, 3) if per_subdomain else None,
         "clocks": clock,

@@ -157,6 +157,20 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
+// Programmatic dependent launch (sm_90+): every kernel of the library is
+// launched with programmatic stream serialisation (pdl_launch in
+// dsx_kernels.cu), so it may become resident while the kernel before it on
+// the stream drains its last wave.  griddepcontrol.wait, the first thing
+// every kernel does, holds it until that kernel has completed and its memory
+// is visible; only then does it let the next kernel launch.  Since each
+// kernel waits for its predecessor before anything else, a kernel's
+// completion still implies the completion of everything enqueued before it.
+// Launched without the attribute, both instructions do nothing.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Read-only (non-coherent) load: the copy kernels read one region and write
 // another, so source loads may be reordered past the stores.
 template <class T>

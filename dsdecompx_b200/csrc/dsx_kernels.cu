@@ -13,6 +13,7 @@
 
 #include <cstdio>
 #include <mutex>
+#include <utility>
 
 namespace dsx {
 namespace {
@@ -173,6 +174,7 @@ __device__ __forceinline__ void fill_tiles(int P, int tile, const int* s_n, cons
 
 __global__ void __launch_bounds__(1024) k_layout(int P, int tile, const int* n, int* obase,
                                                   int* tile_start, int4* tiles) {
+    pdl_begin();
     __shared__ int ws[33];
     __shared__ int s_n[kMaxRanks + 1], s_ob[kMaxRanks + 1], s_ts[kMaxRanks + 1];
     const int t = threadIdx.x;
@@ -205,6 +207,7 @@ __device__ __forceinline__ void scan_counter(const int* cnt, int* pre, int strid
 
 __global__ void __launch_bounds__(1024) k_scan_counters(const int* cnt, int* pre, int stride,
                                                          const int* tile_start_end) {
+    pdl_begin();
     scan_counter(cnt, pre, stride, tile_start_end);
 }
 
@@ -263,6 +266,7 @@ __global__ void __launch_bounds__(NT, 4) k_mig_classify(Grid G, const double* __
                                                      const double* __restrict__ y,
                                                      const double* __restrict__ z, int* cnt,
                                                      int stride, int* imm_total) {
+    pdl_begin();
     __shared__ int ws[33];
     const int g = G.tile_first + blockIdx.x;
     const int P = G.P;
@@ -324,6 +328,7 @@ __global__ void __launch_bounds__(NT, 4) k_mig_classify(Grid G, const double* __
 __global__ void __launch_bounds__(1024) k_mig_layout(Grid G, const int* pre, int stride,
                                                       const int* imm_total, int* imm_base,
                                                       int* emig_info, long long* results) {
+    pdl_begin();
     __shared__ int ws[33];
     const int P = G.P;
     const int t = threadIdx.x;
@@ -376,6 +381,7 @@ __global__ void __launch_bounds__(1024) k_mig_layout(Grid G, const int* pre, int
 __global__ void __launch_bounds__(NT, 4) k_mig_move(Grid G, Arrays A, long long src_off,
                                                  long long dst_off, const int* pre, int stride,
                                                  int* emig_src, int* emig_dst) {
+    pdl_begin();
     __shared__ int s_stay[NW], s_emig[NW];
     const int g = G.tile_first + blockIdx.x;
     const int P = G.P;
@@ -448,6 +454,7 @@ __global__ void __launch_bounds__(NT, 4) k_mig_move(Grid G, Arrays A, long long 
 // K3a: per chunk of the emigrant list, how many go to each destination.
 __global__ void __launch_bounds__(NT) k_emig_hist(int P, const int* emig_info,
                                                   const int* __restrict__ emig_dst, int* hist) {
+    pdl_begin();
     extern __shared__ int sm[];  // [NW][P]
     const int E = emig_info[0], nchunks = emig_info[1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -475,6 +482,7 @@ __global__ void __launch_bounds__(NT) k_emig_hist(int P, const int* emig_info,
 // K3b: per destination, exclusive prefix of its chunk counts.
 __global__ void __launch_bounds__(NT) k_emig_colscan(int P, const int* emig_info, int* hist,
                                                      const int* imm_total, unsigned* status) {
+    pdl_begin();
     __shared__ int ws[33];
     const int d = blockIdx.x;
     const int nchunks = emig_info[1];
@@ -499,6 +507,7 @@ __global__ void __launch_bounds__(NT) k_emig_place(Grid G, Arrays A, long long s
                                                    const int* __restrict__ emig_dst,
                                                    const int* hist, const int* imm_base,
                                                    const int* __restrict__ gap) {
+    pdl_begin();
     extern __shared__ int sm[];  // [NW][P]
     const int P = G.P;
     const int E = emig_info[0], nchunks = emig_info[1];
@@ -723,6 +732,7 @@ __global__ void __launch_bounds__(NT) k_halo_classify(Grid G, const int4* __rest
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z,
                                                       unsigned* mask, int* cnt, int stride) {
+    pdl_begin();
     const int nt = tile_limit(G, ntiles);
     for (int g = G.tile_first + blockIdx.x; g < nt; g += gridDim.x) {
         halo_classify_tile(g, G, tiles, x, y, z, mask, cnt, stride);
@@ -737,6 +747,7 @@ __global__ void __launch_bounds__(1024) k_halo_layout(Grid G, const int* pre, in
                                                        int* list_len, int* send_base, int* gq,
                                                        int* gbase, int* boff, int* info,
                                                        int* cbase) {
+    pdl_begin();
     __shared__ int ws[33];
     __shared__ int s_rcv[kMaxRanks + 1];
     const int P = G.P;
@@ -965,6 +976,7 @@ __global__ void __launch_bounds__(NT) k_halo_scatter(Grid G, Arrays A, long long
                                                      const int* cbase, int* ghost_owner,
                                                      int* ghost_entry, int* bowner, int* boff,
                                                      int* bslot, int* bfirst) {
+    pdl_begin();
     if (*G.status & kStatusGhostOverflow) return;
     const int nt = tile_limit(G, ntiles);
     for (int g = G.tile_first + blockIdx.x; g < nt; g += gridDim.x) {
@@ -1008,6 +1020,7 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                                                       unsigned short* __restrict__ dest_out,
                                                       unsigned* __restrict__ mask_out,
                                                       int* pairs) {
+    pdl_begin();
     constexpr int CI = TILE / CT;   // 32-particle groups per warp
     constexpr int CW = CT / 32;
     static_assert(CI * CT == TILE && CW >= 1, "tile split");
@@ -1153,6 +1166,7 @@ __device__ __forceinline__ void step_layout_body(const Grid& G, const int* pre, 
 __global__ void __launch_bounds__(1024) k_step_scan_layout(Grid G, const int* cnt, int* pre,
                                                             int stride, StepTables T,
                                                             unsigned* ticket) {
+    pdl_begin();
     __shared__ bool s_last;
     scan_counter(cnt, pre, stride, G.tile_start + G.P);
     __syncthreads();
@@ -1325,6 +1339,7 @@ __global__ void __launch_bounds__(NT, 4) k_step_move(Grid G, Arrays A, long long
                                                   int* emig_src, int* emig_dst, int* ghost_owner,
                                                   int* ghost_entry, int* bowner, int* boff,
                                                   int* bslot, int* bfirst) {
+    pdl_begin();
     __shared__ int s_cnt[NW][32];
     __shared__ int s_base[32];
     __shared__ int s_off[kMaxNeighbors + 1];
@@ -1725,6 +1740,7 @@ __global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int s
                                                    const int* cbase_ret, int* tile_bases,
                                                    const int* imm_in, const int* imm_base,
                                                    const int* imm_ts, int4* imm_tiles) {
+    pdl_begin();
     const int ntiles = G.tile_start[G.P];
     for (long long idx = blockIdx.x * static_cast<long long>(NT) + threadIdx.x;
          idx < static_cast<long long>(ntiles) * 32; idx += static_cast<long long>(gridDim.x) * NT) {
@@ -1741,6 +1757,7 @@ __global__ void __launch_bounds__(NT) k_tile_bases(Grid G, const int* pre, int s
 // their images (the retained parts), [3P, 3P + 26P) the retained part of
 // every send list, and out[29P] the emigrants of this shard.
 __global__ void __launch_bounds__(1024) k_step_export(Grid G, const int* pre, int stride, int* out) {
+    pdl_begin();
     const int P = G.P;
     const int* ts = G.tile_start;
     auto tile_sum = [&](int k, int r) {
@@ -1774,6 +1791,7 @@ __global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     const unsigned* __restrict__ mask_in, const int* __restrict__ tile_bases, int* emig_src,
     int* emig_dst, int* ghost_owner, int* ghost_entry, int* bowner, int* boff, int* bslot, int* bfirst, int a0,
     int a1, int index_outputs) {
+    pdl_begin();
     extern __shared__ __align__(16) unsigned char s_rec[];
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ int s_seg[kStagedArrays];
@@ -2024,6 +2042,7 @@ __global__ void __launch_bounds__(NT) k_halo_refresh(Grid G, Arrays A, long long
                                                      const int* info,
                                                      const int* __restrict__ ghost_owner,
                                                      const int* __restrict__ ghost_entry) {
+    pdl_begin();
     if (*G.status & kStatusGhostOverflow) return;
     const int total = info[0];
     // four ghosts per thread and pass: their owner indices, then their
@@ -2084,6 +2103,7 @@ __global__ void __launch_bounds__(NT) k_halo_refresh_owners(Grid G, Arrays A, lo
                                                             const int* __restrict__ bslot,
                                                             const int* __restrict__ bfirst,
                                                             const int* __restrict__ ghost_entry) {
+    pdl_begin();
     if (*G.status & kStatusGhostOverflow) return;
     const int B = info[1];
     constexpr int U = 2;
@@ -2139,6 +2159,7 @@ __global__ void __launch_bounds__(NT) k_forward_fields(Arrays A, long long owned
                                                        const int* info,
                                                        const int* __restrict__ ghost_owner,
                                                        const unsigned* status) {
+    pdl_begin();
     if (*status & kStatusGhostOverflow) return;
     const int total = info[0];
     for (int slot = blockIdx.x * NT + threadIdx.x; slot < total; slot += gridDim.x * NT) {
@@ -2179,6 +2200,7 @@ __global__ void __launch_bounds__(NT) k_reverse_sum3(const int* info, const int*
                                                      const double* __restrict__ gz,
                                                      const unsigned* status, int b_first,
                                                      int b_end) {
+    pdl_begin();
     if (*status & kStatusGhostOverflow) return;
     const int B = b_end >= 0 ? b_end : info[1];
     for (int b = b_first + blockIdx.x * NT + threadIdx.x; b < B; b += gridDim.x * NT) {
@@ -2268,6 +2290,7 @@ __global__ void __launch_bounds__(NT) k_reverse_fields(Arrays A, long long owned
                                                        const int* __restrict__ boff,
                                                        const int* __restrict__ bslot,
                                                        const unsigned* status) {
+    pdl_begin();
     if (*status & kStatusGhostOverflow) return;
     const int B = info[1];
     for (int b = blockIdx.x * NT + threadIdx.x; b < B; b += gridDim.x * NT) {
@@ -2294,20 +2317,37 @@ __global__ void __launch_bounds__(NT) k_reverse_fields(Arrays A, long long owned
 // Dynamic cut planes (dsDecompX src/runtime.cpp:345-447) evaluated by one
 // warp, every value with the reference's operations in the reference's
 // order, on the device so that it can sit inside a captured step.
+//
+// The serial sums run in one loop over the subdomains in index order, each
+// on its own lane: lane 31 the total and the maximum, lanes 0..30 one
+// (axis, slab) sum each (more slabs take further passes).  Every lane adds
+// its terms in the order the reference's single loop does, so each sum has
+// the reference's bits; the lanes only run side by side.
 __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
                                                   RebalanceParams p, long long* call_counter,
                                                   double* result) {
-    // one warp: the serial parts (the totals, each axis's slab sums and
-    // clamps) run in the reference's order on one lane each; the cut
-    // searches, independent per boundary, run one per lane
+    pdl_begin();
     __shared__ double s_work[kMaxRanks];
     __shared__ int s_coord[kMaxRanks];         // packed grid coordinates, staged once
-    __shared__ double s_next[kMaxRanks + 4];   // next cuts, axis a at G.cut_offset[a]
+    __shared__ double s_old[kMaxRanks + 4];    // current cuts, axis a at G.cut_offset[a]
+    __shared__ double s_next[kMaxRanks + 4];   // next cuts, same places
     __shared__ double s_slab[kMaxRanks + 3];   // slab work, axis a at slab_off[a]
-    __shared__ double s_total;
+    __shared__ double s_total, s_max;
     __shared__ int s_go, s_bad;
     const int lane = threadIdx.x;
     if (blockIdx.x != 0) return;
+    const int P = G.P;
+    const int ncuts = G.cut_offset[2] + G.dims[2] + 1;
+    // everything the warp reads, in one round trip
+    for (int s = lane; s < P; s += 32) {
+        s_work[s] = work_in ? work_in[s] : static_cast<double>(G.n[s]);
+        s_coord[s] = G.coord[s];
+    }
+    for (int k = lane; k < ncuts; k += 32) {
+        const double c = G.cuts[k];
+        s_old[k] = c;
+        s_next[k] = c;
+    }
     if (lane == 0) {
         result[0] = 0.0;
         result[1] = 0.0;
@@ -2322,19 +2362,39 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
     }
     __syncwarp();
     if (!s_go) return;
-    const int P = G.P;
-    for (int s = lane; s < P; s += 32) {
-        s_work[s] = work_in ? work_in[s] : static_cast<double>(G.n[s]);
-        s_coord[s] = G.coord[s];
+    const int slab_off[3] = {0, G.dims[0], G.dims[0] + G.dims[1]};
+    const int nslabs = G.dims[0] + G.dims[1] + G.dims[2];
+    for (int first = 0; first == 0 || first < nslabs; first += 31) {
+        // this lane's sum: the total (lane 31, first pass) or slab `pair`
+        const int pair = first + lane;
+        const bool total_lane = lane == 31 && first == 0;
+        const bool slab_lane = lane < 31 && pair < nslabs;
+        int slab = 0, shift = 20;
+        if (slab_lane) {
+            const int axis = pair < slab_off[1] ? 0 : pair < slab_off[2] ? 1 : 2;
+            slab = pair - slab_off[axis];
+            shift = axis == 0 ? 20 : axis == 1 ? 10 : 0;
+        }
+        double acc = 0.0, maximum = 0.0;
+        for (int s = 0; s < P; ++s) {
+            const double w = s_work[s];
+            if (total_lane) {
+                acc = __dadd_rn(acc, w);
+                if (maximum < w) maximum = w;
+            } else if (slab_lane && ((s_coord[s] >> shift) & 1023) == slab) {
+                acc = __dadd_rn(acc, w);
+            }
+        }
+        if (total_lane) {
+            s_total = acc;
+            s_max = maximum;
+        } else if (slab_lane) {
+            s_slab[pair] = acc;
+        }
     }
     __syncwarp();
     if (lane == 0) {
-        double total = 0.0, maximum = 0.0;
-        for (int s = 0; s < P; ++s) {
-            const double w = s_work[s];
-            total = __dadd_rn(total, w);
-            if (maximum < w) maximum = w;
-        }
+        const double total = s_total, maximum = s_max;
         result[0] = 1.0;
         int go = 1;
         if (total <= 0.0 || P <= 1) {
@@ -2345,31 +2405,14 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
             if (!p.force && imbalance < p.threshold) go = 0;
         }
         s_go = go;
-        s_total = total;
     }
     __syncwarp();
     if (!s_go) return;
     const double total = s_total;
-    const int slab_off[3] = {0, G.dims[0], G.dims[0] + G.dims[1]};
-    const int ncuts = G.cut_offset[2] + G.dims[2] + 1;
-    for (int k = lane; k < ncuts; k += 32) s_next[k] = G.cuts[k];
-    if (lane < 3) {
-        const int a = lane, slabs = G.dims[a];
-        double* sw = s_slab + slab_off[a];
-        if (slabs > 1) {
-            for (int i = 0; i < slabs; ++i) sw[i] = 0.0;
-            const int shift = a == 0 ? 20 : a == 1 ? 10 : 0;
-            for (int s = 0; s < P; ++s) {
-                const int c = (s_coord[s] >> shift) & 1023;
-                sw[c] = __dadd_rn(sw[c], s_work[s]);
-            }
-        }
-    }
-    __syncwarp();
     for (int a = 0; a < 3; ++a) {
         const int slabs = G.dims[a];
         if (slabs <= 1) continue;
-        const double* old = G.cuts + G.cut_offset[a];
+        const double* old = s_old + G.cut_offset[a];
         const double* sw = s_slab + slab_off[a];
         double* next = s_next + G.cut_offset[a];
         const double target = __ddiv_rn(total, static_cast<double>(slabs));
@@ -2416,7 +2459,7 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
     __syncwarp();
     bool moved = false;
     for (int k = lane; k < ncuts; k += 32)
-        if (fabs(__dsub_rn(s_next[k], G.cuts[k])) > 1.0e-12) moved = true;
+        if (fabs(__dsub_rn(s_next[k], s_old[k])) > 1.0e-12) moved = true;
     if (!__any_sync(0xffffffffu, moved)) return;
     // Decomposition::set_axis_cuts validation (dsDecompX src/decomp.cpp:146-163)
     if (lane < 3) {
@@ -2454,25 +2497,9 @@ __device__ __forceinline__ int axis_coordinate_count(const double* cuts, int dim
 
 // Decomposition::owner_rank (dsDecompX src/migration.cpp:74-98) of arbitrary
 // positions: one periodic wrap, then the cut search, with the cut planes in
-// shared memory (s_cuts: G.cuts staged, the axes at G.cut_offset): counted on
-// small axes, bisected on long ones.
-__device__ __forceinline__ int owner_of_staged(const Grid& G, const double* s_cuts, double px,
-                                               double py, double pz) {
-    const double p[3] = {px, py, pz};
-    int c[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double v = wrap_if(G, a, p[a]);
-        const double* cuts = s_cuts + G.cut_offset[a];
-        c[a] = G.dims[a] <= kCountedCells ? axis_coordinate_count(cuts, G.dims[a], v)
-                                          : axis_coordinate(cuts, G.dims[a], v);
-    }
-    return (c[0] * G.dims[1] + c[1]) * G.dims[2] + c[2];
-}
-
-// The owner search through a coarse table: each axis is split into kGuessBins
-// equal bins, and the table holds the cell of every bin's lower edge (found
-// with the exact rule).  A position starts at its bin's cell and steps
+// shared memory.  The search goes through a coarse table: each axis is split
+// into kGuessBins equal bins, and the table holds the cell of every bin's
+// lower edge (found with the exact rule).  A position starts at its bin's cell and steps
 // forward while it is not below the next cut, backward while it is below its
 // cell's own cut: the cuts increase strictly, so the steps end at the cell
 // the full search returns (clamped at both ends; a NaN, below no cut, ends
@@ -2541,6 +2568,7 @@ __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restr
                                                    const double* __restrict__ y,
                                                    const double* __restrict__ z, long long n,
                                                    int* out) {
+    pdl_begin();
     __shared__ double s_cuts[kMaxRanks + 16];   // cut_offset[a] + kCountedCells <= 1036
     __shared__ unsigned short s_bins[3 * kGuessBins];
     stage_cuts(G, s_cuts);
@@ -2570,66 +2598,88 @@ __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restr
 // Decomp::has_out_of_domain_particles (dsDecompX src/runtime.cpp:828-840) for
 // every subdomain at once: flags[s] = 1 if an owned particle of s belongs to
 // another subdomain.
+//
+// Each warp takes chunks of 128 consecutive owned particles (four
+// coalesced rows of 32, loaded together).  The warp finds the chunk's
+// subdomain once (the layout's bases in shared memory) and its cell planes
+// once; a position inside its subdomain's own planes is owned there (the wrap
+// leaves a position inside the box as it is, -0 aside, which lies in the same
+// cell), only the others are searched.  A chunk that runs past the end of
+// its subdomain (rare: subdomains hold thousands of particles) finds the
+// later particles' subdomains lane by lane.  One flag atomic per chunk for
+// the chunk's own subdomain.
+__device__ __forceinline__ int subdomain_of_index(const int* s_ob, int lo, int hi, int i) {
+    while (hi - lo > 1) {   // largest s in [lo, hi) with s_ob[s] <= i
+        const int mid = (lo + hi) >> 1;
+        if (s_ob[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool inside_planes(const Grid& G, const double* s_cuts,
+                                              const int* s_coord, int s, double px, double py,
+                                              double pz) {
+    const int packed = s_coord[s];
+    const int c[3] = {packed >> 20, (packed >> 10) & 1023, packed & 1023};
+    const double p[3] = {px, py, pz};
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double* cuts = s_cuts + G.cut_offset[a] + c[a];
+        inside = inside && cuts[0] <= p[a] && p[a] < cuts[1];
+    }
+    return inside;
+}
+
 __global__ void __launch_bounds__(NT) k_out_of_domain(Grid G, const double* __restrict__ x,
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z, int* flags) {
+    pdl_begin();
     __shared__ double s_cuts[kMaxRanks + 16];   // cut_offset[a] + kCountedCells <= 1036
     __shared__ unsigned short s_bins[3 * kGuessBins];
     __shared__ int s_ob[kMaxRanks + 1];
+    __shared__ int s_coord[kMaxRanks];
     const int P = G.P;
-    for (int k = threadIdx.x; k <= P; k += blockDim.x) s_ob[k] = G.obase[k];
+    for (int k = threadIdx.x; k <= P; k += blockDim.x) {
+        s_ob[k] = G.obase[k];
+        if (k < P) s_coord[k] = G.coord[k];
+    }
     stage_cuts(G, s_cuts);
     stage_bins(G, s_cuts, s_bins);
     const CellGuess guess = cell_guess(G);
-    // every owned particle in one grid-stride pass (four per thread and
-    // pass, loaded together); its subdomain from the layout's bases.  A
-    // position inside the subdomain's own cut planes is owned there (the
-    // wrap leaves a position inside the box as it is, -0 aside, which lies in
-    // the same cell); only the others are searched
     const int n = s_ob[P];
     const int lane = threadIdx.x & 31;
-    constexpr int U = 4;
-    const int step = gridDim.x * NT;
-    for (int i0 = blockIdx.x * NT + threadIdx.x; i0 - threadIdx.x % 32 < n; i0 += U * step) {
+    constexpr int U = 4, CHUNK = 32 * U;
+    const int warps = gridDim.x * NW;
+    const long long nchunks = (static_cast<long long>(n) + CHUNK - 1) / CHUNK;
+    for (long long ch = static_cast<long long>(blockIdx.x) * NW + (threadIdx.x >> 5); ch < nchunks;
+         ch += warps) {
+        const int base = static_cast<int>(ch * CHUNK);
+        const int s0 = subdomain_of_index(s_ob, 0, P, base);   // the same on every lane
+        const int end = s_ob[s0 + 1];
         double px[U], py[U], pz[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int i = i0 + u * step;
+            const int i = base + u * 32 + lane;
             if (i < n) {
                 px[u] = ro(x + i);
                 py[u] = ro(y + i);
                 pz[u] = ro(z + i);
             }
         }
+        bool leaves = false;   // a particle of s0 belongs elsewhere
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int i = i0 + u * step;
-            int key = -1;   // the subdomain this particle leaves
-            if (i < n) {
-                int lo = 0, hi = P;   // largest s with s_ob[s] <= i
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (s_ob[mid] <= i) lo = mid;
-                    else hi = mid;
-                }
-                const int packed = G.coord[lo];
-                const int c[3] = {packed >> 20, (packed >> 10) & 1023, packed & 1023};
-                const double p[3] = {px[u], py[u], pz[u]};
-                bool inside = true;
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    const double* cuts = s_cuts + G.cut_offset[a];
-                    inside = inside && cuts[c[a]] <= p[a] && p[a] < cuts[c[a] + 1];
-                }
-                if (!inside && owner_of_binned(G, guess, s_cuts, s_bins, px[u], py[u], pz[u]) != lo)
-                    key = lo;
-            }
-            // one atomic per subdomain and warp
-            if (__any_sync(0xffffffffu, key >= 0)) {
-                const unsigned peers = __match_any_sync(0xffffffffu, key);
-                if (key >= 0 && lane == __ffs(peers) - 1) atomicOr(&flags[key], 1);
-            }
+            const int i = base + u * 32 + lane;
+            if (i >= n) continue;
+            const int s = i < end ? s0 : subdomain_of_index(s_ob, s0 + 1, P, i);
+            if (inside_planes(G, s_cuts, s_coord, s, px[u], py[u], pz[u])) continue;
+            if (owner_of_binned(G, guess, s_cuts, s_bins, px[u], py[u], pz[u]) == s) continue;
+            if (s == s0) leaves = true;
+            else atomicOr(&flags[s], 1);
         }
+        if (__any_sync(0xffffffffu, leaves) && lane == 0) atomicOr(&flags[s0], 1);
     }
 }
 
@@ -2642,6 +2692,7 @@ __global__ void __launch_bounds__(NT) k_pair_counts(int P, const int* __restrict
                                                     const int* __restrict__ emig_src,
                                                     const int* __restrict__ emig_dst,
                                                     const int* __restrict__ obase_old, int* pairs) {
+    pdl_begin();
     const int E = info[0];
     const int lane = threadIdx.x & 31;
     // whole warps walk the list; lanes with the same (destination, source)
@@ -2696,6 +2747,7 @@ __device__ __forceinline__ void copy_words(const unsigned char* __restrict__ src
 // words when source and destination agree modulo 16, else 8, 4 or 1.
 __global__ void __launch_bounds__(NT) k_copy_pieces(const CopyPiece* __restrict__ pieces,
                                                     long long n) {
+    pdl_begin();
     for (long long j = blockIdx.x; j < n; j += gridDim.x) {
         const CopyPiece c = pieces[j];
         const uintptr_t mis = reinterpret_cast<uintptr_t>(c.src) ^ reinterpret_cast<uintptr_t>(c.dst);
@@ -2711,6 +2763,7 @@ __global__ void __launch_bounds__(NT) k_copy_pieces(const CopyPiece* __restrict_
 // src/migration.cpp:106-116).  Only changed values are written back.
 __global__ void __launch_bounds__(NT) k_wrap_inplace(double* x, double* y, double* z, long long n,
                                                      double3 lower, double3 extent, int3 periodic) {
+    pdl_begin();
     for (long long i = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i < n;
          i += static_cast<long long>(gridDim.x) * NT) {
         // all three reads go out before any compare
@@ -2740,6 +2793,26 @@ int sm_count() {
         if (g_sm_count <= 0) g_sm_count = 148;
     }
     return g_sm_count;
+}
+
+// Every kernel launch of the library: programmatic stream serialisation lets
+// the kernel's CTAs become resident (and then wait, pdl_begin) while the
+// previous kernel on the stream drains, inside captured graphs too; errors
+// surface through cudaGetLastError like those of triple-chevron launches.
+template <class... Params, class... Args>
+void pdl_launch(void (*kernel)(Params...), int grid, int block, std::size_t smem, cudaStream_t s,
+                Args&&... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t config = {};
+    config.gridDim = dim3(static_cast<unsigned>(grid));
+    config.blockDim = dim3(static_cast<unsigned>(block));
+    config.dynamicSmemBytes = smem;
+    config.stream = s;
+    config.attrs = attr;
+    config.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&config, kernel, std::forward<Args>(args)...);
 }
 
 int stream_grid(long long items) {
@@ -2776,7 +2849,7 @@ int resident_grid(const void* kernel, long long items) {
 
 void launch_layout(const Grid& G, const int* n, int* obase, int* tile_start, int4* tiles,
                    cudaStream_t s) {
-    k_layout<<<1, 1024, 0, s>>>(G.P, G.tile, n, obase, tile_start, tiles);
+    pdl_launch(k_layout, 1, 1024, 0, s, G.P, G.tile, n, obase, tile_start, tiles);
 }
 
 // Runs launch(Gs, grid) once over all tiles, or, in plain mode, once per
@@ -2801,28 +2874,28 @@ void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long
                     const Scratch& S, cudaStream_t s, const PlainLaunch* plain) {
     cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P, s);
     per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
-        k_mig_classify<<<grid, NT, 0, s>>>(Gs, A.d[0] + src_off, A.d[1] + src_off,
+        pdl_launch(k_mig_classify, grid, NT, 0, s, Gs, A.d[0] + src_off, A.d[1] + src_off,
                                            A.d[2] + src_off, S.cnt, S.stride, S.imm_total);
     });
     if (S.marks) S.marks->mark(s, "mig_classify");
-    k_scan_counters<<<2, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    pdl_launch(k_scan_counters, 2, 1024, 0, s, S.cnt, S.pre, S.stride, G.tile_start + G.P);
     if (S.marks) S.marks->mark(s, "mig_scan");
-    k_mig_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.imm_total, S.imm_base, S.emig_info,
+    pdl_launch(k_mig_layout, 1, 1024, 0, s, G, S.pre, S.stride, S.imm_total, S.imm_base, S.emig_info,
                                      S.mig_results);
     if (S.marks) S.marks->mark(s, "mig_layout");
     per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
-        k_mig_move<<<grid, NT, 0, s>>>(Gs, A, src_off, dst_off, S.pre, S.stride, S.emig_src,
+        pdl_launch(k_mig_move, grid, NT, 0, s, Gs, A, src_off, dst_off, S.pre, S.stride, S.emig_src,
                                        S.emig_dst);
     });
     if (S.marks) S.marks->mark(s, "mig_move");
     const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
     const size_t smem = sizeof(int) * NW * G.P;
-    k_emig_hist<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(G.P, S.emig_info, S.emig_dst,
+    pdl_launch(k_emig_hist, chunk_grid > 0 ? chunk_grid : 1, NT, smem, s, G.P, S.emig_info, S.emig_dst,
                                                                   S.emig_hist);
     if (S.marks) S.marks->mark(s, "emig_hist");
-    k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, S.imm_total, G.status);
+    pdl_launch(k_emig_colscan, G.P, NT, 0, s, G.P, S.emig_info, S.emig_hist, S.imm_total, G.status);
     if (S.marks) S.marks->mark(s, "emig_colscan");
-    k_emig_place<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(
+    pdl_launch(k_emig_place, chunk_grid > 0 ? chunk_grid : 1, NT, smem, s,
         G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base,
         nullptr);
     if (S.marks) S.marks->mark(s, "emig_place");
@@ -2831,18 +2904,18 @@ void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long
 void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                        const Scratch& S, cudaStream_t s, const PlainLaunch* plain) {
     per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
-        k_halo_classify<<<grid, NT, 0, s>>>(Gs, G.tiles, G.tile_start + G.P, A.d[0] + owned_off,
+        pdl_launch(k_halo_classify, grid, NT, 0, s, Gs, G.tiles, G.tile_start + G.P, A.d[0] + owned_off,
                                             A.d[1] + owned_off, A.d[2] + owned_off, S.mask,
                                             S.cnt, S.stride);
     });
     if (S.marks) S.marks->mark(s, "halo_classify");
-    k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    pdl_launch(k_scan_counters, kHaloCounters, 1024, 0, s, S.cnt, S.pre, S.stride, G.tile_start + G.P);
     if (S.marks) S.marks->mark(s, "halo_scan");
-    k_halo_layout<<<1, 1024, 0, s>>>(G, S.pre, S.stride, S.list_len, S.send_base, S.g, S.gbase,
+    pdl_launch(k_halo_layout, 1, 1024, 0, s, G, S.pre, S.stride, S.list_len, S.send_base, S.g, S.gbase,
                                       S.boff, S.halo_info, S.cbase);
     if (S.marks) S.marks->mark(s, "halo_layout");
     per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
-        k_halo_scatter<<<grid, NT, 0, s>>>(Gs, A, owned_off, ghost_off, G.tiles,
+        pdl_launch(k_halo_scatter, grid, NT, 0, s, Gs, A, owned_off, ghost_off, G.tiles,
                                            G.tile_start + G.P, S.mask, S.pre, S.stride, S.cbase,
                                            S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
                                            S.bslot, S.bfirst);
@@ -2893,17 +2966,17 @@ void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, con
     auto pick = [&](auto plain, auto combined) { return S.classify_combine ? combined : plain; };
     switch (S.classify_threads) {
     case 64:
-        pick(k_step_classify<64, 16, false>, k_step_classify<64, 16, true>)<<<G.max_tiles, 64, 0, s>>>(
+        pdl_launch(pick(k_step_classify<64, 16, false>, k_step_classify<64, 16, true>), G.max_tiles, 64, 0, s,
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
             S.mask, S.pairs);
         break;
     case 256:
-        pick(k_step_classify<256, 5, false>, k_step_classify<256, 5, true>)<<<G.max_tiles, 256, 0, s>>>(
+        pdl_launch(pick(k_step_classify<256, 5, false>, k_step_classify<256, 5, true>), G.max_tiles, 256, 0, s,
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
             S.mask, S.pairs);
         break;
     default:
-        pick(k_step_classify<128, 12, false>, k_step_classify<128, 12, true>)<<<G.max_tiles, 128, 0, s>>>(
+        pdl_launch(pick(k_step_classify<128, 12, false>, k_step_classify<128, 12, true>), G.max_tiles, 128, 0, s,
             G, x, y, z, S.cnt, S.stride, S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.dest16,
             S.mask, S.pairs);
     }
@@ -2913,8 +2986,8 @@ void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s) {
     StepTables T{S.imm_total, S.imm_list, S.imm_bnd, S.imm_img, S.imm_base, S.emig_info,
                  S.mig_results, S.list_ret, S.list_len, S.send_base, S.g, S.gbase, S.boff,
                  S.halo_info, S.cbase, S.cbase_imm, S.imm_tile_start, S.imm_tiles};
-    k_step_scan_layout<<<kStepCounters, 1024, 0, s>>>(G, S.cnt, S.pre, S.stride, T, S.ticket);
-    k_tile_bases<<<stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s>>>(
+    pdl_launch(k_step_scan_layout, kStepCounters, 1024, 0, s, G, S.cnt, S.pre, S.stride, T, S.ticket);
+    pdl_launch(k_tile_bases, stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s,
         G, S.pre, S.stride, S.cbase, S.tile_bases, S.imm_total, S.imm_base, S.imm_tile_start,
         S.imm_tiles);
 }
@@ -2949,18 +3022,18 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
     auto staged = [&](bool full, int a0, int a1, int index_outputs) {
         const int bytes = staged_range_bytes(A, a0, a1);
         if (full)
-            k_step_move_staged<true, false><<<G.max_tiles, NT, bytes, s>>>(
+            pdl_launch(k_step_move_staged<true, false>, G.max_tiles, NT, bytes, s,
                 G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
                 S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
                 S.boff, S.bslot, S.bfirst, a0, a1, index_outputs);
         else
-            k_step_move_staged<false, false><<<G.max_tiles, NT, bytes, s>>>(
+            pdl_launch(k_step_move_staged<false, false>, G.max_tiles, NT, bytes, s,
                 G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
                 S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner,
                 S.boff, S.bslot, S.bfirst, a0, a1, index_outputs);
     };
     if (S.move_staged == 3 && whole - kForceStageBytes <= kStagedMaxBytes) {
-        k_step_move_staged<true, true><<<G.max_tiles, NT, whole - kForceStageBytes, s>>>(
+        pdl_launch(k_step_move_staged<true, true>, G.max_tiles, NT, whole - kForceStageBytes, s,
             G, A, src_off, dst_off, ghost_off, S.pre, S.stride, S.cbase, S.dest16, S.mask,
             S.tile_bases, S.emig_src, S.emig_dst, S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
             S.bslot, S.bfirst, 0, narrays, 1);
@@ -2974,7 +3047,7 @@ void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long lo
                 staged(false, a0, ends[p], p == 0 ? 1 : 0);
         }
     } else {
-        k_step_move<<<G.max_tiles, NT, 0, s>>>(G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
+        pdl_launch(k_step_move, G.max_tiles, NT, 0, s, G, A, src_off, dst_off, ghost_off, S.pre, S.stride,
                                                S.cbase, S.dest16, S.mask, S.emig_src, S.emig_dst,
                                                S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
                                                S.bslot, S.bfirst);
@@ -2985,24 +3058,24 @@ void launch_step_emigrants(const Grid& G, const Arrays& A, long long src_off, lo
                            const Scratch& S, const int* local_imm, const int* gap, cudaStream_t s) {
     const int chunk_grid = S.max_chunks < sm_count() * 4 ? S.max_chunks : sm_count() * 4;
     const size_t smem = sizeof(int) * NW * G.P;
-    k_emig_hist<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(G.P, S.emig_info, S.emig_dst,
+    pdl_launch(k_emig_hist, chunk_grid > 0 ? chunk_grid : 1, NT, smem, s, G.P, S.emig_info, S.emig_dst,
                                                                   S.emig_hist);
-    k_emig_colscan<<<G.P, NT, 0, s>>>(G.P, S.emig_info, S.emig_hist, local_imm, G.status);
-    k_emig_place<<<chunk_grid > 0 ? chunk_grid : 1, NT, smem, s>>>(
+    pdl_launch(k_emig_colscan, G.P, NT, 0, s, G.P, S.emig_info, S.emig_hist, local_imm, G.status);
+    pdl_launch(k_emig_place, chunk_grid > 0 ? chunk_grid : 1, NT, smem, s,
         G, A, src_off, dst_off, S.emig_info, S.emig_src, S.emig_dst, S.emig_hist, S.imm_base, gap);
     if (S.marks) S.marks->mark(s, "emig_place");
 }
 
 void launch_step_scan(const Grid& G, const Scratch& S, cudaStream_t s) {
-    k_scan_counters<<<kStepCounters, 1024, 0, s>>>(S.cnt, S.pre, S.stride, G.tile_start + G.P);
+    pdl_launch(k_scan_counters, kStepCounters, 1024, 0, s, S.cnt, S.pre, S.stride, G.tile_start + G.P);
 }
 
 void launch_step_export(const Grid& G, const Scratch& S, int* out, cudaStream_t s) {
-    k_step_export<<<1, 1024, 0, s>>>(G, S.pre, S.stride, out);
+    pdl_launch(k_step_export, 1, 1024, 0, s, G, S.pre, S.stride, out);
 }
 
 void launch_step_bases(const Grid& G, const Scratch& S, const int* imm_in, cudaStream_t s) {
-    k_tile_bases<<<stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s>>>(
+    pdl_launch(k_tile_bases, stream_grid(static_cast<long long>(G.max_tiles) * 32), NT, 0, s,
         G, S.pre, S.stride, S.cbase, S.tile_bases, imm_in, S.imm_base, S.imm_tile_start,
         S.imm_tiles);
 }
@@ -3018,12 +3091,12 @@ void launch_step_immigrant_halo(const Grid& Gn, const Arrays& A, long long dst_o
     const Grid& G = Gn;
     // immigrants: masks, list ranks and ghost images over their segments
     const int imm_grid = G.max_tiles < sm_count() * 4 ? G.max_tiles : sm_count() * 4;
-    k_halo_classify<<<imm_grid, NT, 0, s>>>(Gn, S.imm_tiles, S.imm_tile_start + G.P,
+    pdl_launch(k_halo_classify, imm_grid, NT, 0, s, Gn, S.imm_tiles, S.imm_tile_start + G.P,
                                             A.d[0] + dst_off, A.d[1] + dst_off, A.d[2] + dst_off,
                                             S.mask, S.cnt2, S.stride);
-    k_scan_counters<<<kHaloCounters, 1024, 0, s>>>(S.cnt2, S.pre2, S.stride,
+    pdl_launch(k_scan_counters, kHaloCounters, 1024, 0, s, S.cnt2, S.pre2, S.stride,
                                                    S.imm_tile_start + G.P);
-    k_halo_scatter<<<imm_grid, NT, 0, s>>>(Gn, A, dst_off, ghost_off, S.imm_tiles,
+    pdl_launch(k_halo_scatter, imm_grid, NT, 0, s, Gn, A, dst_off, ghost_off, S.imm_tiles,
                                            S.imm_tile_start + G.P, S.mask, S.pre2, S.stride,
                                            S.cbase_imm, S.ghost_owner, S.ghost_entry, S.bowner,
                                            S.boff, S.bslot, S.bfirst);
@@ -3046,14 +3119,14 @@ void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, lo
     if (S.refresh_owners) {
         int grid = resident_grid(reinterpret_cast<const void*>(k_halo_refresh_owners), G.ncap);
         if (ctas_per_sm > 0 && grid > sm_count() * ctas_per_sm) grid = sm_count() * ctas_per_sm;
-        k_halo_refresh_owners<<<grid, NT, 0, s>>>(G, A, owned_off, ghost_off, positions_only ? 1 : 0,
+        pdl_launch(k_halo_refresh_owners, grid, NT, 0, s, G, A, owned_off, ghost_off, positions_only ? 1 : 0,
                                                   S.halo_info, S.bowner, S.boff, S.bslot,
                                                   S.bfirst, S.ghost_entry);
         return;
     }
     int grid = resident_grid(reinterpret_cast<const void*>(k_halo_refresh), G.gcap);
     if (ctas_per_sm > 0 && grid > sm_count() * ctas_per_sm) grid = sm_count() * ctas_per_sm;
-    k_halo_refresh<<<grid, NT, 0, s>>>(G, A, owned_off, ghost_off,
+    pdl_launch(k_halo_refresh, grid, NT, 0, s, G, A, owned_off, ghost_off,
                                                       positions_only ? 1 : 0, S.halo_info,
                                                       S.ghost_owner, S.ghost_entry);
 }
@@ -3061,7 +3134,7 @@ void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, lo
 void launch_forward_fields(const Grid& G, const Arrays& A, long long owned_off,
                            long long ghost_off, const FieldOps& F, const Scratch& S,
                            cudaStream_t s) {
-    k_forward_fields<<<resident_grid(reinterpret_cast<const void*>(k_forward_fields), G.gcap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
+    pdl_launch(k_forward_fields, resident_grid(reinterpret_cast<const void*>(k_forward_fields), G.gcap), NT, 0, s, A, owned_off, ghost_off, F, S.halo_info,
                                                         S.ghost_owner, G.status);
 }
 
@@ -3072,13 +3145,13 @@ void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, cons
         for (int r = 0; r < G.P; ++r) {
             const int b0 = plain->boundary_start[r], b1 = plain->boundary_start[r + 1];
             if (b1 <= b0) continue;
-            k_reverse_sum3<<<stream_grid(b1 - b0), NT, 0, s>>>(S.halo_info, S.bowner, S.boff,
+            pdl_launch(k_reverse_sum3, stream_grid(b1 - b0), NT, 0, s, S.halo_info, S.bowner, S.boff,
                                                                S.bslot, S.bfirst, ox, oy, oz, gx, gy, gz,
                                                                G.status, b0, b1);
         }
     } else {
         const int grid = S.reverse_per_sm > 0 ? sm_count() * S.reverse_per_sm : stream_grid(G.ncap);
-        k_reverse_sum3<<<grid, NT, 0, s>>>(S.halo_info, S.bowner, S.boff, S.bslot, S.bfirst, ox, oy, oz, gx,
+        pdl_launch(k_reverse_sum3, grid, NT, 0, s, S.halo_info, S.bowner, S.boff, S.bslot, S.bfirst, ox, oy, oz, gx,
                                            gy, gz, G.status, 0, -1);
     }
     if (S.marks) S.marks->mark(s, "reverse_sum");
@@ -3087,25 +3160,24 @@ void launch_reverse_sum3(const Grid& G, double* ox, double* oy, double* oz, cons
 void launch_reverse_fields(const Grid& G, const Arrays& A, long long owned_off,
                            long long ghost_off, const FieldOps& F, const Scratch& S,
                            cudaStream_t s) {
-    k_reverse_fields<<<resident_grid(reinterpret_cast<const void*>(k_reverse_fields), G.ncap), NT, 0, s>>>(A, owned_off, ghost_off, F, S.halo_info,
+    pdl_launch(k_reverse_fields, resident_grid(reinterpret_cast<const void*>(k_reverse_fields), G.ncap), NT, 0, s, A, owned_off, ghost_off, F, S.halo_info,
                                                         S.bowner, S.boff, S.bslot, G.status);
 }
 
 void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
                       long long* call_counter, double* result, cudaStream_t s) {
-    k_rebalance<<<1, 32, 0, s>>>(G, work, params, call_counter, result);
+    pdl_launch(k_rebalance, 1, 32, 0, s, G, work, params, call_counter, result);
 }
 
 void launch_owner_rank(const Grid& G, const double* x, const double* y, const double* z,
                        long long n, int* out, cudaStream_t s) {
-    if (n > 0) k_owner_rank<<<resident_grid(reinterpret_cast<const void*>(k_owner_rank), n), NT, 0, s>>>(G, x, y, z, n, out);
+    if (n > 0) pdl_launch(k_owner_rank, resident_grid(reinterpret_cast<const void*>(k_owner_rank), n), NT, 0, s, G, x, y, z, n, out);
 }
 
 void launch_out_of_domain(const Grid& G, const double* x, const double* y, const double* z,
                           int* flags, cudaStream_t s) {
     cudaMemsetAsync(flags, 0, sizeof(int) * G.P, s);
-    k_out_of_domain<<<resident_grid(reinterpret_cast<const void*>(k_out_of_domain), G.ncap), NT, 0,
-                      s>>>(G, x, y, z, flags);
+    pdl_launch(k_out_of_domain, resident_grid(reinterpret_cast<const void*>(k_out_of_domain), G.ncap), NT, 0, s, G, x, y, z, flags);
 }
 
 void mark(const Scratch& S, cudaStream_t s, const char* what) {
@@ -3117,7 +3189,7 @@ void launch_pair_counts(int P, const Scratch& S, const int* obase_old, long long
     cudaMemsetAsync(pairs, 0, sizeof(int) * static_cast<std::size_t>(P) * P, s);
     if (ncap > 0) {
         const long long want = (ncap + NT - 1) / NT, cap = static_cast<long long>(sm_count()) * 4;
-        k_pair_counts<<<static_cast<int>(want < cap ? want : cap), NT, 0, s>>>(
+        pdl_launch(k_pair_counts, static_cast<int>(want < cap ? want : cap), NT, 0, s,
             P, S.emig_info, S.emig_src, S.emig_dst, obase_old, pairs);
     }
 }
@@ -3164,7 +3236,7 @@ cudaError_t launch_copies(const std::vector<CopyPiece>& copies, cudaStream_t s) 
     if (e != cudaSuccess) return e;
     const long long cap = static_cast<long long>(sm_count()) * 8;
     const long long count = static_cast<long long>(n);
-    k_copy_pieces<<<static_cast<int>(count < cap ? count : cap), NT, 0, s>>>(st.device, count);
+    pdl_launch(k_copy_pieces, static_cast<int>(count < cap ? count : cap), NT, 0, s, st.device, count);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return cudaEventRecord(st.done, s);
 }
@@ -3173,7 +3245,7 @@ void launch_wrap_inplace(double* x, double* y, double* z, long long n, const dou
                          const double* extent, const int* periodic, cudaStream_t s) {
     if (n <= 0) return;
     const long long blocks = (n + NT - 1) / NT;   // one particle per thread
-    k_wrap_inplace<<<static_cast<int>(blocks < 1 ? 1 : (blocks < (1 << 30) ? blocks : (1 << 30))), NT, 0, s>>>(
+    pdl_launch(k_wrap_inplace, static_cast<int>(blocks < 1 ? 1 : (blocks < (1 << 30) ? blocks : (1 << 30))), NT, 0, s,
         x, y, z, n, make_double3(lower[0], lower[1], lower[2]),
         make_double3(extent[0], extent[1], extent[2]),
         make_int3(periodic[0], periodic[1], periodic[2]));

@@ -182,3 +182,27 @@ def test_noalloc_refuses_overlapping_arrays():
 def test_noalloc_refuses_bad_cuts(cuts):
     status, msg = _noalloc_call(2, (2, 1, 1), [0, 0], [0] * 13, [0] * 13, cuts=cuts)
     assert status == -1 and b"strictly increasing and span" in msg
+
+
+def test_every_library_kernel_waits_for_its_predecessor():
+    """The library launches its kernels with programmatic stream serialisation
+    (a kernel may become resident while the one before it drains).  That is
+    only ordered if every such kernel waits (griddepcontrol.wait, through
+    pdl_begin) before it touches memory: each kernel body of dsx_kernels.cu
+    must open with pdl_begin(), and every launch there must go through
+    pdl_launch (no triple-chevron launch)."""
+    src = open(os.path.join(ROOT, "dsdecompx_b200", "csrc", "dsx_kernels.cu")).read()
+    code = re.sub(r"//[^\n]*", "", src)
+    kernels = 0
+    for m in re.finditer(r"__global__[^{;]*?\b(k_\w+)\s*\(", code):
+        depth, k = 0, m.end() - 1
+        while True:
+            depth += {"(": 1, ")": -1}.get(code[k], 0)
+            if depth == 0:
+                break
+            k += 1
+        body = code[code.index("{", k) + 1:]
+        assert body.lstrip().startswith("pdl_begin();"), m.group(1)
+        kernels += 1
+    assert kernels >= 20
+    assert "<<<" not in code
