@@ -445,6 +445,7 @@ struct dsx_grid {
     double* d_shift = nullptr;
     signed char* d_dir = nullptr;
     unsigned* d_lut = nullptr;
+    unsigned* d_lut_empty = nullptr;   // the same shape, every mask 0 (no halo)
     int* d_coord = nullptr;
     // plain launches (per-call operations, one launch per subdomain)
     bool plain = false;
@@ -664,6 +665,7 @@ struct dsx_grid {
         d_shift = device_alloc<double>(fixed_owned, shift.size());
         d_dir = device_alloc<signed char>(fixed_owned, dir.size());
         d_lut = device_alloc<unsigned>(fixed_owned, lut.size());
+        d_lut_empty = device_alloc<unsigned>(fixed_owned, lut.size());
         std::vector<int> coord(static_cast<std::size_t>(P));
         for (int s = 0; s < P; ++s) {
             const auto& c = coords[static_cast<std::size_t>(s)];
@@ -672,6 +674,7 @@ struct dsx_grid {
         d_coord = device_alloc<int>(fixed_owned, coord.size());
         up(d_nn, nn); up(d_nbr, nbr); up(d_recv_entry, recv_entry); up(d_sender_of, sender_of);
         up(d_shift, shift); up(d_dir, dir); up(d_lut, lut); up(d_coord, coord);
+        up(d_lut_empty, std::vector<unsigned>(lut.size(), 0u));
 
         // uniform cuts (dsDecompX src/topology.cpp:63-75)
         std::vector<double> c;
@@ -902,7 +905,16 @@ struct dsx_grid {
                                 plain_layout(stream));
         } else {
             enqueue_rebalance(stream, automatic_rebalance, work_in);
-            dsx::launch_migrate(params(), A, owned_off(), next_off(), S, stream);
+            // the batched step's classify, layout and staged move over an
+            // empty halo table: every halo mask is 0, so the pipeline lays
+            // out and writes no ghost and leaves what migrate alone leaves
+            // (the old layout's plan is dropped either way)
+            dsx::Grid G = params();
+            G.lut = d_lut_empty;
+            dsx::launch_step_classify(G, A, owned_off(), S, stream);
+            dsx::launch_step_layout(G, S, stream);
+            dsx::launch_step_move(G, A, owned_off(), next_off(), ghost_off(), S, stream);
+            dsx::launch_step_emigrants(G, A, owned_off(), next_off(), S, S.imm_total, nullptr, stream);
         }
         commit_migrate();
         if (results) {
@@ -922,6 +934,8 @@ struct dsx_grid {
             clear_status(stream);
             enqueue_halo_build(stream, plain_layout(stream));
             const unsigned st = read_status(stream);
+            if (st & dsx::kStatusCopyTimeout)
+                fail(DSX_E_RUNTIME, "a bulk copy of particle records did not complete within 1 s");
             if (!(st & dsx::kStatusGhostOverflow)) break;
             grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
         }
@@ -1046,6 +1060,8 @@ struct dsx_grid {
             } else {
                 st = read_status(stream);
             }
+            if (st & dsx::kStatusCopyTimeout)
+                fail(DSX_E_RUNTIME, "a bulk copy of particle records did not complete within 1 s");
             if (st & dsx::kStatusGhostOverflow) {
                 grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
                 build_checked(stream);

@@ -1713,6 +1713,178 @@ __device__ __forceinline__ void ghost_array_from_stage(const Grid& G, const Arra
     }
 }
 
+// Ghost image of staged record l for a plan rebuild: the position as it is
+// (the rebuild copies it without a wrap, like write_ghost) + shift,
+// velocities, zero force, mass, charge, type, id, fields.
+__device__ __forceinline__ void ghost_from_stage_unwrapped(const Arrays& A, const unsigned char* rec,
+                                                           const int* sg, const int* fseg, int l,
+                                                           long long gi, const double* sh) {
+    double v[11];
+#pragma unroll
+    for (int a = 0; a < 11; ++a)
+        if (a < 6 || a > 8) v[a] = srd(rec, sg[a], l);
+    const int ty = sri(rec, sg[11], l), id = sri(rec, sg[12], l);
+    A.d[0][gi] = __dadd_rn(v[0], sh[0]);
+    A.d[1][gi] = __dadd_rn(v[1], sh[1]);
+    A.d[2][gi] = __dadd_rn(v[2], sh[2]);
+#pragma unroll
+    for (int a = 3; a < 6; ++a) A.d[a][gi] = v[a];
+    A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+    A.d[9][gi] = v[9];
+    A.d[10][gi] = v[10];
+    A.type[gi] = ty;
+    A.gid[gi] = id;
+    fields_from_stage(A.f, rec, fseg, l, gi);
+}
+
+// The plan build's scatter (same outputs as k_halo_scatter, one tile per
+// block) with the tile's records brought into shared memory by bulk copies
+// (every array but the forces, which a ghost does not carry) while the block
+// ranks the tile's hits from the masks.  The images are then written list by
+// list from shared memory, consecutive threads on consecutive ghost slots:
+// the records cross HBM once, as whole tiles, instead of as one 32-byte
+// sector per array and image.  A tile with more images than the staging
+// list holds writes them from HBM reads during the ranking, as k_halo_scatter
+// does.
+__global__ void __launch_bounds__(NT, 4) k_halo_scatter_staged(
+    Grid G, Arrays A, long long owned_off, long long ghost_off, const int4* __restrict__ tiles,
+    const int* ntiles, const unsigned* __restrict__ mask, const int* pre, int stride,
+    const int* cbase, int* ghost_owner, int* ghost_entry, int* bowner, int* boff, int* bslot,
+    int* bfirst) {
+    pdl_begin();
+    extern __shared__ __align__(16) unsigned char s_rec[];
+    __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ int s_seg[kStagedArrays];
+    __shared__ int s_cnt[NW][32];
+    __shared__ int s_base[32];
+    __shared__ int s_off[kMaxNeighbors + 1];
+    __shared__ unsigned short s_own[kStageCap];
+    const int g = G.tile_first + blockIdx.x;
+    if (g >= tile_limit(G, ntiles) || (*G.status & kStatusGhostOverflow)) return;
+    const int4 td = tiles[g];
+    const int s = td.x, begin = td.y, end = td.z;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbegin = begin + warp * 32 * ITEMS;
+    const unsigned bar = smem_u32(&s_bar);
+    if (warp == 0) {
+        if (lane == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+        stage_issue(A, owned_off, begin, end, s_rec, bar, s_seg, lane, 0, 13 + A.f.count, true);
+    }
+    const int nn = G.nn[s];
+    const unsigned lt = lanemask_lt();
+    unsigned m[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = wbegin + j * 32 + lane;
+        m[j] = i < end ? mask[i] : 0u;
+    }
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) count_group(m[j], nn, lane, acc);
+    s_cnt[warp][lane] = acc;
+    if (threadIdx.x < kHaloCounters) {
+        const int k = threadIdx.x;
+        s_base[k] = cbase[s * kHaloCounters + k] + pre[k * stride + g] - pre[k * stride + td.w];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int tot = 0;
+        if (lane < nn)
+            for (int w = 0; w < NW; ++w) tot += s_cnt[w][lane];
+        const int incl = warp_inclusive_sum(tot);
+        if (lane < nn) s_off[lane] = incl - tot;
+        if (lane == 31) s_off[nn] = incl;
+    }
+    __syncthreads();
+    const int Q = s_off[nn];
+    const bool staged = Q <= kStageCap;
+    int run = 0, lrun = 0;
+    if (lane < kHaloCounters) {
+        run = s_base[lane];
+        if (lane < nn) lrun = s_off[lane];
+        for (int w = 0; w < warp; ++w) {
+            run += s_cnt[w][lane];
+            lrun += s_cnt[w][lane];
+        }
+    }
+    const double* shift = G.shift + static_cast<long long>(s) * kMaxNeighbors * 3;
+#pragma unroll 1
+    for (int j = 0; j < ITEMS; ++j) {
+        const unsigned mj = m[j];
+        const unsigned any = __ballot_sync(0xffffffffu, mj != 0);
+        if (!any) continue;
+        const int i = wbegin + j * 32 + lane;
+        const int b = __shfl_sync(0xffffffffu, run, kBoundaryCounter) + __popc(any & lt);
+        const int pm = __popc(mj);
+        const int incl = warp_inclusive_sum(pm);
+        const int img = __shfl_sync(0xffffffffu, run, kImageCounter) + incl - pm;
+        if (mj) {
+            bowner[b] = i;
+            boff[b] = img;
+        }
+        int k = 0;
+        const unsigned used = __reduce_or_sync(0xffffffffu, mj);
+        for (unsigned rest = used; rest; rest &= rest - 1) {
+            const int n = __ffs(rest) - 1;
+            const unsigned hit = __ballot_sync(0xffffffffu, (mj >> n) & 1u);
+            const int list_base = __shfl_sync(0xffffffffu, run, n);
+            const int stage_base = __shfl_sync(0xffffffffu, lrun, n);
+            if ((mj >> n) & 1u) {
+                const int rank = __popc(hit & lt);
+                const int slot = list_base + rank;
+                bslot[img + k] = slot;
+                if (k == 0) bfirst[b] = slot;
+                ++k;
+                if (staged) {
+                    s_own[stage_base + rank] = static_cast<unsigned short>(i - begin);
+                } else {
+                    write_ghost(A, owned_off + i, ghost_off + slot, shift + 3 * n);
+                    ghost_owner[slot] = i;
+                    ghost_entry[slot] = s * kMaxNeighbors + n;
+                }
+            }
+            if (lane == n) {
+                run += __popc(hit);
+                lrun += __popc(hit);
+            }
+        }
+        const int group_images = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane == kBoundaryCounter) run += __popc(any);
+        if (lane == kImageCounter) run += group_images;
+    }
+    // the records must have landed (and every warp's staging list be
+    // visible) before the images are written from shared memory
+    const bool lost = !bulk_wait(bar);
+    if (__syncthreads_or(lost)) {
+        if (lost) bulk_wait(bar);   // copies still in flight get one more bounded wait
+        if (threadIdx.x == 0) atomicOr(G.status, kStatusCopyTimeout);
+        return;
+    }
+    if (!staged) return;
+    int sg[13];
+#pragma unroll
+    for (int a = 0; a < 13; ++a) sg[a] = s_seg[a];
+    const int* fseg = s_seg + 13;
+    for (int q = threadIdx.x; q < Q; q += NT) {
+        int lo = 0, hi = nn;   // largest n with s_off[n] <= q
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_off[mid] <= q) lo = mid;
+            else hi = mid;
+        }
+        const int n = lo;
+        const int slot = s_base[n] + (q - s_off[n]);
+        const int l = s_own[q];
+        ghost_from_stage_unwrapped(A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
+        ghost_owner[slot] = begin + l;
+        ghost_entry[slot] = s * kMaxNeighbors + n;
+    }
+}
+
 // Tile descriptors {s, begin, end, first tile of s} of a layout given by its
 // global counts, bases and tile starts (P + 1 entries each), the tiles
 // strided over the threads of the grid.
@@ -2901,6 +3073,18 @@ void launch_migrate(const Grid& G, const Arrays& A, long long src_off, long long
     if (S.marks) S.marks->mark(s, "emig_place");
 }
 
+// Shared memory the staged move needs for one tile of arrays [a0, a1).
+int staged_range_bytes(const Arrays& A, int a0, int a1) {
+    int bytes = 0;
+    for (int k = a0; k < a1; ++k) bytes += TILE * (k < 11 ? 8 : k < 13 ? 4 : A.f.bytes[k - 13]) + 32;
+    return bytes;
+}
+
+int staged_bytes(const Arrays& A) { return staged_range_bytes(A, 0, 13 + A.f.count); }
+
+// Shared memory of the three force arrays of one staged tile.
+constexpr int kForceStageBytes = 3 * (TILE * 8 + 32);
+
 void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                        const Scratch& S, cudaStream_t s, const PlainLaunch* plain) {
     per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
@@ -2914,26 +3098,29 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off, long
     pdl_launch(k_halo_layout, 1, 1024, 0, s, G, S.pre, S.stride, S.list_len, S.send_base, S.g, S.gbase,
                                       S.boff, S.halo_info, S.cbase);
     if (S.marks) S.marks->mark(s, "halo_layout");
-    per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
-        pdl_launch(k_halo_scatter, grid, NT, 0, s, Gs, A, owned_off, ghost_off, G.tiles,
-                                           G.tile_start + G.P, S.mask, S.pre, S.stride, S.cbase,
-                                           S.ghost_owner, S.ghost_entry, S.bowner, S.boff,
-                                           S.bslot, S.bfirst);
-    });
+    // the tile's records staged in shared memory (all but the forces) when
+    // they fit; plain launches keep the per-image reads
+    const int stage = staged_bytes(A) - kForceStageBytes;
+    if (!plain && stage <= kStagedMaxBytes) {
+        static bool attribute_set = false;   // once per process (one device per process)
+        if (!attribute_set) {
+            cudaFuncSetAttribute(k_halo_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kStagedMaxBytes);
+            attribute_set = true;
+        }
+        pdl_launch(k_halo_scatter_staged, G.max_tiles, NT, static_cast<std::size_t>(stage), s, G, A,
+                   owned_off, ghost_off, G.tiles, G.tile_start + G.P, S.mask, S.pre, S.stride,
+                   S.cbase, S.ghost_owner, S.ghost_entry, S.bowner, S.boff, S.bslot, S.bfirst);
+    } else {
+        per_subdomain(G, plain, [&](const Grid& Gs, int grid) {
+            pdl_launch(k_halo_scatter, grid, NT, 0, s, Gs, A, owned_off, ghost_off, G.tiles,
+                       G.tile_start + G.P, S.mask, S.pre, S.stride, S.cbase, S.ghost_owner,
+                       S.ghost_entry, S.bowner, S.boff, S.bslot, S.bfirst);
+        });
+    }
     if (S.marks) S.marks->mark(s, "halo_scatter");
 }
 
-// Shared memory the staged move needs for one tile of arrays [a0, a1).
-int staged_range_bytes(const Arrays& A, int a0, int a1) {
-    int bytes = 0;
-    for (int k = a0; k < a1; ++k) bytes += TILE * (k < 11 ? 8 : k < 13 ? 4 : A.f.bytes[k - 13]) + 32;
-    return bytes;
-}
-
-int staged_bytes(const Arrays& A) { return staged_range_bytes(A, 0, 13 + A.f.count); }
-
-// Shared memory of the three force arrays of one staged tile.
-constexpr int kForceStageBytes = 3 * (TILE * 8 + 32);
 
 // A staged pass holds at most this much of the record, so that three CTAs
 // (their tiles in flight at once) fit an SM's shared memory.
