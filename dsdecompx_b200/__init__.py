@@ -131,6 +131,8 @@ def lib() -> C.CDLL:
             "dsx_grid_invalidate_halo": [vp],
             "dsx_grid_halo_backward": [vp, vp, vp, vp, vp, vp, vp, vp],
             "dsx_grid_step": [vp, STEP_CALLBACK, vp, C.c_int, vp, C.POINTER(C.c_uint)],
+            "dsx_grid_step_async": [vp, STEP_CALLBACK, vp, vp],
+            "dsx_grid_step_wait": [vp, C.POINTER(C.c_uint)],
             "dsx_grid_step_kernel_count": [vp],
             "dsx_grid_profile": [vp, C.c_int],
             "dsx_grid_set_plain": [vp, C.c_int],
@@ -480,9 +482,7 @@ class VirtualGrid:
             owner_grad[0].data_ptr(), owner_grad[1].data_ptr(), owner_grad[2].data_ptr(),
             _stream(stream)))
 
-    def step(self, callback=None, capture: bool = False, stream=None) -> int:
-        """One batched step: migrate -> halo build -> callback(view, stream)
-        -> reverse_halo.  Returns the device status bits (0 == ok)."""
+    def _step_callback(self, callback):
         # one C function pointer per Python callback: the engine keeps its
         # captured graphs only while the callback pointer stays the same
         cache = self.__dict__.setdefault("_cb_cache", {})
@@ -492,7 +492,31 @@ class VirtualGrid:
                 cache[key] = (None, STEP_CALLBACK())
             else:
                 cache[key] = (callback, STEP_CALLBACK(_trampoline(callback, self)))
-        cb = cache[key][1]
+        return cache[key][1]
+
+    def step_async(self, callback=None, stream=None) -> None:
+        """Queues one captured batched step (dsx_grid_step_async) and returns:
+        the previous queued step's build is checked (and an overflow redone)
+        before this one is queued.  step_wait() completes the queue."""
+        cb = self._step_callback(callback)
+        self._callback_error = None
+        status = self.L.dsx_grid_step_async(self.h, cb, None, _stream(stream))
+        _raise_callback_error(self)
+        _check(status)
+
+    def step_wait(self) -> int:
+        """Completes the queued steps; the OR of their status bits."""
+        st = C.c_uint()
+        self._callback_error = None
+        status = self.L.dsx_grid_step_wait(self.h, C.byref(st))
+        _raise_callback_error(self)
+        _check(status)
+        return st.value
+
+    def step(self, callback=None, capture: bool = False, stream=None) -> int:
+        """One batched step: migrate -> halo build -> callback(view, stream)
+        -> reverse_halo.  Returns the device status bits (0 == ok)."""
+        cb = self._step_callback(callback)
         st = C.c_uint()
         self._callback_error = None
         status = self.L.dsx_grid_step(self.h, cb, None, 1 if capture else 0, _stream(stream),

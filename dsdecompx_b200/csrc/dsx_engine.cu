@@ -462,9 +462,23 @@ struct dsx_grid {
     dsx_step_callback graph_callback = nullptr;
     void* graph_user = nullptr;
     cudaStream_t graph_stream = nullptr;
+    // Asynchronous steps: each step graph copies its build status (before the
+    // callback) to pinned_build[4 * parity] and records build_done[parity]
+    // there, so the next step can check it while this one's callback and
+    // reverse sum still run.
+    unsigned* pinned_build = nullptr;             // [8]: per parity status, G, B, pad
+    cudaEvent_t build_done[2] = {nullptr, nullptr};
+    bool async_inflight = false;                  // a step whose status is unchecked
+    int async_parity = 0;
+    unsigned async_status = 0;                    // bits of the checked asynchronous steps
+    cudaStream_t async_stream = nullptr;
 
     ~dsx_grid() {
+        if (async_inflight) cudaStreamSynchronize(async_stream);
+        async_inflight = false;
         destroy_graphs();
+        for (auto& e : build_done) if (e) cudaEventDestroy(e);
+        if (pinned_build) cudaFreeHost(pinned_build);
         free_shard_buffers();
         for (auto& e : marks.ev) if (e) cudaEventDestroy(e);
         for (void* p : arrays_owned) cudaFree(p);
@@ -483,6 +497,7 @@ struct dsx_grid {
     int split_ctas_per_sm = 0;
 
     void destroy_graphs() {
+        settle_async();
         for (auto& g : graph) {
             if (g) cudaGraphExecDestroy(g);
             g = nullptr;
@@ -601,6 +616,10 @@ struct dsx_grid {
         allocate_ghost_scratch();
         cuda_check(cudaMallocHost(reinterpret_cast<void**>(&pinned_status), 4 * sizeof(unsigned)),
                    "cudaMallocHost");
+        cuda_check(cudaMallocHost(reinterpret_cast<void**>(&pinned_build), 8 * sizeof(unsigned)),
+                   "cudaMallocHost");
+        for (auto& e : build_done)
+            cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
         S.marks = &marks;
         last_ghosts.assign(static_cast<std::size_t>(P), 0);
     }
@@ -996,6 +1015,7 @@ struct dsx_grid {
     bool halo_pending = false, pending_rebuild = false, pending_reused = false, pending_build = false;
 
     void not_pending(const char* what) {
+        settle_async();
         if (halo_pending)
             fail(DSX_E_LOGIC, std::string(what) + " while a split halo exchange is in progress");
     }
@@ -1180,7 +1200,7 @@ struct dsx_grid {
         return v;
     }
 
-    void enqueue_step(dsx_step_callback cb, void* user, cudaStream_t stream) {
+    void enqueue_step(dsx_step_callback cb, void* user, cudaStream_t stream, bool build_event = false) {
         marks.count = 0;
         clear_status(stream);
         marks.mark(stream, "start");
@@ -1191,6 +1211,17 @@ struct dsx_grid {
             const dsx::Grid Gn = params();
             cur ^= 1;
             dsx::launch_fused_step(G, Gn, A, owned_off(), next_off(), ghost_off(), S, stream);
+        }
+        if (build_event) {
+            // the build's status and totals, then the event the next
+            // asynchronous step waits on (an event node of the graph)
+            unsigned* out = pinned_build + 4 * parity;
+            cuda_check(cudaMemcpyAsync(out, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
+                       "read build status");
+            cuda_check(cudaMemcpyAsync(out + 1, S.halo_info, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                                       stream), "read build status");
+            cuda_check(cudaEventRecordWithFlags(build_done[parity], stream, cudaEventRecordExternal),
+                       "record build event");
         }
         // the rest of the step reads the next layout
         parity ^= 1;
@@ -1521,7 +1552,7 @@ struct dsx_grid {
             if (!exec) {
                 cudaGraph_t g = nullptr;
                 cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-                enqueue_step(cb, user, stream);
+                enqueue_step(cb, user, stream, true);
                 cuda_check(cudaStreamEndCapture(stream, &g), "end capture");
                 cuda_check(cudaGraphInstantiate(&exec, g, 0), "instantiate graph");
                 cudaGraphDestroy(g);
@@ -1534,11 +1565,18 @@ struct dsx_grid {
         plan_valid = true;
         ghosts_valid = true;
         cuda_check(cudaStreamSynchronize(stream), "synchronize step");
-        unsigned st = pinned_status[0];
+        const unsigned st = finish_step(pinned_status[0], static_cast<int>(pinned_status[1]), cb, user,
+                                        stream);
+        if (status_out) *status_out = st;
+    }
+
+    // A step whose graph has run: after a ghost-region overflow the owned
+    // half is intact, so the capacity grows and the halo build, the callback
+    // and the reverse sum are redone; other failures raise.
+    unsigned finish_step(unsigned st, int ghosts_needed, dsx_step_callback cb, void* user,
+                         cudaStream_t stream) {
         if (st & dsx::kStatusGhostOverflow) {
-            // the owned half of this step is intact: grow, then redo the
-            // halo build, the callback and the reverse sum
-            grow_ghosts(static_cast<long long>(static_cast<int>(pinned_status[1])), stream);
+            grow_ghosts(static_cast<long long>(ghosts_needed), stream);
             build_checked(stream);
             const dsx_grid_view v = view();
             if (cb) cb(user, stream, &v);
@@ -1550,7 +1588,72 @@ struct dsx_grid {
         if (st & dsx::kStatusMigrationMismatch) fail(DSX_E_RUNTIME, "migration count mismatch");
         if (st & dsx::kStatusCutsInvalid)
             fail(DSX_E_INVALID, "dynamic cuts must be strictly increasing and span the domain");
-        if (status_out) *status_out = st;
+        return st;
+    }
+
+    // Asynchronous batched steps: the step's graph is queued and the call
+    // returns.  Before it is queued, the previous asynchronous step's build
+    // status is read at that step's build event (its callback and reverse
+    // sum may still be running), so the GPU always has the next step in line
+    // and a failed build is handled (grown and redone, as in step) before
+    // anything builds on it.
+    void step_async(dsx_step_callback cb, void* user, cudaStream_t stream) {
+        if (halo_pending)
+            fail(DSX_E_LOGIC, "the batched step while a split halo exchange is in progress");
+        if (async_inflight && async_stream != stream) settle_async();
+        if (graph_callback != cb || graph_user != user || graph_stream != stream) {
+            destroy_graphs();   // settles a pending step first
+            graph_callback = cb;
+            graph_user = user;
+            graph_stream = stream;
+        }
+        if (async_inflight) check_async();
+        cudaGraphExec_t& exec = graph[parity];
+        if (!exec) {
+            cudaGraph_t g = nullptr;
+            cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            enqueue_step(cb, user, stream, true);
+            cuda_check(cudaStreamEndCapture(stream, &g), "end capture");
+            cuda_check(cudaGraphInstantiate(&exec, g, 0), "instantiate graph");
+            cudaGraphDestroy(g);
+        }
+        const int p = parity;
+        cuda_check(cudaGraphLaunch(exec, stream), "launch graph");
+        commit_migrate();
+        plan_valid = true;
+        ghosts_valid = true;
+        async_inflight = true;
+        async_parity = p;
+        async_stream = stream;
+    }
+
+    // The pending asynchronous step's build, checked at its event.
+    void check_async() {
+        async_inflight = false;
+        cuda_check(cudaEventSynchronize(build_done[async_parity]), "wait for the step's build");
+        const unsigned* b = pinned_build + 4 * async_parity;
+        unsigned st = b[0];
+        const unsigned failed = dsx::kStatusGhostOverflow | dsx::kStatusCopyTimeout |
+                                dsx::kStatusMigrationMismatch | dsx::kStatusCutsInvalid;
+        if (st & failed) {
+            cuda_check(cudaStreamSynchronize(async_stream), "synchronize step");
+            st = finish_step(st, static_cast<int>(b[1]), graph_callback, graph_user, async_stream);
+        }
+        async_status |= st;
+    }
+
+    // Every other call first completes the pending asynchronous step.
+    void settle_async() {
+        if (!async_inflight) return;
+        check_async();
+        cuda_check(cudaStreamSynchronize(async_stream), "synchronize step");
+    }
+
+    unsigned step_wait() {
+        settle_async();
+        const unsigned st = async_status;
+        async_status = 0;
+        return st;
     }
 
     // ------------------------------------------------------ sharded step
@@ -2190,6 +2293,7 @@ int dsx_grid_neighbors(dsx_grid* grid, int rank, int* count, int* info, double* 
 
 int dsx_grid_cuts(dsx_grid* grid, double* out, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         int total = 0;
         for (int a = 0; a < 3; ++a) total += grid->dims[a] + 1;
         cuda_check(cudaMemcpyAsync(out, grid->cuts, sizeof(double) * total, cudaMemcpyDeviceToHost,
@@ -2200,6 +2304,7 @@ int dsx_grid_cuts(dsx_grid* grid, double* out, void* stream) {
 
 int dsx_grid_upload(dsx_grid* grid, const long long* counts, const void* const* arrays, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || !counts) fail(DSX_E_INVALID, "null argument");
         grid->upload(counts, arrays, static_cast<cudaStream_t>(stream));
     });
@@ -2207,6 +2312,7 @@ int dsx_grid_upload(dsx_grid* grid, const long long* counts, const void* const* 
 
 int dsx_grid_download(dsx_grid* grid, long long* counts, void* const* arrays, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         const auto s = static_cast<cudaStream_t>(stream);
         const std::vector<int> n = grid->read_ints(grid->layout[grid->cur][0], grid->P, s);
         for (int r = 0; r < grid->P; ++r) if (counts) counts[r] = n[static_cast<std::size_t>(r)];
@@ -2231,6 +2337,7 @@ int dsx_grid_download(dsx_grid* grid, long long* counts, void* const* arrays, vo
 
 int dsx_grid_totals(dsx_grid* grid, long long* out4, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         const auto s = static_cast<cudaStream_t>(stream);
         const std::vector<int> e = grid->read_ints(grid->S.emig_info, 1, s);
         const std::vector<int> h = grid->read_ints(grid->S.halo_info, 2, s);
@@ -2243,6 +2350,7 @@ int dsx_grid_totals(dsx_grid* grid, long long* out4, void* stream) {
 
 int dsx_grid_counts(dsx_grid* grid, long long* owned, long long* ghosts, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         const auto s = static_cast<cudaStream_t>(stream);
         const std::vector<int> n = grid->read_ints(grid->layout[grid->cur][0], grid->P, s);
         std::vector<int> g(static_cast<std::size_t>(grid->P), 0);
@@ -2256,12 +2364,16 @@ int dsx_grid_counts(dsx_grid* grid, long long* owned, long long* ghosts, void* s
 
 int dsx_grid_read(dsx_grid* grid, int rank, int array, long long start, long long count, void* host_out,
                   void* stream) {
-    return guarded([&] { grid->access(rank, array, start, count, host_out, false, static_cast<cudaStream_t>(stream)); });
+    return guarded([&] {
+        grid->settle_async();
+        grid->access(rank, array, start, count, host_out, false, static_cast<cudaStream_t>(stream));
+    });
 }
 
 int dsx_grid_write(dsx_grid* grid, int rank, int array, long long start, long long count, const void* host_in,
                    void* stream) {
     return guarded([&] {
+        grid->settle_async();
         grid->access(rank, array, start, count, const_cast<void*>(host_in), true, static_cast<cudaStream_t>(stream));
     });
 }
@@ -2272,6 +2384,7 @@ int dsx_grid_view_get(dsx_grid* grid, dsx_grid_view* out) {
 
 int dsx_grid_migrate(dsx_grid* grid, void* stream, long long* results) {
     return guarded([&] {
+        grid->settle_async();
         grid->migrate(static_cast<cudaStream_t>(stream), results);
         cuda_check(cudaGetLastError(), "launch migrate");
     });
@@ -2279,6 +2392,7 @@ int dsx_grid_migrate(dsx_grid* grid, void* stream, long long* results) {
 
 int dsx_grid_exchange_halo(dsx_grid* grid, int rebuild, int positions_only, void* stream, long long* results) {
     return guarded([&] {
+        grid->settle_async();
         grid->exchange_halo(rebuild != 0, positions_only != 0, static_cast<cudaStream_t>(stream), results);
         cuda_check(cudaGetLastError(), "launch halo");
     });
@@ -2286,6 +2400,7 @@ int dsx_grid_exchange_halo(dsx_grid* grid, int rebuild, int positions_only, void
 
 int dsx_grid_reverse_halo(dsx_grid* grid, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         grid->reverse_halo(static_cast<cudaStream_t>(stream));
         cuda_check(cudaGetLastError(), "launch reverse halo");
     });
@@ -2293,6 +2408,7 @@ int dsx_grid_reverse_halo(dsx_grid* grid, void* stream) {
 
 int dsx_grid_reverse_exchange(dsx_grid* grid, int nfields, const int* field_ids, const int* ops, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         grid->reverse_exchange(nfields, field_ids, ops, static_cast<cudaStream_t>(stream));
         cuda_check(cudaGetLastError(), "launch reverse exchange");
     });
@@ -2300,6 +2416,7 @@ int dsx_grid_reverse_exchange(dsx_grid* grid, int nfields, const int* field_ids,
 
 int dsx_grid_forward_exchange(dsx_grid* grid, int nfields, const int* field_ids, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         grid->forward_exchange(nfields, field_ids, static_cast<cudaStream_t>(stream));
         cuda_check(cudaGetLastError(), "launch forward exchange");
     });
@@ -2308,12 +2425,14 @@ int dsx_grid_forward_exchange(dsx_grid* grid, int nfields, const int* field_ids,
 int dsx_grid_rebalance(dsx_grid* grid, const double* work, int force, void* stream, long long* results,
                        double* imbalance) {
     return guarded([&] {
+        grid->settle_async();
         grid->rebalance(work, force != 0, static_cast<cudaStream_t>(stream), results, imbalance);
     });
 }
 
 int dsx_grid_set_halo_width(dsx_grid* grid, double width) {
     return guarded([&] {
+        grid->settle_async();
         if (width < 0.0) fail(DSX_E_INVALID, "halo width cannot be negative");
         grid->not_pending("set_halo_width");
         if (grid->halo_width != width) {
@@ -2326,6 +2445,7 @@ int dsx_grid_set_halo_width(dsx_grid* grid, double width) {
 
 int dsx_grid_set_refresh_kind(dsx_grid* grid, int owner_by_owner) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->not_pending("set_refresh_kind");
         const int kind = owner_by_owner ? 1 : 0;
@@ -2338,6 +2458,7 @@ int dsx_grid_set_refresh_kind(dsx_grid* grid, int owner_by_owner) {
 
 int dsx_grid_set_split_share(dsx_grid* grid, int ctas_per_sm) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         if (ctas_per_sm < 0) fail(DSX_E_INVALID, "CTAs per SM cannot be negative");
         grid->not_pending("set_split_share");
@@ -2349,12 +2470,16 @@ int dsx_grid_set_split_share(dsx_grid* grid, int ctas_per_sm) {
 }
 
 int dsx_grid_invalidate_halo(dsx_grid* grid) {
-    return guarded([&] { grid->plan_valid = false; });
+    return guarded([&] {
+        grid->settle_async();
+        grid->plan_valid = false;
+    });
 }
 
 int dsx_grid_halo_backward(dsx_grid* grid, const double* cx, const double* cy, const double* cz,
                            double* gx, double* gy, double* gz, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (grid->P == 1 || !grid->ghosts_valid) return;
         dsx::launch_reverse_sum3(grid->params(), gx, gy, gz, cx, cy, cz, grid->S,
                                  static_cast<cudaStream_t>(stream));
@@ -2365,6 +2490,7 @@ int dsx_grid_halo_backward(dsx_grid* grid, const double* cx, const double* cy, c
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture, void* stream,
                   unsigned* status) {
     return guarded([&] {
+        grid->settle_async();
         if (grid->P == 1) fail(DSX_E_INVALID, "the batched step needs at least two subdomains");
         if (capture && (stream == nullptr || static_cast<cudaStream_t>(stream) == cudaStreamLegacy ||
                         static_cast<cudaStream_t>(stream) == cudaStreamPerThread))
@@ -2374,10 +2500,29 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
     });
 }
 
+int dsx_grid_step_async(dsx_grid* grid, dsx_step_callback callback, void* user, void* stream) {
+    return guarded([&] {
+        if (grid->P == 1) fail(DSX_E_INVALID, "the batched step needs at least two subdomains");
+        if (stream == nullptr || static_cast<cudaStream_t>(stream) == cudaStreamLegacy ||
+            static_cast<cudaStream_t>(stream) == cudaStreamPerThread)
+            fail(DSX_E_INVALID, "asynchronous steps need a created stream, not the default stream");
+        grid->step_async(callback, user, static_cast<cudaStream_t>(stream));
+        cuda_check(cudaGetLastError(), "launch step");
+    });
+}
+
+int dsx_grid_step_wait(dsx_grid* grid, unsigned* status) {
+    return guarded([&] {
+        const unsigned st = grid->step_wait();
+        if (status) *status = st;
+    });
+}
+
 int dsx_grid_sharded_step(dsx_grid* grid, const int* owners, int shard, int nshards,
                           const dsx_transport* transport, dsx_step_callback callback, void* user,
                           void* stream, unsigned* status) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || !owners || !transport) fail(DSX_E_INVALID, "null argument");
         if (grid->P == 1) fail(DSX_E_INVALID, "the sharded step needs at least two subdomains");
         grid->sharded_step(owners, shard, nshards, *transport, callback, user,
@@ -2432,6 +2577,7 @@ int dsx_shard_plan_step(const dsx_grid_desc* desc, const int* owners, int shard,
 
 int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->autotune(static_cast<cudaStream_t>(stream), report);
     });
@@ -2439,6 +2585,7 @@ int dsx_grid_autotune(dsx_grid* grid, void* stream, dsx_tune_report* report) {
 
 int dsx_grid_begin_halo_exchange(dsx_grid* grid, int rebuild, int positions_only, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->begin_halo(rebuild != 0, positions_only != 0, static_cast<cudaStream_t>(stream));
         cuda_check(cudaGetLastError(), "launch halo exchange");
@@ -2447,6 +2594,7 @@ int dsx_grid_begin_halo_exchange(dsx_grid* grid, int rebuild, int positions_only
 
 int dsx_grid_end_halo_exchange(dsx_grid* grid, void* stream, long long* results) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->end_halo(static_cast<cudaStream_t>(stream), results);
     });
@@ -2455,6 +2603,7 @@ int dsx_grid_end_halo_exchange(dsx_grid* grid, void* stream, long long* results)
 int dsx_grid_owner_rank(dsx_grid* grid, const double* x, const double* y, const double* z,
                         long long n, int* out, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || n < 0 || (n > 0 && (!x || !y || !z || !out))) fail(DSX_E_INVALID, "null argument");
         dsx::launch_owner_rank(grid->params(), x, y, z, n, out, static_cast<cudaStream_t>(stream));
         cuda_check(cudaGetLastError(), "launch owner_rank");
@@ -2463,6 +2612,7 @@ int dsx_grid_owner_rank(dsx_grid* grid, const double* x, const double* y, const 
 
 int dsx_grid_out_of_domain(dsx_grid* grid, int* flags, int* any, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
         const long long o = grid->owned_off();
@@ -2478,6 +2628,7 @@ int dsx_grid_out_of_domain(dsx_grid* grid, int* flags, int* any, void* stream) {
 
 int dsx_grid_set_cuts(dsx_grid* grid, const double* cuts, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || !cuts) fail(DSX_E_INVALID, "null argument");
         grid->set_cuts(cuts, static_cast<cudaStream_t>(stream));
     });
@@ -2486,6 +2637,7 @@ int dsx_grid_set_cuts(dsx_grid* grid, const double* cuts, void* stream) {
 int dsx_grid_rescale_domain(dsx_grid* grid, const double* lower, const double* upper,
                             int invalidate_plan, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || !lower || !upper) fail(DSX_E_INVALID, "null argument");
         grid->rescale_domain(lower, upper, invalidate_plan != 0, static_cast<cudaStream_t>(stream));
     });
@@ -2493,6 +2645,7 @@ int dsx_grid_rescale_domain(dsx_grid* grid, const double* lower, const double* u
 
 int dsx_grid_migration_pairs(dsx_grid* grid, long long* pairs, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || !pairs) fail(DSX_E_INVALID, "null argument");
         grid->migration_pairs(pairs, static_cast<cudaStream_t>(stream));
     });
@@ -2500,6 +2653,7 @@ int dsx_grid_migration_pairs(dsx_grid* grid, long long* pairs, void* stream) {
 
 int dsx_grid_send_lists(dsx_grid* grid, int* length, int* first_slot, void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || !length || !first_slot) fail(DSX_E_INVALID, "null argument");
         grid->send_lists(length, first_slot, static_cast<cudaStream_t>(stream));
     });
@@ -2509,6 +2663,7 @@ int dsx_grid_assemble(dsx_grid* grid, const long long* counts, int nsources,
                       const void* const* sources, long long nsegments, const dsx_segment* segments,
                       void* stream) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid || !counts || (nsegments > 0 && !segments) || (nsources > 0 && !sources) ||
             nsources < 0 || nsegments < 0)
             fail(DSX_E_INVALID, "null argument");
@@ -2518,6 +2673,7 @@ int dsx_grid_assemble(dsx_grid* grid, const long long* counts, int nsources,
 
 int dsx_grid_set_rebalance_work(dsx_grid* grid, const double* work) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->set_rebalance_work(work);
     });
@@ -2541,6 +2697,7 @@ int dsx_copy_segments(const dsx_copy* copies, long long n, void* stream) {
 int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
                         int reverse_ctas_per_sm, int classify_combine) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         if (classify_threads != 64 && classify_threads != 128 && classify_threads != 256)
             fail(DSX_E_INVALID, "classify threads must be 64, 128 or 256");
@@ -2558,6 +2715,7 @@ int dsx_grid_set_tuning(dsx_grid* grid, int classify_threads, int move_kind,
 
 int dsx_grid_set_plain(dsx_grid* grid, int plain) {
     return guarded([&] {
+        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->plain = plain != 0;
         grid->plain_bounds.clear();
@@ -2566,6 +2724,7 @@ int dsx_grid_set_plain(dsx_grid* grid, int plain) {
 
 int dsx_grid_profile(dsx_grid* grid, int enable) {
     return guarded([&] {
+        grid->settle_async();
         if (enable && !grid->marks.ev[0])
             for (auto& e : grid->marks.ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         if ((enable != 0) != grid->marks.on) grid->destroy_graphs();
@@ -2577,6 +2736,7 @@ int dsx_grid_profile(dsx_grid* grid, int enable) {
 int dsx_grid_kernel_times(dsx_grid* grid, int max, const char** names, float* ms) {
     int n = 0;
     const int status = guarded([&] {
+        grid->settle_async();
         const dsx::Marks& m = grid->marks;
         if (!m.on || m.count < 2) return;
         cuda_check(cudaEventSynchronize(m.ev[m.count - 1]), "event synchronize");

@@ -70,6 +70,7 @@ __global__ void k_ghost_forces(double* fx, double* fy, double* fz, const int* to
 }
 
 __global__ void k_advance() { ++g_step; }
+__global__ void k_set_step(unsigned long long v) { g_step = v; }
 
 // Drift of the owned particles and ghost forces in one launch (the step
 // callback's work): a grid-stride pass over the owned particles (two per
@@ -209,6 +210,12 @@ int dsxw_interior(const dsx_grid_view* v, int rounds, double* out, void* stream)
 // moves the device step counter on (call once per step, after the draws)
 int dsxw_advance(void* stream) {
     k_advance<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>();
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+// sets the device step counter (to replay the same draws on a second grid)
+int dsxw_set_step(unsigned long long value, void* stream) {
+    k_set_step<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(value);
     return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

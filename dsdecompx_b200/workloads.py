@@ -133,6 +133,7 @@ def harness() -> C.CDLL:
         _WL.dsxw_drift.argtypes = [C.c_void_p, C.c_ulonglong, C.c_longlong, C.c_double, C.c_void_p]
         _WL.dsxw_ghost_forces.argtypes = [C.c_void_p, C.c_ulonglong, C.c_longlong, C.c_void_p]
         _WL.dsxw_advance.argtypes = [C.c_void_p]
+        _WL.dsxw_set_step.argtypes = [C.c_ulonglong, C.c_void_p]
         _WL.dsxw_interior.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         _WL.dsxw_step_work.argtypes = [C.c_void_p, C.c_ulonglong, C.c_double, C.c_void_p]
         _WL.dsxw_drift_arrays.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -235,6 +235,23 @@ typedef void (*dsx_step_callback)(void* user, void* stream, const dsx_grid_view*
 int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int capture,
                   void* stream, unsigned* status);
 
+/* Batched steps queued back to back (no counterpart call in the reference,
+ * whose ranks finish each call before the next): the step's graph (captured
+ * as dsx_grid_step with capture != 0 does, same callback contract) is queued
+ * on `stream` and the call returns.  The previous asynchronous step is checked
+ * first, at the end of its halo build (its callback and reverse sum may still
+ * be running), so the GPU is never left without the next step; an overflowed
+ * ghost region is grown and that step's build, callback and reverse sum are
+ * redone there, before anything builds on it (so the callback must be
+ * idempotent, as for dsx_grid_step).  dsx_grid_step_wait completes the
+ * pending step and returns the OR of the status bits of the asynchronous
+ * steps since the last wait; every other dsx_grid_* call on the grid (but
+ * dsx_grid_view_get and the topology queries) completes the pending step
+ * first, and so reports its failure.  Needs a created stream (DSX_E_INVALID
+ * for a default stream). */
+int dsx_grid_step_async(dsx_grid* grid, dsx_step_callback callback, void* user, void* stream);
+int dsx_grid_step_wait(dsx_grid* grid, unsigned* status);
+
 /* Split-phase halo exchange (Decomp::begin_halo_exchange /
  * end_halo_exchange, dsDecompX src/halo.cpp:296-872): begin enqueues the
  * refresh along the plan or the plan build on stream and returns at once, so

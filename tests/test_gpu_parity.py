@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from helpers import ALL_FIELDS, Pair, same, split_by_owner, uniform_particles
+from oracle import Grid
 
 pytestmark = pytest.mark.gpu
 
@@ -928,3 +929,59 @@ def test_step_callback_exception_reaches_the_caller(cuda):
         assert pair.gpu.step(None, capture=False) == 0   # the grid goes on
     finally:
         pair.close()
+
+
+@pytest.mark.parametrize("ghost_capacity", [30000, 500], ids=["ample", "overflow"])
+def test_async_steps_match_synchronous_steps(cuda, ghost_capacity):
+    """dsx_grid_step_async queues each step before the previous one has
+    finished (it checks that one's build at its event) and dsx_grid_step_wait
+    completes them; the arrays, counts and cut planes must equal those of the
+    same steps run one at a time by dsx_grid_step, bit for bit.  The tiny
+    ghost capacity makes the first steps overflow, so the redo (grow, build,
+    callback, reverse sum) runs on the queued path too.  The callback draws
+    the drift and the ghost forces from the harness's device step counter,
+    reset before each grid, so both grids see the same draws."""
+    import ctypes as C
+
+    import torch
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import workloads as W
+    wl = W.harness()
+    rng = np.random.default_rng(31)
+    n = 20000
+    kw = dict(nranks=8, dims=(0, 0, 0), policy="dynamic", lower=(0, 0, 0), upper=(16, 16, 16),
+              halo_width=0.8, fields=ALL_FIELDS[:2], particles=n,
+              ghost_capacity=ghost_capacity, dynamic=(1.0, 1.05, 0.5, 0.10))
+    data = uniform_particles(rng, n, (0, 0, 0), (16, 16, 16), ALL_FIELDS[:2])
+    grids = [dsx.VirtualGrid(**kw) for _ in range(2)]
+    with Grid("port", 8, (0, 0, 0), "dynamic", (0, 0, 0), (16, 16, 16), (True,) * 3, 0.8,
+              dynamic=kw["dynamic"]) as probe:
+        owner = probe.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    per = split_by_owner(owner, data, 8)
+    for g in grids:
+        g.upload(per)
+    stream = torch.cuda.Stream()
+
+    def work(view, s):
+        assert wl.dsxw_step_work(C.byref(view), 7, 0.25, s) == 0
+
+    steps = 6
+    torch.cuda.synchronize()
+    wl.dsxw_set_step(0, stream.cuda_stream)
+    for _ in range(steps):
+        assert grids[0].step(work, capture=True, stream=stream) == 0
+    stream.synchronize()
+    wl.dsxw_set_step(0, stream.cuda_stream)
+    for _ in range(steps):
+        grids[1].step_async(work, stream=stream)
+    assert grids[1].step_wait() == 0
+    stream.synchronize()
+    for r in range(8):
+        a, b = grids[0].snapshot(r), grids[1].snapshot(r)
+        for k in a:
+            assert same(a[k], b[k]), (ghost_capacity, r, k)
+    for ca, cb in zip(grids[0].cuts(), grids[1].cuts()):
+        assert same(ca, cb)
+    for g in grids:
+        g.close()
