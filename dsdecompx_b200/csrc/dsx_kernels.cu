@@ -1957,7 +1957,7 @@ __global__ void __launch_bounds__(1024) k_step_export(Grid G, const int* pre, in
 // several passes); every pass redoes the index work from the destinations
 // and masks, and only the pass with index_outputs writes its results.
 template <bool FULL, bool DIRECT_FORCES>
-__global__ void __launch_bounds__(NT, DIRECT_FORCES ? 4 : 3) k_step_move_staged(
+__global__ void __launch_bounds__(NT, 3) k_step_move_staged(
     Grid G, Arrays A, long long src_off, long long dst_off, long long ghost_off, const int* pre,
     int stride, const int* cbase_ret, const unsigned short* __restrict__ dest_in,
     const unsigned* __restrict__ mask_in, const int* __restrict__ tile_bases, int* emig_src,
