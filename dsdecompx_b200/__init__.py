@@ -558,9 +558,15 @@ class VirtualGrid:
                                                  res.ctypes.data_as(C.POINTER(C.c_longlong))))
         return res
 
-    def set_refresh_kind(self, owner_by_owner: bool = False):
-        """Refresh walk: ghost by ghost (default) or owner by owner."""
-        _check(self.L.dsx_grid_set_refresh_kind(self.h, 1 if owner_by_owner else 0))
+    REFRESH_KINDS = {"ghosts": 0, "owners": 1, "tiles": 2}
+
+    def set_refresh_kind(self, kind="tiles"):
+        """Refresh walk: "tiles" (default; the tile's owners staged whole),
+        "owners" (each boundary owner once) or "ghosts" (each ghost's owner
+        gathered); True / False stand for "owners" / "ghosts"."""
+        if isinstance(kind, bool):
+            kind = "owners" if kind else "ghosts"
+        _check(self.L.dsx_grid_set_refresh_kind(self.h, self.REFRESH_KINDS[kind]))
 
     def set_split_share(self, ctas_per_sm: int = 0):
         """CTAs per SM the split-phase refresh may occupy (0: all resident)."""

@@ -764,6 +764,7 @@ struct dsx_grid {
         S.bowner = device_alloc<int>(fixed_owned, ncap);
         S.boff = device_alloc<int>(fixed_owned, ncap + 1);
         S.bfirst = device_alloc<int>(fixed_owned, ncap);
+        S.tile_b0 = device_alloc<int>(fixed_owned, static_cast<std::size_t>(max_tiles) + 1);
         S.cbase = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * dsx::kHaloCounters);
         S.halo_info = device_alloc<int>(fixed_owned, 4);
         cuda_check(cudaMemset(S.halo_info, 0, 4 * sizeof(int)), "memset");
@@ -2443,14 +2444,14 @@ int dsx_grid_set_halo_width(dsx_grid* grid, double width) {
     });
 }
 
-int dsx_grid_set_refresh_kind(dsx_grid* grid, int owner_by_owner) {
+int dsx_grid_set_refresh_kind(dsx_grid* grid, int kind) {
     return guarded([&] {
-        grid->settle_async();
         if (!grid) fail(DSX_E_INVALID, "null grid");
+        grid->settle_async();
         grid->not_pending("set_refresh_kind");
-        const int kind = owner_by_owner ? 1 : 0;
-        if (grid->S.refresh_owners != kind) {
-            grid->S.refresh_owners = kind;
+        if (kind < 0 || kind > 2) fail(DSX_E_INVALID, "refresh kind must be 0, 1 or 2");
+        if (grid->S.refresh_kind != kind) {
+            grid->S.refresh_kind = kind;
             grid->destroy_graphs();
         }
     });

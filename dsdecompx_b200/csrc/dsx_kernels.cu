@@ -1885,6 +1885,207 @@ __global__ void __launch_bounds__(NT, 4) k_halo_scatter_staged(
     }
 }
 
+// Polls the mbarrier's phase `parity` for at most kBulkWaitNs; false if it
+// never completed.
+__device__ __forceinline__ bool bulk_wait_parity(unsigned bar, unsigned parity) {
+    const unsigned long long start = global_ns();
+    for (;;) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+        if (global_ns() - start > kBulkWaitNs) return false;
+    }
+}
+
+// First boundary owner of every tile of the current layout (tile_b0[g]; the
+// boundary owners are in owned order in every plan) and tile_b0[ntiles] = B.
+__global__ void __launch_bounds__(NT) k_tile_boundary_starts(Grid G, const int* info,
+                                                             const int* __restrict__ bowner,
+                                                             int* tile_b0) {
+    pdl_begin();
+    const int ntiles = G.tile_start[G.P];
+    const int B = info[1];
+    for (int g = blockIdx.x * NT + threadIdx.x; g <= ntiles; g += gridDim.x * NT) {
+        if (g == ntiles) {
+            tile_b0[g] = B;
+            continue;
+        }
+        const int begin = G.tiles[g].y;
+        int lo = 0, hi = B;   // first b with bowner[b] >= begin
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (ro(bowner + mid) < begin) lo = mid + 1;
+            else hi = mid;
+        }
+        tile_b0[g] = lo;
+    }
+}
+
+// Refresh along the plan, one tile of owners at a time: the arrays the
+// refresh copies (x, y, z; with velocities and the registered fields for a
+// full refresh) come into shared memory by bulk copies of the whole tile,
+// while the block sorts the tile's images by ghost slot from the CSR (the
+// images of one send list from one tile are a run of consecutive slots,
+// every list being in owned order); then consecutive threads write
+// consecutive ghost slots from shared memory.  Owned data crosses HBM once,
+// as whole tiles, instead of one sector per array and ghost.  A tile whose
+// images do not fit the staging list, or break the run order, writes each
+// image straight to its slot from shared memory.
+__global__ void __launch_bounds__(NT) k_halo_refresh_staged(Grid G, Arrays A, long long owned_off,
+                                                           long long ghost_off, int positions_only,
+                                                           const int* __restrict__ bowner,
+                                                           const int* __restrict__ boff,
+                                                           const int* __restrict__ bslot,
+                                                           const int* __restrict__ bfirst,
+                                                           const int* __restrict__ ghost_entry,
+                                                           const int* __restrict__ tile_b0) {
+    pdl_begin();
+    extern __shared__ __align__(16) unsigned char s_rec[];
+    __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ int s_seg[6 + kMaxFields];
+    __shared__ int s_min[kMaxNeighbors];
+    __shared__ int s_cnt[kMaxNeighbors];
+    __shared__ int s_off[kMaxNeighbors + 1];
+    __shared__ int s_bad;
+    __shared__ unsigned short s_own[kStageCap];
+    if (*G.status & kStatusGhostOverflow) return;
+    const int ntiles = G.tile_start[G.P];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int narr = positions_only ? 3 : 6 + A.f.count;
+    const unsigned bar = smem_u32(&s_bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    unsigned phase = 0;
+    for (int g = blockIdx.x; g < ntiles; g += gridDim.x) {
+        const int b0 = tile_b0[g], b1 = tile_b0[g + 1];
+        if (b0 == b1) continue;   // uniform: no owner of this tile has an image
+        const int4 td = G.tiles[g];
+        const int s = td.x, begin = td.y, end = td.z;
+        if (warp == 0) {
+            // lane -> array: x, y, z, then vx, vy, vz and the fields
+            const int k = lane < 6 ? lane : 13 + (lane - 6);
+            int b = 0;
+            const unsigned char* base = nullptr;
+            if (lane < narr) {
+                b = array_bytes(A, k);
+                base = array_base(A, k);
+            }
+            const int size = b ? TILE * b + 32 : 0;
+            const int soff = warp_inclusive_sum(size) - size;
+            long long gl = 0, lo = 0, hi = 0;
+            if (b) {
+                gl = (owned_off + begin) * b;
+                lo = gl & ~15LL;
+                hi = ((owned_off + end) * b + 15) & ~15LL;
+            }
+            const unsigned bytes = static_cast<unsigned>(hi - lo);
+            const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                             "r"(total) : "memory");
+            __syncwarp();
+            if (b) {
+                bulk_load(smem_u32(s_rec + soff), base + lo, bytes, bar);
+                s_seg[lane] = soff + static_cast<int>(gl - lo);
+            }
+        }
+        if (threadIdx.x < kMaxNeighbors) {
+            s_min[threadIdx.x] = INT_MAX;
+            s_cnt[threadIdx.x] = 0;
+        }
+        if (threadIdx.x == 0) s_bad = 0;
+        __syncthreads();
+        // pass 1: each list's first slot and image count in this tile
+        for (int b = b0 + threadIdx.x; b < b1; b += NT) {
+            const int k0 = boff[b], k1 = boff[b + 1];
+            for (int k = k0; k < k1; ++k) {
+                const int slot = k == k0 ? bfirst[b] : bslot[k];
+                const int n = ghost_entry[slot] - s * kMaxNeighbors;
+                if (n < 0 || n >= kMaxNeighbors) {   // not this tile's sender: direct writes
+                    s_bad = 1;
+                    continue;
+                }
+                atomicMin(&s_min[n], slot);
+                atomicAdd(&s_cnt[n], 1);
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const int c = lane < kMaxNeighbors ? s_cnt[lane] : 0;
+            const int incl = warp_inclusive_sum(c);
+            if (lane < kMaxNeighbors) s_off[lane] = incl - c;
+            if (lane == 31) s_off[kMaxNeighbors] = incl;
+        }
+        __syncthreads();
+        const int Q = s_off[kMaxNeighbors];
+        const bool listed = Q <= kStageCap && !s_bad;
+        // pass 2: every image's place in its list's run (a run that is not
+        // one block of slots sends the tile to the direct writes)
+        if (listed) {
+            for (int b = b0 + threadIdx.x; b < b1; b += NT) {
+                const int l = bowner[b] - begin;
+                const int k0 = boff[b], k1 = boff[b + 1];
+                for (int k = k0; k < k1; ++k) {
+                    const int slot = k == k0 ? bfirst[b] : bslot[k];
+                    const int n = ghost_entry[slot] - s * kMaxNeighbors;
+                    const int rel = slot - s_min[n];
+                    if (rel >= 0 && rel < s_cnt[n]) s_own[s_off[n] + rel] = static_cast<unsigned short>(l);
+                    else s_bad = 1;
+                }
+            }
+        }
+        const bool lost = !bulk_wait_parity(bar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(lost)) {
+            if (lost) bulk_wait_parity(bar, phase ^ 1u);
+            if (threadIdx.x == 0) atomicOr(G.status, kStatusCopyTimeout);
+            return;
+        }
+        const double* shift = G.shift;
+        auto write_image = [&](int l, long long gi, int entry) {
+            const double* sh = shift + 3ll * entry;
+            A.d[0][gi] = __dadd_rn(srd(s_rec, s_seg[0], l), sh[0]);
+            A.d[1][gi] = __dadd_rn(srd(s_rec, s_seg[1], l), sh[1]);
+            A.d[2][gi] = __dadd_rn(srd(s_rec, s_seg[2], l), sh[2]);
+            A.d[6][gi] = 0.0; A.d[7][gi] = 0.0; A.d[8][gi] = 0.0;
+            if (!positions_only) {
+                A.d[3][gi] = srd(s_rec, s_seg[3], l);
+                A.d[4][gi] = srd(s_rec, s_seg[4], l);
+                A.d[5][gi] = srd(s_rec, s_seg[5], l);
+                fields_from_stage(A.f, s_rec, s_seg + 6, l, gi);
+            }
+        };
+        if (listed && !s_bad) {
+            for (int q = threadIdx.x; q < Q; q += NT) {
+                int lo = 0, hi = kMaxNeighbors;   // largest n with s_off[n] <= q
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_off[mid] <= q) lo = mid;
+                    else hi = mid;
+                }
+                const int n = lo;
+                write_image(s_own[q], ghost_off + s_min[n] + (q - s_off[n]), s * kMaxNeighbors + n);
+            }
+        } else {
+            for (int b = b0 + threadIdx.x; b < b1; b += NT) {
+                const int l = bowner[b] - begin;
+                const int k0 = boff[b], k1 = boff[b + 1];
+                for (int k = k0; k < k1; ++k) {
+                    const int slot = k == k0 ? bfirst[b] : bslot[k];
+                    write_image(l, ghost_off + slot, ghost_entry[slot]);
+                }
+            }
+        }
+        __syncthreads();   // the stage and the lists are reused by the next tile
+    }
+}
+
 // Tile descriptors {s, begin, end, first tile of s} of a layout given by its
 // global counts, bases and tile starts (P + 1 entries each), the tiles
 // strided over the threads of the grid.
@@ -3301,9 +3502,51 @@ void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long
     if (S.marks) S.marks->mark(s, "immigrant_halo");
 }
 
+// Shared memory of one tile of the arrays a refresh copies (x, y, z; with
+// velocities and the fields for a full refresh).
+int refresh_stage_bytes(const Arrays& A, bool positions_only) {
+    int bytes = (positions_only ? 3 : 6) * (TILE * 8 + 32);
+    if (!positions_only)
+        for (int f = 0; f < A.f.count; ++f) bytes += TILE * A.f.bytes[f] + 32;
+    return bytes;
+}
+
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                          bool positions_only, const Scratch& S, cudaStream_t s, int ctas_per_sm) {
-    if (S.refresh_owners) {
+    const int stage = refresh_stage_bytes(A, positions_only);
+    if (S.refresh_kind == 2 && stage <= kStagedMaxBytes) {
+        static bool attribute_set = false;   // once per process (one device per process)
+        static std::mutex lock;
+        static std::vector<std::pair<int, int>> per_sm_of;   // stage bytes -> CTAs per SM
+        int per_sm = 0;
+        {
+            std::lock_guard<std::mutex> hold(lock);
+            if (!attribute_set) {
+                cudaFuncSetAttribute(k_halo_refresh_staged,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedMaxBytes);
+                attribute_set = true;
+            }
+            for (const auto& e : per_sm_of)
+                if (e.first == stage) per_sm = e.second;
+            if (!per_sm) {
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_halo_refresh_staged, NT,
+                                                                  stage) != cudaSuccess ||
+                    per_sm < 1)
+                    per_sm = 1;
+                per_sm_of.emplace_back(stage, per_sm);
+            }
+        }
+        if (ctas_per_sm > 0 && per_sm > ctas_per_sm) per_sm = ctas_per_sm;
+        int grid = sm_count() * per_sm;
+        if (grid > G.max_tiles) grid = G.max_tiles > 0 ? G.max_tiles : 1;
+        pdl_launch(k_tile_boundary_starts, stream_grid(static_cast<long long>(G.max_tiles) + 1), NT, 0, s,
+                   G, S.halo_info, S.bowner, S.tile_b0);
+        pdl_launch(k_halo_refresh_staged, grid, NT, static_cast<std::size_t>(stage), s, G, A, owned_off,
+                   ghost_off, positions_only ? 1 : 0, S.bowner, S.boff, S.bslot, S.bfirst,
+                   S.ghost_entry, S.tile_b0);
+        return;
+    }
+    if (S.refresh_kind == 1) {
         int grid = resident_grid(reinterpret_cast<const void*>(k_halo_refresh_owners), G.ncap);
         if (ctas_per_sm > 0 && grid > sm_count() * ctas_per_sm) grid = sm_count() * ctas_per_sm;
         pdl_launch(k_halo_refresh_owners, grid, NT, 0, s, G, A, owned_off, ghost_off, positions_only ? 1 : 0,

@@ -53,6 +53,7 @@ struct Scratch {
     int* boff = nullptr;       // [ncap+1] CSR offsets into bslot
     int* bslot = nullptr;      // [gcap] ghost slots of each boundary owner, n ascending
     int* bfirst = nullptr;     // [ncap] ghost slot of each boundary owner's first image
+    int* tile_b0 = nullptr;    // [max_tiles + 1] first boundary owner of each tile (refresh)
     // sharded step only (null otherwise): emigrants per (destination, source)
     // from the classify, and the gap before each source's group of
     // immigrants that other shards fill
@@ -78,7 +79,8 @@ struct Scratch {
     int classify_combine = 0;     // immigrant counters combined per warp before the atomics
     int move_staged = 1;          // 1: staged (one pass if it fits), 2: staged in passes,
                                   // 3: staged without forces, 0: direct reads
-    int refresh_owners = 0;       // refresh owner by owner (the CSR) instead of ghost by ghost
+    int refresh_kind = 2;         // refresh walk: 0 ghost by ghost, 1 owner by owner (the CSR),
+                                  // 2 tile by tile with the owners staged (when the stage fits)
     int reverse_per_sm = 0;       // CTAs per SM of the reverse sum; 0: one wave of the default shape
 };
 

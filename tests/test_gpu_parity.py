@@ -155,16 +155,16 @@ def test_rebalance_api(cuda):
     pair.close()
 
 
-@pytest.mark.parametrize("owner_by_owner", [True, False], ids=["owners", "ghosts"])
-def test_refresh_kinds_follow_the_reference(cuda, owner_by_owner):
+@pytest.mark.parametrize("kind", ["owners", "ghosts", "tiles"])
+def test_refresh_kinds_follow_the_reference(cuda, kind):
     """Full refreshes along the plan (every field type, a halo wider than
-    half a cell so that owners have many images) walked owner by owner and
-    ghost by ghost give the oracle's ghosts."""
+    half a cell so that owners have many images) walked owner by owner,
+    ghost by ghost and tile by tile give the oracle's ghosts."""
     rng = np.random.default_rng(41)
     pair = run_scenario(cuda, P=12, dims=(3, 2, 2), L=(9.0, 7.0, 6.0), halo=1.9, N=6000,
                         steps=1, seed=40)
     try:
-        pair.gpu.set_refresh_kind(owner_by_owner)
+        pair.gpu.set_refresh_kind(kind)
         for k in range(3):
             pair.displace(rng, 0.05)
             hg, hr = pair.gpu.exchange_halo(), pair.ref.exchange_halo()
@@ -174,11 +174,11 @@ def test_refresh_kinds_follow_the_reference(cuda, owner_by_owner):
         pair.close()
 
 
-@pytest.mark.parametrize("owner_by_owner", [True, False], ids=["owners", "ghosts"])
-def test_positions_only_refresh(cuda, owner_by_owner):
+@pytest.mark.parametrize("kind", ["owners", "ghosts", "tiles"])
+def test_positions_only_refresh(cuda, kind):
     pair = run_scenario(cuda, P=8, dims=(2, 2, 2), L=(10.0, 10.0, 10.0), halo=1.0, N=5000,
                         steps=1, seed=10, fields=ALL_FIELDS[:2])
-    pair.gpu.set_refresh_kind(owner_by_owner)
+    pair.gpu.set_refresh_kind(kind)
     rng = np.random.default_rng(11)
     before = [pair.gpu.snapshot(r) for r in range(8)]
     pair.displace(rng, 0.05)
