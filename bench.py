@@ -591,15 +591,15 @@ def measure_calls(grid, w, N, S, stream, device, reps=10):
             positions_only=True, stream=stream, results=False)), 80 * G)
         out["refresh_full"] = row(timed(lambda: grid.exchange_halo(
             stream=stream, results=False)), (128 + 2 * fb) * G)
-        # the same refreshes walked owner by owner and ghost by ghost (the
-        # other refresh kinds; the default walks the plan tile by tile)
-        for kind in ("owners", "ghosts"):
+        # the same refreshes walked by each kind (the default picks ghosts or
+        # tiles by what the refresh copies)
+        for kind in ("owners", "ghosts", "tiles"):
             grid.set_refresh_kind(kind)
             out[f"refresh_positions_by_{kind[:-1]}"] = row(timed(lambda: grid.exchange_halo(
                 positions_only=True, stream=stream, results=False)), 80 * G)
             out[f"refresh_full_by_{kind[:-1]}"] = row(timed(lambda: grid.exchange_halo(
                 stream=stream, results=False)), (128 + 2 * fb) * G)
-        grid.set_refresh_kind("tiles")
+        grid.set_refresh_kind("auto")
         # split phase: begin launches the refresh (one captured graph) and
         # returns; interior work that needs the SMs, not HBM (the harness's
         # FP64 multiply-add stand-in over the owned positions), runs on

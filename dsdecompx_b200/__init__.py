@@ -558,12 +558,13 @@ class VirtualGrid:
                                                  res.ctypes.data_as(C.POINTER(C.c_longlong))))
         return res
 
-    REFRESH_KINDS = {"ghosts": 0, "owners": 1, "tiles": 2}
+    REFRESH_KINDS = {"ghosts": 0, "owners": 1, "tiles": 2, "auto": 3}
 
-    def set_refresh_kind(self, kind="tiles"):
-        """Refresh walk: "tiles" (default; the tile's owners staged whole),
-        "owners" (each boundary owner once) or "ghosts" (each ghost's owner
-        gathered); True / False stand for "owners" / "ghosts"."""
+    def set_refresh_kind(self, kind="auto"):
+        """Refresh walk: "ghosts" (each ghost's owner gathered), "owners"
+        (each boundary owner once), "tiles" (each tile's owners staged whole)
+        or "auto" (the default: tiles for a full refresh of nine arrays or
+        more, else ghosts); True / False stand for "owners" / "ghosts"."""
         if isinstance(kind, bool):
             kind = "owners" if kind else "ghosts"
         _check(self.L.dsx_grid_set_refresh_kind(self.h, self.REFRESH_KINDS[kind]))

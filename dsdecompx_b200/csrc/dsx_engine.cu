@@ -2449,7 +2449,7 @@ int dsx_grid_set_refresh_kind(dsx_grid* grid, int kind) {
         if (!grid) fail(DSX_E_INVALID, "null grid");
         grid->settle_async();
         grid->not_pending("set_refresh_kind");
-        if (kind < 0 || kind > 2) fail(DSX_E_INVALID, "refresh kind must be 0, 1 or 2");
+        if (kind < 0 || kind > 3) fail(DSX_E_INVALID, "refresh kind must be 0, 1, 2 or 3");
         if (grid->S.refresh_kind != kind) {
             grid->S.refresh_kind = kind;
             grid->destroy_graphs();

@@ -3514,7 +3514,13 @@ int refresh_stage_bytes(const Arrays& A, bool positions_only) {
 void launch_halo_refresh(const Grid& G, const Arrays& A, long long owned_off, long long ghost_off,
                          bool positions_only, const Scratch& S, cudaStream_t s, int ctas_per_sm) {
     const int stage = refresh_stage_bytes(A, positions_only);
-    if (S.refresh_kind == 2 && stage <= kStagedMaxBytes) {
+    // the tile walk pays a fixed latency per tile, the ghost walk one sector
+    // per copied array and ghost: the tiles win once a full refresh copies
+    // nine arrays or more (measured: 11 arrays 1.19 against 1.50 ms, 7 arrays
+    // 0.39 against 0.31 ms, positions 0.30 against 0.15 ms)
+    const bool tiles = S.refresh_kind == 2 || (S.refresh_kind == 3 && !positions_only &&
+                                                6 + A.f.count >= 9);
+    if (tiles && stage <= kStagedMaxBytes) {
         static bool attribute_set = false;   // once per process (one device per process)
         static std::mutex lock;
         static std::vector<std::pair<int, int>> per_sm_of;   // stage bytes -> CTAs per SM

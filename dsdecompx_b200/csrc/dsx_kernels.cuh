@@ -79,8 +79,9 @@ struct Scratch {
     int classify_combine = 0;     // immigrant counters combined per warp before the atomics
     int move_staged = 1;          // 1: staged (one pass if it fits), 2: staged in passes,
                                   // 3: staged without forces, 0: direct reads
-    int refresh_kind = 2;         // refresh walk: 0 ghost by ghost, 1 owner by owner (the CSR),
-                                  // 2 tile by tile with the owners staged (when the stage fits)
+    int refresh_kind = 3;         // refresh walk: 0 ghost by ghost, 1 owner by owner (the CSR),
+                                  // 2 tile by tile with the owners staged (when the stage fits),
+                                  // 3 tile by tile for a full refresh of 9 or more arrays, else 0
     int reverse_per_sm = 0;       // CTAs per SM of the reverse sum; 0: one wave of the default shape
 };
 

@@ -268,10 +268,12 @@ int dsx_grid_end_halo_exchange(dsx_grid* grid, void* stream, long long* results)
 /* How a halo refresh (exchange_halo along a valid plan, full or positions
  * only) walks the plan: 0 ghost by ghost, gathering the owner of every
  * ghost; 1 owner by owner, reading each boundary owner once and writing all
- * its images; 2 (the default) tile by tile, the tile's owners brought into
- * shared memory whole and the images written in ghost-slot order (a record
- * whose copied arrays exceed 100 KB per tile falls back to 0).  All write
- * the same values; DSX_E_INVALID for another kind. */
+ * its images; 2 tile by tile, the tile's owners brought into shared memory
+ * whole and the images written in ghost-slot order (a record whose copied
+ * arrays exceed 100 KB per tile falls back to 0); 3 (the default) 2 for a
+ * full refresh that copies nine arrays or more (positions, velocities and
+ * at least three fields), else 0.  All write the same values; DSX_E_INVALID
+ * for another kind. */
 int dsx_grid_set_refresh_kind(dsx_grid* grid, int kind);
 
 /* CTAs per SM that begin_halo_exchange's refresh may occupy (0, the default:

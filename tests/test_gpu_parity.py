@@ -155,7 +155,7 @@ def test_rebalance_api(cuda):
     pair.close()
 
 
-@pytest.mark.parametrize("kind", ["owners", "ghosts", "tiles"])
+@pytest.mark.parametrize("kind", ["owners", "ghosts", "tiles", "auto"])
 def test_refresh_kinds_follow_the_reference(cuda, kind):
     """Full refreshes along the plan (every field type, a halo wider than
     half a cell so that owners have many images) walked owner by owner,
