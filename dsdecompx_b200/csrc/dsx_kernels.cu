@@ -1514,20 +1514,23 @@ __device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigne
         ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
 
-// Polls phase 0 of the mbarrier for at most kBulkWaitNs; false if it never
-// completed.
-__device__ __forceinline__ bool bulk_wait(unsigned bar) {
+// Polls the mbarrier's phase `parity` for at most kBulkWaitNs; false if it
+// never completed.
+__device__ __forceinline__ bool bulk_wait_parity(unsigned bar, unsigned parity) {
     const unsigned long long start = global_ns();
     for (;;) {
         unsigned ok;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
             " selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(ok) : "r"(bar) : "memory");
+            : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
         if (ok) return true;
         if (global_ns() - start > kBulkWaitNs) return false;
     }
 }
+
+// Phase 0 (a barrier that completes once).
+__device__ __forceinline__ bool bulk_wait(unsigned bar) { return bulk_wait_parity(bar, 0u); }
 
 // Array k of the record (0..10 doubles, 11 type, 12 id, 13.. fields).
 __device__ __forceinline__ int array_bytes(const Arrays& A, int k) {
@@ -1882,21 +1885,6 @@ __global__ void __launch_bounds__(NT, 4) k_halo_scatter_staged(
         ghost_from_stage_unwrapped(A, s_rec, sg, fseg, l, ghost_off + slot, shift + 3 * n);
         ghost_owner[slot] = begin + l;
         ghost_entry[slot] = s * kMaxNeighbors + n;
-    }
-}
-
-// Polls the mbarrier's phase `parity` for at most kBulkWaitNs; false if it
-// never completed.
-__device__ __forceinline__ bool bulk_wait_parity(unsigned bar, unsigned parity) {
-    const unsigned long long start = global_ns();
-    for (;;) {
-        unsigned ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-            " selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
-        if (ok) return true;
-        if (global_ns() - start > kBulkWaitNs) return false;
     }
 }
 
