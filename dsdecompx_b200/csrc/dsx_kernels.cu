@@ -2908,11 +2908,22 @@ __device__ __forceinline__ int owner_of_binned(const Grid& G, const CellGuess& g
         const double v = wrap_if(G, a, p[a]);
         const double* cuts = s_cuts + G.cut_offset[a];
         const int dims = G.dims[a];
-        int b = static_cast<int>((v - g.lower[a]) * g.inv[a]);   // saturating: NaN gives 0
+        // the bin, rounded to nearest by the 1.5 x 2^52 shift (its low word
+        // is the integer; any value, NaN's included, is clamped, and a guess
+        // one bin off is stepped away like any other)
+        int b = __double2loint(__fma_rn(v - g.lower[a], g.inv[a], 6755399441055744.0));
         b = b < 0 ? 0 : (b > kGuessBins - 1 ? kGuessBins - 1 : b);
         int k = s_bins[a * kGuessBins + b];
-        while (k < dims - 1 && !(v < cuts[k + 1])) ++k;
-        while (k > 0 && v < cuts[k]) --k;
+        // one step either way without a branch; a position two or more
+        // cells from the guess (cuts closer than a bin) keeps stepping
+        const bool up = k < dims - 1 && !(v < cuts[k + 1]);
+        const bool down = k > 0 && v < cuts[k];
+        k += up ? 1 : 0;
+        k -= down ? 1 : 0;
+        if ((up && k < dims - 1 && !(v < cuts[k + 1])) || (down && k > 0 && v < cuts[k])) {
+            while (k < dims - 1 && !(v < cuts[k + 1])) ++k;
+            while (k > 0 && v < cuts[k]) --k;
+        }
         c[a] = k;
     }
     return (c[0] * G.dims[1] + c[1]) * G.dims[2] + c[2];
@@ -2993,7 +3004,7 @@ __device__ __forceinline__ bool inside_planes(const Grid& G, const double* s_cut
     return inside;
 }
 
-__global__ void __launch_bounds__(NT) k_out_of_domain(Grid G, const double* __restrict__ x,
+__global__ void __launch_bounds__(NT, 4) k_out_of_domain(Grid G, const double* __restrict__ x,
                                                       const double* __restrict__ y,
                                                       const double* __restrict__ z, int* flags) {
     pdl_begin();
