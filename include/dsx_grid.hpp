@@ -210,6 +210,20 @@ public:
                             capture ? 1 : 0, stream, &status));
         return status;
     }
+    // The same step queued behind the previous one (dsx_grid_step_async; a
+    // created stream); step_wait completes the queue and returns the OR of
+    // the queued steps' status bits.
+    void step_async(void* stream) {
+        check(dsx_grid_step_async(handle_, callback_ ? &trampoline : nullptr, callback_.get(),
+                                  stream));
+    }
+    unsigned step_wait() {
+        unsigned status = 0;
+        check(dsx_grid_step_wait(handle_, &status));
+        return status;
+    }
+    // Refresh walk (dsx_grid_set_refresh_kind): 0 ghosts, 1 owners, 2 tiles, 3 auto
+    void set_refresh_kind(int kind) { check(dsx_grid_set_refresh_kind(handle_, kind)); }
     // classify_threads 64/128/256, move_kind as dsx_tune_report.move_staged,
     // reverse_ctas_per_sm 0..32, classify_combine as dsx_tune_report's
     void set_tuning(int classify_threads, int move_kind, int reverse_ctas_per_sm,

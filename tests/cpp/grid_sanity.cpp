@@ -161,6 +161,10 @@ int main() {
                    "step: sum of reverse == #ghosts");
             expect(sorted_ids(grid) == want, "step: ids conserved");
         }
+        // the same steps queued back to back, completed by one wait
+        for (int step = 0; step < 3; ++step) grid.step_async(stream);
+        expect(grid.step_wait() == 0, "queued steps' status");
+        expect(sorted_ids(grid) == want, "queued steps: ids conserved");
 
         // split phase and its misuse (std::logic_error), bad cuts (invalid_argument)
         grid.begin_halo_exchange(true);
