@@ -1026,6 +1026,8 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
     static_assert(CI * CT == TILE && CW >= 1, "tile split");
     __shared__ int s_cnt[CW][32];
     __shared__ unsigned s_lut[64];   // the subdomain's halo flags -> neighbor mask
+    __shared__ unsigned short s_queue[TILE];   // tile slots left to the general path
+    __shared__ int s_qn;
     const int g = blockIdx.x;
     // the descriptor is read together with the tile count (the table has a
     // row for every block of the launch)
@@ -1047,6 +1049,7 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
     const TileBounds bs = halo_bounds(G, s);
     const Cell cell = cell_of(G, s);
     for (int f = threadIdx.x; f < 64; f += CT) s_lut[f] = G.lut[s * 64 + f];
+    if (threadIdx.x == 0) s_qn = 0;
     __syncthreads();
     const unsigned* lut = s_lut;
     const int nn = G.nn[s];
@@ -1057,8 +1060,8 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                         (!G.periodic[2] || G.lower[2] == 0.0);
     int acc = 0;
     unsigned m[CI];
-    int fast = 0;         // this lane's particles that took the warp-uniform path
-    unsigned slow = 0;    // groups left to the general path (the same in every lane)
+    int fast = 0;   // this lane's particles that stay inside their own cell
+    const unsigned lt = lanemask_lt();
 #pragma unroll
     for (int j = 0; j < CI; ++j) {
         const int i = wbegin + j * 32 + lane;
@@ -1067,30 +1070,38 @@ __global__ void __launch_bounds__(CT, MINB) k_step_classify(Grid G, const double
                          cell.lo[1] <= py[j] && py[j] < cell.hi[1] && cell.lo[2] <= pz[j] &&
                          pz[j] < cell.hi[2];
         m[j] = 0;
-        if (__all_sync(0xffffffffu, own || !valid)) {
-            // the whole group stays: destination s, mask of the own subdomain
-            if (valid) {
-                const double wx = G.periodic[0] && px[j] == 0.0 ? 0.0 : px[j];
-                const double wy = G.periodic[1] && py[j] == 0.0 ? 0.0 : py[j];
-                const double wz = G.periodic[2] && pz[j] == 0.0 ? 0.0 : pz[j];
-                m[j] = halo_mask(bs, lut, wx, wy, wz);
-                dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(s);
-                mask_out[static_cast<long long>(g) * TILE + (i - begin)] = m[j];
-                ++fast;
-            }
-        } else {
-            slow |= 1u << j;
+        if (own) {
+            // stays: destination s, mask of the own subdomain
+            const double wx = G.periodic[0] && px[j] == 0.0 ? 0.0 : px[j];
+            const double wy = G.periodic[1] && py[j] == 0.0 ? 0.0 : py[j];
+            const double wz = G.periodic[2] && pz[j] == 0.0 ? 0.0 : pz[j];
+            m[j] = halo_mask(bs, lut, wx, wy, wz);
+            dest_out[static_cast<long long>(g) * TILE + (i - begin)] = static_cast<unsigned short>(s);
+            mask_out[static_cast<long long>(g) * TILE + (i - begin)] = m[j];
+            ++fast;
+        }
+        // every other particle of the tile waits in a queue for the
+        // general path (one slot per particle; one shared atomic per group)
+        const unsigned queued = __ballot_sync(0xffffffffu, valid && !own);
+        if (queued) {
+            int at = 0;
+            if (lane == 0) at = atomicAdd(&s_qn, __popc(queued));
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (valid && !own) s_queue[at + __popc(queued & lt)] = static_cast<unsigned short>(i - begin);
         }
     }
     count_groups<CI>(m, lane, acc);
     const int fast_stays = __reduce_add_sync(0xffffffffu, fast);
     if (lane == kStepStay) acc += fast_stays;
-    // The general path, one group per pass: its code appears once (the
-    // unrolled path above stays small enough for the instruction cache) and
-    // re-reads the group's positions, still in L1.
+    __syncthreads();
+    // The general path, 32 queued particles per warp and pass (a group with
+    // one leaver no longer runs it for all 32 lanes); it re-reads the
+    // positions, still in L1.
+    const int nq = s_qn;
 #pragma unroll 1
-    for (; slow; slow &= slow - 1) {
-        const int i = wbegin + (__ffs(slow) - 1) * 32 + lane;
+    for (int q0 = warp * 32; q0 < nq; q0 += CW * 32) {
+        const int q = q0 + lane;
+        const int i = q < nq ? begin + s_queue[q] : end;
         int d = -1;
         unsigned mg = 0, me = 0;
         if (i < end) {
