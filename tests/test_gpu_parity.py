@@ -117,6 +117,32 @@ def test_dynamic_boundaries_follow_the_reference(cuda):
     pair.close()
 
 
+def test_largest_grid_with_dynamic_boundaries(cuda):
+    """The engine's largest grid (1024 subdomains, 16x8x8 here): the layout
+    runs one thread per subdomain, and the Dynamic rebalance has 32 slab sums,
+    more than one pass of its lanes.  Clustered particles so that the cut
+    planes move; every call compared with the oracle."""
+    def clustered(rng, n, lower, upper):
+        lower, upper = np.asarray(lower), np.asarray(upper)
+        d = uniform_particles(rng, n, lower, upper, ALL_FIELDS[:1])
+        k = int(0.7 * n)
+        centre = rng.uniform(lower, upper, size=(6, 3))
+        pos = centre[rng.integers(0, 6, k)] + rng.normal(0, 3.0, size=(k, 3))
+        pos = lower + np.mod(pos - lower, upper - lower)
+        d["x"][:k], d["y"][:k], d["z"][:k] = pos[:, 0], pos[:, 1], pos[:, 2]
+        return d
+
+    pair = run_scenario(cuda, P=1024, dims=(0, 0, 0), L=(96.0, 48.0, 48.0), halo=0.7, N=60000,
+                        steps=3, seed=77, policy="dynamic", fields=ALL_FIELDS[:1],
+                        dynamic=(1.0, 1.05, 0.5, 0.10), data_fn=clustered)
+    try:
+        dims = pair.gpu.topology(0)[0]
+        assert sum(dims) > 31, dims
+        assert not np.allclose(pair.gpu.cuts()[0], np.linspace(0, 96, dims[0] + 1))
+    finally:
+        pair.close()
+
+
 def test_ghost_overflow_grows_and_rebuilds(cuda):
     # a deliberately tiny ghost capacity: the build must detect the overflow,
     # grow the ghost region and rebuild, with results identical to the oracle
