@@ -1561,20 +1561,35 @@ __device__ __forceinline__ int sri(const unsigned char* rec, int seg, int l) {
     return *reinterpret_cast<const int*>(rec + seg + l * 4);
 }
 
+// Words of one field, four at a time: the four shared-memory loads are
+// issued before the four stores (the generic pointers could otherwise alias,
+// which would order every store before the next load).
+template <class W>
+__device__ __forceinline__ void copy_words_staged(const W* __restrict__ src, W* __restrict__ out,
+                                                  int n) {
+    for (int w0 = 0; w0 < n; w0 += 4) {
+        W t[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (w0 + u < n) t[u] = src[w0 + u];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (w0 + u < n) out[w0 + u] = t[u];
+    }
+}
+
 __device__ __forceinline__ void fields_from_stage(const FieldSet& f, const unsigned char* rec,
                                                   const int* seg, int l, long long dst) {
     for (int k = 0; k < f.count; ++k) {
         const int b = f.bytes[k];
         const unsigned char* src = rec + seg[k] + l * b;
         unsigned char* out = f.base[k] + dst * b;
-        if ((b & 7) == 0) {
-            for (int w = 0; w < (b >> 3); ++w)
-                reinterpret_cast<unsigned long long*>(out)[w] =
-                    reinterpret_cast<const unsigned long long*>(src)[w];
-        } else {
-            for (int w = 0; w < (b >> 2); ++w)
-                reinterpret_cast<unsigned*>(out)[w] = reinterpret_cast<const unsigned*>(src)[w];
-        }
+        if ((b & 7) == 0)
+            copy_words_staged(reinterpret_cast<const unsigned long long*>(src),
+                              reinterpret_cast<unsigned long long*>(out), b >> 3);
+        else
+            copy_words_staged(reinterpret_cast<const unsigned*>(src), reinterpret_cast<unsigned*>(out),
+                              b >> 2);
     }
 }
 
