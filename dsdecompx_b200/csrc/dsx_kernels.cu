@@ -2961,7 +2961,9 @@ __device__ __forceinline__ void stage_cuts(const Grid& G, double* s_cuts) {
     __syncthreads();
 }
 
-// Two positions per thread and pass, both loaded before any search.
+// One position per thread and pass, the next pass's position loaded before
+// this one is searched (software pipelining: the loads stay in flight while
+// the search runs).
 __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restrict__ x,
                                                    const double* __restrict__ y,
                                                    const double* __restrict__ z, long long n,
@@ -2972,24 +2974,26 @@ __global__ void __launch_bounds__(NT) k_owner_rank(Grid G, const double* __restr
     stage_cuts(G, s_cuts);
     stage_bins(G, s_cuts, s_bins);
     const CellGuess guess = cell_guess(G);
-    constexpr int U = 2;
     const long long step = static_cast<long long>(gridDim.x) * NT;
-    for (long long i0 = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; i0 < n; i0 += U * step) {
-        double px[U], py[U], pz[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const long long i = i0 + u * step;
-            if (i < n) {
-                px[u] = ro(x + i);
-                py[u] = ro(y + i);
-                pz[u] = ro(z + i);
-            }
+    long long i = blockIdx.x * static_cast<long long>(NT) + threadIdx.x;
+    double px = 0.0, py = 0.0, pz = 0.0;
+    if (i < n) {
+        px = ro(x + i);
+        py = ro(y + i);
+        pz = ro(z + i);
+    }
+    for (; i < n; i += step) {
+        const long long j = i + step;
+        double qx = 0.0, qy = 0.0, qz = 0.0;
+        if (j < n) {
+            qx = ro(x + j);
+            qy = ro(y + j);
+            qz = ro(z + j);
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const long long i = i0 + u * step;
-            if (i < n) out[i] = owner_of_binned(G, guess, s_cuts, s_bins, px[u], py[u], pz[u]);
-        }
+        out[i] = owner_of_binned(G, guess, s_cuts, s_bins, px, py, pz);
+        px = qx;
+        py = qy;
+        pz = qz;
     }
 }
 
