@@ -246,8 +246,8 @@ int dsx_grid_step(dsx_grid* grid, dsx_step_callback callback, void* user, int ca
  * idempotent, as for dsx_grid_step).  dsx_grid_step_wait completes the
  * pending step and returns the OR of the status bits of the asynchronous
  * steps since the last wait; every other dsx_grid_* call on the grid (but
- * dsx_grid_view_get and the topology queries) completes the pending step
- * first, and so reports its failure.  Needs a created stream (DSX_E_INVALID
+ * dsx_grid_view_get, dsx_grid_step_kernel_count and the topology queries)
+ * completes the pending step first, and so reports its failure.  Needs a created stream (DSX_E_INVALID
  * for a default stream). */
 int dsx_grid_step_async(dsx_grid* grid, dsx_step_callback callback, void* user, void* stream);
 int dsx_grid_step_wait(dsx_grid* grid, unsigned* status);
