@@ -1011,3 +1011,62 @@ def test_async_steps_match_synchronous_steps(cuda, ghost_capacity):
         assert same(ca, cb)
     for g in grids:
         g.close()
+
+
+def test_calls_between_queued_steps_complete_them(cuda):
+    """A per-call operation after dsx_grid_step_async first completes the
+    queued step (its build checked, its graph finished): the same sequence
+    of steps and calls, queued on one grid and one call at a time on the
+    other, leaves the same arrays, counts and cut planes."""
+    import ctypes as C
+
+    import torch
+
+    import dsdecompx_b200 as dsx
+    from dsdecompx_b200 import workloads as W
+    wl = W.harness()
+    rng = np.random.default_rng(33)
+    n = 12000
+    kw = dict(nranks=8, dims=(2, 2, 2), policy="dynamic", lower=(0, 0, 0), upper=(12, 12, 12),
+              halo_width=0.8, fields=ALL_FIELDS[:1], particles=n, ghost_capacity=20000,
+              dynamic=(1.0, 1.05, 0.5, 0.10))
+    data = uniform_particles(rng, n, (0, 0, 0), (12, 12, 12), ALL_FIELDS[:1])
+    grids = [dsx.VirtualGrid(**kw) for _ in range(2)]
+    with Grid("port", 8, (2, 2, 2), "dynamic", (0, 0, 0), (12, 12, 12), (True,) * 3, 0.8,
+              dynamic=kw["dynamic"]) as probe:
+        owner = probe.owner_rank(np.stack([data["x"], data["y"], data["z"]], 1))
+    per = split_by_owner(owner, data, 8)
+    for g in grids:
+        g.upload(per)
+    stream = torch.cuda.Stream()
+
+    def work(view, s):
+        assert wl.dsxw_step_work(C.byref(view), 5, 0.2, s) == 0
+
+    torch.cuda.synchronize()
+    for k, g in enumerate(grids):
+        wl.dsxw_set_step(0, stream.cuda_stream)
+        for _ in range(2):
+            if k == 0:
+                assert g.step(work, capture=True, stream=stream) == 0
+            else:
+                g.step_async(work, stream=stream)
+        g.migrate(stream=stream)                     # completes a queued step first
+        g.exchange_halo(rebuild=True, stream=stream)
+        g.reverse_halo(stream=stream)
+        for _ in range(2):
+            if k == 0:
+                assert g.step(work, capture=True, stream=stream) == 0
+            else:
+                g.step_async(work, stream=stream)
+        if k == 1:
+            assert g.step_wait() == 0
+        stream.synchronize()
+    for r in range(8):
+        a, b = grids[0].snapshot(r), grids[1].snapshot(r)
+        for key in a:
+            assert same(a[key], b[key]), (r, key)
+    for ca, cb in zip(grids[0].cuts(), grids[1].cuts()):
+        assert same(ca, cb)
+    for g in grids:
+        g.close()
