@@ -845,8 +845,10 @@ struct dsx_grid {
         plain_bounds[static_cast<std::size_t>(P)] = info[1];
     }
 
+    // first_of_step: the batched step's rebalance, which also clears the
+    // status word and the step's immigrant counters (their memsets skipped)
     void enqueue_rebalance(cudaStream_t stream, bool automatic_rebalance,
-                           const double* work_in = nullptr) {
+                           const double* work_in = nullptr, bool first_of_step = false) {
         const dsx::Grid G = params();
         if (desc.policy == DSX_DYNAMIC) {
             // Decomp::migrate: ++migration_calls, automatic rebalance every
@@ -859,6 +861,11 @@ struct dsx_grid {
             p.halo_width = halo_width;
             p.automatic = 1;
             p.interval = automatic_rebalance ? static_cast<long long>(desc.dyn_interval) : 0;
+            if (first_of_step) {
+                p.clear_status = 1;
+                p.zero = S.imm_total;
+                p.nzero = P * (3 + dsx::kMaxNeighbors);
+            }
             dsx::launch_rebalance(G, work_in, p, call_counter, rebalance_result, stream);
             dsx::mark(S, stream, "rebalance");
         }
@@ -1203,15 +1210,18 @@ struct dsx_grid {
 
     void enqueue_step(dsx_step_callback cb, void* user, cudaStream_t stream, bool build_event = false) {
         marks.count = 0;
-        clear_status(stream);
+        // a Dynamic grid's rebalance opens the step and clears the status and
+        // the immigrant counters itself
+        const bool dynamic = desc.policy == DSX_DYNAMIC;
+        if (!dynamic) clear_status(stream);
         marks.mark(stream, "start");
-        enqueue_rebalance(stream, true);
+        enqueue_rebalance(stream, true, nullptr, dynamic);
         {
             const dsx::Grid G = params();
             cur ^= 1;
             const dsx::Grid Gn = params();
             cur ^= 1;
-            dsx::launch_fused_step(G, Gn, A, owned_off(), next_off(), ghost_off(), S, stream);
+            dsx::launch_fused_step(G, Gn, A, owned_off(), next_off(), ghost_off(), S, stream, dynamic);
         }
         if (build_event) {
             // the build's status and totals, then the event the next

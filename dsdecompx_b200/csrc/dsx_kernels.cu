@@ -2723,6 +2723,8 @@ __global__ void __launch_bounds__(32) k_rebalance(Grid G, const double* work_in,
     __shared__ int s_go, s_bad;
     const int lane = threadIdx.x;
     if (blockIdx.x != 0) return;
+    if (p.clear_status && lane == 0) *G.status = 0u;
+    for (int k = lane; k < p.nzero; k += 32) p.zero[k] = 0;
     const int P = G.P;
     const int ncuts = G.cut_offset[2] + G.dims[2] + 1;
     // everything the warp reads, in one round trip
@@ -3373,8 +3375,8 @@ bool staged_passes(const Arrays& A, int* ends, int& passes) {
 }
 
 void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, const Scratch& S,
-                          cudaStream_t s) {
-    cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P * (3 + kMaxNeighbors), s);
+                          cudaStream_t s, bool counters_zeroed) {
+    if (!counters_zeroed) cudaMemsetAsync(S.imm_total, 0, sizeof(int) * G.P * (3 + kMaxNeighbors), s);
     if (S.pairs) cudaMemsetAsync(S.pairs, 0, sizeof(int) * G.P * G.P, s);
     const double* x = A.d[0] + src_off;
     const double* y = A.d[1] + src_off;
@@ -3520,8 +3522,9 @@ void launch_step_immigrant_halo(const Grid& Gn, const Arrays& A, long long dst_o
 }
 
 void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
-                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s) {
-    launch_step_classify(G, A, src_off, S, s);
+                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s,
+                       bool counters_zeroed) {
+    launch_step_classify(G, A, src_off, S, s, counters_zeroed);
     if (S.marks) S.marks->mark(s, "step_classify");
     launch_step_layout(G, S, s);
     if (S.marks) S.marks->mark(s, "step_layout");

@@ -107,14 +107,15 @@ void launch_halo_build(const Grid& G, const Arrays& A, long long owned_off,
 // migrate + plan build as one pipeline (the batched step); G: current layout,
 // Gn: the same grid with the next layout current.
 void launch_fused_step(const Grid& G, const Grid& Gn, const Arrays& A, long long src_off,
-                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s);
+                       long long dst_off, long long ghost_off, const Scratch& S, cudaStream_t s,
+                       bool counters_zeroed = false);
 
 // The pipeline's parts, in order (the autotuner replays them one by one):
 // classify (destinations, masks, tile counters), the counter scan and the
 // next layout, the move (idempotent for a fixed current half), and the
 // emigrant placement plus the immigrants' ghost images.
 void launch_step_classify(const Grid& G, const Arrays& A, long long src_off, const Scratch& S,
-                          cudaStream_t s);
+                          cudaStream_t s, bool counters_zeroed = false);
 void launch_step_layout(const Grid& G, const Scratch& S, cudaStream_t s);
 void launch_step_move(const Grid& G, const Arrays& A, long long src_off, long long dst_off,
                       long long ghost_off, const Scratch& S, cudaStream_t s);
@@ -181,6 +182,11 @@ struct RebalanceParams {
     int force = 0;
     long long interval = 1;   // 0: automatic rebalance disabled
     int automatic = 0;        // 1: the migrate-time check (counts the call)
+    // the batched step's first kernel also clears the status word and the
+    // step's immigrant counters (instead of two memset nodes before it)
+    int clear_status = 0;
+    int* zero = nullptr;
+    int nzero = 0;
 };
 // out: {attempted, changed, imbalance(bits)} written to `result` (3 doubles)
 void launch_rebalance(const Grid& G, const double* work, RebalanceParams params,
