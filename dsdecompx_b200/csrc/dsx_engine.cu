@@ -1247,10 +1247,14 @@ struct dsx_grid {
         ghosts_valid = saved_ghosts;
         marks.mark(stream, "callback");
         enqueue_reverse(stream);
-        cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
-                   "read status");
-        cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream),
-                   "read status");
+        // the status after the build is the step's (nothing later sets a
+        // bit): a step with the build's copy needs no second one
+        if (!build_event) {
+            cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                       stream), "read status");
+            cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int),
+                                       cudaMemcpyDeviceToHost, stream), "read status");
+        }
         parity ^= 1;
         cur ^= 1;
         ++layout_version;
@@ -1558,6 +1562,9 @@ struct dsx_grid {
             graph_user = user;
             graph_stream = stream;
         }
+        // where the step's status lands: the build's copy of a captured
+        // step (per owned half), else the copy at the end of the step
+        const unsigned* st_at = capture ? pinned_build + 4 * parity : pinned_status;
         if (capture) {
             cudaGraphExec_t& exec = graph[parity];
             if (!exec) {
@@ -1576,8 +1583,7 @@ struct dsx_grid {
         plan_valid = true;
         ghosts_valid = true;
         cuda_check(cudaStreamSynchronize(stream), "synchronize step");
-        const unsigned st = finish_step(pinned_status[0], static_cast<int>(pinned_status[1]), cb, user,
-                                        stream);
+        const unsigned st = finish_step(st_at[0], static_cast<int>(st_at[1]), cb, user, stream);
         if (status_out) *status_out = st;
     }
 
