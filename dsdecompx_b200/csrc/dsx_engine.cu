@@ -716,8 +716,10 @@ struct dsx_grid {
         }
         const int tiles_cap = static_cast<int>((ncap + dsx::kTile - 1) / dsx::kTile) + P;
         for (auto& t : layout_tiles) t = device_alloc<int4>(fixed_owned, tiles_cap);
-        status = device_alloc<unsigned>(fixed_owned, 4);
-        cuda_check(cudaMemset(status, 0, 4 * sizeof(unsigned)), "memset");
+        // the status word, then the plan's totals {G, B} (S.halo_info, four
+        // words): one copy brings the status and the totals to the host
+        status = device_alloc<unsigned>(fixed_owned, 8);
+        cuda_check(cudaMemset(status, 0, 8 * sizeof(unsigned)), "memset");
         call_counter = device_alloc<long long>(fixed_owned, 1);
         cuda_check(cudaMemset(call_counter, 0, sizeof(long long)), "memset");
         rebalance_result = device_alloc<double>(fixed_owned, 6);
@@ -766,8 +768,7 @@ struct dsx_grid {
         S.bfirst = device_alloc<int>(fixed_owned, ncap);
         S.tile_b0 = device_alloc<int>(fixed_owned, static_cast<std::size_t>(max_tiles) + 1);
         S.cbase = device_alloc<int>(fixed_owned, static_cast<std::size_t>(P) * dsx::kHaloCounters);
-        S.halo_info = device_alloc<int>(fixed_owned, 4);
-        cuda_check(cudaMemset(S.halo_info, 0, 4 * sizeof(int)), "memset");
+        S.halo_info = reinterpret_cast<int*>(status + 1);
     }
 
     // particle arrays [owned A | owned B | ghosts]
@@ -894,10 +895,8 @@ struct dsx_grid {
     }
 
     unsigned read_status(cudaStream_t stream) {
-        cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
-                   "read status");
-        cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream),
-                   "read status");
+        cuda_check(cudaMemcpyAsync(pinned_status, status, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                   stream), "read status");
         cuda_check(cudaStreamSynchronize(stream), "synchronize");
         return pinned_status[0];
     }
@@ -1078,9 +1077,7 @@ struct dsx_grid {
             if (pending_graphs) {
                 // segment 2: the build's status and totals to the host
                 run_captured(split_end[parity], stream, [&] {
-                    cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned),
-                                               cudaMemcpyDeviceToHost, stream), "read status");
-                    cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int),
+                    cuda_check(cudaMemcpyAsync(pinned_status, status, 3 * sizeof(unsigned),
                                                cudaMemcpyDeviceToHost, stream), "read status");
                 });
                 cuda_check(cudaStreamSynchronize(stream), "synchronize");
@@ -1227,10 +1224,8 @@ struct dsx_grid {
             // the build's status and totals, then the event the next
             // asynchronous step waits on (an event node of the graph)
             unsigned* out = pinned_build + 4 * parity;
-            cuda_check(cudaMemcpyAsync(out, status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
+            cuda_check(cudaMemcpyAsync(out, status, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
                        "read build status");
-            cuda_check(cudaMemcpyAsync(out + 1, S.halo_info, 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                                       stream), "read build status");
             cuda_check(cudaEventRecordWithFlags(build_done[parity], stream, cudaEventRecordExternal),
                        "record build event");
         }
@@ -1249,12 +1244,9 @@ struct dsx_grid {
         enqueue_reverse(stream);
         // the status after the build is the step's (nothing later sets a
         // bit): a step with the build's copy needs no second one
-        if (!build_event) {
-            cuda_check(cudaMemcpyAsync(pinned_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+        if (!build_event)
+            cuda_check(cudaMemcpyAsync(pinned_status, status, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                                        stream), "read status");
-            cuda_check(cudaMemcpyAsync(pinned_status + 1, S.halo_info, 2 * sizeof(int),
-                                       cudaMemcpyDeviceToHost, stream), "read status");
-        }
         parity ^= 1;
         cur ^= 1;
         ++layout_version;
