@@ -468,6 +468,10 @@ struct dsx_grid {
     // reverse sum still run.
     unsigned* pinned_build = nullptr;             // [8]: per parity status, G, B, pad
     cudaEvent_t build_done[2] = {nullptr, nullptr};
+    // the build-status copy runs on a branch of the step graph, so the
+    // callback does not wait for it (fork and join events, side stream)
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool async_inflight = false;                  // a step whose status is unchecked
     int async_parity = 0;
     unsigned async_status = 0;                    // bits of the checked asynchronous steps
@@ -478,6 +482,9 @@ struct dsx_grid {
         async_inflight = false;
         destroy_graphs();
         for (auto& e : build_done) if (e) cudaEventDestroy(e);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        if (join_ev) cudaEventDestroy(join_ev);
+        if (side_stream) cudaStreamDestroy(side_stream);
         if (pinned_build) cudaFreeHost(pinned_build);
         free_shard_buffers();
         for (auto& e : marks.ev) if (e) cudaEventDestroy(e);
@@ -620,6 +627,9 @@ struct dsx_grid {
                    "cudaMallocHost");
         for (auto& e : build_done)
             cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
+        cuda_check(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming), "create event");
+        cuda_check(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming), "create event");
+        cuda_check(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking), "create stream");
         S.marks = &marks;
         last_ghosts.assign(static_cast<std::size_t>(P), 0);
     }
@@ -1222,12 +1232,16 @@ struct dsx_grid {
         }
         if (build_event) {
             // the build's status and totals, then the event the next
-            // asynchronous step waits on (an event node of the graph)
+            // asynchronous step waits on (an event node of the graph), on a
+            // branch that joins the step again after the reverse sum
             unsigned* out = pinned_build + 4 * parity;
-            cuda_check(cudaMemcpyAsync(out, status, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
-                       "read build status");
-            cuda_check(cudaEventRecordWithFlags(build_done[parity], stream, cudaEventRecordExternal),
+            cuda_check(cudaEventRecord(fork_ev, stream), "fork");
+            cuda_check(cudaStreamWaitEvent(side_stream, fork_ev, 0), "fork");
+            cuda_check(cudaMemcpyAsync(out, status, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                       side_stream), "read build status");
+            cuda_check(cudaEventRecordWithFlags(build_done[parity], side_stream, cudaEventRecordExternal),
                        "record build event");
+            cuda_check(cudaEventRecord(join_ev, side_stream), "join");
         }
         // the rest of the step reads the next layout
         parity ^= 1;
@@ -1247,6 +1261,8 @@ struct dsx_grid {
         if (!build_event)
             cuda_check(cudaMemcpyAsync(pinned_status, status, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                                        stream), "read status");
+        else
+            cuda_check(cudaStreamWaitEvent(stream, join_ev, 0), "join");
         parity ^= 1;
         cur ^= 1;
         ++layout_version;

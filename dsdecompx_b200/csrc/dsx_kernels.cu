@@ -537,36 +537,60 @@ __global__ void __launch_bounds__(NT) k_emig_place(Grid G, Arrays A, long long s
             }
         }
         __syncthreads();
+        // every emigrant's slot first (the counters step group by group),
+        // then both records gathered before either is written
+        int pos[ITEMS];
+        long long src[ITEMS];
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             const int e = base + j * 32 + lane;
             const int d = dj[j];
             const unsigned peers = __match_any_sync(0xffffffffu, d);
+            pos[j] = 0;
+            src[j] = 0;
             if (d >= 0) {
-                int pos = imm_base[d] + hist[static_cast<long long>(c) * P + d] +
-                          sm[warp * P + d] + __popc(peers & lt);
+                pos[j] = imm_base[d] + hist[static_cast<long long>(c) * P + d] + sm[warp * P + d] +
+                         __popc(peers & lt);
+                const int i = emig_src[e];
                 if (gap) {
                     // a sharded step: other shards' groups of immigrants of
                     // d that come before this emigrant's source q
-                    const int i = emig_src[e];
                     int lo = 0, hi = P;   // largest q with obase[q] <= i
                     while (hi - lo > 1) {
                         const int mid = (lo + hi) >> 1;
                         if (G.obase[mid] <= i) lo = mid;
                         else hi = mid;
                     }
-                    pos += gap[d * P + lo];
+                    pos[j] += gap[d * P + lo];
                 }
-                const long long src = src_off + emig_src[e];
-                const double ox = ro(A.d[0] + src), oy = ro(A.d[1] + src), oz = ro(A.d[2] + src);
-                const double wx = G.periodic[0] ? wrap_axis(ox, G.lower[0], G.extent[0]) : ox;
-                const double wy = G.periodic[1] ? wrap_axis(oy, G.lower[1], G.extent[1]) : oy;
-                const double wz = G.periodic[2] ? wrap_axis(oz, G.lower[2], G.extent[2]) : oz;
-                move_record(A, src, dst_off + pos, wx, wy, wz);
+                src[j] = src_off + i;
             }
             __syncwarp();
             if (d >= 0 && lane == __ffs(peers) - 1) sm[warp * P + d] += __popc(peers);
             __syncwarp();
+        }
+        double v[ITEMS][11];
+        int ty[ITEMS], id[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (dj[j] < 0) continue;
+#pragma unroll
+            for (int a = 0; a < 11; ++a) v[j][a] = ro(A.d[a] + src[j]);
+            ty[j] = ro(A.type + src[j]);
+            id[j] = ro(A.gid + src[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (dj[j] < 0) continue;
+            const long long dst = dst_off + pos[j];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                A.d[a][dst] = G.periodic[a] ? wrap_axis(v[j][a], G.lower[a], G.extent[a]) : v[j][a];
+#pragma unroll
+            for (int a = 3; a < 11; ++a) A.d[a][dst] = v[j][a];
+            A.type[dst] = ty[j];
+            A.gid[dst] = id[j];
+            copy_fields(A.f, src[j], dst);
         }
         __syncthreads();
     }
